@@ -1,0 +1,451 @@
+#!/usr/bin/env python
+"""Benchmark of the CSR analytics path on B200.
+
+Workload (one "step"): BFS from each of 64 seeded random non-isolated
+sources on an undirected RMAT graph, scale 24, edge factor 16, seed 7,
+a/b/c/d = .57/.19/.19/.05, permuted ids, duplicates and self-loops removed
+(16.8 M vertices, ~0.5 G CSR entries; ~2.1 GB of col, larger than the
+126 MB L2, so no L2 flush is needed between steps).
+
+  value  GTEPS = sum over sources of m_r (CSR entries out of reached
+         vertices) / device time, inputs resident in HBM
+  e2e    the same metric through the C ABI with the depth vector of every
+         BFS copied to pinned host memory inside the timed region (the
+         reference's Cuda_BFS returns a host vector too)
+
+Also measured (in "extra"): SSSP GTEPS, PageRank GB/s (FP32+Kahan, FP64),
+WCC / CDLP / TC times, the 64-source bitmask BFS, and the 4096x4096 grid.
+
+--impl reference times the reference's own CPU BFS (oracle/_ref, compiled
+from the reference's sources) on the same graph, built on the host.
+Under torchrun every rank runs its own sources on its own copy of the graph
+(replicas, weak scaling; no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GTEPS BFS/SSSP, PR GB/s vs HBM peak; learned+batched vs plain, 1x B200"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--edge-factor", type=int, default=16)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--sources", type=int, default=64)
+    ap.add_argument("--extras", type=int, default=1, help="also measure the other algorithms")
+    ap.add_argument("--cpu-sample", type=int, default=1, help="number of BFS sources in the CPU baseline")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", FALLBACK_HBM_GBS)), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def pick_sources(rowptr_host: np.ndarray, count: int, seed: int, salt: int = 0):
+    """Seeded random non-isolated sources (splitmix64 draws, first hits)."""
+    n = len(rowptr_host) - 1
+    deg = np.diff(rowptr_host)
+    out = []
+    k = 0
+    mask = (1 << 64) - 1
+
+    def mix(z):
+        z = (z + 0x9E3779B97F4A7C15) & mask
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        return z ^ (z >> 31)
+
+    base = mix(seed * 1000003 + 5 + salt * 7919)
+    while len(out) < count and k < 100 * count + 1000:
+        v = mix(base ^ k) % n
+        k += 1
+        if deg[v] > 0:
+            out.append(int(v))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        if args.impl == "ours":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=1800))
+    return world, rank, local
+
+
+def barrier_sync(world):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(world, x: float) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- ours
+def run_ours(args, world, rank, local):
+    import ctypes
+
+    import torch
+
+    import graphhet_b200 as G
+
+    torch.cuda.set_device(local)
+    ws = G.default_workspace()
+    t0 = time.time()
+    g = G.rmat_graph(args.scale, args.edge_factor, args.seed, directed=False)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    n, m = g.n, g.m
+    rp_host = g.rowptr.cpu().numpy()
+    srcs = pick_sources(rp_host, args.sources, args.seed, salt=rank)
+    depth = torch.empty(n, dtype=torch.int32, device="cuda")
+    L = G.lib()
+    wsh = ws.handle
+    opt_plain = G.BfsOptions(policy=G.POLICY_HEURISTIC)
+    trace_cap = 64
+    trace = (ctypes.c_float * (trace_cap * G.TRACE_COLS))()
+    opt_trace = G.BfsOptions(policy=G.POLICY_HEURISTIC, record_trace=1, trace=ctypes.cast(trace, ctypes.c_void_p),
+                             trace_cap=trace_cap)
+    st = G.TraversalStats()
+    rp_p, col_p, d_p = G._ptr(g.rowptr), G._ptr(g.col), G._ptr(depth)
+
+    def one_bfs(s, opt):
+        G._check(L.ghb_bfs(wsh, n, rp_p, col_p, rp_p, col_p, s, G.INT32_MAX, d_p, ctypes.byref(opt),
+                           ctypes.byref(st)), "ghb_bfs")
+        return st.edges_reached
+
+    # m_r per source (deterministic) and warm-up.
+    mr = {}
+    for s in srcs:
+        mr[s] = one_bfs(s, opt_plain)
+    for _ in range(max(0, args.warmup - 1)):
+        for s in srcs:
+            one_bfs(s, opt_plain)
+    l0, _ = ws.counters()
+
+    # ---- timed region: K steps, every step = BFS from every source.
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    level_rows = []
+    with ClockSampler(local) as clk:
+        barrier_sync(world)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            for s in srcs:
+                one_bfs(s, opt_trace)
+                level_rows.append(np.frombuffer(trace, dtype=np.float32).reshape(trace_cap, G.TRACE_COLS)
+                                  [: st.levels].copy())
+        ev1.record(stream)
+        barrier_sync(world)
+    l1, _ = ws.counters()
+    ms = max_over_ranks(world, ev0.elapsed_time(ev1))
+    edges_per_step = sum(mr[s] for s in srcs)
+    total_edges = edges_per_step * args.steps * world
+    value = total_edges / (ms / 1e3) / 1e9
+    launches = int(l1 - l0)
+
+    # ---- roofline of the dominant kernel class (BFS levels by direction).
+    levels = np.concatenate(level_rows, axis=0)
+    by_dir = {}
+    for d in (0, 1):
+        sel = levels[levels[:, 12] == d]
+        if len(sel):
+            by_dir[d] = (float(sel[:, 13].sum()), len(sel), float(sel[:, 19].sum()))
+    dom = max(by_dir, key=lambda d: by_dir[d][0])
+    dom_ms, dom_launches, dom_bytes = by_dir[dom]
+    hbm, peak_kind = measured_peaks()
+    achieved = (dom_bytes / dom_launches) / ((dom_ms / dom_launches) / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "bfs_pull_kernel" if dom == 1 else "bfs_push_kernel+bfs_big_kernel",
+                "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_source": peak_kind,
+                "traffic": None, "share_of_step": round(dom_ms / ms, 3) if world == 1 else None,
+                "bytes_per_launch": round(dom_bytes / dom_launches), "launches": dom_launches}
+
+    # ---- e2e: through the C ABI, depth vector to pinned host memory.
+    host_depth = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    barrier_sync(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        for s in srcs:
+            one_bfs(s, opt_plain)
+            host_depth.copy_(depth, non_blocking=True)
+    e1.record(stream)
+    barrier_sync(world)
+    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
+    e2e = {"value": round(total_edges / (e2e_ms / 1e3) / 1e9, 3), "unit": "GTEPS",
+           "h2d_bytes_per_step": 4 * len(srcs), "d2h_bytes_per_step": 4 * n * len(srcs)}
+
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"BFS from {len(srcs)} random non-isolated sources, undirected RMAT "
+                               f"scale {args.scale} edge factor {args.edge_factor} seed {args.seed}",
+                   "n": n, "m": m, "sources_per_step": len(srcs), "policy": "heuristic (alpha 14, beta 24)",
+                   "l2": "inputs larger than L2 (col %.2f GB)" % (4 * m / 1e9),
+                   "parallelism": f"replicas x{world}"},
+        "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "build_s": round(build_s, 2),
+    }
+    out["clocks"] = clk.summary()
+
+    if rank == 0 and args.extras:
+        out["extra"] = extras(args, G, g, srcs, ws)
+    if rank == 0 and args.cpu_sample > 0:
+        out["cpu_baseline"] = cpu_baseline_port(g, srcs[: args.cpu_sample])
+    return out
+
+
+def timed(fn, reps=1):
+    import torch
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record()
+    r = None
+    for _ in range(reps):
+        r = fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps, r
+
+
+def extras(args, G, g, srcs, ws):
+    import torch
+    hbm, _ = measured_peaks()
+    n, m = g.n, g.m
+    ex = {}
+    # SSSP over 4 sources
+    dist = torch.empty(n, dtype=torch.float64, device="cuda")
+    G.sssp(g, srcs[0], out=dist)
+    t_tot, e_tot = 0.0, 0
+    for s in srcs[:4]:
+        ms, (d, st) = timed(lambda: G.sssp(g, s, out=dist))
+        t_tot += ms
+        e_tot += st["edges_reached"]
+    ex["sssp_gteps"] = round(e_tot / (t_tot / 1e3) / 1e9, 3)
+    ex["sssp_ms_per_source"] = round(t_tot / 4, 3)
+    # PageRank: 10 iterations, FP32+Kahan and FP64
+    rank = torch.empty(n, dtype=torch.float64, device="cuda")
+    for prec, name, vb in ((G.PR_FP32_KAHAN, "fp32_kahan", 8), (G.PR_FP64, "fp64", 16)):
+        G.pagerank(g, 10, 0.85, precision=prec, out=rank)
+        ms, _ = timed(lambda: G.pagerank(g, 10, 0.85, precision=prec, out=rank), reps=2)
+        per_it = ms / 10
+        bytes_it = 4 * (n + 1) + 4 * m + vb * n
+        ex[f"pr_{name}_ms_per_iter"] = round(per_it, 4)
+        ex[f"pr_{name}_gbs"] = round(bytes_it / (per_it / 1e3) / 1e9, 1)
+        ex[f"pr_{name}_frac_hbm"] = round(bytes_it / (per_it / 1e3) / 1e9 / hbm, 4)
+    lab = torch.empty(n, dtype=torch.int32, device="cuda")
+    G.wcc(g, out=lab)
+    ms, _ = timed(lambda: G.wcc(g, out=lab), reps=3)
+    ex["wcc_ms"] = round(ms, 3)
+    ex["wcc_gbs"] = round((4 * (n + 1) + 4 * m + 4 * n) / (ms / 1e3) / 1e9, 1)
+    G.cdlp(g, 10, out=lab)
+    ms, _ = timed(lambda: G.cdlp(g, 10, out=lab))
+    ex["cdlp_ms_per_iter"] = round(ms / 10, 3)
+    ex["cdlp_gbs"] = round((4 * (n + 1) + 4 * m + 8 * n) / (ms / 10 / 1e3) / 1e9, 1)
+    ms, (c64, c32, tri) = timed(lambda: G.tc(g))
+    ex["tc_ms"] = round(ms, 2)
+    ex["tc_triangles"] = int(tri)
+    ex["tc_edges_per_s"] = round(m / (ms / 1e3) / 1e9, 3)
+    # 64-source bitmask BFS vs 64 single-source runs
+    import ctypes
+    k = min(64, len(srcs))
+    sd = torch.tensor(srcs[:k], dtype=torch.int32, device="cuda")
+    out = torch.empty(k * n, dtype=torch.int32, device="cuda")
+    stt = G.TraversalStats()
+
+    def ms_bfs():
+        G._check(G.lib().ghb_msbfs(ws.handle, n, G._ptr(g.rowptr), G._ptr(g.col), G._ptr(g.rowptr), G._ptr(g.col),
+                                   G._ptr(sd), k, G._ptr(out), ctypes.byref(stt)), "ghb_msbfs")
+    ms_bfs()
+    ms, _ = timed(ms_bfs)
+    mr_sum = 0
+    for s in srcs[:k]:
+        mr_sum += G.bfs(g, s, out=lab)[1]["edges_reached"]
+    ex["msbfs64_ms"] = round(ms, 2)
+    ex["msbfs64_gteps"] = round(mr_sum / (ms / 1e3) / 1e9, 3)
+    del out
+    torch.cuda.empty_cache()
+    # 4096 x 4096 grid: BFS and SSSP from its centre
+    gg = G.grid_graph(4096, 4096, weight_seed=args.seed)
+    c = 2048 * 4096 + 2048
+    dg = torch.empty(gg.n, dtype=torch.int32, device="cuda")
+    G.bfs(gg, c, out=dg)
+    ms, (_, st) = timed(lambda: G.bfs(gg, c, out=dg))
+    ex["grid_bfs_ms"] = round(ms, 2)
+    ex["grid_bfs_levels"] = st["levels"]
+    ex["grid_bfs_gteps"] = round(st["edges_reached"] / (ms / 1e3) / 1e9, 3)
+    dgs = torch.empty(gg.n, dtype=torch.float64, device="cuda")
+    ms, (_, st) = timed(lambda: G.sssp(gg, c, out=dgs))
+    ex["grid_sssp_ms"] = round(ms, 2)
+    ex["grid_sssp_gteps"] = round(st["edges_reached"] / (ms / 1e3) / 1e9, 3)
+    return ex
+
+
+def cpu_baseline_port(g, srcs):
+    """The oracle (C restatement of the reference's CPU BFS) on the host."""
+    import oracle as O
+    og = O.Graph(g.n, g.rowptr.cpu().numpy(), g.col.cpu().numpy(), None, False, None, None, None)
+    og.in_rowptr, og.in_col = og.rowptr, og.col
+    deg = np.diff(og.rowptr)
+    t_tot, e_tot = 0.0, 0
+    for s in srcs:
+        t0 = time.perf_counter()
+        d = O.bfs(og, s)
+        t_tot += time.perf_counter() - t0
+        e_tot += int(deg[d != 2**31 - 1].sum())
+    return {"value": round(e_tot / t_tot / 1e9, 4), "unit": "GTEPS", "cores": 1, "kind": "port",
+            "sample": f"BFS from {len(srcs)} of the same sources on the same graph (single-threaded FIFO BFS, "
+                      f"CPU_BFS.hpp:10-41), {t_tot:.1f} s"}
+
+
+# ----------------------------------------------------------- reference
+def run_reference(args, world, rank):
+    import oracle as O
+    if rank != 0:
+        return None
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref.so was not built (reference tree absent)"}
+    t0 = time.time()
+    og = O.rmat_graph(args.scale, args.edge_factor, args.seed, directed=False)
+    build_s = time.time() - t0
+    r = O.Ref().load(og)
+    srcs = pick_sources(og.rowptr, args.sources, args.seed)
+    deg = np.diff(og.rowptr)
+    # Each step: BFS from one source (a bounded sample of the 64-source step).
+    for i in range(args.warmup):
+        r.bfs(srcs[i % len(srcs)])
+    t_tot, e_tot = 0.0, 0
+    for i in range(args.steps):
+        s = srcs[i % len(srcs)]
+        t = time.perf_counter()
+        d = r.bfs(s)
+        t_tot += time.perf_counter() - t
+        e_tot += int(deg[d != 2**31 - 1].sum())
+    v = e_tot / t_tot / 1e9
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "GTEPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t_tot / args.steps, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"BFS from {len(srcs)} random non-isolated sources, undirected RMAT scale "
+                               f"{args.scale} edge factor {args.edge_factor} seed {args.seed}",
+                   "n": og.n, "m": og.m, "sources_per_step": 1},
+        "cpu_baseline": {"value": round(v, 4), "unit": "GTEPS", "cores": 1, "kind": "reference",
+                         "sample": f"reference CPU_BFS (single-threaded by design) from 1 source per step, "
+                                   f"{args.steps} steps; host has {os.cpu_count()} threads"},
+        "e2e": {"value": round(v, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "build_s": round(build_s, 1),
+    }
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+    else:
+        out = run_ours(args, world, rank, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,429 @@
+"""graphhet_b200: GraphHET's CSR analytics path (BFS, SSSP, WCC, PageRank,
+CDLP, triangle counting) on B200 (sm_100a).
+
+The compute lives in ``libghb.so`` (hand-written CUDA behind the C ABI of
+``include/ghb.h``).  This module is a thin host layer over that ABI: torch
+tensors hold the device memory, ctypes passes their pointers.  There is no
+CPU fallback: if the library is missing every call raises.
+
+Entry points mirror the reference's (include/GPU_csr/algorithm/*.cuh):
+``bfs`` ~ Cuda_BFS, ``sssp`` ~ Cuda_SSSP, ``wcc`` ~ Cuda_WCC,
+``pagerank`` ~ Cuda_PR, ``cdlp`` ~ Cuda_CDLP, ``tc`` ~ Cuda_TC, and
+``bfs_pred`` / ``sssp_pred`` ~ Cuda_BFS_pre / Cuda_SSSP_pre.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libghb.so")
+
+INT32_MAX = 2**31 - 1
+DBL_MAX = 1.7976931348623157e308
+
+POLICY_HEURISTIC, POLICY_LEARNED, POLICY_PUSH, POLICY_PULL, POLICY_SCHEDULE = 0, 1, 2, 3, 4
+PR_FP64, PR_FP32_KAHAN = 0, 1
+BUILD_SYMMETRIZE, BUILD_DROP_SELF_LOOPS, BUILD_TRANSPOSE = 1, 2, 4
+WEIGHT_NONE, WEIGHT_UNIFORM01, WEIGHT_INT100 = 0, 1, 2
+TRACE_FEATURES, TRACE_COLS = 12, 20
+
+_p = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+_u64 = ctypes.c_uint64
+_f64 = ctypes.c_double
+
+
+class BfsOptions(ctypes.Structure):
+    _fields_ = [("policy", _i32), ("alpha", ctypes.c_float), ("beta", ctypes.c_float),
+                ("schedule", _p), ("schedule_len", _i32), ("record_trace", _i32),
+                ("trace", _p), ("trace_cap", _i32), ("oracle_timing", _i32)]
+
+
+class SsspOptions(ctypes.Structure):
+    _fields_ = [("delta", _f64), ("policy", _i32), ("record_trace", _i32), ("trace", _p),
+                ("trace_cap", _i32)]
+
+
+class TraversalStats(ctypes.Structure):
+    _fields_ = [("levels", _i32), ("pull_levels", _i32), ("reached", _i64),
+                ("edges_reached", _i64), ("edges_examined", _i64), ("device_ms", _f64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class PrOptions(ctypes.Structure):
+    _fields_ = [("iterations", _i32), ("damping", _f64), ("precision", _i32),
+                ("tolerance", _f64), ("l1_history", _p)]
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "ghb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "ghb_last_error": (ctypes.c_char_p, []),
+    "ghb_version": (ctypes.c_int, []),
+    "ghb_workspace_create": (ctypes.c_int, [ctypes.POINTER(_p)]),
+    "ghb_workspace_destroy": (ctypes.c_int, [_p]),
+    "ghb_workspace_set_stream": (ctypes.c_int, [_p, _p]),
+    "ghb_workspace_get_stream": (_p, [_p]),
+    "ghb_workspace_trim": (ctypes.c_int, [_p]),
+    "ghb_workspace_counters": (ctypes.c_int, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "ghb_default_workspace": (_p, []),
+    "ghb_gen_rmat": (ctypes.c_int, [_p, _i32, _i64, _u64, _f64, _f64, _f64, _i32, _p, _p]),
+    "ghb_gen_grid": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
+    "ghb_gen_er": (ctypes.c_int, [_p, _i32, _i64, _u64, _p, _p]),
+    "ghb_csr_build": (ctypes.c_int, [_p, _i32, _p, _p, _p, _i64, _i32, _i32, _u64, _p, _p, _p,
+                                     ctypes.POINTER(_i64)]),
+    "ghb_csr_transpose": (ctypes.c_int, [_p, _i32, _i64, _p, _p, _p, _p, _p, _p]),
+    "ghb_csr_merge_in_out": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _p]),
+    "ghb_bfs": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _i32, _i32, _p, _p, _p]),
+    "ghb_bfs_pred": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _i32, _i32, _p, _p, _p, _p]),
+    "ghb_msbfs": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _i32, _p, _p]),
+    "ghb_sssp": (ctypes.c_int, [_p, _i32, _p, _p, _p, _i32, _f64, _p, _p, _p]),
+    "ghb_sssp_pred": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _p, _i32, _f64, _p, _p, _p, _p]),
+    "ghb_mssssp": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _i32, _f64, _p, _p]),
+    "ghb_wcc": (ctypes.c_int, [_p, _i32, _p, _p, _p]),
+    "ghb_pagerank": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _p]),
+    "ghb_cdlp": (ctypes.c_int, [_p, _i32, _p, _p, _i32, _p]),
+    "ghb_tc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p]),
+    "ghb_batch_wcc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p]),
+    "ghb_batch_tc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _p]),
+}
+
+_lib = None
+
+
+class GhbError(RuntimeError):
+    pass
+
+
+def lib() -> ctypes.CDLL:
+    """Load libghb.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GhbError(f"{LIB_PATH} is missing: build it with `make` (or __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status: int, what: str) -> None:
+    if status != 0:
+        L = lib()
+        raise GhbError(f"{what}: {L.ghb_status_string(status).decode()} "
+                       f"({L.ghb_last_error().decode()})")
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise GhbError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise GhbError("expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Workspace:
+    """A libghb workspace bound to torch's current CUDA stream."""
+
+    def __init__(self):
+        self._h = _p()
+        _check(lib().ghb_workspace_create(ctypes.byref(self._h)), "ghb_workspace_create")
+
+    @property
+    def handle(self):
+        lib().ghb_workspace_set_stream(self._h, _p(torch.cuda.current_stream().cuda_stream))
+        return self._h
+
+    def counters(self):
+        launches, scratch = _i64(), _i64()
+        _check(lib().ghb_workspace_counters(self._h, ctypes.byref(launches), ctypes.byref(scratch)),
+               "ghb_workspace_counters")
+        return launches.value, scratch.value
+
+    def trim(self):
+        _check(lib().ghb_workspace_trim(self._h), "ghb_workspace_trim")
+
+    def close(self):
+        if self._h:
+            lib().ghb_workspace_destroy(self._h)
+            self._h = _p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ws: dict = {}
+
+
+def default_workspace() -> Workspace:
+    dev = torch.cuda.current_device()
+    ws = _default_ws.get(dev)
+    if ws is None:
+        ws = _default_ws[dev] = Workspace()
+    return ws
+
+
+def _ws(ws):
+    return (ws or default_workspace()).handle
+
+
+# --------------------------------------------------------------- graphs
+@dataclass
+class CSRGraph:
+    """Device CSR in the reference's layout (CSR_graph, GPU_csr.hpp:97-110).
+
+    For an undirected graph the in/all arrays are the out arrays, as toCSR
+    aliases them (GPU_csr.hpp:133-140)."""
+    n: int
+    rowptr: torch.Tensor
+    col: torch.Tensor
+    w: Optional[torch.Tensor] = None
+    directed: bool = False
+    in_rowptr: Optional[torch.Tensor] = None
+    in_col: Optional[torch.Tensor] = None
+    in_w: Optional[torch.Tensor] = None
+    _all: Optional[tuple] = field(default=None, repr=False)
+
+    @property
+    def m(self) -> int:
+        return int(self.col.numel())
+
+    def in_csr(self):
+        if not self.directed:
+            return self.rowptr, self.col, self.w
+        return self.in_rowptr, self.in_col, self.in_w
+
+    def all_csr(self, ws=None):
+        """Row v = in-neighbours then out-neighbours (toCSR, GPU_csr.hpp:315-330)."""
+        if not self.directed:
+            return self.rowptr, self.col
+        if self._all is None:
+            arp = torch.empty(self.n + 1, dtype=torch.int32, device=self.rowptr.device)
+            acol = torch.empty(max(1, self.m + int(self.in_col.numel())), dtype=torch.int32,
+                               device=self.rowptr.device)
+            _check(lib().ghb_csr_merge_in_out(_ws(ws), self.n, _ptr(self.in_rowptr), _ptr(self.in_col),
+                                              _ptr(self.rowptr), _ptr(self.col), _ptr(arp), _ptr(acol)),
+                   "ghb_csr_merge_in_out")
+            self._all = (arp, acol[: self.m + int(self.in_col.numel())])
+        return self._all
+
+
+def _dev(device):
+    return torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+
+
+def gen_rmat(scale: int, n_edges: int, seed: int, a=0.57, b=0.19, c=0.19, permute=True, device=None, ws=None):
+    d = _dev(device)
+    src = torch.empty(max(1, n_edges), dtype=torch.int32, device=d)
+    dst = torch.empty(max(1, n_edges), dtype=torch.int32, device=d)
+    _check(lib().ghb_gen_rmat(_ws(ws), scale, n_edges, seed, a, b, c, int(permute), _ptr(src), _ptr(dst)),
+           "ghb_gen_rmat")
+    return src[:n_edges], dst[:n_edges]
+
+
+def gen_grid(rows: int, cols: int, device=None, ws=None):
+    d = _dev(device)
+    ne = rows * (cols - 1) + (rows - 1) * cols
+    src = torch.empty(max(1, ne), dtype=torch.int32, device=d)
+    dst = torch.empty(max(1, ne), dtype=torch.int32, device=d)
+    _check(lib().ghb_gen_grid(_ws(ws), rows, cols, _ptr(src), _ptr(dst)), "ghb_gen_grid")
+    return src[:ne], dst[:ne]
+
+
+def gen_er(n: int, n_edges: int, seed: int, device=None, ws=None):
+    d = _dev(device)
+    src = torch.empty(max(1, n_edges), dtype=torch.int32, device=d)
+    dst = torch.empty(max(1, n_edges), dtype=torch.int32, device=d)
+    _check(lib().ghb_gen_er(_ws(ws), n, n_edges, seed, _ptr(src), _ptr(dst)), "ghb_gen_er")
+    return src[:n_edges], dst[:n_edges]
+
+
+def build_csr(n: int, src: torch.Tensor, dst: torch.Tensor, w: Optional[torch.Tensor] = None,
+              symmetrize=False, drop_self_loops=True, transpose=False, weight_mode=WEIGHT_UNIFORM01,
+              weight_seed=0, ws=None):
+    """Edge list -> (rowptr, col, w) with sorted, deduplicated rows (ghb_csr_build)."""
+    ne = int(src.numel())
+    cap = max(1, ne * (2 if symmetrize else 1))
+    dev = src.device
+    rowptr = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    col = torch.empty(cap, dtype=torch.int32, device=dev)
+    want_w = w is not None or weight_mode != WEIGHT_NONE
+    wout = torch.empty(cap, dtype=torch.float64, device=dev) if want_w else None
+    flags = (BUILD_SYMMETRIZE if symmetrize else 0) | (BUILD_DROP_SELF_LOOPS if drop_self_loops else 0) | \
+            (BUILD_TRANSPOSE if transpose else 0)
+    m = _i64()
+    _check(lib().ghb_csr_build(_ws(ws), n, _ptr(src.contiguous()), _ptr(dst.contiguous()),
+                               _ptr(w.contiguous()) if w is not None else None, ne, flags, weight_mode,
+                               weight_seed, _ptr(rowptr), _ptr(col), _ptr(wout), ctypes.byref(m)),
+           "ghb_csr_build")
+    mm = m.value
+    # Shrink to the entry count (frees the worst-case allocation).
+    col = col[:mm].clone()
+    wout = wout[:mm].clone() if wout is not None else None
+    return rowptr, col, wout
+
+
+def transpose_csr(n: int, rowptr, col, w=None, ws=None):
+    m = int(col.numel())
+    trp = torch.empty(n + 1, dtype=torch.int32, device=rowptr.device)
+    tcol = torch.empty(max(1, m), dtype=torch.int32, device=rowptr.device)
+    tw = torch.empty(max(1, m), dtype=torch.float64, device=rowptr.device) if w is not None else None
+    _check(lib().ghb_csr_transpose(_ws(ws), n, m, _ptr(rowptr), _ptr(col) if m else None,
+                                   _ptr(w) if (w is not None and m) else None, _ptr(trp), _ptr(tcol),
+                                   _ptr(tw) if tw is not None else None), "ghb_csr_transpose")
+    return trp, tcol[:m], (tw[:m] if tw is not None else None)
+
+
+def make_graph(n: int, src, dst, directed: bool, weight_mode=WEIGHT_UNIFORM01, weight_seed=0, w=None,
+               drop_self_loops=True, ws=None) -> CSRGraph:
+    rp, col, wt = build_csr(n, src, dst, w=w, symmetrize=not directed, drop_self_loops=drop_self_loops,
+                            weight_mode=weight_mode, weight_seed=weight_seed, ws=ws)
+    g = CSRGraph(n=n, rowptr=rp, col=col, w=wt, directed=directed)
+    if directed:
+        g.in_rowptr, g.in_col, g.in_w = transpose_csr(n, rp, col, wt, ws=ws)
+    return g
+
+
+def rmat_graph(scale: int, edge_factor: int, seed: int, directed=False, a=0.57, b=0.19, c=0.19,
+               weight_mode=WEIGHT_UNIFORM01, device=None, ws=None) -> CSRGraph:
+    """RMAT(scale, edge_factor) with permuted ids, duplicates and self-loops removed."""
+    src, dst = gen_rmat(scale, edge_factor << scale, seed, a, b, c, True, device=device, ws=ws)
+    g = make_graph(1 << scale, src, dst, directed, weight_mode=weight_mode, weight_seed=seed, ws=ws)
+    del src, dst
+    return g
+
+
+def grid_graph(rows: int, cols: int, weight_seed=0, device=None, ws=None) -> CSRGraph:
+    """rows x cols 4-neighbour grid, integer weights in [1, 100]."""
+    src, dst = gen_grid(rows, cols, device=device, ws=ws)
+    return make_graph(rows * cols, src, dst, False, weight_mode=WEIGHT_INT100, weight_seed=weight_seed, ws=ws)
+
+
+# ----------------------------------------------------------- algorithms
+def _stats_out(stats: TraversalStats):
+    return stats.as_dict()
+
+
+def bfs(g: CSRGraph, src: int, max_depth: int = INT32_MAX, policy: int = POLICY_HEURISTIC, alpha=0.0,
+        beta=0.0, schedule=None, trace_cap: int = 0, oracle_timing=False, out=None, ws=None):
+    """Depths from src (INT32_MAX = unreached).  Returns (depth, stats[, trace])."""
+    depth = out if out is not None else torch.empty(g.n, dtype=torch.int32, device=g.rowptr.device)
+    irp, icol, _ = g.in_csr()
+    opt = BfsOptions(policy=policy, alpha=alpha, beta=beta)
+    sched_buf = None
+    if schedule is not None:
+        sched_buf = (ctypes.c_int8 * len(schedule))(*[int(x) for x in schedule])
+        opt.schedule = ctypes.cast(sched_buf, _p)
+        opt.schedule_len = len(schedule)
+    trace = None
+    if trace_cap > 0:
+        trace = (ctypes.c_float * (trace_cap * TRACE_COLS))()
+        opt.record_trace = 1
+        opt.trace = ctypes.cast(trace, _p)
+        opt.trace_cap = trace_cap
+        opt.oracle_timing = int(oracle_timing)
+    st = TraversalStats()
+    _check(lib().ghb_bfs(_ws(ws), g.n, _ptr(g.rowptr), _ptr(g.col) if g.m else None, _ptr(irp),
+                         _ptr(icol) if icol is not None and icol.numel() else None, src, max_depth,
+                         _ptr(depth), ctypes.byref(opt), ctypes.byref(st)), "ghb_bfs")
+    if trace is not None:
+        import numpy as np
+        rows = min(trace_cap, st.levels)
+        tr = np.frombuffer(trace, dtype=np.float32).reshape(trace_cap, TRACE_COLS)[:rows].copy()
+        return depth, _stats_out(st), tr
+    return depth, _stats_out(st)
+
+
+def bfs_pred(g: CSRGraph, src: int, max_depth: int = INT32_MAX, ws=None):
+    depth = torch.empty(g.n, dtype=torch.int32, device=g.rowptr.device)
+    pred = torch.empty(g.n, dtype=torch.int32, device=g.rowptr.device)
+    irp, icol, _ = g.in_csr()
+    st = TraversalStats()
+    _check(lib().ghb_bfs_pred(_ws(ws), g.n, _ptr(g.rowptr), _ptr(g.col) if g.m else None, _ptr(irp),
+                              _ptr(icol) if icol is not None and icol.numel() else None, src, max_depth,
+                              _ptr(depth), _ptr(pred), None, ctypes.byref(st)), "ghb_bfs_pred")
+    return depth, pred
+
+
+def sssp(g: CSRGraph, src: int, inf: float = DBL_MAX, delta: float = 0.0, out=None, ws=None):
+    """FP64 distances from src (`inf` = unreached).  Returns (dist, stats)."""
+    dist = out if out is not None else torch.empty(g.n, dtype=torch.float64, device=g.rowptr.device)
+    opt = SsspOptions(delta=delta)
+    st = TraversalStats()
+    _check(lib().ghb_sssp(_ws(ws), g.n, _ptr(g.rowptr), _ptr(g.col) if g.m else None,
+                          _ptr(g.w) if g.m else None, src, inf, _ptr(dist), ctypes.byref(opt),
+                          ctypes.byref(st)), "ghb_sssp")
+    return dist, _stats_out(st)
+
+
+def sssp_pred(g: CSRGraph, src: int, inf: float = DBL_MAX, ws=None):
+    dist = torch.empty(g.n, dtype=torch.float64, device=g.rowptr.device)
+    pred = torch.empty(g.n, dtype=torch.int32, device=g.rowptr.device)
+    irp, icol, iw = g.in_csr()
+    st = TraversalStats()
+    has = g.m > 0
+    _check(lib().ghb_sssp_pred(_ws(ws), g.n, _ptr(g.rowptr), _ptr(g.col) if has else None,
+                               _ptr(g.w) if has else None, _ptr(irp), _ptr(icol) if has else None,
+                               _ptr(iw) if has else None, src, inf, _ptr(dist), _ptr(pred), None,
+                               ctypes.byref(st)), "ghb_sssp_pred")
+    return dist, pred
+
+
+def wcc(g: CSRGraph, out=None, ws=None):
+    """Smallest vertex id of each vertex's weak component."""
+    lab = out if out is not None else torch.empty(g.n, dtype=torch.int32, device=g.rowptr.device)
+    _check(lib().ghb_wcc(_ws(ws), g.n, _ptr(g.rowptr), _ptr(g.col) if g.m else None, _ptr(lab)), "ghb_wcc")
+    return lab
+
+
+def pagerank(g: CSRGraph, iterations: int = 10, damping: float = 0.85, precision: int = PR_FP64,
+             tolerance: float = 0.0, l1_history=False, out=None, ws=None):
+    """LDBC PageRank.  Returns (rank, iterations_run, l1_per_iteration or None)."""
+    rank = out if out is not None else torch.empty(g.n, dtype=torch.float64, device=g.rowptr.device)
+    irp, icol, _ = g.in_csr()
+    hist = (ctypes.c_double * max(1, iterations))() if l1_history else None
+    opt = PrOptions(iterations=iterations, damping=damping, precision=precision, tolerance=tolerance,
+                    l1_history=ctypes.cast(hist, _p) if hist is not None else None)
+    ran = _i32()
+    _check(lib().ghb_pagerank(_ws(ws), g.n, _ptr(irp), _ptr(icol) if icol.numel() else None, _ptr(g.rowptr),
+                              ctypes.byref(opt), _ptr(rank), ctypes.byref(ran)), "ghb_pagerank")
+    h = list(hist)[: ran.value] if hist is not None else None
+    return rank, ran.value, h
+
+
+def cdlp(g: CSRGraph, iterations: int = 10, out=None, ws=None):
+    """Label propagation over in+out neighbours, smallest label on ties."""
+    lab = out if out is not None else torch.empty(g.n, dtype=torch.int32, device=g.rowptr.device)
+    arp, acol = g.all_csr(ws)
+    _check(lib().ghb_cdlp(_ws(ws), g.n, _ptr(arp), _ptr(acol) if acol.numel() else None, iterations,
+                          _ptr(lab)), "ghb_cdlp")
+    return lab
+
+
+def tc(g: CSRGraph, ws=None):
+    """Per-vertex counts as the reference computes them.  Returns
+    (counts64, counts32 (the reference's wrapping int32), triangles)."""
+    c64 = torch.empty(g.n, dtype=torch.int64, device=g.rowptr.device)
+    c32 = torch.empty(g.n, dtype=torch.int32, device=g.rowptr.device)
+    total = _i64()
+    _check(lib().ghb_tc(_ws(ws), g.n, _ptr(g.rowptr), _ptr(g.col) if g.m else None, _ptr(c64), _ptr(c32),
+                        ctypes.byref(total)), "ghb_tc")
+    return c64, c32, total.value

@@ -1,0 +1,202 @@
+// Single-source BFS: direction-optimising (top-down push over a vertex queue,
+// bottom-up pull over a frontier bitmap), replacing the reference's
+// expand/contract queue BFS (GPU_BFS_csr.cuh:15-327) and its push/pull
+// variant (GPU_BFS_pre_csr.cuh:18-124).  Output semantics follow the CPU
+// oracle (CPU_BFS.hpp:10-41): depth[v] = hop distance from src, INT32_MAX when
+// unreached or deeper than max_depth.
+//
+// Layout in HBM: depth int32[n] (the output, written once per vertex); a
+// visited bitmap and two frontier bitmaps of ceil(n/32) words (L2 resident:
+// 2 MiB each at n = 2^24); two int32[n] vertex queues.
+#include <cmath>
+#include <vector>
+
+#include "bfs_kernels.cuh"
+#include "common.cuh"
+#include "policy.cuh"
+
+namespace ghb {
+
+int bfs_run(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32_t* out_col,
+            const int32_t* in_rowptr, const int32_t* in_col, int32_t src, int32_t max_depth,
+            int32_t* depth, const ghb_bfs_options* opt, ghb_traversal_stats* stats) {
+    GHB_REQUIRE(n >= 1, "n must be >= 1");
+    GHB_REQUIRE(out_rowptr && depth, "NULL graph or output");
+    GHB_REQUIRE(src >= 0 && src < n, "source outside [0, n)");
+    GHB_REQUIRE(max_depth >= 0, "max_depth < 0");
+    ghb_bfs_options defaults = {};
+    if (!opt) opt = &defaults;
+    const bool can_pull = in_rowptr != nullptr && in_col != nullptr;
+    int policy = opt->policy;
+    if ((policy == GHB_POLICY_PULL || policy == GHB_POLICY_SCHEDULE || policy == GHB_POLICY_LEARNED ||
+         policy == GHB_POLICY_HEURISTIC) && !can_pull)
+        policy = GHB_POLICY_PUSH;
+    GHB_REQUIRE(!(opt->record_trace && (!opt->trace || opt->trace_cap <= 0)), "trace buffer missing");
+    const float alpha = opt->alpha > 0 ? opt->alpha : 14.0f;
+    const float beta = opt->beta > 0 ? opt->beta : 24.0f;
+
+    const int64_t words = ((int64_t)n + 31) / 32;
+    Carver sizing(nullptr);
+    BfsBuffers::carve(sizing, n, words);
+    GHB_TRY(ws_reserve(ws, sizing.off));
+    Carver c(ws->scratch);
+    BfsBuffers B = BfsBuffers::carve(c, n, words);
+
+    cudaStream_t st = ws->stream;
+    // m (total CSR entries) and deg(src) from rowptr.
+    int32_t* hp32 = reinterpret_cast<int32_t*>(ws->host_pinned);
+    GHB_CUDA_TRY(cudaMemcpyAsync(hp32, out_rowptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaMemcpyAsync(hp32 + 1, out_rowptr + src, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GHB_TRY(launch(ws, bfs_init_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n,
+                   words, src, depth, B.visited, B.front_a, B.queue_a));
+    if (stats || opt->record_trace) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    const int64_t m_total = hp32[0];
+    const int64_t deg_src = (int64_t)hp32[2] - hp32[1];
+
+    int64_t n_f = 1, m_f = deg_src, m_r = deg_src, examined = 0, reached = 1;
+    double deg2_f = (double)deg_src * deg_src, degmax_f = (double)deg_src;
+    int level = 0, pull_levels = 0, dir = 0 /* 0 push, 1 pull */, prev_dir = 0;
+    float prev_ms = 0.f;
+    int32_t *q_cur = B.queue_a, *q_next = B.queue_b;
+    uint32_t *f_cur = B.front_a, *f_next = B.front_b;
+    const int threads = 256;
+    const unsigned gmax = ws->num_sms * 8;
+
+    while (n_f > 0 && level < max_depth) {
+        // ---- direction for this level
+        const int64_t m_u = m_total - m_r;
+        if (policy == GHB_POLICY_PUSH) {
+            dir = 0;
+        } else if (policy == GHB_POLICY_PULL) {
+            dir = level == 0 ? 0 : 1;
+        } else if (policy == GHB_POLICY_SCHEDULE) {
+            dir = (opt->schedule && level < opt->schedule_len) ? (opt->schedule[level] ? 1 : 0) : dir;
+        } else {
+            int heur = dir;
+            if (dir == 0 && (double)m_f > (double)m_u / alpha) heur = 1;
+            else if (dir == 1 && (double)n_f < (double)n / beta) heur = 0;
+            dir = heur;
+            if (policy == GHB_POLICY_LEARNED) {
+                float feat[GHB_TRACE_FEATURES];
+                bfs_features(feat, n, m_total, n_f, m_f, m_u, level, deg2_f, degmax_f, prev_dir, prev_ms);
+                int d = policy_pick_direction(feat);
+                if (d >= 0) dir = d;
+            }
+        }
+        float row[GHB_TRACE_COLS];
+        if (opt->record_trace && level < opt->trace_cap) {
+            bfs_features(row, n, m_total, n_f, m_f, m_u, level, deg2_f, degmax_f, prev_dir, prev_ms);
+            row[13] = row[14] = row[15] = -1.f;
+        }
+
+        float t_push = -1.f, t_pull = -1.f;
+        if (opt->oracle_timing && can_pull && opt->record_trace) {
+            // Time both directions on a snapshot; the state after a level does
+            // not depend on the direction, so the run continues unchanged.
+            GHB_TRY(bfs_time_both(ws, B, n, words, out_rowptr, out_col, in_rowptr, in_col, q_cur, n_f,
+                                  f_cur, level, depth, &t_push, &t_pull));
+        }
+
+        GHB_CUDA_TRY(cudaMemsetAsync(B.counters, 0, sizeof(BfsCounters), st));
+        GHB_CUDA_TRY(cudaMemsetAsync(f_next, 0, words * sizeof(uint32_t), st));
+        if (opt->record_trace) GHB_CUDA_TRY(cudaEventRecord(ws->ev_a, st));
+        if (dir == 0) {
+            GHB_TRY(bfs_push_level(ws, B, n, out_rowptr, out_col, q_cur, n_f, level + 1, depth,
+                                   q_next, f_next));
+        } else {
+            GHB_TRY(launch(ws, bfs_pull_kernel, dim3(grid_for(words * 32, threads, gmax)),
+                           dim3(threads), 0, n, words, in_rowptr, in_col, out_rowptr,
+                           (const uint32_t*)f_cur, B.visited, f_next, depth, level + 1, q_next,
+                           B.counters));
+            pull_levels++;
+        }
+        if (opt->record_trace) GHB_CUDA_TRY(cudaEventRecord(ws->ev_b, st));
+        GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, B.counters, sizeof(BfsCounters),
+                                     cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        const BfsCounters* hc = reinterpret_cast<const BfsCounters*>(ws->host_pinned);
+        float ms = 0.f;
+        if (opt->record_trace) GHB_CUDA_TRY(cudaEventElapsedTime(&ms, ws->ev_a, ws->ev_b));
+        if (opt->record_trace && level < opt->trace_cap) {
+            row[12] = (float)dir;
+            row[13] = ms;
+            row[14] = t_push;
+            row[15] = t_pull;
+            const double unvisited = (double)(n - reached);
+            row[16] = (float)hc->examined;
+            row[17] = (float)hc->tail;
+            row[18] = (float)unvisited;
+            // Pull reads the rowptr of every unvisited vertex; push reads the
+            // rowptr of every frontier vertex.  Both read 4 B per entry
+            // examined and write 4 B of depth per vertex reached.
+            row[19] = (float)(4.0 * (dir ? unvisited : (double)n_f) + 4.0 * (double)hc->examined +
+                              4.0 * (double)hc->tail);
+            for (int k = 0; k < GHB_TRACE_COLS; ++k) opt->trace[(size_t)level * GHB_TRACE_COLS + k] = row[k];
+        }
+        prev_dir = dir;
+        prev_ms = ms;
+        n_f = hc->tail;
+        m_f = (int64_t)hc->m_f;
+        deg2_f = (double)hc->deg2;
+        degmax_f = (double)hc->degmax;
+        examined += (int64_t)hc->examined;
+        m_r += m_f;
+        reached += n_f;
+        std::swap(q_cur, q_next);
+        std::swap(f_cur, f_next);
+        ++level;
+    }
+    if (stats) {
+        GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
+        GHB_CUDA_TRY(cudaEventSynchronize(ws->ev_stop));
+        float ms = 0.f;
+        GHB_CUDA_TRY(cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop));
+        stats->levels = level;
+        stats->pull_levels = pull_levels;
+        stats->reached = reached;
+        stats->edges_reached = m_r;
+        stats->edges_examined = examined;
+        stats->device_ms = ms;
+    }
+    return GHB_OK;
+}
+
+}  // namespace ghb
+
+using namespace ghb;
+
+extern "C" {
+
+int ghb_bfs(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32_t* out_col,
+            const int32_t* in_rowptr, const int32_t* in_col, int32_t src, int32_t max_depth,
+            int32_t* depth, const ghb_bfs_options* options, ghb_traversal_stats* stats) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    return bfs_run(ws, n, out_rowptr, out_col, in_rowptr, in_col, src, max_depth, depth, options,
+                   stats);
+}
+
+int ghb_bfs_pred(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32_t* out_col,
+                 const int32_t* in_rowptr, const int32_t* in_col, int32_t src, int32_t max_depth,
+                 int32_t* depth, int32_t* pred, const ghb_bfs_options* options,
+                 ghb_traversal_stats* stats) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    GHB_REQUIRE(pred != nullptr, "NULL pred");
+    GHB_TRY(bfs_run(ws, n, out_rowptr, out_col, in_rowptr, in_col, src, max_depth, depth, options,
+                    stats));
+    const unsigned gmax = ws->num_sms * 8;
+    if (in_rowptr && in_col) {
+        // Smallest-id parent: first entry of the (sorted) in-row one level up.
+        return launch(ws, bfs_pred_pull_kernel, dim3(grid_for((int64_t)n * 32, 256, gmax)), dim3(256),
+                      0, n, in_rowptr, in_col, (const int32_t*)depth, src, pred);
+    }
+    GHB_TRY(launch(ws, fill_i32_kernel, dim3(grid_for(n, 256, gmax)), dim3(256), 0, pred, (int64_t)n,
+                   (int32_t)0x7fffffff));
+    GHB_TRY(launch(ws, bfs_pred_push_kernel, dim3(grid_for((int64_t)n * 32, 256, gmax)), dim3(256), 0,
+                   n, out_rowptr, out_col, (const int32_t*)depth, pred));
+    return launch(ws, bfs_pred_finish_kernel, dim3(grid_for(n, 256, gmax)), dim3(256), 0, n, src, pred);
+}
+
+}  // extern "C"

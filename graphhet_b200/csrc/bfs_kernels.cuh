@@ -1,0 +1,84 @@
+// Device kernels of the single-source BFS (see bfs.cu for the driver).
+#pragma once
+
+#include "common.cuh"
+
+namespace ghb {
+
+// Lists at least this long are expanded edge-parallel across the whole grid
+// instead of by one warp.
+constexpr int32_t kBigList = 4096;
+
+struct BfsCounters {
+    int32_t tail;       // next-queue length
+    int32_t big_tail;   // deferred long lists this level
+    unsigned long long m_f;       // sum of out-degrees of newly reached vertices
+    unsigned long long examined;  // CSR entries read
+    double deg2;                  // sum of squared out-degrees (trace features)
+    unsigned int degmax;
+    int32_t pad;
+    unsigned long long big_edges;  // entries in the deferred long lists
+};
+
+struct BfsBuffers {
+    uint32_t* visited;
+    uint32_t* front_a;
+    uint32_t* front_b;
+    int32_t* queue_a;
+    int32_t* queue_b;
+    int32_t* big;          // deferred long-list vertices
+    int64_t* big_prefix;   // exclusive prefix of their degrees (+ total)
+    int32_t* depth_snap;   // snapshots for oracle timing
+    uint32_t* visited_snap;
+    BfsCounters* counters;
+
+    static BfsBuffers carve(Carver& c, int32_t n, int64_t words) {
+        BfsBuffers b;
+        b.visited = c.take<uint32_t>(words);
+        b.front_a = c.take<uint32_t>(words);
+        b.front_b = c.take<uint32_t>(words);
+        b.queue_a = c.take<int32_t>(n);
+        b.queue_b = c.take<int32_t>(n);
+        b.big = c.take<int32_t>(n);
+        b.big_prefix = c.take<int64_t>((size_t)n + 1);
+        b.depth_snap = c.take<int32_t>(n);
+        b.visited_snap = c.take<uint32_t>(words);
+        b.counters = c.take<BfsCounters>(1);
+        return b;
+    }
+};
+
+__global__ void fill_i32_kernel(int32_t* p, int64_t count, int32_t value);
+
+__global__ void bfs_init_kernel(int32_t n, int64_t words, int32_t src, int32_t* depth,
+                                uint32_t* visited, uint32_t* front, int32_t* queue);
+
+__global__ void bfs_pull_kernel(int32_t n, int64_t words, const int32_t* __restrict__ in_rp,
+                                const int32_t* __restrict__ in_col,
+                                const int32_t* __restrict__ out_rp,
+                                const uint32_t* __restrict__ f_cur, uint32_t* visited,
+                                uint32_t* f_next, int32_t* depth, int32_t next_depth,
+                                int32_t* q_next, BfsCounters* cnt);
+
+__global__ void bfs_pred_pull_kernel(int32_t n, const int32_t* __restrict__ in_rp,
+                                     const int32_t* __restrict__ in_col,
+                                     const int32_t* __restrict__ depth, int32_t src,
+                                     int32_t* __restrict__ pred);
+__global__ void bfs_pred_push_kernel(int32_t n, const int32_t* __restrict__ out_rp,
+                                     const int32_t* __restrict__ out_col,
+                                     const int32_t* __restrict__ depth, int32_t* pred);
+__global__ void bfs_pred_finish_kernel(int32_t n, int32_t src, int32_t* pred);
+
+// One top-down level: the queue kernel (short and medium lists), then the
+// long lists edge-parallel.
+int bfs_push_level(ghb_workspace* ws, const BfsBuffers& B, int32_t n, const int32_t* rowptr,
+                   const int32_t* col, const int32_t* q_cur, int64_t n_f, int32_t next_depth,
+                   int32_t* depth, int32_t* q_next, uint32_t* f_next);
+
+// Oracle timing of both directions for one level (state restored after each).
+int bfs_time_both(ghb_workspace* ws, const BfsBuffers& B, int32_t n, int64_t words,
+                  const int32_t* out_rowptr, const int32_t* out_col, const int32_t* in_rowptr,
+                  const int32_t* in_col, const int32_t* q_cur, int64_t n_f, const uint32_t* f_cur,
+                  int level, int32_t* depth, float* t_push, float* t_pull);
+
+}  // namespace ghb

@@ -1,0 +1,107 @@
+// Seeded synthetic graph generators (RMAT, 2-D grid, Erdos-Renyi).  The edge
+// lists are pure functions of (seed, edge number) defined in ghb_gen.h, so a
+// CPU restatement reproduces them exactly.
+#include "common.cuh"
+#include "ghb_gen.h"
+
+namespace ghb {
+namespace {
+
+__global__ void rmat_kernel(int scale, int64_t n_edges, uint64_t stream, ghb_rmat_thresholds t,
+                            int permute, ghb_perm perm, int32_t* __restrict__ src,
+                            int32_t* __restrict__ dst) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_edges;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t u, v;
+        ghb_rmat_edge(stream, t, scale, (uint64_t)e, &u, &v);
+        if (permute) {
+            u = ghb_perm_apply(&perm, u);
+            v = ghb_perm_apply(&perm, v);
+        }
+        src[e] = (int32_t)u;
+        dst[e] = (int32_t)v;
+    }
+}
+
+__global__ void grid_kernel(int32_t rows, int32_t cols, int32_t* __restrict__ src,
+                            int32_t* __restrict__ dst) {
+    // Edges 0 .. rows*(cols-1)-1 go right, the rest go down.
+    int64_t right = (int64_t)rows * (cols - 1);
+    int64_t down = (int64_t)(rows - 1) * cols;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < right + down;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t u, v;
+        if (e < right) {
+            int64_t r = e / (cols - 1), c = e % (cols - 1);
+            u = r * cols + c;
+            v = u + 1;
+        } else {
+            int64_t k = e - right;
+            u = k;
+            v = k + cols;
+        }
+        src[e] = (int32_t)u;
+        dst[e] = (int32_t)v;
+    }
+}
+
+__global__ void er_kernel(uint32_t n, int64_t n_edges, uint64_t stream, int32_t* __restrict__ src,
+                          int32_t* __restrict__ dst) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_edges;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t u, v;
+        ghb_er_edge(stream, n, (uint64_t)e, &u, &v);
+        src[e] = (int32_t)u;
+        dst[e] = (int32_t)v;
+    }
+}
+
+}  // namespace
+}  // namespace ghb
+
+using namespace ghb;
+
+extern "C" {
+
+int ghb_gen_rmat(ghb_workspace* ws, int32_t scale, int64_t n_edges, uint64_t seed, double a,
+                 double b, double c, int32_t permute, int32_t* src, int32_t* dst) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    GHB_REQUIRE(scale >= 0 && scale <= 30, "scale must be in [0, 30]");
+    GHB_REQUIRE(n_edges >= 0, "n_edges < 0");
+    GHB_REQUIRE(n_edges == 0 || (src && dst), "NULL output");
+    GHB_REQUIRE(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0, "bad RMAT probabilities");
+    ghb_rmat_thresholds t = ghb_rmat_make_thresholds(a, b, c);
+    ghb_perm perm = ghb_perm_make(seed, scale);
+    uint64_t stream = ghb_stream(seed, GHB_PURPOSE_RMAT);
+    unsigned g = grid_for(n_edges, 256, ws->num_sms * 16);
+    return launch(ws, rmat_kernel, dim3(g), dim3(256), 0, (int)scale, n_edges, stream, t,
+                  (int)permute, perm, src, dst);
+}
+
+int ghb_gen_grid(ghb_workspace* ws, int32_t rows, int32_t cols, int32_t* src, int32_t* dst) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    GHB_REQUIRE(rows >= 1 && cols >= 1, "rows and cols must be >= 1");
+    GHB_REQUIRE((int64_t)rows * cols < (1ll << 31), "grid too large for int32 ids");
+    int64_t ne = (int64_t)rows * (cols - 1) + (int64_t)(rows - 1) * cols;
+    if (ne == 0) return GHB_OK;
+    GHB_REQUIRE(src && dst, "NULL output");
+    unsigned g = grid_for(ne, 256, ws->num_sms * 16);
+    return launch(ws, grid_kernel, dim3(g), dim3(256), 0, rows, cols, src, dst);
+}
+
+int ghb_gen_er(ghb_workspace* ws, int32_t n, int64_t n_edges, uint64_t seed, int32_t* src,
+               int32_t* dst) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    GHB_REQUIRE(n >= 1, "n must be >= 1");
+    GHB_REQUIRE(n_edges >= 0, "n_edges < 0");
+    if (n_edges == 0) return GHB_OK;
+    GHB_REQUIRE(src && dst, "NULL output");
+    unsigned g = grid_for(n_edges, 256, ws->num_sms * 16);
+    return launch(ws, er_kernel, dim3(g), dim3(256), 0, (uint32_t)n, n_edges,
+                  ghb_stream(seed, GHB_PURPOSE_ER), src, dst);
+}
+
+}  // extern "C"

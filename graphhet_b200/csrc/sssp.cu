@@ -1,0 +1,410 @@
+// Single-source shortest paths, FP64, by delta-stepping in its near/far form
+// (replaces the reference's frontier Bellman-Ford, GPU_SSSP_csr.cuh:23-327,
+// which materialises an 8-byte entry per improving edge and syncs the host
+// every round).  Semantics: the CPU Dijkstra (CPU_shortest_paths.hpp:19-64).
+//
+// Both compute, for every vertex, the minimum over paths of the
+// left-to-right FP64 sum of the path's weights: a relaxation only ever
+// lowers dist[v] to fl(dist[u] + w), fl is monotone and fl(x + w) >= x for
+// w >= 0, so any relaxation order reaches the same least fixpoint, bit for
+// bit.  dist is updated with a 64-bit atomicMin on the bit pattern, which
+// orders non-negative doubles like the values themselves.
+//
+// Phase loop: vertices whose tentative distance is below the threshold form
+// the near queue and are relaxed until the queue is empty (one load-balanced
+// pass over their out-rows per round, edge_walk.cuh); improvements at or
+// above the threshold go to the far list.  Then the threshold moves up by
+// delta and the far list is split.  A vertex enters a queue at most once per
+// round (stamp arrays).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "edge_walk.cuh"
+#include "policy.cuh"
+
+namespace ghb {
+namespace {
+
+struct SsspCounters {
+    int32_t near_tail;
+    int32_t far_tail;
+    int32_t split_near;
+    int32_t pad;
+    unsigned long long examined;
+    unsigned long long improved;
+};
+
+__device__ __forceinline__ double ld_dist(const unsigned long long* d, int32_t v) {
+    return __longlong_as_double((long long)__ldcg(d + v));
+}
+
+struct RelaxVisitor {
+    const double* w;
+    unsigned long long* dist;
+    double threshold;
+    int32_t* near_next;
+    int32_t* near_stamp;
+    int32_t round;
+    int32_t* far;
+    int32_t* far_stamp;
+    int32_t phase;
+    SsspCounters* cnt;
+    unsigned long long examined;
+    __device__ bool want_row(int32_t) const { return true; }
+    __device__ void operator()(int32_t u, int32_t v, int32_t j) {
+        ++examined;
+        const double nd = ld_dist(dist, u) + w[j];
+        if (nd < ld_dist(dist, v)) {
+            const unsigned long long nb = (unsigned long long)__double_as_longlong(nd);
+            const unsigned long long old = atomicMin(dist + v, nb);
+            if (nb < old) {
+                if (nd < threshold) {
+                    if (atomicExch(near_stamp + v, round) != round) {
+                        const int32_t pos = atomicAdd(&cnt->near_tail, 1);
+                        near_next[pos] = v;
+                    }
+                } else {
+                    if (atomicExch(far_stamp + v, phase) != phase) {
+                        const int32_t pos = atomicAdd(&cnt->far_tail, 1);
+                        far[pos] = v;
+                    }
+                }
+            }
+        }
+    }
+    __device__ void finish() {
+        unsigned long long e = warp_sum(examined);
+        if (lane_id() == 0 && e) atomicAdd(&cnt->examined, e);
+    }
+};
+
+__global__ void sssp_init_kernel(int32_t n, int32_t src, double inf, unsigned long long* dist,
+                                 int32_t* near_stamp, int32_t* far_stamp, int32_t* near_q) {
+    const unsigned long long ib = (unsigned long long)__double_as_longlong(inf);
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        dist[v] = (v == src) ? 0ull : ib;
+        near_stamp[v] = -1;
+        far_stamp[v] = -1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) near_q[0] = src;
+}
+
+// Split the far list at a new threshold: entries already settled (below the
+// old threshold) are dropped, entries below the new one go to the near
+// queue, the rest to the next far list.
+__global__ void sssp_split_kernel(const int32_t* __restrict__ far, int32_t far_count,
+                                  const unsigned long long* dist, double old_thr, double new_thr,
+                                  int32_t* near_q, int32_t* near_stamp, int32_t round, int32_t* far_next,
+                                  int32_t* far_stamp, int32_t phase, SsspCounters* cnt,
+                                  double* min_far) {
+    double mn = INFINITY;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < far_count;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = far[i];
+        const double d = ld_dist(dist, v);
+        if (d < old_thr) continue;
+        if (d < new_thr) {
+            if (atomicExch(near_stamp + v, round) != round) near_q[atomicAdd(&cnt->split_near, 1)] = v;
+        } else {
+            if (atomicExch(far_stamp + v, phase) != phase) far_next[atomicAdd(&cnt->far_tail, 1)] = v;
+            mn = d < mn ? d : mn;
+        }
+    }
+    // Smallest distance left in the far list, to skip empty buckets.
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double x = __shfl_xor_sync(0xffffffffu, mn, o);
+        mn = x < mn ? x : mn;
+    }
+    if (lane_id() == 0 && mn < INFINITY)
+        atomicMin(reinterpret_cast<unsigned long long*>(min_far), (unsigned long long)__double_as_longlong(mn));
+}
+
+__global__ void mean_weight_kernel(const double* __restrict__ w, int64_t m, int64_t stride, double* out) {
+    double s = 0.0;
+    int64_t c = 0;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * stride; i < m;
+         i += (int64_t)gridDim.x * blockDim.x * stride) {
+        s += w[i];
+        ++c;
+    }
+    s = warp_sum(s);
+    double cd = warp_sum((double)c);
+    if (lane_id() == 0) {
+        atomicAdd(out, s);
+        atomicAdd(out + 1, cd);
+    }
+}
+
+// Predecessors after the distances are final: the smallest-id u in v's
+// in-row with dist[u] + w(u, v) == dist[v] exactly.
+__global__ void sssp_pred_pull_kernel(int32_t n, int32_t src, const int32_t* __restrict__ in_rp,
+                                      const int32_t* __restrict__ in_col, const double* __restrict__ in_w,
+                                      const double* __restrict__ dist, double inf, int32_t* __restrict__ pred) {
+    const int lane = lane_id();
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t v = warp; v < n; v += nwarps) {
+        const double dv = dist[v];
+        int32_t p = -1;
+        if (v != src && dv != inf) {
+            const int32_t b = in_rp[v], e = in_rp[v + 1];
+            for (int32_t k0 = b; k0 < e; k0 += 32) {
+                const int32_t k = k0 + lane;
+                bool h = false;
+                int32_t u = -1;
+                if (k < e) {
+                    u = in_col[k];
+                    const double du = dist[u];
+                    h = du != inf && du + in_w[k] == dv;
+                }
+                const unsigned hm = __ballot_sync(0xffffffffu, h);
+                if (hm) {
+                    p = __shfl_sync(0xffffffffu, u, __ffs(hm) - 1);
+                    break;
+                }
+            }
+        }
+        if (lane == 0) pred[v] = p;
+    }
+}
+
+__global__ void sssp_pred_push_kernel(int32_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                                      const double* __restrict__ w, const double* __restrict__ dist, double inf,
+                                      int32_t* pred) {
+    const int lane = lane_id();
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t u = warp; u < n; u += nwarps) {
+        const double du = dist[u];
+        if (du == inf) continue;
+        for (int32_t k = rp[u] + lane; k < rp[u + 1]; k += 32) {
+            const int32_t v = col[k];
+            if (du + w[k] == dist[v]) atomicMin(pred + v, (int32_t)u);
+        }
+    }
+}
+
+__global__ void sssp_pred_finish_kernel(int32_t n, int32_t src, int32_t* pred) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x)
+        if (v == src || pred[v] == 0x7fffffff) pred[v] = -1;
+}
+
+__global__ void reached_edges_kernel(int32_t n, const int32_t* __restrict__ rp, const double* __restrict__ dist,
+                                     double inf, unsigned long long* out) {
+    unsigned long long e = 0, r = 0;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        if (dist[v] != inf) {
+            e += (unsigned long long)(rp[v + 1] - rp[v]);
+            ++r;
+        }
+    }
+    e = warp_sum(e);
+    r = warp_sum(r);
+    if (lane_id() == 0) {
+        atomicAdd(out, e);
+        atomicAdd(out + 1, r);
+    }
+}
+
+__global__ void fill_i32(int32_t* p, int64_t count, int32_t value) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = value;
+}
+
+}  // namespace
+
+// Bucket width from a weight sample when the caller gives none: the mean
+// weight times 32 over the mean degree (wider buckets on sparse graphs,
+// where rounds are latency-bound).
+int sssp_pick_delta(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const double* w, double* delta) {
+    cudaStream_t st = ws->stream;
+    int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
+    GHB_CUDA_TRY(cudaMemcpyAsync(hp, rowptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    const int64_t m = hp[0];
+    if (m == 0) {
+        *delta = 1.0;
+        return GHB_OK;
+    }
+    double* acc = reinterpret_cast<double*>(ws->dev_small);
+    GHB_CUDA_TRY(cudaMemsetAsync(acc, 0, 2 * sizeof(double), st));
+    const int64_t stride = std::max<int64_t>(1, m / (1 << 20));
+    GHB_TRY(launch(ws, mean_weight_kernel, dim3(64), dim3(256), 0, w, m, stride, acc));
+    GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, acc, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    const double* h = reinterpret_cast<const double*>(ws->host_pinned);
+    const double mean_w = h[1] > 0 ? h[0] / h[1] : 1.0;
+    const double mean_d = (double)m / (double)n;
+    double d = mean_w * 32.0 / std::max(1.0, mean_d);
+    if (!(d > 0)) d = 1.0;
+    *delta = d;
+    return GHB_OK;
+}
+
+int sssp_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, const double* w,
+             int32_t src, double inf, double* dist_out, const ghb_sssp_options* opt,
+             ghb_traversal_stats* stats) {
+    GHB_REQUIRE(n >= 1, "n must be >= 1");
+    GHB_REQUIRE(rowptr && dist_out, "NULL argument");
+    GHB_REQUIRE(src >= 0 && src < n, "source outside [0, n)");
+    GHB_REQUIRE(inf >= 0, "inf must be >= 0");
+    ghb_sssp_options defaults = {};
+    if (!opt) opt = &defaults;
+    cudaStream_t st = ws->stream;
+    double delta = opt->delta;
+    if (!(delta > 0)) GHB_TRY(sssp_pick_delta(ws, n, rowptr, w, &delta));
+
+    Carver sizing(nullptr);
+    auto carve = [&](Carver& c, WalkBuffers* wb, int32_t** qa, int32_t** qb, int32_t** fa, int32_t** fb,
+                     int32_t** ns, int32_t** fs, SsspCounters** cnt, double** minfar) {
+        *wb = WalkBuffers::carve(c, n);
+        *qa = c.take<int32_t>(n);
+        *qb = c.take<int32_t>(n);
+        *fa = c.take<int32_t>(n);
+        *fb = c.take<int32_t>(n);
+        *ns = c.take<int32_t>(n);
+        *fs = c.take<int32_t>(n);
+        *cnt = c.take<SsspCounters>(1);
+        *minfar = c.take<double>(1);
+    };
+    WalkBuffers wb;
+    int32_t *qa, *qb, *fa, *fb, *ns, *fs;
+    SsspCounters* cnt;
+    double* minfar;
+    carve(sizing, &wb, &qa, &qb, &fa, &fb, &ns, &fs, &cnt, &minfar);
+    GHB_TRY(ws_reserve(ws, sizing.off));
+    Carver c(ws->scratch);
+    carve(c, &wb, &qa, &qb, &fa, &fb, &ns, &fs, &cnt, &minfar);
+
+    unsigned long long* dist = reinterpret_cast<unsigned long long*>(dist_out);
+    const unsigned g = grid_for(n, 256, ws->num_sms * 8);
+    if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
+    GHB_TRY(launch(ws, sssp_init_kernel, dim3(g), dim3(256), 0, n, src, inf, dist, ns, fs, qa));
+    GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(SsspCounters), st));
+    int64_t near_count = 1, far_count = 0, examined = 0, rounds = 0;
+    int32_t round = 0, phase = 0;
+    double thr = delta;
+    const SsspCounters* hc = reinterpret_cast<const SsspCounters*>(ws->host_pinned);
+    // Budget: every productive round lowers some distance; n rounds per phase
+    // and n phases with work bound any correct run.
+    const int64_t round_budget = 64ll * n + 1024;
+    while (true) {
+        while (near_count > 0) {
+            if (++rounds > round_budget) {
+                set_error("SSSP round budget exhausted");
+                return GHB_ERR_LIMIT;
+            }
+            ++round;
+            GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, offsetof(SsspCounters, far_tail), st));
+            GHB_CUDA_TRY(cudaMemsetAsync(&cnt->examined, 0, sizeof(unsigned long long), st));
+            RelaxVisitor f{w, dist, thr, qb, ns, round, fa, fs, phase, cnt, 0ull};
+            GHB_TRY(walk(ws, rowptr, col, (const int32_t*)qa, (const int32_t*)nullptr, near_count, near_count,
+                         wb, f));
+            GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, cnt, sizeof(SsspCounters), cudaMemcpyDeviceToHost, st));
+            GHB_CUDA_TRY(cudaStreamSynchronize(st));
+            near_count = hc->near_tail;
+            far_count = hc->far_tail;
+            examined += (int64_t)hc->examined;
+            std::swap(qa, qb);
+        }
+        if (far_count == 0) break;
+        // Advance the threshold past empty buckets: to the first multiple of
+        // delta above the smallest far distance.
+        ++phase;
+        ++round;
+        const double old_thr = thr;
+        GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(SsspCounters), st));
+        const double big = INFINITY;
+        GHB_CUDA_TRY(cudaMemcpyAsync(minfar, &big, sizeof(double), cudaMemcpyHostToDevice, st));
+        // Two steps: find the minimum (no moves: new_thr = old_thr), then split.
+        GHB_TRY(launch(ws, sssp_split_kernel, dim3(grid_for(far_count, 256, ws->num_sms * 8)), dim3(256), 0,
+                       (const int32_t*)fa, (int32_t)far_count, (const unsigned long long*)dist, old_thr, old_thr,
+                       qa, ns, round, fb, fs, phase, cnt, minfar));
+        GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, cnt, sizeof(SsspCounters), cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(ws->host_pinned) + 256, minfar, sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        const int64_t kept = hc->far_tail;
+        const double mn = *reinterpret_cast<const double*>(reinterpret_cast<const char*>(ws->host_pinned) + 256);
+        if (kept == 0) break;
+        double nthr = old_thr + delta;
+        if (mn >= nthr) nthr = old_thr + delta * std::floor((mn - old_thr) / delta + 1.0);
+        if (!(nthr > mn)) nthr = mn + delta;  // guards rounding
+        ++phase;
+        ++round;
+        GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(SsspCounters), st));
+        GHB_TRY(launch(ws, sssp_split_kernel, dim3(grid_for(kept, 256, ws->num_sms * 8)), dim3(256), 0,
+                       (const int32_t*)fb, (int32_t)kept, (const unsigned long long*)dist, old_thr, nthr, qa, ns,
+                       round, fa, fs, phase, cnt, minfar));
+        GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, cnt, sizeof(SsspCounters), cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        near_count = hc->split_near;
+        far_count = hc->far_tail;
+        thr = nthr;
+    }
+    if (stats) {
+        GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
+        unsigned long long* acc = reinterpret_cast<unsigned long long*>(ws->dev_small);
+        GHB_CUDA_TRY(cudaMemsetAsync(acc, 0, 2 * sizeof(unsigned long long), st));
+        GHB_TRY(launch(ws, reached_edges_kernel, dim3(g), dim3(256), 0, n, rowptr, (const double*)dist_out, inf, acc));
+        GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, acc, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaEventSynchronize(ws->ev_stop));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        float ms = 0.f;
+        GHB_CUDA_TRY(cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop));
+        const unsigned long long* ha = reinterpret_cast<const unsigned long long*>(ws->host_pinned);
+        stats->levels = (int32_t)rounds;
+        stats->pull_levels = phase;
+        stats->edges_reached = (int64_t)ha[0];
+        stats->reached = (int64_t)ha[1];
+        stats->edges_examined = examined;
+        stats->device_ms = ms;
+    }
+    return GHB_OK;
+}
+
+int sssp_pred_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, const double* w,
+                  const int32_t* in_rp, const int32_t* in_col, const double* in_w, int32_t src, double inf,
+                  const double* dist, int32_t* pred) {
+    const unsigned g = ws->num_sms * 8;
+    if (in_rp && in_w) {
+        return launch(ws, sssp_pred_pull_kernel, dim3(grid_for((int64_t)n * 32, 256, g)), dim3(256), 0, n, src,
+                      in_rp, in_col, in_w, dist, inf, pred);
+    }
+    GHB_TRY(launch(ws, fill_i32, dim3(grid_for(n, 256, g)), dim3(256), 0, pred, (int64_t)n, (int32_t)0x7fffffff));
+    GHB_TRY(launch(ws, sssp_pred_push_kernel, dim3(grid_for((int64_t)n * 32, 256, g)), dim3(256), 0, n, rowptr, col,
+                   w, dist, inf, pred));
+    return launch(ws, sssp_pred_finish_kernel, dim3(grid_for(n, 256, g)), dim3(256), 0, n, src, pred);
+}
+
+}  // namespace ghb
+
+using namespace ghb;
+
+extern "C" {
+
+int ghb_sssp(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, const double* w,
+             int32_t src, double inf, double* dist, const ghb_sssp_options* options, ghb_traversal_stats* stats) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    return sssp_run(ws, n, rowptr, col, w, src, inf, dist, options, stats);
+}
+
+int ghb_sssp_pred(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, const double* w,
+                  const int32_t* in_rowptr, const int32_t* in_col, const double* in_w, int32_t src, double inf,
+                  double* dist, int32_t* pred, const ghb_sssp_options* options, ghb_traversal_stats* stats) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    GHB_REQUIRE(pred, "NULL pred");
+    GHB_TRY(sssp_run(ws, n, rowptr, col, w, src, inf, dist, options, stats));
+    return sssp_pred_run(ws, n, rowptr, col, w, in_rowptr, in_col, in_w, src, inf, dist, pred);
+}
+
+}  // extern "C"

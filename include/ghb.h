@@ -1,0 +1,261 @@
+/*
+ * ghb.h - C ABI of the B200 (sm_100a) CSR analytics library (libghb.so).
+ *
+ * Every entry point takes plain device pointers and sizes, runs on the
+ * workspace's CUDA stream, and returns a status code (GHB_OK on success).
+ * A failed call leaves a message for ghb_last_error() (per host thread).
+ *
+ * Graph layout (the reference's CSR_graph, include/GPU_csr/GPU_csr.hpp:97-110):
+ *   rowptr  int32[n + 1]   offsets into col
+ *   col     int32[m]       neighbour ids, sorted ascending inside each row
+ *   w       double[m]      edge weights (SSSP only)
+ * An undirected graph stores both directions; then the "in" arrays may alias
+ * the "out" arrays, exactly as toCSR does for is_directed == false
+ * (GPU_csr.hpp:133-140).
+ *
+ * The header-inline C++ entry points in include/GPU_csr/algorithm/*.cuh
+ * (Cuda_BFS, Cuda_SSSP, ...) are the reference-facing API; they call these.
+ */
+#ifndef GHB_H
+#define GHB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+    GHB_OK = 0,
+    GHB_ERR_INVALID_ARGUMENT = 1,
+    GHB_ERR_CUDA = 2,
+    GHB_ERR_OUT_OF_MEMORY = 3,
+    GHB_ERR_TIMEOUT = 4,   /* a bounded device-side wait gave up           */
+    GHB_ERR_LIMIT = 5,     /* a level / phase / iteration budget ran out     */
+    GHB_ERR_UNSUPPORTED = 6
+};
+
+const char* ghb_status_string(int status);
+/* Detail of the last failure on this host thread ("" if none). */
+const char* ghb_last_error(void);
+/* Library version, major * 10000 + minor * 100 + patch. */
+int ghb_version(void);
+
+/* ------------------------------------------------------------- workspace */
+/* A workspace owns a CUDA stream binding, cached scratch memory, pinned host
+ * counters and timing events.  Calls on one workspace are serialised on its
+ * stream; use one workspace per host thread.  The reference allocates and
+ * frees scratch inside every call (e.g. GPU_BFS_csr.cuh:258-283); the
+ * workspace keeps it across calls instead. */
+typedef struct ghb_workspace ghb_workspace;
+
+int ghb_workspace_create(ghb_workspace** out);
+int ghb_workspace_destroy(ghb_workspace* ws);
+/* Bind a cudaStream_t (NULL = legacy default stream). */
+int ghb_workspace_set_stream(ghb_workspace* ws, void* stream);
+void* ghb_workspace_get_stream(ghb_workspace* ws);
+/* Free cached scratch. */
+int ghb_workspace_trim(ghb_workspace* ws);
+/* Launch counter of this library's kernels on this workspace and the scratch
+ * bytes currently reserved. */
+int ghb_workspace_counters(ghb_workspace* ws, int64_t* kernel_launches, int64_t* scratch_bytes);
+/* Process-wide workspace on the current device (used by the C++ wrappers). */
+ghb_workspace* ghb_default_workspace(void);
+
+/* ------------------------------------------------------------ generators */
+/* Seeded synthetic inputs (include/ghb_gen.h).  Outputs are device arrays of
+ * n_edges entries.  They stand in for the LDBC/Graph500 datasets that the
+ * reference loads from text (include/LDBC/ldbc.hpp:181-253). */
+int ghb_gen_rmat(ghb_workspace* ws, int32_t scale, int64_t n_edges, uint64_t seed,
+                 double a, double b, double c, int32_t permute,
+                 int32_t* src, int32_t* dst);
+/* rows x cols 4-neighbour grid, one entry per undirected edge (right, down):
+ * n_edges = rows*(cols-1) + (rows-1)*cols. */
+int ghb_gen_grid(ghb_workspace* ws, int32_t rows, int32_t cols, int32_t* src, int32_t* dst);
+int ghb_gen_er(ghb_workspace* ws, int32_t n, int64_t n_edges, uint64_t seed,
+               int32_t* src, int32_t* dst);
+
+/* ----------------------------------------------------------- CSR builder */
+/* Build a CSR from an edge list (replaces the host flattening in toCSR,
+ * GPU_csr.hpp:282-339, for edge-list inputs).  Flags: */
+#define GHB_BUILD_SYMMETRIZE 1      /* add (v,u) for every (u,v)                */
+#define GHB_BUILD_DROP_SELF_LOOPS 2 /* drop (u,u)                              */
+#define GHB_BUILD_TRANSPOSE 4       /* build the in-CSR (rows = destinations)  */
+/* Duplicates are always merged (graph_structure::add_edge keeps one entry per
+ * pair, sorted_vector_binary_operations.hpp:89-101).  Weights: if w_in is not
+ * NULL the LAST occurrence of a pair wins (add_edge overwrites); otherwise
+ * weight_mode / weight_seed generate ghb_pair_weight(); mode 0 writes none.
+ * col / w must hold the worst case (n_edges, doubled when symmetrising);
+ * *m_out receives the entry count. */
+int ghb_csr_build(ghb_workspace* ws, int32_t n, const int32_t* src, const int32_t* dst,
+                  const double* w_in, int64_t n_edges, int32_t flags,
+                  int32_t weight_mode, uint64_t weight_seed,
+                  int32_t* rowptr, int32_t* col, double* w, int64_t* m_out);
+/* Transpose an existing CSR (out -> in), weights optional. */
+int ghb_csr_transpose(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* rowptr,
+                      const int32_t* col, const double* w, int32_t* t_rowptr,
+                      int32_t* t_col, double* t_w);
+/* all-CSR of a directed graph: row v = in-neighbours of v then out-neighbours
+ * of v (toCSR, GPU_csr.hpp:315-330). */
+int ghb_csr_merge_in_out(ghb_workspace* ws, int32_t n, const int32_t* in_rowptr,
+                         const int32_t* in_col, const int32_t* out_rowptr,
+                         const int32_t* out_col, int32_t* all_rowptr, int32_t* all_col);
+
+/* ------------------------------------------------------------------- BFS */
+/* Direction policy per level. */
+#define GHB_POLICY_HEURISTIC 0 /* Beamer alpha/beta rule                      */
+#define GHB_POLICY_LEARNED 1   /* the trained MLP (ghb_policy_*); falls back   */
+#define GHB_POLICY_PUSH 2      /* top-down every level                        */
+#define GHB_POLICY_PULL 3      /* bottom-up every level after the first       */
+#define GHB_POLICY_SCHEDULE 4  /* options.schedule[level] (0 push, 1 pull)    */
+
+typedef struct {
+    int32_t policy;
+    float alpha;             /* switch to pull when m_f > m_u / alpha (0: 14) */
+    float beta;              /* back to push when n_f < n / beta (0: 24)      */
+    const int8_t* schedule;  /* host array for GHB_POLICY_SCHEDULE            */
+    int32_t schedule_len;
+    int32_t record_trace;    /* 1: fill trace[] with one row per level         */
+    float* trace;            /* host, trace_cap x GHB_TRACE_COLS               */
+    int32_t trace_cap;
+    int32_t oracle_timing;   /* 1: time push and pull at every level (slow)   */
+} ghb_bfs_options;
+
+/* Trace row: 12 policy features, then direction used, level time (ms),
+ * push time (ms) and pull time (ms) when oracle_timing is set (else -1),
+ * CSR entries read, vertices reached by the level, vertices unvisited
+ * before it, and the level's algorithmic bytes (rowptr + col + depth). */
+#define GHB_TRACE_FEATURES 12
+#define GHB_TRACE_COLS 20
+
+typedef struct {
+    int32_t levels;          /* frontier expansions run                      */
+    int32_t pull_levels;     /* of which bottom-up                           */
+    int64_t reached;         /* vertices with a finite depth                 */
+    int64_t edges_reached;   /* m_r: CSR entries out of reached vertices      */
+    int64_t edges_examined;  /* CSR entries the kernels read                 */
+    double device_ms;        /* CUDA-event time of the traversal             */
+} ghb_traversal_stats;
+
+/* Unweighted depths from src over the out-CSR (Cuda_BFS / csr_bfs,
+ * GPU_BFS_csr.cuh:13, 258-327; CPU_BFS.hpp:10-41).  depth[v] = INT32_MAX when
+ * v is unreached or deeper than max_depth.  in_rowptr/in_col enable bottom-up
+ * levels (pass the out arrays for an undirected graph, NULL to force push). */
+int ghb_bfs(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32_t* out_col,
+            const int32_t* in_rowptr, const int32_t* in_col, int32_t src, int32_t max_depth,
+            int32_t* depth, const ghb_bfs_options* options, ghb_traversal_stats* stats);
+
+/* BFS with predecessors (Cuda_BFS_pre / bfs_pre, GPU_BFS_pre_csr.cuh:15,
+ * 62-124).  pred[v] = an out-neighbour parent at depth[v]-1 (the smallest
+ * such id), -1 for the source and for unreached vertices. */
+int ghb_bfs_pred(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr,
+                 const int32_t* out_col, const int32_t* in_rowptr, const int32_t* in_col,
+                 int32_t src, int32_t max_depth, int32_t* depth, int32_t* pred,
+                 const ghb_bfs_options* options, ghb_traversal_stats* stats);
+
+/* Many sources at once: 64 sources per uint64 bitmask word.  depth is
+ * n_src x n, row s holding the depths from srcs[s]. */
+int ghb_msbfs(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32_t* out_col,
+              const int32_t* in_rowptr, const int32_t* in_col, const int32_t* srcs,
+              int32_t n_src, int32_t* depth, ghb_traversal_stats* stats);
+
+/* ------------------------------------------------------------------ SSSP */
+typedef struct {
+    double delta;            /* bucket width; <= 0 picks one from the weights */
+    int32_t policy;          /* GHB_POLICY_HEURISTIC or GHB_POLICY_LEARNED     */
+    int32_t record_trace;
+    float* trace;
+    int32_t trace_cap;
+} ghb_sssp_options;
+
+/* FP64 distances from src over the out-CSR (Cuda_SSSP / csr_sssp,
+ * GPU_SSSP_csr.cuh:253-327; CPU_shortest_paths.hpp:19-64).  Unreached
+ * vertices get `inf` (LDBC passes DBL_MAX).  Weights must be >= 0. */
+int ghb_sssp(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col,
+             const double* w, int32_t src, double inf, double* dist,
+             const ghb_sssp_options* options, ghb_traversal_stats* stats);
+
+/* With predecessors (Cuda_SSSP_pre, GPU_SSSP_pre_csr.cuh:332-368): pred[v] is
+ * the smallest-id u with dist[u] + w(u,v) == dist[v] (exact FP64), -1 for the
+ * source and for unreached vertices.  in_* is the transposed CSR with its
+ * weights (the out-CSR of an undirected graph). */
+int ghb_sssp_pred(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col,
+                  const double* w, const int32_t* in_rowptr, const int32_t* in_col,
+                  const double* in_w, int32_t src, double inf, double* dist, int32_t* pred,
+                  const ghb_sssp_options* options, ghb_traversal_stats* stats);
+
+/* Many sources: dist is n_src x n. */
+int ghb_mssssp(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col,
+               const double* w, const int32_t* srcs, int32_t n_src, double inf, double* dist,
+               ghb_traversal_stats* stats);
+
+/* ------------------------------------------------------------------- WCC */
+/* Weakly connected components (Cuda_WCC / WCC_GPU, GPU_WCC_csr.cuh:83-129;
+ * CPU_connected_components.hpp:12-66).  label[v] = the smallest vertex id in
+ * v's component.  Either direction of a directed graph covers every edge. */
+int ghb_wcc(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col,
+            int32_t* label);
+
+/* -------------------------------------------------------------- PageRank */
+#define GHB_PR_FP64 0
+#define GHB_PR_FP32_KAHAN 1
+
+typedef struct {
+    int32_t iterations;      /* maximum iterations                            */
+    double damping;
+    int32_t precision;       /* GHB_PR_FP64 or GHB_PR_FP32_KAHAN               */
+    double tolerance;        /* > 0: stop once the L1 change <= tolerance      */
+    double* l1_history;      /* host, optional: L1 change per iteration        */
+} ghb_pr_options;
+
+/* LDBC PageRank, pull form (Cuda_PR / GPU_PR, GPU_PR_csr.cuh:34-117, 193-197;
+ * CPU_PageRank.hpp:12-56): pr' = (1-d)/N + d*S/N + d*sum_{u in in(v)} pr[u]/out(u),
+ * S = sum of the ranks of vertices with no out-edges.  `rank` is FP64 either
+ * way; FP32 mode stores ranks and contributions in FP32 with per-row Kahan
+ * sums and keeps S and the L1 norm in FP64.  *iterations_run may be NULL. */
+int ghb_pagerank(ghb_workspace* ws, int32_t n, const int32_t* in_rowptr, const int32_t* in_col,
+                 const int32_t* out_rowptr, const ghb_pr_options* options, double* rank,
+                 int32_t* iterations_run);
+
+/* ------------------------------------------------------------------ CDLP */
+/* Synchronous label propagation (Cuda_CDLP / CDLP_GPU, GPU_CDLP_csr.cuh:75-210;
+ * CPU_Community_Detection.hpp:12-64): new label = the most frequent label
+ * among the row's entries, smallest label on ties; a vertex with an empty row
+ * keeps its label.  Labels start as vertex ids.  Pass the all-CSR (in then
+ * out) of a directed graph, the out-CSR of an undirected one. */
+int ghb_cdlp(ghb_workspace* ws, int32_t n, const int32_t* all_rowptr, const int32_t* all_col,
+             int32_t iterations, int32_t* labels);
+
+/* -------------------------------------------------------------------- TC */
+/* Per-vertex triangle incidences with the reference's counting
+ * (Cuda_TC / Cuda_TC_PerNode, GPU_TC_csr.cuh:15-68; CPU_TC.hpp:31-60): for
+ * every entry u->v and every w in row(u) and row(v), add 1 to u, v and w.
+ * On a symmetric graph without self-loops that is 6 x triangles(x).
+ * counts64 (exact) and counts32 (the reference's wrapping int32) may each be
+ * NULL; *total receives sum(counts64) / 3 (may be NULL). */
+int ghb_tc(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col,
+           int64_t* counts64, int32_t* counts32, int64_t* total);
+
+/* ------------------------------------------------------ batched graphs */
+/* Many independent graphs packed back to back.  vbase / ebase are HOST
+ * arrays of n_graphs + 1 int64: graph g owns global vertices
+ * [vbase[g], vbase[g+1]) and entries [ebase[g], ebase[g+1]) (a batch may hold
+ * more than 2^31 entries); its rowptr (n_g + 1 int32 LOCAL offsets) starts at
+ * rowptr[vbase[g] + g]; col holds LOCAL ids.  Outputs are indexed by global
+ * vertex and hold local values. */
+/* WCC of every graph (label = smallest local id of the component). */
+int ghb_batch_wcc(ghb_workspace* ws, int32_t n_graphs, const int64_t* vbase,
+                  const int64_t* ebase, const int32_t* rowptr, const int32_t* col,
+                  int32_t* label);
+/* Triangle counts of every graph: counts64 per vertex (device, may be NULL),
+ * totals[g] triangles of graph g (host, may be NULL). */
+int ghb_batch_tc(ghb_workspace* ws, int32_t n_graphs, const int64_t* vbase,
+                 const int64_t* ebase, const int32_t* rowptr, const int32_t* col,
+                 int64_t* counts64, int64_t* totals);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GHB_H */

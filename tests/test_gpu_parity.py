@@ -1,0 +1,280 @@
+"""GPU parity: every algorithm through the C ABI against the CPU oracle
+(oracle/oracle.c, itself pinned to the reference) and the golden fixtures.
+Integer outputs and SSSP distances must match bit for bit; PageRank within
+1e-6 relative L1 of the FP64 oracle."""
+import glob
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+PR_TOL = 1e-6  # relative L1 vs FP64
+
+FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+@pytest.fixture(scope="module")
+def G():
+    import graphhet_b200 as G
+    assert torch.cuda.is_available()
+    G.lib()
+    return G
+
+
+def to_gpu(G, og: O.Graph):
+    dev = torch.device("cuda")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    g = G.CSRGraph(n=og.n, rowptr=t(og.rowptr), col=t(og.col), w=t(og.w) if og.w is not None else None,
+                   directed=og.directed)
+    if og.directed:
+        g.in_rowptr, g.in_col = t(og.in_rowptr), t(og.in_col)
+        g.in_w = t(og.in_w) if og.in_w is not None else None
+    return g
+
+
+def rel_l1(a, b):
+    return float(np.abs(a - b).sum() / np.abs(b).sum())
+
+
+def check_all(G, g, og, src, pr_tol=PR_TOL):
+    d, st = G.bfs(g, src)
+    assert np.array_equal(d.cpu().numpy(), O.bfs(og, src)), "bfs"
+    for pol in (G.POLICY_PUSH, G.POLICY_PULL):
+        d2, _ = G.bfs(g, src, policy=pol)
+        assert np.array_equal(d2.cpu().numpy(), O.bfs(og, src)), f"bfs policy {pol}"
+    dist, _ = G.sssp(g, src)
+    assert np.array_equal(dist.cpu().numpy(), O.sssp(og, src)), "sssp"
+    assert np.array_equal(G.wcc(g).cpu().numpy(), O.wcc(og)), "wcc"
+    ref_pr = O.pagerank(og, 10, 0.85)
+    for prec in (G.PR_FP64, G.PR_FP32_KAHAN):
+        pr, _, _ = G.pagerank(g, 10, 0.85, precision=prec)
+        assert rel_l1(pr.cpu().numpy(), ref_pr) <= pr_tol, f"pagerank precision {prec}"
+    assert np.array_equal(G.cdlp(g, 10).cpu().numpy(), O.cdlp(og, 10)), "cdlp"
+    c64, c32, total = G.tc(g)
+    ref_tc = O.tc(og)
+    assert np.array_equal(c32.cpu().numpy(), ref_tc), "tc int32"
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p)[:-4] for p in FIXTURES])
+def test_golden_fixtures(G, path):
+    z = np.load(path)
+    n = int(z["n"])
+    og = O.Graph(n, z["rowptr"], z["col"], z["w"] if z["w"].size else None, bool(int(z["directed"])),
+                 z["in_rowptr"], z["in_col"], None)
+    g = to_gpu(G, og)
+    src = int(z["src"])
+    assert np.array_equal(G.bfs(g, src)[0].cpu().numpy(), z["bfs"])
+    if og.w is not None:
+        assert np.array_equal(G.sssp(g, src)[0].cpu().numpy(), z["sssp"])
+    assert np.array_equal(G.wcc(g).cpu().numpy(), z["wcc"])
+    pr, _, _ = G.pagerank(g, 10, 0.85)
+    assert rel_l1(pr.cpu().numpy(), z["pagerank"]) <= PR_TOL
+    assert np.array_equal(G.cdlp(g, 10).cpu().numpy(), z["cdlp"])
+    assert np.array_equal(G.tc(g)[1].cpu().numpy(), z["tc"])
+
+
+@pytest.mark.parametrize("directed", [False, True])
+def test_gpu_builder_matches_cpu_builder(G, directed):
+    src, dst = G.gen_rmat(12, 16 << 12, 42)
+    s_cpu, d_cpu = O.rmat_edges(12, 16 << 12, 42)
+    assert np.array_equal(src.cpu().numpy(), s_cpu) and np.array_equal(dst.cpu().numpy(), d_cpu)
+    g = G.make_graph(1 << 12, src, dst, directed, weight_seed=42)
+    og = O.make_graph(1 << 12, s_cpu, d_cpu, directed, weight_seed=42)
+    assert np.array_equal(g.rowptr.cpu().numpy(), og.rowptr)
+    assert np.array_equal(g.col.cpu().numpy(), og.col)
+    assert np.array_equal(g.w.cpu().numpy(), og.w)
+    if directed:
+        assert np.array_equal(g.in_rowptr.cpu().numpy(), og.in_rowptr)
+        assert np.array_equal(g.in_col.cpu().numpy(), og.in_col)
+        assert np.array_equal(g.in_w.cpu().numpy(), og.in_w)
+
+
+def test_builder_duplicates_last_weight_wins(G):
+    s = torch.tensor([0, 0, 1, 2, 1, 3, 1], dtype=torch.int32, device="cuda")
+    d = torch.tensor([1, 1, 0, 2, 2, 1, 2], dtype=torch.int32, device="cuda")
+    w = torch.tensor([0.5, 0.25, 0.75, 1.0, 0.125, 2.0, 0.0625], dtype=torch.float64, device="cuda")
+    rp, col, wt = G.build_csr(5, s, d, w=w, symmetrize=False)
+    orp, ocol, ow = O.build_csr(5, s.cpu().numpy(), d.cpu().numpy(), w=w.cpu().numpy())
+    assert np.array_equal(rp.cpu().numpy(), orp) and np.array_equal(col.cpu().numpy(), ocol)
+    assert np.array_equal(wt.cpu().numpy(), ow)
+
+
+def test_builder_rejects_bad_endpoint(G):
+    s = torch.tensor([0, 5], dtype=torch.int32, device="cuda")
+    d = torch.tensor([1, 1], dtype=torch.int32, device="cuda")
+    with pytest.raises(G.GhbError):
+        G.build_csr(5, s, d)
+
+
+@pytest.mark.parametrize("directed", [False, True])
+def test_rmat16_config0_all_algorithms(G, directed):
+    """RMAT seed 42, scale 16, edge factor 16, sources = highest degree vertex."""
+    g = G.rmat_graph(16, 16, 42, directed=directed)
+    og = O.rmat_graph(16, 16, 42, directed=directed)
+    assert np.array_equal(g.col.cpu().numpy(), og.col)
+    deg = np.diff(og.rowptr)
+    src = int(np.argmax(deg))  # first maximum = smallest id among ties
+    check_all(G, g, og, src)
+
+
+def test_grid_high_diameter(G):
+    g = G.grid_graph(96, 80, weight_seed=3)
+    og = O.grid_graph(96, 80, weight_seed=3)
+    assert np.array_equal(g.w.cpu().numpy(), og.w)
+    check_all(G, g, og, 0)
+    check_all(G, g, og, 96 * 80 // 2 + 7)
+
+
+def test_er_sparse_many_components(G):
+    s, d = O.er_edges(20000, 12000, 11)
+    og = O.make_graph(20000, s, d, False, weight_mode=1, weight_seed=11)
+    g = to_gpu(G, og)
+    check_all(G, g, og, int(np.argmax(np.diff(og.rowptr))))
+    check_all(G, g, og, 5)
+
+
+def test_edge_cases(G):
+    # no edges at all
+    og = O.make_graph(7, np.zeros(0, np.int32), np.zeros(0, np.int32), False)
+    g = to_gpu(G, og)
+    assert G.bfs(g, 3)[0].cpu().tolist() == [2**31 - 1] * 3 + [0] + [2**31 - 1] * 3
+    assert G.wcc(g).cpu().tolist() == list(range(7))
+    assert G.cdlp(g, 5).cpu().tolist() == list(range(7))
+    assert G.tc(g)[1].cpu().tolist() == [0] * 7
+    pr, _, _ = G.pagerank(g, 10, 0.85)
+    assert rel_l1(pr.cpu().numpy(), O.pagerank(og, 10, 0.85)) <= PR_TOL
+    dist = G.sssp(g, 2)[0].cpu().numpy()
+    assert dist[2] == 0 and np.all(np.delete(dist, 2) == O.DBL_MAX)
+    # single vertex
+    og1 = O.make_graph(1, np.zeros(0, np.int32), np.zeros(0, np.int32), False)
+    g1 = to_gpu(G, og1)
+    assert G.bfs(g1, 0)[0].cpu().tolist() == [0]
+    # star: hub row far longer than a warp
+    hub = np.zeros(9000, np.int32)
+    leaves = np.arange(1, 9001, dtype=np.int32)
+    og2 = O.make_graph(9001, hub, leaves, False, weight_mode=1, weight_seed=2)
+    check_all(G, to_gpu(G, og2), og2, 17)
+    # max_depth
+    og3 = O.rmat_graph(12, 8, 5)
+    g3 = to_gpu(G, og3)
+    for md in (0, 1, 2, 3):
+        assert np.array_equal(G.bfs(g3, 1, max_depth=md)[0].cpu().numpy(), O.bfs(og3, 1, md))
+    # invalid source is an error, not a fault
+    with pytest.raises(G.GhbError):
+        G.bfs(g3, og3.n)
+    with pytest.raises(G.GhbError):
+        G.sssp(g3, -1)
+
+
+def test_sssp_custom_inf_and_delta(G):
+    og = O.rmat_graph(13, 8, 9, directed=True)
+    g = to_gpu(G, og)
+    ref = O.sssp(og, 0)
+    for delta in (0.01, 0.3, 5.0):
+        dist, _ = G.sssp(g, 0, delta=delta)
+        assert np.array_equal(dist.cpu().numpy(), ref)
+    # finite inf: vertices at distance >= inf stay at inf (reference semantics)
+    dist, _ = G.sssp(g, 0, inf=1.0)
+    exp = np.where(ref < 1.0, ref, 1.0)
+    assert np.array_equal(dist.cpu().numpy(), exp)
+
+
+def test_bfs_schedule_and_trace(G):
+    og = O.rmat_graph(14, 16, 4)
+    g = to_gpu(G, og)
+    ref = O.bfs(og, 10)
+    d, st, tr = G.bfs(g, 10, trace_cap=64, oracle_timing=True)
+    assert np.array_equal(d.cpu().numpy(), ref)
+    assert tr.shape[0] == st["levels"] and tr.shape[1] == 20
+    assert np.all(tr[:, 14] >= 0) and np.all(tr[:, 15] >= 0)
+    sched = [0, 1, 0, 1, 1, 0, 0, 1, 0, 1, 1, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0]
+    d2, _ = G.bfs(g, 10, policy=G.POLICY_SCHEDULE, schedule=sched)
+    assert np.array_equal(d2.cpu().numpy(), ref)
+
+
+def test_bfs_and_sssp_predecessors(G):
+    for directed in (False, True):
+        og = O.rmat_graph(12, 16, 21, directed=directed)
+        g = to_gpu(G, og)
+        src = int(np.argmax(np.diff(og.rowptr)))
+        depth, pred = G.bfs_pred(g, src)
+        depth, pred = depth.cpu().numpy(), pred.cpu().numpy()
+        assert np.array_equal(depth, O.bfs(og, src))
+        for v in range(og.n):
+            p = pred[v]
+            if v == src or depth[v] == 2**31 - 1:
+                assert p == -1
+                continue
+            row = og.col[og.rowptr[p]:og.rowptr[p + 1]]
+            assert depth[p] == depth[v] - 1 and v in row
+        dist, pr = G.sssp_pred(g, src)
+        dist, pr = dist.cpu().numpy(), pr.cpu().numpy()
+        assert np.array_equal(dist, O.sssp(og, src))
+        for v in range(og.n):
+            p = pr[v]
+            if v == src or dist[v] == O.DBL_MAX:
+                assert p == -1
+                continue
+            lo, hi = og.rowptr[p], og.rowptr[p + 1]
+            j = lo + np.searchsorted(og.col[lo:hi], v)
+            assert og.col[j] == v and dist[p] + og.w[j] == dist[v]
+
+
+def test_msbfs_matches_single_source(G):
+    og = O.rmat_graph(13, 16, 8)
+    g = to_gpu(G, og)
+    rng = np.random.default_rng(0)
+    srcs = rng.integers(0, og.n, 70).astype(np.int32)
+    srcs[3] = srcs[4]  # duplicate source
+    d = torch.empty(len(srcs) * og.n, dtype=torch.int32, device="cuda")
+    st = G.TraversalStats()
+    import ctypes
+    G._check(G.lib().ghb_msbfs(G._ws(None), og.n, G._ptr(g.rowptr), G._ptr(g.col), G._ptr(g.rowptr),
+                               G._ptr(g.col), G._ptr(torch.from_numpy(srcs).cuda()), len(srcs), G._ptr(d),
+                               ctypes.byref(st)), "ghb_msbfs")
+    d = d.cpu().numpy().reshape(len(srcs), og.n)
+    for i in range(0, len(srcs), 7):
+        assert np.array_equal(d[i], O.bfs(og, int(srcs[i])))
+    assert np.array_equal(d[4], O.bfs(og, int(srcs[4])))
+    assert np.array_equal(d[69], O.bfs(og, int(srcs[69])))
+
+
+def test_batch_wcc_and_tc(G):
+    import ctypes
+    rng = np.random.default_rng(5)
+    graphs = []
+    for i in range(12):
+        n = int(rng.integers(50, 3000))
+        m = int(rng.integers(n // 2, 6 * n))
+        s, d = O.er_edges(n, m, 100 + i)
+        graphs.append(O.make_graph(n, s, d, False, weight_mode=0))
+    vbase = np.zeros(len(graphs) + 1, np.int64)
+    ebase = np.zeros(len(graphs) + 1, np.int64)
+    for i, og in enumerate(graphs):
+        vbase[i + 1] = vbase[i] + og.n
+        ebase[i + 1] = ebase[i] + og.m
+    rp = torch.from_numpy(np.concatenate([og.rowptr for og in graphs])).cuda()
+    col = torch.from_numpy(np.concatenate([og.col for og in graphs])).cuda()
+    lab = torch.empty(int(vbase[-1]), dtype=torch.int32, device="cuda")
+    P = ctypes.POINTER(ctypes.c_int64)
+    G._check(G.lib().ghb_batch_wcc(G._ws(None), len(graphs), vbase.ctypes.data_as(ctypes.c_void_p),
+                                   ebase.ctypes.data_as(ctypes.c_void_p), G._ptr(rp), G._ptr(col), G._ptr(lab)),
+             "ghb_batch_wcc")
+    c64 = torch.empty(int(vbase[-1]), dtype=torch.int64, device="cuda")
+    totals = np.zeros(len(graphs), np.int64)
+    G._check(G.lib().ghb_batch_tc(G._ws(None), len(graphs), vbase.ctypes.data_as(ctypes.c_void_p),
+                                  ebase.ctypes.data_as(ctypes.c_void_p), G._ptr(rp), G._ptr(col), G._ptr(c64),
+                                  totals.ctypes.data_as(ctypes.c_void_p)), "ghb_batch_tc")
+    lab, c64 = lab.cpu().numpy(), c64.cpu().numpy()
+    for i, og in enumerate(graphs):
+        a, b = vbase[i], vbase[i + 1]
+        assert np.array_equal(lab[a:b], O.wcc(og))
+        ref = O.tc(og)
+        assert np.array_equal(c64[a:b].astype(np.int32), ref)
+        assert totals[i] == int(ref.astype(np.int64).sum()) // 18

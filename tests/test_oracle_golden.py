@@ -1,0 +1,93 @@
+"""Pins the CPU oracle (oracle/oracle.c): against the golden fixtures made by
+the reference's own CPU code (tests/golden/make_golden.py), against the
+known answers of the reference's example graph, and, where the compiled
+reference is present, against it directly on fresh seeded graphs."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import GOLDEN
+
+FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load_fixture(path):
+    z = np.load(path)
+    n = int(z["n"])
+    directed = bool(int(z["directed"]))
+    if "edge_src" in z:
+        g = O.make_graph(n, z["edge_src"], z["edge_dst"], directed, w=z["edge_w"])
+    elif "scale" in z:
+        g = O.rmat_graph(int(z["scale"]), int(z["edge_factor"]), int(z["seed"]), directed=directed)
+    elif "rows" in z:
+        g = O.grid_graph(int(z["rows"]), int(z["cols"]), weight_seed=int(z["seed"]))
+    else:
+        s, d = O.er_edges(int(z["er_n"]), int(z["er_m"]), int(z["seed"]))
+        g = O.make_graph(n, s, d, False, weight_mode=1, weight_seed=int(z["seed"]))
+    return z, g
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p)[:-4] for p in FIXTURES])
+def test_builder_reproduces_fixture_csr(path):
+    z, g = load_fixture(path)
+    assert np.array_equal(g.rowptr, z["rowptr"])
+    assert np.array_equal(g.col, z["col"])
+    if z["w"].size:
+        assert np.array_equal(g.w, z["w"])
+    assert np.array_equal(g.in_rowptr, z["in_rowptr"])
+    assert np.array_equal(g.in_col, z["in_col"])
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p)[:-4] for p in FIXTURES])
+def test_oracle_matches_reference_outputs(path):
+    z, g = load_fixture(path)
+    src = int(z["src"])
+    assert np.array_equal(O.bfs(g, src), z["bfs"])
+    assert np.array_equal(O.sssp(g, src), z["sssp"])  # bit-exact FP64
+    assert np.array_equal(O.wcc(g), z["wcc"])
+    pr = O.pagerank(g, 10, 0.85)
+    assert np.abs(pr - z["pagerank"]).sum() <= 1e-12 * np.abs(z["pagerank"]).sum()
+    assert np.array_equal(O.cdlp(g, 10), z["cdlp"])
+    assert np.array_equal(O.tc(g), z["tc"])
+
+
+def test_reference_example_known_answers():
+    """GPU_csr_example.cu's graph, source "one" (ids one=0 .. six=5)."""
+    z = np.load(os.path.join(GOLDEN, "toy_example_directed.npz"))
+    assert z["bfs"].tolist() == [0, 1, 1, 1, 2, 1]
+    assert z["sssp"].tolist() == [0.0, 0.8, 1.0, 1.0, 2.0, 1.0]
+    assert z["wcc"].tolist() == [0] * 6
+    assert z["cdlp"].tolist() == [0] * 6
+    expect = [0.11221769699688859, 0.13606398563018426, 0.30954548324429865, 0.13606398563018426,
+              0.17004486286826004, 0.13606398563018426]
+    assert np.allclose(z["pagerank"], expect, rtol=0, atol=1e-15)
+    t = np.load(os.path.join(GOLDEN, "triangle_pendant_isolated.npz"))
+    assert t["tc"].tolist() == [6, 6, 6, 0, 0]
+    assert t["cdlp"].tolist() == [0, 0, 0, 0, 4]
+    assert t["wcc"].tolist() == [0, 0, 0, 0, 4]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="compiled reference (oracle/_ref) not built")
+@pytest.mark.parametrize("directed", [False, True])
+def test_oracle_matches_compiled_reference_rmat12(directed):
+    g = O.rmat_graph(12, 16, 7, directed=directed)
+    r = O.Ref().load(g)
+    src = int(np.argmax(np.diff(g.rowptr)))
+    assert np.array_equal(O.bfs(g, src), r.bfs(src))
+    assert np.array_equal(O.bfs(g, src, 2), r.bfs(src, 2))
+    assert np.array_equal(O.sssp(g, src), r.sssp(src))
+    assert np.array_equal(O.wcc(g), r.wcc())
+    assert np.array_equal(O.pagerank(g, 10, 0.85), r.pagerank(10, 0.85))
+    assert np.array_equal(O.cdlp(g, 10), r.cdlp(10))
+    assert np.array_equal(O.tc(g), r.tc())
+
+
+def test_oracle_planted_mistake_is_caught():
+    """A wrong answer planted in the oracle's output must fail the comparison."""
+    z, g = load_fixture(os.path.join(GOLDEN, "rmat10_seed42_undirected.npz"))
+    d = O.bfs(g, int(z["src"]))
+    d[np.argmax(d < 2**31 - 1)] += 1
+    assert not np.array_equal(d, z["bfs"])
