@@ -14,7 +14,7 @@ CU_SRC    := $(wildcard graphhet_b200/csrc/*.cu)
 CU_OBJ    := $(patsubst graphhet_b200/csrc/%.cu,$(BUILD)/%.o,$(CU_SRC))
 CU_HDR    := $(wildcard graphhet_b200/csrc/*.cuh) include/ghb.h include/ghb_gen.h
 
-all: graphhet_b200/libghb.so oracle
+all: graphhet_b200/libghb.so oracle dropin
 
 graphhet_b200/libghb.so: $(CU_OBJ)
 	$(NVCC) $(ARCH) -shared -cudart static -o $@ $^ -lrt -ldl -lpthread
@@ -26,8 +26,21 @@ $(BUILD)/%.o: graphhet_b200/csrc/%.cu $(CU_HDR)
 oracle:
 	$(MAKE) -C oracle REF_ROOT=$(REF_ROOT)
 
+# The reference's own GPU-CSR drivers (GPU_csr_example.cu, LDBC_GPU_csr.cu),
+# compiled unchanged from where they lie against this repository's
+# include/GPU_csr headers and linked to libghb.so: the drop-in check.
+DROPIN    := build/dropin
+dropin: graphhet_b200/libghb.so
+	@if [ -f "$(REF_ROOT)/src/LDBC/LDBC_GPU_csr.cu" ]; then \
+	  mkdir -p $(DROPIN) && \
+	  $(NVCC) $(ARCH) -O2 -std=c++17 -Iinclude -I$(REF_ROOT)/include $(REF_ROOT)/src/GPU_csr/GPU_csr_example.cu \
+	    -o $(DROPIN)/GPU_csr_example -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' && \
+	  $(NVCC) $(ARCH) -O2 -std=c++17 -Iinclude -I$(REF_ROOT)/include $(REF_ROOT)/src/LDBC/LDBC_GPU_csr.cu \
+	    -o $(DROPIN)/LDBC_GPU_csr -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' ; \
+	else echo "reference drivers not found under $(REF_ROOT): skipping the drop-in build"; fi
+
 clean:
 	rm -rf build graphhet_b200/libghb.so
 	$(MAKE) -C oracle clean
 
-.PHONY: all oracle clean
+.PHONY: all oracle dropin clean
