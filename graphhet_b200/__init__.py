@@ -94,6 +94,20 @@ _SIGS = {
     "ghb_tc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p]),
     "ghb_batch_wcc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p]),
     "ghb_batch_tc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _p]),
+    "ghb_graph_create": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _p, ctypes.POINTER(_p)]),
+    "ghb_graph_destroy": (ctypes.c_int, [_p]),
+    "ghb_graph_info": (ctypes.c_int, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i32), ctypes.POINTER(_i64),
+                                      ctypes.POINTER(ctypes.c_float)]),
+    "ghb_graph_perm": (ctypes.c_int, [_p, ctypes.POINTER(_p), ctypes.POINTER(_p)]),
+    "ghb_graph_bfs": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p]),
+    "ghb_graph_bfs_pred": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p, _p]),
+    "ghb_graph_msbfs": (ctypes.c_int, [_p, _p, _p, _i32, _p, _p]),
+    "ghb_graph_sssp": (ctypes.c_int, [_p, _p, _i32, _f64, _p, _p, _p]),
+    "ghb_graph_sssp_pred": (ctypes.c_int, [_p, _p, _i32, _f64, _p, _p, _p, _p]),
+    "ghb_graph_wcc": (ctypes.c_int, [_p, _p, _p]),
+    "ghb_graph_pagerank": (ctypes.c_int, [_p, _p, _p, _p, _p]),
+    "ghb_graph_cdlp": (ctypes.c_int, [_p, _p, _i32, _p]),
+    "ghb_graph_tc": (ctypes.c_int, [_p, _p, _p, _p, _p]),
 }
 
 _lib = None
@@ -427,3 +441,124 @@ def tc(g: CSRGraph, ws=None):
     _check(lib().ghb_tc(_ws(ws), g.n, _ptr(g.rowptr), _ptr(g.col) if g.m else None, _ptr(c64), _ptr(c32),
                         ctypes.byref(total)), "ghb_tc")
     return c64, c32, total.value
+
+
+# ------------------------------------------------------- resident graphs
+class ResidentGraph:
+    """A graph relabelled once by degree on the GPU (ghb_graph_create); every
+    method returns the same values as the module-level function of the same
+    name, in the caller's vertex ids."""
+
+    def __init__(self, g: CSRGraph, ws=None):
+        self.n = g.n
+        self.directed = g.directed
+        self._dev = g.rowptr.device
+        self._h = _p()
+        irp, icol, iw = g.in_csr()
+        has = g.m > 0
+        _check(lib().ghb_graph_create(_ws(ws), g.n, _ptr(g.rowptr), _ptr(g.col) if has else None,
+                                      _ptr(g.w) if (g.w is not None and has) else None,
+                                      _ptr(irp) if g.directed else None,
+                                      _ptr(icol) if (g.directed and icol.numel()) else None,
+                                      _ptr(iw) if (g.directed and iw is not None and iw.numel()) else None,
+                                      ctypes.byref(self._h)), "ghb_graph_create")
+        m, na, nb, ms = _i64(), _i32(), _i64(), ctypes.c_float()
+        _check(lib().ghb_graph_info(self._h, ctypes.byref(m), ctypes.byref(na), ctypes.byref(nb), ctypes.byref(ms)),
+               "ghb_graph_info")
+        self.m, self.n_active, self.device_bytes, self.build_ms = m.value, na.value, nb.value, ms.value
+
+    def close(self):
+        if self._h:
+            lib().ghb_graph_destroy(self._h)
+            self._h = _p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _i32(self, k=1):
+        return torch.empty(self.n * k, dtype=torch.int32, device=self._dev)
+
+    def bfs(self, src, max_depth=INT32_MAX, policy=POLICY_HEURISTIC, schedule=None, trace_cap=0,
+            oracle_timing=False, out=None, ws=None):
+        depth = out if out is not None else self._i32()
+        opt = BfsOptions(policy=policy)
+        keep = None
+        if schedule is not None:
+            keep = (ctypes.c_int8 * len(schedule))(*[int(x) for x in schedule])
+            opt.schedule = ctypes.cast(keep, _p)
+            opt.schedule_len = len(schedule)
+        trace = None
+        if trace_cap > 0:
+            trace = (ctypes.c_float * (trace_cap * TRACE_COLS))()
+            opt.record_trace, opt.trace, opt.trace_cap = 1, ctypes.cast(trace, _p), trace_cap
+            opt.oracle_timing = int(oracle_timing)
+        st = TraversalStats()
+        _check(lib().ghb_graph_bfs(_ws(ws), self._h, src, max_depth, _ptr(depth), ctypes.byref(opt),
+                                   ctypes.byref(st)), "ghb_graph_bfs")
+        if trace is not None:
+            import numpy as np
+            rows = min(trace_cap, st.levels)
+            return depth, st.as_dict(), np.frombuffer(trace, dtype=np.float32).reshape(trace_cap, TRACE_COLS)[:rows].copy()
+        return depth, st.as_dict()
+
+    def bfs_pred(self, src, max_depth=INT32_MAX, ws=None):
+        depth, pred = self._i32(), self._i32()
+        st = TraversalStats()
+        _check(lib().ghb_graph_bfs_pred(_ws(ws), self._h, src, max_depth, _ptr(depth), _ptr(pred), None,
+                                        ctypes.byref(st)), "ghb_graph_bfs_pred")
+        return depth, pred
+
+    def msbfs(self, srcs, out=None, ws=None):
+        sd = torch.as_tensor(srcs, dtype=torch.int32, device=self._dev)
+        depth = out if out is not None else self._i32(len(sd))
+        st = TraversalStats()
+        _check(lib().ghb_graph_msbfs(_ws(ws), self._h, _ptr(sd), len(sd), _ptr(depth), ctypes.byref(st)),
+               "ghb_graph_msbfs")
+        return depth.view(len(sd), self.n), st.as_dict()
+
+    def sssp(self, src, inf=DBL_MAX, delta=0.0, out=None, ws=None):
+        dist = out if out is not None else torch.empty(self.n, dtype=torch.float64, device=self._dev)
+        opt = SsspOptions(delta=delta)
+        st = TraversalStats()
+        _check(lib().ghb_graph_sssp(_ws(ws), self._h, src, inf, _ptr(dist), ctypes.byref(opt), ctypes.byref(st)),
+               "ghb_graph_sssp")
+        return dist, st.as_dict()
+
+    def sssp_pred(self, src, inf=DBL_MAX, ws=None):
+        dist = torch.empty(self.n, dtype=torch.float64, device=self._dev)
+        pred = self._i32()
+        st = TraversalStats()
+        _check(lib().ghb_graph_sssp_pred(_ws(ws), self._h, src, inf, _ptr(dist), _ptr(pred), None,
+                                         ctypes.byref(st)), "ghb_graph_sssp_pred")
+        return dist, pred
+
+    def wcc(self, out=None, ws=None):
+        lab = out if out is not None else self._i32()
+        _check(lib().ghb_graph_wcc(_ws(ws), self._h, _ptr(lab)), "ghb_graph_wcc")
+        return lab
+
+    def pagerank(self, iterations=10, damping=0.85, precision=PR_FP64, tolerance=0.0, l1_history=False, out=None,
+                 ws=None):
+        rank = out if out is not None else torch.empty(self.n, dtype=torch.float64, device=self._dev)
+        hist = (ctypes.c_double * max(1, iterations))() if l1_history else None
+        opt = PrOptions(iterations=iterations, damping=damping, precision=precision, tolerance=tolerance,
+                        l1_history=ctypes.cast(hist, _p) if hist is not None else None)
+        ran = _i32()
+        _check(lib().ghb_graph_pagerank(_ws(ws), self._h, ctypes.byref(opt), _ptr(rank), ctypes.byref(ran)),
+               "ghb_graph_pagerank")
+        return rank, ran.value, (list(hist)[: ran.value] if hist is not None else None)
+
+    def cdlp(self, iterations=10, out=None, ws=None):
+        lab = out if out is not None else self._i32()
+        _check(lib().ghb_graph_cdlp(_ws(ws), self._h, iterations, _ptr(lab)), "ghb_graph_cdlp")
+        return lab
+
+    def tc(self, ws=None):
+        c64 = torch.empty(self.n, dtype=torch.int64, device=self._dev)
+        c32 = self._i32()
+        total = _i64()
+        _check(lib().ghb_graph_tc(_ws(ws), self._h, _ptr(c64), _ptr(c32), ctypes.byref(total)), "ghb_graph_tc")
+        return c64, c32, total.value

@@ -17,10 +17,13 @@
 
 namespace ghb {
 
-int bfs_run(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32_t* out_col,
+// n_active: vertices [n_active, n) have no entries at all (a relabelled
+// graph puts them last); bottom-up levels skip them.
+int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_rowptr, const int32_t* out_col,
             const int32_t* in_rowptr, const int32_t* in_col, int32_t src, int32_t max_depth,
             int32_t* depth, const ghb_bfs_options* opt, ghb_traversal_stats* stats) {
     GHB_REQUIRE(n >= 1, "n must be >= 1");
+    GHB_REQUIRE(n_active >= 0 && n_active <= n, "n_active outside [0, n]");
     GHB_REQUIRE(out_rowptr && depth, "NULL graph or output");
     GHB_REQUIRE(src >= 0 && src < n, "source outside [0, n)");
     GHB_REQUIRE(max_depth >= 0, "max_depth < 0");
@@ -32,8 +35,14 @@ int bfs_run(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32
          policy == GHB_POLICY_HEURISTIC) && !can_pull)
         policy = GHB_POLICY_PUSH;
     GHB_REQUIRE(!(opt->record_trace && (!opt->trace || opt->trace_cap <= 0)), "trace buffer missing");
-    const float alpha = opt->alpha > 0 ? opt->alpha : 14.0f;
+    // Beamer's rule with thresholds measured on B200 (a top-down level costs
+    // ~0.13 ms per million frontier entries, a bottom-up level ~0.03-0.2 ms
+    // on an RMAT scale-24 graph): switch to bottom-up once the frontier's
+    // out-entries exceed 1/256 of the unexplored ones, back to top-down when
+    // the frontier is under 1/24 of the vertices.
+    const float alpha = opt->alpha > 0 ? opt->alpha : 256.0f;
     const float beta = opt->beta > 0 ? opt->beta : 24.0f;
+    static_assert(sizeof(BfsPersistState) <= 16 * sizeof(unsigned long long), "persist state slot");
 
     const int64_t words = ((int64_t)n + 31) / 32;
     Carver sizing(nullptr);
@@ -62,6 +71,27 @@ int bfs_run(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32
     uint32_t *f_cur = B.front_a, *f_next = B.front_b;
     const int threads = 256;
     const unsigned gmax = ws->num_sms * 8;
+    const int64_t words_active = ((int64_t)n_active + 31) / 32;
+    bool queue_valid = true;   // q_cur holds the frontier (false after a bottom-up level)
+    bool bitmap_valid = true;  // f_cur holds the frontier (false after a persistent run)
+    int coop_blocks = 0;       // co-resident 1024-thread blocks for the persistent kernel
+    {
+        int coop = 0, per_sm = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ws->device);
+        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_push_persistent_kernel, 1024, 0) ==
+                        cudaSuccess &&
+            per_sm >= 1)
+            coop_blocks = ws->num_sms;
+    }
+    auto ensure_queue = [&]() -> int {
+        if (queue_valid) return GHB_OK;
+        GHB_CUDA_TRY(cudaMemsetAsync(&B.counters->big_tail, 0, sizeof(int32_t), st));
+        GHB_TRY(launch(ws, bfs_queue_from_bitmap_kernel, dim3(grid_for(words * 32, threads, gmax)),
+                       dim3(threads), 0, words, (const uint32_t*)f_cur, out_rowptr, q_cur,
+                       &B.counters->big_tail, (BfsCounters*)nullptr));
+        queue_valid = true;
+        return GHB_OK;
+    };
 
     while (n_f > 0 && level < max_depth) {
         // ---- direction for this level
@@ -91,10 +121,52 @@ int bfs_run(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32
         }
 
         float t_push = -1.f, t_pull = -1.f;
+        if (dir == 0 || (opt->oracle_timing && can_pull && opt->record_trace)) GHB_TRY(ensure_queue());
+        // Runs of small top-down levels: one cooperative launch, no host
+        // round trip per level (high-diameter graphs, BFS tails).
+        const bool persist_policy = policy == GHB_POLICY_HEURISTIC || policy == GHB_POLICY_PUSH;
+        if (dir == 0 && persist_policy && coop_blocks > 0 && !opt->record_trace && m_f < kPersistMaxEdges &&
+            degmax_f < (double)kBigList && queue_valid) {
+            BfsPersistState* ps = B.persist;
+            GHB_CUDA_TRY(cudaMemsetAsync(ps, 0, sizeof(BfsPersistState), st));
+            const int32_t nf32 = (int32_t)n_f;
+            GHB_CUDA_TRY(cudaMemcpyAsync(&ps->tail[0], &nf32, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+            GHB_TRY(launch_coop(ws, bfs_push_persistent_kernel, dim3(coop_blocks), dim3(1024), 0,
+                                (const int32_t*)out_rowptr, (const int32_t*)out_col, q_cur, q_next, B.visited, depth,
+                                (int32_t)level, (int32_t)max_depth, (int64_t)kPersistMaxEdges, (int64_t)m_total,
+                                (int64_t)m_r, policy == GHB_POLICY_PUSH || !can_pull ? 0.f : alpha, ps));
+            GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, ps, sizeof(BfsPersistState), cudaMemcpyDeviceToHost, st));
+            GHB_CUDA_TRY(cudaStreamSynchronize(st));
+            const BfsPersistState* hs = reinterpret_cast<const BfsPersistState*>(ws->host_pinned);
+            if (hs->status != kDevOk) {
+                set_error("BFS persistent kernel: grid barrier timed out");
+                return GHB_ERR_TIMEOUT;
+            }
+            const int L = hs->levels_done;
+            n_f = hs->tail[L % 3];
+            m_f = (int64_t)hs->mf[L % 3];
+            deg2_f = 0.0;
+            degmax_f = (double)hs->dmax[L % 3];
+            examined += (int64_t)hs->examined;
+            m_r += (int64_t)hs->m_r;
+            reached += (int64_t)hs->reached;
+            if (L & 1) std::swap(q_cur, q_next);
+            level += L;
+            prev_dir = 0;
+            dir = 0;
+            bitmap_valid = false;
+            continue;
+        }
+        if (dir == 1 && !bitmap_valid) {
+            GHB_CUDA_TRY(cudaMemsetAsync(f_cur, 0, words * sizeof(uint32_t), st));
+            GHB_TRY(launch(ws, bfs_bitmap_from_queue_kernel, dim3(grid_for(n_f, 256, gmax)), dim3(256), 0,
+                           (const int32_t*)q_cur, (int32_t)n_f, f_cur));
+            bitmap_valid = true;
+        }
         if (opt->oracle_timing && can_pull && opt->record_trace) {
             // Time both directions on a snapshot; the state after a level does
             // not depend on the direction, so the run continues unchanged.
-            GHB_TRY(bfs_time_both(ws, B, n, words, out_rowptr, out_col, in_rowptr, in_col, q_cur, n_f,
+            GHB_TRY(bfs_time_both(ws, B, n, words, out_rowptr, out_col, in_rowptr, in_col, q_cur, n_f, m_f,
                                   f_cur, level, depth, &t_push, &t_pull));
         }
 
@@ -102,11 +174,16 @@ int bfs_run(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32
         GHB_CUDA_TRY(cudaMemsetAsync(f_next, 0, words * sizeof(uint32_t), st));
         if (opt->record_trace) GHB_CUDA_TRY(cudaEventRecord(ws->ev_a, st));
         if (dir == 0) {
+            const bool append = m_f < kAppendMaxEdges;
             GHB_TRY(bfs_push_level(ws, B, n, out_rowptr, out_col, q_cur, n_f, level + 1, depth,
-                                   q_next, f_next));
+                                   append ? q_next : (int32_t*)nullptr, f_next));
+            if (!append)
+                GHB_TRY(launch(ws, bfs_queue_from_bitmap_kernel, dim3(grid_for(words * 32, threads, gmax)),
+                               dim3(threads), 0, words, (const uint32_t*)f_next, out_rowptr, q_next,
+                               &B.counters->tail, B.counters));
         } else {
-            GHB_TRY(launch(ws, bfs_pull_kernel, dim3(grid_for(words * 32, threads, gmax)),
-                           dim3(threads), 0, n, words, in_rowptr, in_col, out_rowptr,
+            GHB_TRY(launch(ws, bfs_pull_kernel, dim3(grid_for(words_active * 32, threads, gmax)),
+                           dim3(threads), 0, n_active, words_active, in_rowptr, in_col, out_rowptr,
                            (const uint32_t*)f_cur, B.visited, f_next, depth, level + 1, q_next,
                            B.counters));
             pull_levels++;
@@ -145,6 +222,8 @@ int bfs_run(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32
         reached += n_f;
         std::swap(q_cur, q_next);
         std::swap(f_cur, f_next);
+        queue_valid = (dir == 0);
+        bitmap_valid = true;
         ++level;
     }
     if (stats) {
@@ -173,7 +252,7 @@ int ghb_bfs(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32
             int32_t* depth, const ghb_bfs_options* options, ghb_traversal_stats* stats) {
     ws = ws_resolve(ws);
     GHB_REQUIRE(ws, "no workspace");
-    return bfs_run(ws, n, out_rowptr, out_col, in_rowptr, in_col, src, max_depth, depth, options,
+    return bfs_run(ws, n, n, out_rowptr, out_col, in_rowptr, in_col, src, max_depth, depth, options,
                    stats);
 }
 
@@ -184,7 +263,7 @@ int ghb_bfs_pred(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const 
     ws = ws_resolve(ws);
     GHB_REQUIRE(ws, "no workspace");
     GHB_REQUIRE(pred != nullptr, "NULL pred");
-    GHB_TRY(bfs_run(ws, n, out_rowptr, out_col, in_rowptr, in_col, src, max_depth, depth, options,
+    GHB_TRY(bfs_run(ws, n, n, out_rowptr, out_col, in_rowptr, in_col, src, max_depth, depth, options,
                     stats));
     const unsigned gmax = ws->num_sms * 8;
     if (in_rowptr && in_col) {

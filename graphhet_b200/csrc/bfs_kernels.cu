@@ -45,7 +45,12 @@ struct LevelAcc {
     unsigned int degmax = 0;
 };
 
+// Block-level reduction of the level counters, then one atomic per counter
+// per block (per-warp atomics on the same four addresses serialise at L2).
 __device__ __forceinline__ void flush_acc(const LevelAcc& a, BfsCounters* cnt) {
+    __shared__ unsigned long long s_mf[32], s_ex[32];
+    __shared__ double s_d2[32];
+    __shared__ unsigned int s_dm[32];
     unsigned long long mf = a.m_f, ex = a.examined;
     double d2 = a.deg2;
     unsigned int dm = a.degmax;
@@ -57,7 +62,22 @@ __device__ __forceinline__ void flush_acc(const LevelAcc& a, BfsCounters* cnt) {
         unsigned int x = __shfl_xor_sync(0xffffffffu, dm, o);
         dm = x > dm ? x : dm;
     }
+    const int w = threadIdx.x >> 5;
     if (lane_id() == 0) {
+        s_mf[w] = mf;
+        s_ex[w] = ex;
+        s_d2[w] = d2;
+        s_dm[w] = dm;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x >> 5;
+        for (int i = 1; i < nw; ++i) {
+            mf += s_mf[i];
+            ex += s_ex[i];
+            d2 += s_d2[i];
+            dm = s_dm[i] > dm ? s_dm[i] : dm;
+        }
         if (mf) atomicAdd(&cnt->m_f, mf);
         if (ex) atomicAdd(&cnt->examined, ex);
         if (d2 != 0.0) atomicAdd(&cnt->deg2, d2);
@@ -65,7 +85,11 @@ __device__ __forceinline__ void flush_acc(const LevelAcc& a, BfsCounters* cnt) {
     }
 }
 
-// Claim v for the next level if nobody has.
+// Claim v for the next level if nobody has.  With q_next (small levels) the
+// claimer also appends v to the next queue and adds its degree to the level
+// statistics; without it (large levels, where one queue counter would
+// serialise millions of appends) only the frontier bitmap is written and
+// bfs_queue_from_bitmap_kernel builds the queue and the statistics later.
 __device__ __forceinline__ void visit(int32_t v, uint32_t* visited, uint32_t* f_next, int32_t* depth,
                                       int32_t next_depth, int32_t* q_next, int32_t* tail,
                                       const int32_t* __restrict__ rowptr, LevelAcc& acc) {
@@ -76,12 +100,14 @@ __device__ __forceinline__ void visit(int32_t v, uint32_t* visited, uint32_t* f_
     if (old & bit) return;
     depth[v] = next_depth;
     atomicOr(f_next + (v >> 5), bit);
-    int32_t pos = warp_append_active(tail);
-    q_next[pos] = v;
-    uint32_t dv = (uint32_t)(rowptr[v + 1] - rowptr[v]);
-    acc.m_f += dv;
-    acc.deg2 += (double)dv * (double)dv;
-    acc.degmax = dv > acc.degmax ? dv : acc.degmax;
+    if (q_next) {
+        int32_t pos = warp_append_active(tail);
+        q_next[pos] = v;
+        uint32_t dv = (uint32_t)(rowptr[v + 1] - rowptr[v]);
+        acc.m_f += dv;
+        acc.deg2 += (double)dv * (double)dv;
+        acc.degmax = dv > acc.degmax ? dv : acc.degmax;
+    }
 }
 
 __global__ void __launch_bounds__(256) bfs_push_kernel(
@@ -237,6 +263,7 @@ __global__ void __launch_bounds__(256) bfs_big_kernel(
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (ok[k]) visit(vs[k], visited, f_next, depth, next_depth, q_next, &cnt->tail, rowptr, acc);
+        acc.examined += (unsigned long long)(ok[0] + ok[1] + ok[2] + ok[3]);
         (void)u1;
     }
     flush_acc(acc, cnt);
@@ -248,7 +275,9 @@ __global__ void __launch_bounds__(256) bfs_pull_kernel(
     int32_t n, int64_t words, const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col,
     const int32_t* __restrict__ out_rp, const uint32_t* __restrict__ f_cur, uint32_t* visited,
     uint32_t* f_next, int32_t* depth, int32_t next_depth, int32_t* q_next, BfsCounters* cnt) {
+    (void)q_next;
     LevelAcc acc;
+    unsigned long long found_total = 0;
     const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -264,14 +293,24 @@ __global__ void __launch_bounds__(256) bfs_pull_kernel(
             e = in_rp[v + 1];
             const int32_t b = j;
             const int32_t lim = min(e, b + 32);
-            for (; j < lim; ++j) {
-                const int32_t u = in_col[j];
-                if ((f_cur[u >> 5] >> (u & 31)) & 1u) {
+            // Probe four entries at a time: the four column loads and the four
+            // frontier-word loads are independent, so they overlap.
+            while (j < lim && !found) {
+                int32_t u[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) u[k] = (j + k < lim) ? in_col[j + k] : -1;
+                bool h[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) h[k] = u[k] >= 0 && ((f_cur[u[k] >> 5] >> (u[k] & 31)) & 1u);
+                int hit = h[0] ? 0 : h[1] ? 1 : h[2] ? 2 : h[3] ? 3 : -1;
+                if (hit >= 0) {
                     found = true;
-                    break;
+                    j += hit + 1;
+                } else {
+                    j = min(j + 4, lim);
                 }
             }
-            acc.examined += (unsigned long long)(j - b + (found ? 1 : 0));
+            acc.examined += (unsigned long long)(j - b);
         }
         unsigned rest = __ballot_sync(0xffffffffu, todo && !found && j < e);
         while (rest) {
@@ -305,11 +344,10 @@ __global__ void __launch_bounds__(256) bfs_pull_kernel(
             if (lane == 0) {
                 visited[w] = vis | fm;
                 f_next[w] = fm;
+                found_total += (unsigned long long)__popc(fm);
             }
             if (found) {
                 depth[v] = next_depth;
-                const int32_t pos = warp_append_active(&cnt->tail);
-                q_next[pos] = (int32_t)v;
                 const uint32_t dv = (uint32_t)(out_rp[v + 1] - out_rp[v]);
                 acc.m_f += dv;
                 acc.deg2 += (double)dv * (double)dv;
@@ -317,7 +355,61 @@ __global__ void __launch_bounds__(256) bfs_pull_kernel(
             }
         }
     }
-    flush_acc(acc, cnt);
+    // New-frontier size: per-block total, one atomic per block.
+    __shared__ unsigned long long s_found[32];
+    found_total = warp_sum(found_total);
+    if (lane == 0) s_found[threadIdx.x >> 5] = found_total;
+    flush_acc(acc, cnt);  // contains __syncthreads
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += s_found[i];
+        if (t) atomicAdd(&cnt->tail, (int32_t)t);
+    }
+}
+
+// The frontier bitmap as a vertex queue (ascending within each warp's 32
+// words), for a top-down level after a bottom-up one or after a large
+// top-down level.  With cnt it also counts the frontier and its degree
+// statistics.
+__global__ void __launch_bounds__(256) bfs_queue_from_bitmap_kernel(int64_t words,
+                                                                    const uint32_t* __restrict__ f,
+                                                                    const int32_t* __restrict__ rowptr,
+                                                                    int32_t* queue, int32_t* tail,
+                                                                    BfsCounters* cnt) {
+    LevelAcc acc;
+    const int lane = lane_id();
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t w0 = warp * 32; w0 < words; w0 += nwarps * 32) {
+        const int64_t w = w0 + lane;
+        uint32_t bits = w < words ? f[w] : 0u;
+        const int32_t c = __popc(bits);
+        int32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += x;
+        }
+        const int32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        if (total == 0) continue;
+        int32_t base = 0;
+        if (lane == 0) base = atomicAdd(tail, total);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        int32_t pos = base + incl - c;
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const int32_t v = (int32_t)(w * 32 + b);
+            queue[pos++] = v;
+            if (cnt) {
+                const uint32_t dv = (uint32_t)(rowptr[v + 1] - rowptr[v]);
+                acc.m_f += dv;
+                acc.deg2 += (double)dv * (double)dv;
+                acc.degmax = dv > acc.degmax ? dv : acc.degmax;
+            }
+        }
+    }
+    if (cnt) flush_acc(acc, cnt);
 }
 
 __global__ void bfs_pred_pull_kernel(int32_t n, const int32_t* __restrict__ in_rp,
@@ -377,6 +469,7 @@ __global__ void bfs_pred_finish_kernel(int32_t n, int32_t src, int32_t* pred) {
 int bfs_push_level(ghb_workspace* ws, const BfsBuffers& B, int32_t n, const int32_t* rowptr,
                    const int32_t* col, const int32_t* q_cur, int64_t n_f, int32_t next_depth,
                    int32_t* depth, int32_t* q_next, uint32_t* f_next) {
+    // q_next == nullptr: bitmap mode (see visit()).
     (void)n;
     const unsigned gmax = ws->num_sms * 8;
     GHB_TRY(launch(ws, bfs_push_kernel, dim3(grid_for(n_f * 32, 256, gmax)), dim3(256), 0, rowptr,
@@ -392,7 +485,7 @@ int bfs_push_level(ghb_workspace* ws, const BfsBuffers& B, int32_t n, const int3
 
 int bfs_time_both(ghb_workspace* ws, const BfsBuffers& B, int32_t n, int64_t words,
                   const int32_t* out_rowptr, const int32_t* out_col, const int32_t* in_rowptr,
-                  const int32_t* in_col, const int32_t* q_cur, int64_t n_f, const uint32_t* f_cur,
+                  const int32_t* in_col, const int32_t* q_cur, int64_t n_f, int64_t m_f, const uint32_t* f_cur,
                   int level, int32_t* depth, float* t_push, float* t_pull) {
     cudaStream_t st = ws->stream;
     const unsigned gmax = ws->num_sms * 8;
@@ -408,8 +501,12 @@ int bfs_time_both(ghb_workspace* ws, const BfsBuffers& B, int32_t n, int64_t wor
         GHB_CUDA_TRY(cudaMemsetAsync(f_tmp, 0, words * sizeof(uint32_t), st));
         GHB_CUDA_TRY(cudaEventRecord(ws->ev_a, st));
         if (pass == 0) {
-            GHB_TRY(bfs_push_level(ws, B, n, out_rowptr, out_col, q_cur, n_f, level + 1, depth, q_tmp,
-                                   f_tmp));
+            const bool append = m_f < kAppendMaxEdges;
+            GHB_TRY(bfs_push_level(ws, B, n, out_rowptr, out_col, q_cur, n_f, level + 1, depth,
+                                   append ? q_tmp : (int32_t*)nullptr, f_tmp));
+            if (!append)
+                GHB_TRY(launch(ws, bfs_queue_from_bitmap_kernel, dim3(grid_for(words * 32, 256, gmax)), dim3(256),
+                               0, words, (const uint32_t*)f_tmp, out_rowptr, q_tmp, &B.counters->tail, B.counters));
         } else {
             GHB_TRY(launch(ws, bfs_pull_kernel, dim3(grid_for(words * 32, 256, gmax)), dim3(256), 0,
                            n, words, in_rowptr, in_col, out_rowptr, f_cur, B.visited, f_tmp, depth,
@@ -425,6 +522,122 @@ int bfs_time_both(ghb_workspace* ws, const BfsBuffers& B, int32_t n, int64_t wor
                                      cudaMemcpyDeviceToDevice, st));
     }
     return GHB_OK;
+}
+
+}  // namespace ghb
+
+namespace ghb {
+
+// Consecutive small top-down levels in one cooperative launch.  Level L reads
+// queue L%2 and appends to queue (L+1)%2; frontier counters are triple-
+// buffered (level L appends to slot (L+1)%3 and block 0 clears slot (L+2)%3,
+// which nobody reads or writes again before the next barrier), so one grid
+// barrier per level suffices.  After each barrier every block reads the same
+// settled counters and takes the same decision: continue, or stop when the
+// frontier is empty, when its out-entries reach exit_edges, at max_depth, or
+// when the direction rule (frontier entries > unexplored entries / alpha)
+// asks for a bottom-up level.
+// The barrier wait is bounded (grid_barrier): on timeout every block leaves
+// and the host reports GHB_ERR_TIMEOUT.
+__global__ void __launch_bounds__(1024) bfs_push_persistent_kernel(
+    const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, int32_t* qa, int32_t* qb,
+    uint32_t* visited, int32_t* depth, int32_t start_level, int32_t max_depth, int64_t exit_edges,
+    int64_t m_total, int64_t m_r_start, float alpha, BfsPersistState* ps) {
+    __shared__ unsigned long long s_mf[32], s_ex[32];
+    const int lane = lane_id();
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    int32_t level = start_level;
+    int L = 0;  // levels done in this launch
+    while (true) {
+        volatile int32_t* vtail = ps->tail;
+        const int32_t n_f = vtail[L % 3];
+        const int32_t* q_cur = (L & 1) ? qb : qa;
+        int32_t* q_next = (L & 1) ? qa : qb;
+        int32_t* tail_next = &ps->tail[(L + 1) % 3];
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            ps->tail[(L + 2) % 3] = 0;
+            ps->mf[(L + 2) % 3] = 0;
+            ps->dmax[(L + 2) % 3] = 0;
+        }
+        unsigned long long mf = 0, ex = 0;
+        unsigned int dm = 0;
+        for (int64_t base = warp * 32; base < n_f; base += nwarps * 32) {
+            const int64_t i = base + lane;
+            int32_t b = 0, e = 0;
+            if (i < n_f) {
+                const int32_t u = q_cur[i];
+                b = rowptr[u];
+                e = rowptr[u + 1];
+            }
+            ex += (unsigned long long)(e - b);
+            // Whole warp per row, 32 entries per step.
+            unsigned todo = __ballot_sync(0xffffffffu, e > b);
+            while (todo) {
+                const int leader = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const int32_t lb = __shfl_sync(0xffffffffu, b, leader);
+                const int32_t le = __shfl_sync(0xffffffffu, e, leader);
+                for (int32_t j = lb + lane; j < le; j += 32) {
+                    const int32_t v = col[j];
+                    const uint32_t bit = 1u << (v & 31);
+                    uint32_t* wp = visited + (v >> 5);
+                    if ((*wp & bit) == 0 && (atomicOr(wp, bit) & bit) == 0) {
+                        depth[v] = level + 1;
+                        q_next[warp_append_active(tail_next)] = v;
+                        const unsigned int dv = (unsigned int)(rowptr[v + 1] - rowptr[v]);
+                        mf += dv;
+                        dm = dv > dm ? dv : dm;
+                    }
+                }
+            }
+        }
+        // Block totals of this level's counters.
+        mf = warp_sum(mf);
+        ex = warp_sum(ex);
+        dm = warp_max(dm);
+        if (lane == 0) {
+            s_mf[threadIdx.x >> 5] = mf;
+            s_ex[threadIdx.x >> 5] = ex;
+            if (dm) atomicMax(&ps->dmax[(L + 1) % 3], dm);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long a = 0, c = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+                a += s_mf[k];
+                c += s_ex[k];
+            }
+            if (a) atomicAdd(&ps->mf[(L + 1) % 3], a);
+            if (c) atomicAdd(&ps->examined, c);
+        }
+        if (!grid_barrier(&ps->bar_count, &ps->bar_gen, &ps->status)) return;
+        ++L;
+        ++level;
+        const int32_t nf_next = vtail[L % 3];
+        const unsigned long long mf_next = ((volatile unsigned long long*)ps->mf)[L % 3];
+        const unsigned int dmax_next = ((volatile unsigned int*)ps->dmax)[L % 3];
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            ps->m_r += mf_next;
+            ps->reached += nf_next;
+            ps->levels_done = L;
+        }
+        // Stop for an empty frontier, at max_depth, when the frontier is too
+        // big for one launch, or when the direction rule asks for bottom-up.
+        const double m_u = (double)(m_total - m_r_start - (int64_t)ps->m_r);
+        // Rows are walked by one warp each here, so a frontier holding a row of
+        // kBigList entries or more goes back to the balanced host-driven path.
+        if (nf_next == 0 || (int64_t)mf_next >= exit_edges || level >= max_depth || dmax_next >= (unsigned)kBigList ||
+            (alpha > 0.f && (double)mf_next > m_u / alpha))
+            return;
+    }
+}
+
+__global__ void bfs_bitmap_from_queue_kernel(const int32_t* __restrict__ q, int32_t count, uint32_t* f) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = q[i];
+        atomicOr(f + (v >> 5), 1u << (v & 31));
+    }
 }
 
 }  // namespace ghb

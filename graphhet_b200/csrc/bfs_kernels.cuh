@@ -20,6 +20,8 @@ struct BfsCounters {
     unsigned long long big_edges;  // entries in the deferred long lists
 };
 
+struct BfsPersistState;
+
 struct BfsBuffers {
     uint32_t* visited;
     uint32_t* front_a;
@@ -31,6 +33,7 @@ struct BfsBuffers {
     int32_t* depth_snap;   // snapshots for oracle timing
     uint32_t* visited_snap;
     BfsCounters* counters;
+    BfsPersistState* persist;
 
     static BfsBuffers carve(Carver& c, int32_t n, int64_t words) {
         BfsBuffers b;
@@ -44,6 +47,7 @@ struct BfsBuffers {
         b.depth_snap = c.take<int32_t>(n);
         b.visited_snap = c.take<uint32_t>(words);
         b.counters = c.take<BfsCounters>(1);
+        b.persist = reinterpret_cast<BfsPersistState*>(c.take<unsigned long long>(16));
         return b;
     }
 };
@@ -59,6 +63,14 @@ __global__ void bfs_pull_kernel(int32_t n, int64_t words, const int32_t* __restr
                                 const uint32_t* __restrict__ f_cur, uint32_t* visited,
                                 uint32_t* f_next, int32_t* depth, int32_t next_depth,
                                 int32_t* q_next, BfsCounters* cnt);
+
+__global__ void bfs_queue_from_bitmap_kernel(int64_t words, const uint32_t* __restrict__ f,
+                                             const int32_t* __restrict__ rowptr, int32_t* queue, int32_t* tail,
+                                             BfsCounters* cnt);
+
+// Top-down levels whose frontier has at least this many out-entries write
+// only the frontier bitmap; the queue is compacted from it afterwards.
+constexpr int64_t kAppendMaxEdges = 1 << 16;
 
 __global__ void bfs_pred_pull_kernel(int32_t n, const int32_t* __restrict__ in_rp,
                                      const int32_t* __restrict__ in_col,
@@ -78,7 +90,36 @@ int bfs_push_level(ghb_workspace* ws, const BfsBuffers& B, int32_t n, const int3
 // Oracle timing of both directions for one level (state restored after each).
 int bfs_time_both(ghb_workspace* ws, const BfsBuffers& B, int32_t n, int64_t words,
                   const int32_t* out_rowptr, const int32_t* out_col, const int32_t* in_rowptr,
-                  const int32_t* in_col, const int32_t* q_cur, int64_t n_f, const uint32_t* f_cur,
+                  const int32_t* in_col, const int32_t* q_cur, int64_t n_f, int64_t m_f, const uint32_t* f_cur,
                   int level, int32_t* depth, float* t_push, float* t_pull);
+
+}  // namespace ghb
+
+namespace ghb {
+
+// State of the persistent top-down kernel (device memory, zeroed before a run).
+struct BfsPersistState {
+    unsigned bar_count, bar_gen;
+    int32_t status;                 // kDevOk or kDevBarrierTimeout
+    int32_t levels_done;            // levels expanded in this run
+    int32_t tail[3];                // frontier sizes, triple-buffered by level
+    int32_t pad;
+    unsigned long long mf[3];       // frontier out-entries, triple-buffered
+    unsigned int dmax[3];           // largest frontier row, triple-buffered
+    unsigned int pad2;
+    unsigned long long examined;
+    unsigned long long m_r;         // out-entries of all vertices reached in this run
+    long long reached;              // vertices reached in this run
+};
+
+// Frontiers with fewer out-entries than this run in the persistent kernel.
+constexpr int64_t kPersistMaxEdges = 1 << 20;
+
+__global__ void bfs_push_persistent_kernel(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                                           int32_t* qa, int32_t* qb, uint32_t* visited, int32_t* depth,
+                                           int32_t start_level, int32_t max_depth, int64_t exit_edges,
+                                           int64_t m_total, int64_t m_r_start, float alpha, BfsPersistState* ps);
+
+__global__ void bfs_bitmap_from_queue_kernel(const int32_t* __restrict__ q, int32_t count, uint32_t* f);
 
 }  // namespace ghb

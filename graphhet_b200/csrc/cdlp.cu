@@ -299,8 +299,9 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_global_kernel(
 
 }  // namespace
 
+// init_labels (device, may be NULL = vertex ids): starting label values.
 int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col, int32_t iterations,
-             int32_t* labels) {
+             int32_t* labels, const int32_t* init_labels) {
     cudaStream_t st = ws->stream;
     // Largest row, for the global table region.
     const unsigned grid_global = ws->num_sms;
@@ -346,7 +347,10 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
     GHB_CUDA_TRY(cudaMemcpyAsync(cursor, hp, kCdlpClasses * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     GHB_TRY(launch(ws, cdlp_fill_classes_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n, rp,
                    cursor, rows));
-    GHB_TRY(launch(ws, cdlp_iota_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, labels, n));
+    if (init_labels)
+        GHB_CUDA_TRY(cudaMemcpyAsync(labels, init_labels, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
+    else
+        GHB_TRY(launch(ws, cdlp_iota_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, labels, n));
 
     GHB_CUDA_TRY(cudaFuncSetAttribute(cdlp_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(2 * kBlockSlots * sizeof(int32_t))));
@@ -382,5 +386,5 @@ extern "C" int ghb_cdlp(ghb_workspace* ws, int32_t n, const int32_t* all_rowptr,
     GHB_REQUIRE(n >= 1, "n must be >= 1");
     GHB_REQUIRE(all_rowptr && labels, "NULL argument");
     GHB_REQUIRE(iterations >= 0, "iterations < 0");
-    return cdlp_run(ws, n, all_rowptr, all_col, iterations, labels);
+    return cdlp_run(ws, n, all_rowptr, all_col, iterations, labels, nullptr);
 }

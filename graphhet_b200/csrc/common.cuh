@@ -63,6 +63,8 @@ struct ghb_workspace {
     cudaStream_t stream = nullptr;
     void* scratch = nullptr;  // cached device scratch (grown on demand)
     size_t scratch_cap = 0;
+    void* stage = nullptr;    // results in relabelled ids before mapping back
+    size_t stage_cap = 0;
     int64_t* host_pinned = nullptr;  // pinned host mirror for small readbacks
     int64_t* dev_small = nullptr;    // small device block (counters, status)
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
@@ -77,6 +79,9 @@ constexpr int kDevSmallWords = 1024;
 
 // Ensure at least `bytes` of scratch; the previous contents are not kept.
 int ws_reserve(ghb_workspace* ws, size_t bytes);
+// Ensure at least `bytes` of the staging area (kept apart from scratch, so an
+// algorithm can write its relabelled result there while using scratch).
+int ws_reserve_stage(ghb_workspace* ws, size_t bytes);
 // Resolve NULL to the default workspace.
 ghb_workspace* ws_resolve(ghb_workspace* ws);
 // Copy `words` int64 counters from dev_small to host_pinned and wait.

@@ -3,7 +3,8 @@
 
 namespace ghb {
 
-__global__ void __launch_bounds__(1024) walk_big_scan_kernel(const int32_t* __restrict__ rowptr,
+__global__ void __launch_bounds__(1024) walk_big_scan_kernel(const int32_t* __restrict__ rb,
+                                                             const int32_t* __restrict__ re,
                                                              const int32_t* __restrict__ big,
                                                              const int32_t* big_tail,
                                                              int64_t* prefix) {
@@ -17,7 +18,7 @@ __global__ void __launch_bounds__(1024) walk_big_scan_kernel(const int32_t* __re
         int64_t d = 0;
         if (i < count) {
             const int32_t u = big[i];
-            d = rowptr[u + 1] - rowptr[u];
+            d = re[u] - rb[u];
         }
         int64_t incl = d;
 #pragma unroll

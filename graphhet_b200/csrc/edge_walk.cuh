@@ -18,8 +18,10 @@ namespace ghb {
 
 constexpr int32_t kWalkBig = 4096;
 
+// Row u spans entries [rb[u], re[u]) (a CSR passes rb = rowptr,
+// re = rowptr + 1; other views select part of every row).
 template <class F>
-__device__ __forceinline__ void walk_rows(const int32_t* __restrict__ rowptr,
+__device__ __forceinline__ void walk_rows(const int32_t* __restrict__ rb, const int32_t* __restrict__ re,
                                           const int32_t* __restrict__ col,
                                           const int32_t* __restrict__ queue, int64_t count,
                                           int32_t* big, int32_t* big_tail, F& f) {
@@ -32,8 +34,8 @@ __device__ __forceinline__ void walk_rows(const int32_t* __restrict__ rowptr,
         if (i < count) {
             u = queue ? queue[i] : (int32_t)i;
             if (f.want_row(u)) {
-                b = rowptr[u];
-                e = rowptr[u + 1];
+                b = rb[u];
+                e = re[u];
                 if (big && e - b >= kWalkBig) {
                     int32_t pos = warp_append_active(big_tail);
                     big[pos] = u;
@@ -81,24 +83,25 @@ __device__ __forceinline__ void walk_rows(const int32_t* __restrict__ rowptr,
 }
 
 template <class F>
-__global__ void __launch_bounds__(256) walk_kernel(const int32_t* __restrict__ rowptr,
+__global__ void __launch_bounds__(256) walk_kernel(const int32_t* __restrict__ rb, const int32_t* __restrict__ re,
                                                    const int32_t* __restrict__ col,
                                                    const int32_t* __restrict__ queue,
                                                    const int32_t* count_dev, int64_t count_host,
                                                    int32_t* big, int32_t* big_tail, F f) {
     const int64_t count = count_dev ? (int64_t)*count_dev : count_host;
-    walk_rows(rowptr, col, queue, count, big, big_tail, f);
+    walk_rows(rb, re, col, queue, count, big, big_tail, f);
     f.finish();
 }
 
 // Exclusive prefix of the deferred rows' lengths; prefix[count] = total.
-__global__ void __launch_bounds__(1024) walk_big_scan_kernel(const int32_t* __restrict__ rowptr,
+__global__ void __launch_bounds__(1024) walk_big_scan_kernel(const int32_t* __restrict__ rb,
+                                                             const int32_t* __restrict__ re,
                                                              const int32_t* __restrict__ big,
                                                              const int32_t* big_tail,
                                                              int64_t* prefix);
 
 template <class F>
-__global__ void __launch_bounds__(256) walk_big_kernel(const int32_t* __restrict__ rowptr,
+__global__ void __launch_bounds__(256) walk_big_kernel(const int32_t* __restrict__ rb,
                                                        const int32_t* __restrict__ col,
                                                        const int32_t* __restrict__ big,
                                                        const int32_t* big_tail,
@@ -120,11 +123,11 @@ __global__ void __launch_bounds__(256) walk_big_kernel(const int32_t* __restrict
             const int64_t start0 = prefix[lo];
             const int64_t start1 = prefix[lo + 1];
             const int32_t u0 = big[lo];
-            const int32_t b0 = rowptr[u0];
+            const int32_t b0 = rb[u0];
             int32_t u1 = u0, b1 = 0;
             if (start1 < c0 + 128 && lo + 1 < count) {
                 u1 = big[lo + 1];
-                b1 = rowptr[u1];
+                b1 = rb[u1];
             }
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -154,22 +157,30 @@ struct WalkBuffers {
     }
 };
 
-// Walk every entry of the given rows (queue == nullptr: rows [0, count)).
-// count_dev, when set, is read on the device instead of count_host.
+// Walk every entry [rb[u], re[u]) of the given rows (queue == nullptr: rows
+// [0, count)).  count_dev, when set, is read on the device instead of
+// count_host.
+template <class F>
+int walk_range(ghb_workspace* ws, const int32_t* rb, const int32_t* re, const int32_t* col, const int32_t* queue,
+               const int32_t* count_dev, int64_t count_host, int64_t grid_rows, const WalkBuffers& wb, const F& f) {
+    const unsigned gmax = ws->num_sms * 8;
+    GHB_CUDA_TRY(cudaMemsetAsync(wb.big_tail, 0, sizeof(int32_t), ws->stream));
+    GHB_TRY(launch(ws, walk_kernel<F>, dim3(grid_for(grid_rows * 32, 256, gmax)), dim3(256), 0,
+                   rb, re, col, queue, count_dev, count_host, wb.big, wb.big_tail, f));
+    GHB_TRY(launch(ws, walk_big_scan_kernel, dim3(1), dim3(1024), 0, rb, re,
+                   (const int32_t*)wb.big, (const int32_t*)wb.big_tail, wb.prefix));
+    GHB_TRY(launch(ws, walk_big_kernel<F>, dim3(gmax), dim3(256), 0, rb, col,
+                   (const int32_t*)wb.big, (const int32_t*)wb.big_tail,
+                   (const int64_t*)wb.prefix, f));
+    return GHB_OK;
+}
+
+// Walk every entry of the given rows of a CSR.
 template <class F>
 int walk(ghb_workspace* ws, const int32_t* rowptr, const int32_t* col, const int32_t* queue,
          const int32_t* count_dev, int64_t count_host, int64_t grid_rows, const WalkBuffers& wb,
          const F& f) {
-    const unsigned gmax = ws->num_sms * 8;
-    GHB_CUDA_TRY(cudaMemsetAsync(wb.big_tail, 0, sizeof(int32_t), ws->stream));
-    GHB_TRY(launch(ws, walk_kernel<F>, dim3(grid_for(grid_rows * 32, 256, gmax)), dim3(256), 0,
-                   rowptr, col, queue, count_dev, count_host, wb.big, wb.big_tail, f));
-    GHB_TRY(launch(ws, walk_big_scan_kernel, dim3(1), dim3(1024), 0, rowptr,
-                   (const int32_t*)wb.big, (const int32_t*)wb.big_tail, wb.prefix));
-    GHB_TRY(launch(ws, walk_big_kernel<F>, dim3(gmax), dim3(256), 0, rowptr, col,
-                   (const int32_t*)wb.big, (const int32_t*)wb.big_tail,
-                   (const int64_t*)wb.prefix, f));
-    return GHB_OK;
+    return walk_range(ws, rowptr, rowptr + 1, col, queue, count_dev, count_host, grid_rows, wb, f);
 }
 
 }  // namespace ghb

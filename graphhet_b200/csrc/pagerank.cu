@@ -10,24 +10,27 @@
 // partials of the next S and of the L1 change; a one-block kernel reduces the
 // partials in a fixed order (deterministic S and norm, FP64 in both modes).
 //
-// Rows are summed by groups of VW lanes (VW picked from the mean in-degree);
-// rows with >= kPrBig entries are split into kPrChunk-entry chunks summed by
-// one warp each and combined per row in chunk order.
+// Rows of up to 32 entries are summed by one thread each; longer rows are
+// cut into 256-entry chunks summed by one warp each and combined per row in
+// chunk order.  Both kernels serve the hubs' contributions from a shared-
+// memory cache (a degree-relabelled graph puts the hubs first).
 //
 // FP32 mode: ranks and contributions are stored as float (half the gather
 // footprint: 64 MiB at n = 2^24, resident in the 126 MB L2); each lane keeps
 // a Kahan-compensated FP32 sum and lanes are merged with an error-free
 // TwoSum; the row total, S and the L1 norm are FP64.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
 #include "common.cuh"
+#include "scan.cuh"
 
 namespace ghb {
 namespace {
 
-constexpr int32_t kPrBig = 8192;
-constexpr int32_t kPrChunk = 2048;
+constexpr int32_t kPrShort = 32;   // rows up to this length are packed
+constexpr int32_t kPrChunk = 256;  // longer rows are cut into chunks of this many entries
 constexpr int kPrThreads = 256;
 
 template <class T>
@@ -111,21 +114,21 @@ __global__ void __launch_bounds__(kPrThreads) pr_init_kernel(int32_t n, const in
 template <class T>
 __device__ __forceinline__ void pr_finish_row(int64_t v, double sum, const PrScalars* sc, double damping,
                                               const int32_t* __restrict__ outdeg, const T* rank_old,
-                                              T* rank_new, T* contrib_new, double& sink, double& l1) {
+                                              T* rank_new, T* contrib_new, int track_l1, double& sink,
+                                              double& l1) {
     const double r = sc->base + damping * sum;
     const T rt = (T)r;
     const int32_t d = outdeg[v];
-    const double old = (double)rank_old[v];
     rank_new[v] = rt;
     contrib_new[v] = d > 0 ? (T)(r / (double)d) : (T)0;
     if (d == 0) sink += (double)rt;
-    l1 += fabs((double)rt - old);
+    if (track_l1) l1 += fabs((double)rt - (double)rank_old[v]);
 }
 
 template <class T>
 __device__ __forceinline__ void block_partials(double sink, double l1, double* part_sink, double* part_l1,
                                                int slot) {
-    __shared__ double red_s[kPrThreads / 32], red_l[kPrThreads / 32];
+    __shared__ double red_s[32], red_l[32];
     sink = warp_sum(sink);
     l1 = warp_sum(l1);
     if (lane_id() == 0) {
@@ -135,7 +138,7 @@ __device__ __forceinline__ void block_partials(double sink, double l1, double* p
     __syncthreads();
     if (threadIdx.x == 0) {
         double s = 0.0, l = 0.0;
-        for (int i = 0; i < kPrThreads / 32; ++i) {
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
             s += red_s[i];
             l += red_l[i];
         }
@@ -144,119 +147,143 @@ __device__ __forceinline__ void block_partials(double sink, double l1, double* p
     }
 }
 
-// Rows with < kPrBig entries: VW lanes per row.
-template <class T, int VW>
-__global__ void __launch_bounds__(kPrThreads) pr_rows_kernel(
+// Shared-memory cache of the first kHubCacheBytes / sizeof(T) contributions.
+// On a degree-relabelled graph these are the hubs' (the top 32K vertices of
+// an RMAT scale-22 graph hold half of all entries), so about half of the
+// gathers are served from shared memory instead of L2 sectors.  The kernels
+// that use it run one persistent 1024-thread block per SM, so each SM fills
+// the cache once per launch.
+constexpr int kPrPersistThreads = 1024;
+constexpr int kHubCacheBytes = 192 * 1024;
+
+template <class T>
+__device__ __forceinline__ int32_t fill_hub_cache(T* cache, const T* __restrict__ contrib_old, int32_t n) {
+    const int32_t K = min((int32_t)(kHubCacheBytes / sizeof(T)), n);
+    for (int32_t i = threadIdx.x; i < K; i += blockDim.x) cache[i] = contrib_old[i];
+    __syncthreads();
+    return K;
+}
+
+template <class T>
+__device__ __forceinline__ T gather(const T* cache, int32_t K, const T* __restrict__ contrib_old, int32_t u,
+                                    uint64_t pol) {
+    return u < K ? cache[u] : load_contrib<T>(contrib_old + u, pol);
+}
+
+// Rows of up to kPrShort entries: one thread per row, gathers four at a time
+// (independent loads), Kahan-summed in row order.  Longer rows are skipped
+// here (chunk path).
+template <class T>
+__global__ void __launch_bounds__(kPrPersistThreads) pr_rows_short_kernel(
     int32_t n, const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col,
     const int32_t* __restrict__ outdeg, const T* __restrict__ contrib_old, const T* rank_old,
-    T* rank_new, T* contrib_new, const PrScalars* sc, double damping, double* part_sink,
+    T* rank_new, T* contrib_new, const PrScalars* sc, double damping, int track_l1, double* part_sink,
     double* part_l1) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* cache = reinterpret_cast<T*>(smem_raw);
+    const int32_t K = fill_hub_cache<T>(cache, contrib_old, n);
     const uint64_t pol_stream = policy_evict_first();
     const uint64_t pol_keep = policy_evict_last();
-    const int sub = threadIdx.x % VW;
-    const int64_t group = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / VW;
-    const int64_t ngroups = ((int64_t)gridDim.x * blockDim.x) / VW;
     double sink = 0.0, l1 = 0.0;
-    // Every lane of a warp runs the same trip count so the shuffles stay
-    // converged.
-    const int64_t rounds = ((int64_t)n + ngroups - 1) / ngroups;
-    for (int64_t r = 0; r < rounds; ++r) {
-        const int64_t v = group + r * ngroups;
-        int32_t b = 0, e = 0;
-        if (v < n) {
-            b = in_rp[v];
-            e = in_rp[v + 1];
-            if (e - b >= kPrBig) e = b - 1;  // handled by the chunk kernels
-        }
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t b = in_rp[r], e = in_rp[r + 1];
+        if (e - b > kPrShort) continue;
         KSum<T> acc;
-        for (int32_t j = b + sub; j < e; j += VW) {
-            const int32_t u = ld_stream(in_col + j, pol_stream);
-            acc.add(load_contrib<T>(contrib_old + u, pol_keep));
-        }
+        for (int32_t j = b; j < e; j += 4) {
+            int32_t u[4];
 #pragma unroll
-        for (int o = VW / 2; o > 0; o >>= 1) acc.merge_from_lane(o, VW);
-        if (sub == 0 && v < n && e >= b)
-            pr_finish_row<T>(v, acc.value(), sc, damping, outdeg, rank_old, rank_new, contrib_new, sink, l1);
+            for (int k = 0; k < 4; ++k) u[k] = (j + k < e) ? ld_stream(in_col + j + k, pol_stream) : -1;
+            T x[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) x[k] = u[k] >= 0 ? gather<T>(cache, K, contrib_old, u[k], pol_keep) : (T)0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (u[k] >= 0) acc.add(x[k]);
+        }
+        pr_finish_row<T>(r, acc.value(), sc, damping, outdeg, rank_old, rank_new, contrib_new, track_l1, sink, l1);
     }
     block_partials<T>(sink, l1, part_sink, part_l1, blockIdx.x);
 }
 
-__global__ void pr_find_big_kernel(int32_t n, const int32_t* __restrict__ in_rp, int32_t* big,
-                                   int32_t* big_tail) {
-    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
-         v += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t d = in_rp[v + 1] - in_rp[v];
-        if (d >= kPrBig) big[atomicAdd(big_tail, 1)] = (int32_t)v;
+__global__ void pr_long_flags_kernel(int32_t n, const int32_t* __restrict__ in_rp, int32_t* flag) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        flag[v] = (in_rp[v + 1] - in_rp[v]) > kPrShort ? 1 : 0;
+}
+
+// Long rows in ascending order, and their chunk counts.
+__global__ void pr_long_compact_kernel(int32_t n, const int32_t* __restrict__ in_rp, const int32_t* __restrict__ flag,
+                                       const int32_t* __restrict__ pos, int32_t* long_rows, int32_t* nchunks) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        if (!flag[v]) continue;
+        const int32_t i = pos[v];
+        long_rows[i] = (int32_t)v;
+        nchunks[i] = (in_rp[v + 1] - in_rp[v] + kPrChunk - 1) / kPrChunk;
     }
 }
 
-// chunk_prefix[i] = chunks before big row i (one block, few rows).
-__global__ void __launch_bounds__(1024) pr_chunk_scan_kernel(const int32_t* __restrict__ in_rp,
-                                                             const int32_t* __restrict__ big,
-                                                             const int32_t* big_tail,
-                                                             int32_t* chunk_prefix) {
-    __shared__ int32_t carry;
-    if (threadIdx.x == 0) {
-        // Sequential: the list is short (rows >= kPrBig entries).
-        int32_t acc = 0;
-        const int32_t count = *big_tail;
-        for (int32_t i = 0; i < count; ++i) {
-            const int32_t u = big[i];
-            chunk_prefix[i] = acc;
-            acc += (in_rp[u + 1] - in_rp[u] + kPrChunk - 1) / kPrChunk;
-        }
-        chunk_prefix[count] = acc;
-        carry = acc;
-    }
+// chunk_row[c] = index (in long_rows) of the row chunk c belongs to.
+__global__ void pr_chunk_rows_kernel(int32_t nlong, const int32_t* __restrict__ chunk_prefix, int32_t* chunk_row) {
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = warp; i < nlong; i += nwarps)
+        for (int32_t c = chunk_prefix[i] + lane_id(); c < chunk_prefix[i + 1]; c += 32) chunk_row[c] = (int32_t)i;
 }
 
+// One warp per chunk of kPrChunk entries: a partial sum, four independent
+// 32-wide loads in flight per lane, hub contributions from shared memory.
 template <class T>
-__global__ void __launch_bounds__(kPrThreads) pr_chunk_kernel(
-    const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col, const int32_t* __restrict__ big,
-    const int32_t* big_tail, const int32_t* __restrict__ chunk_prefix, const T* __restrict__ contrib_old,
-    double* chunk_sum) {
+__global__ void __launch_bounds__(kPrPersistThreads) pr_chunk_kernel(
+    int32_t n, const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col,
+    const int32_t* __restrict__ long_rows, const int32_t* __restrict__ chunk_prefix,
+    const int32_t* __restrict__ chunk_row, int32_t nchunks, const T* __restrict__ contrib_old, double* chunk_sum) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* cache = reinterpret_cast<T*>(smem_raw);
+    const int32_t K = fill_hub_cache<T>(cache, contrib_old, n);
     const uint64_t pol_stream = policy_evict_first();
     const uint64_t pol_keep = policy_evict_last();
-    const int32_t count = *big_tail;
-    if (count == 0) return;
-    const int32_t nchunks = chunk_prefix[count];
+    const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t ch = warp; ch < nchunks; ch += nwarps) {
-        int32_t lo = 0, hi = count - 1;
-        while (lo < hi) {
-            const int32_t mid = (lo + hi + 1) >> 1;
-            if (chunk_prefix[mid] <= ch) lo = mid;
-            else hi = mid - 1;
-        }
-        const int32_t u = big[lo];
+        const int32_t i = chunk_row[ch];
+        const int32_t u = long_rows[i];
         const int32_t rb = in_rp[u], re = in_rp[u + 1];
-        const int32_t b = rb + (int32_t)(ch - chunk_prefix[lo]) * kPrChunk;
+        const int32_t b = rb + (int32_t)(ch - chunk_prefix[i]) * kPrChunk;
         const int32_t e = min(re, b + kPrChunk);
         KSum<T> acc;
-        for (int32_t j = b + lane_id(); j < e; j += 32) {
-            const int32_t x = ld_stream(in_col + j, pol_stream);
-            acc.add(load_contrib<T>(contrib_old + x, pol_keep));
+        for (int32_t j0 = b; j0 < e; j0 += 128) {
+            int32_t x[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int32_t j = j0 + lane + 32 * k;
+                x[k] = j < e ? ld_stream(in_col + j, pol_stream) : -1;
+            }
+            T y[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) y[k] = x[k] >= 0 ? gather<T>(cache, K, contrib_old, x[k], pol_keep) : (T)0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (x[k] >= 0) acc.add(y[k]);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc.merge_from_lane(o, 32);
-        if (lane_id() == 0) chunk_sum[ch] = acc.value();
+        if (lane == 0) chunk_sum[ch] = acc.value();
     }
 }
 
+// Long rows: the chunk partials summed in chunk order, then the row update.
 template <class T>
-__global__ void __launch_bounds__(kPrThreads) pr_big_finish_kernel(
-    const int32_t* __restrict__ big, const int32_t* big_tail, const int32_t* __restrict__ chunk_prefix,
-    const double* __restrict__ chunk_sum, const int32_t* __restrict__ outdeg, const T* rank_old,
-    T* rank_new, T* contrib_new, const PrScalars* sc, double damping, double* part_sink,
-    double* part_l1, int slot0) {
-    const int32_t count = *big_tail;
+__global__ void __launch_bounds__(kPrThreads) pr_long_finish_kernel(
+    int32_t nlong, const int32_t* __restrict__ long_rows, const int32_t* __restrict__ chunk_prefix,
+    const double* __restrict__ chunk_sum, const int32_t* __restrict__ outdeg, const T* rank_old, T* rank_new,
+    T* contrib_new, const PrScalars* sc, double damping, int track_l1, double* part_sink, double* part_l1,
+    int slot0) {
     double sink = 0.0, l1 = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nlong;
          i += (int64_t)gridDim.x * blockDim.x) {
         double s = 0.0;
         for (int32_t c = chunk_prefix[i]; c < chunk_prefix[i + 1]; ++c) s += chunk_sum[c];
-        pr_finish_row<T>(big[i], s, sc, damping, outdeg, rank_old, rank_new, contrib_new, sink, l1);
+        pr_finish_row<T>(long_rows[i], s, sc, damping, outdeg, rank_old, rank_new, contrib_new, track_l1, sink, l1);
     }
     block_partials<T>(sink, l1, part_sink, part_l1, slot0 + blockIdx.x);
 }
@@ -300,91 +327,101 @@ __global__ void pr_to_f64_kernel(const T* src, double* dst, int32_t n) {
         dst[v] = (double)src[v];
 }
 
-template <class T, int VW>
-int launch_rows(ghb_workspace* ws, unsigned grid, int32_t n, const int32_t* in_rp, const int32_t* in_col,
-                const int32_t* outdeg, const T* c_old, const T* r_old, T* r_new, T* c_new,
-                const PrScalars* sc, double d, double* ps, double* pl) {
-    return launch(ws, pr_rows_kernel<T, VW>, dim3(grid), dim3(kPrThreads), 0, n, in_rp, in_col, outdeg,
-                  c_old, r_old, r_new, c_new, sc, d, ps, pl);
-}
-
 template <class T>
 int pagerank_impl(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int32_t* in_col,
                   const int32_t* out_rp, const ghb_pr_options* o, double* rank_out, int32_t* iters_run) {
     cudaStream_t st = ws->stream;
-    const unsigned grid_rows = ws->num_sms * 8;
-    const unsigned grid_big = ws->num_sms * 2;
-    const int nparts = grid_rows + grid_big;
-    Carver sizing(nullptr);
-    auto carve = [&](Carver& c, T** ra, T** rb, T** ca, T** cb, int32_t** outdeg, int32_t** big,
-                     int32_t** big_tail, int32_t** chunk_prefix, double** chunk_sum, double** ps,
-                     double** pl, PrScalars** sc, double** hist) {
+    const unsigned grid_rows = ws->num_sms;  // persistent: one block per SM
+    const unsigned grid_long = ws->num_sms * 2;
+    const int nparts = grid_rows + grid_long;
+    int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
+    GHB_CUDA_TRY(cudaMemcpyAsync(hp, in_rp + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    const int64_t m = hp[0];
+    // Upper bounds: long rows <= min(n, m / (kPrShort + 1)), chunks <= m / kPrChunk + long rows.
+    const int64_t max_long = std::min<int64_t>(n, m / (kPrShort + 1) + 1);
+    const int64_t max_chunks = m / kPrChunk + max_long + 1;
+    auto carve = [&](Carver& c, T** ra, T** rb, T** ca, T** cb, int32_t** outdeg, int32_t** flag, int32_t** pos,
+                     int32_t** long_rows, int32_t** nch, int32_t** cpre, int32_t** crow, double** csum, int64_t** bs,
+                     double** ps, double** pl, PrScalars** sc, double** hist) {
         *ra = c.take<T>(n);
         *rb = c.take<T>(n);
         *ca = c.take<T>(n);
         *cb = c.take<T>(n);
         *outdeg = c.take<int32_t>(n);
-        const int64_t max_big = 1 + (int64_t)n / 1;  // bounded by n
-        *big = c.take<int32_t>(max_big);
-        *big_tail = c.take<int32_t>(8);
-        *chunk_prefix = c.take<int32_t>(max_big + 1);
-        // chunk count <= m / kPrChunk + big rows; m < 2^31.
-        *chunk_sum = c.take<double>(((int64_t)1 << 31) / kPrChunk + max_big + 1);
+        *flag = c.take<int32_t>(n);
+        *pos = c.take<int32_t>((size_t)n + 1);
+        *long_rows = c.take<int32_t>(max_long);
+        *nch = c.take<int32_t>(max_long);
+        *cpre = c.take<int32_t>(max_long + 1);
+        *crow = c.take<int32_t>(max_chunks);
+        *csum = c.take<double>(max_chunks);
+        *bs = c.take<int64_t>(scan_scratch_words(n > max_long ? n : max_long));
         *ps = c.take<double>(nparts);
         *pl = c.take<double>(nparts);
         *sc = c.take<PrScalars>(1);
         *hist = c.take<double>(o->iterations > 0 ? o->iterations : 1);
     };
     T *ra, *rb, *ca, *cb;
-    int32_t *outdeg, *big, *big_tail, *chunk_prefix;
-    double *chunk_sum, *ps, *pl, *hist;
+    int32_t *outdeg, *flag, *pos, *long_rows, *nch, *cpre, *crow;
+    double *csum, *ps, *pl, *hist;
+    int64_t* bs;
     PrScalars* sc;
-    carve(sizing, &ra, &rb, &ca, &cb, &outdeg, &big, &big_tail, &chunk_prefix, &chunk_sum, &ps, &pl, &sc,
+    Carver sizing(nullptr);
+    carve(sizing, &ra, &rb, &ca, &cb, &outdeg, &flag, &pos, &long_rows, &nch, &cpre, &crow, &csum, &bs, &ps, &pl, &sc,
           &hist);
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
-    carve(c, &ra, &rb, &ca, &cb, &outdeg, &big, &big_tail, &chunk_prefix, &chunk_sum, &ps, &pl, &sc, &hist);
+    carve(c, &ra, &rb, &ca, &cb, &outdeg, &flag, &pos, &long_rows, &nch, &cpre, &crow, &csum, &bs, &ps, &pl, &sc,
+          &hist);
 
     const double d = o->damping;
+    const unsigned g = ws->num_sms * 8;
+    GHB_CUDA_TRY(cudaFuncSetAttribute(pr_rows_short_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kHubCacheBytes));
+    GHB_CUDA_TRY(cudaFuncSetAttribute(pr_chunk_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kHubCacheBytes));
     GHB_CUDA_TRY(cudaMemsetAsync(ps, 0, sizeof(double) * nparts, st));
     GHB_CUDA_TRY(cudaMemsetAsync(pl, 0, sizeof(double) * nparts, st));
-    GHB_CUDA_TRY(cudaMemsetAsync(big_tail, 0, sizeof(int32_t), st));
     GHB_TRY(launch(ws, pr_init_kernel<T>, dim3(grid_rows), dim3(kPrThreads), 0, n, out_rp, outdeg, ra, ca, ps));
-    GHB_TRY(launch(ws, pr_reduce_kernel, dim3(1), dim3(1024), 0, (const double*)ps, (const double*)pl,
-                   nparts, n, d, sc, (double*)nullptr, 0, 0));
-    GHB_TRY(launch(ws, pr_find_big_kernel, dim3(grid_for(n, 256, ws->num_sms * 4)), dim3(256), 0, n, in_rp,
-                   big, big_tail));
-    GHB_TRY(launch(ws, pr_chunk_scan_kernel, dim3(1), dim3(32), 0, in_rp, (const int32_t*)big,
-                   (const int32_t*)big_tail, chunk_prefix));
-
-    // Mean in-degree picks the lanes per row.
-    int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
-    GHB_CUDA_TRY(cudaMemcpyAsync(hp, in_rp + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GHB_TRY(launch(ws, pr_reduce_kernel, dim3(1), dim3(1024), 0, (const double*)ps, (const double*)pl, nparts, n, d,
+                   sc, (double*)nullptr, 0, 0));
+    // Long-row list (ascending) and its chunks.
+    GHB_TRY(launch(ws, pr_long_flags_kernel, dim3(grid_for(n, 256, g)), dim3(256), 0, n, in_rp, flag));
+    GHB_TRY(scan_exclusive_i32(ws, flag, pos, n, bs));
+    GHB_CUDA_TRY(cudaMemcpyAsync(hp, pos + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     GHB_CUDA_TRY(cudaStreamSynchronize(st));
-    const double mean = (double)hp[0] / (double)n;
-    const int vw = mean >= 24 ? 16 : mean >= 10 ? 8 : mean >= 4 ? 4 : 2;
+    const int32_t nlong = hp[0];
+    int32_t nchunks = 0;
+    if (nlong > 0) {
+        GHB_TRY(launch(ws, pr_long_compact_kernel, dim3(grid_for(n, 256, g)), dim3(256), 0, n, in_rp,
+                       (const int32_t*)flag, (const int32_t*)pos, long_rows, nch));
+        GHB_TRY(scan_exclusive_i32(ws, nch, cpre, nlong, bs));
+        GHB_CUDA_TRY(cudaMemcpyAsync(hp, cpre + nlong, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        nchunks = hp[0];
+        GHB_TRY(launch(ws, pr_chunk_rows_kernel, dim3(grid_for((int64_t)nlong * 32, 256, g)), dim3(256), 0, nlong,
+                       (const int32_t*)cpre, crow));
+    }
 
     T *r_cur = ra, *r_nxt = rb, *c_cur = ca, *c_nxt = cb;
     const bool track = o->tolerance > 0 || o->l1_history != nullptr;
     int it = 0;
     for (; it < o->iterations; ++it) {
-        int s;
-        switch (vw) {
-            case 16: s = launch_rows<T, 16>(ws, grid_rows, n, in_rp, in_col, outdeg, c_cur, r_cur, r_nxt, c_nxt, sc, d, ps, pl); break;
-            case 8: s = launch_rows<T, 8>(ws, grid_rows, n, in_rp, in_col, outdeg, c_cur, r_cur, r_nxt, c_nxt, sc, d, ps, pl); break;
-            case 4: s = launch_rows<T, 4>(ws, grid_rows, n, in_rp, in_col, outdeg, c_cur, r_cur, r_nxt, c_nxt, sc, d, ps, pl); break;
-            default: s = launch_rows<T, 2>(ws, grid_rows, n, in_rp, in_col, outdeg, c_cur, r_cur, r_nxt, c_nxt, sc, d, ps, pl); break;
+        GHB_TRY(launch(ws, pr_rows_short_kernel<T>, dim3(grid_rows), dim3(kPrPersistThreads), (size_t)kHubCacheBytes,
+                       n, in_rp, in_col, (const int32_t*)outdeg, (const T*)c_cur, (const T*)r_cur, r_nxt, c_nxt,
+                       (const PrScalars*)sc, d, track ? 1 : 0, ps, pl));
+        if (nlong > 0) {
+            GHB_TRY(launch(ws, pr_chunk_kernel<T>, dim3(ws->num_sms), dim3(kPrPersistThreads), (size_t)kHubCacheBytes,
+                           n, in_rp, in_col, (const int32_t*)long_rows, (const int32_t*)cpre, (const int32_t*)crow,
+                           nchunks, (const T*)c_cur, csum));
         }
-        GHB_TRY(s);
-        GHB_TRY(launch(ws, pr_chunk_kernel<T>, dim3(ws->num_sms * 4), dim3(kPrThreads), 0, in_rp, in_col,
-                       (const int32_t*)big, (const int32_t*)big_tail, (const int32_t*)chunk_prefix,
-                       (const T*)c_cur, chunk_sum));
-        GHB_TRY(launch(ws, pr_big_finish_kernel<T>, dim3(grid_big), dim3(kPrThreads), 0, (const int32_t*)big,
-                       (const int32_t*)big_tail, (const int32_t*)chunk_prefix, (const double*)chunk_sum,
-                       (const int32_t*)outdeg, (const T*)r_cur, r_nxt, c_nxt, (const PrScalars*)sc, d, ps, pl,
+        GHB_TRY(launch(ws, pr_long_finish_kernel<T>, dim3(grid_long), dim3(kPrThreads), 0, nlong,
+                       (const int32_t*)long_rows, (const int32_t*)cpre, (const double*)csum, (const int32_t*)outdeg,
+                       (const T*)r_cur, r_nxt, c_nxt, (const PrScalars*)sc, d, track ? 1 : 0, ps, pl,
                        (int)grid_rows));
-        GHB_TRY(launch(ws, pr_reduce_kernel, dim3(1), dim3(1024), 0, (const double*)ps, (const double*)pl,
-                       nparts, n, d, sc, hist, it, track ? 1 : 0));
+        GHB_TRY(launch(ws, pr_reduce_kernel, dim3(1), dim3(1024), 0, (const double*)ps, (const double*)pl, nparts, n,
+                       d, sc, hist, it, track ? 1 : 0));
         std::swap(r_cur, r_nxt);
         std::swap(c_cur, c_nxt);
         if (o->tolerance > 0) {
@@ -397,8 +434,8 @@ int pagerank_impl(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int3
             }
         }
     }
-    GHB_TRY(launch(ws, pr_to_f64_kernel<T>, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0,
-                   (const T*)r_cur, rank_out, n));
+    GHB_TRY(launch(ws, pr_to_f64_kernel<T>, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, (const T*)r_cur,
+                   rank_out, n));
     if (o->l1_history && it > 0) {
         GHB_CUDA_TRY(cudaMemcpyAsync(o->l1_history, hist, sizeof(double) * it, cudaMemcpyDeviceToHost, st));
         GHB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -408,6 +445,13 @@ int pagerank_impl(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int3
 }
 
 }  // namespace
+
+int pagerank_run(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int32_t* in_col, const int32_t* out_rp,
+                 const ghb_pr_options* o, double* rank, int32_t* iters_run) {
+    if (o->precision == GHB_PR_FP64) return pagerank_impl<double>(ws, n, in_rp, in_col, out_rp, o, rank, iters_run);
+    return pagerank_impl<float>(ws, n, in_rp, in_col, out_rp, o, rank, iters_run);
+}
+
 }  // namespace ghb
 
 using namespace ghb;

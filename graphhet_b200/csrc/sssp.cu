@@ -16,12 +16,16 @@
 // above the threshold go to the far list.  Then the threshold moves up by
 // delta and the far list is split.  A vertex enters a queue at most once per
 // round (stamp arrays).
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
 #include "edge_walk.cuh"
+#include "graph.cuh"
 #include "policy.cuh"
 
 namespace ghb {
@@ -212,6 +216,57 @@ __global__ void reached_edges_kernel(int32_t n, const int32_t* __restrict__ rp, 
     }
 }
 
+// ---- delta-stepping with a light/heavy split (resident graphs)
+
+// Sort key of entry j of row u: row, then the weight's top 39 bits (sign,
+// exponent and 28 mantissa bits).  Rows must fit in 25 bits.
+__global__ void weight_key_kernel(int32_t n, const int32_t* __restrict__ rp, const double* __restrict__ w,
+                                  uint64_t* keys, uint32_t* vals) {
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t u = warp; u < n; u += nwarps) {
+        for (int32_t j = rp[u] + lane_id(); j < rp[u + 1]; j += 32) {
+            const uint64_t wb = (uint64_t)__double_as_longlong(w[j]);
+            keys[j] = ((uint64_t)u << 39) | (wb >> 25);
+            vals[j] = (uint32_t)j;
+        }
+    }
+}
+
+__global__ void weight_gather_kernel(int64_t m, const uint32_t* __restrict__ vals, const int32_t* __restrict__ col,
+                                     const double* __restrict__ w, int32_t* sw_col, double* sw_w) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = vals[i];
+        sw_col[i] = col[j];
+        sw_w[i] = w[j];
+    }
+}
+
+// light_end[u] = first entry of row u with weight >= delta (rows sorted by
+// the truncated weight, and delta itself has no bits below the truncation,
+// so the comparison is exact).
+__global__ void light_end_kernel(int32_t n, const int32_t* __restrict__ rp, const double* __restrict__ sw_w,
+                                 double delta, int32_t* light_end) {
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+        int32_t lo = rp[u], hi = rp[u + 1];
+        while (lo < hi) {
+            const int32_t mid = (lo + hi) >> 1;
+            if (sw_w[mid] < delta) lo = mid + 1;
+            else hi = mid;
+        }
+        light_end[u] = lo;
+    }
+}
+
+// Adds the vertices of the near queue to the settled list R (once per phase).
+__global__ void mark_settled_kernel(const int32_t* __restrict__ q, int32_t count, int32_t* r_stamp, int32_t phase,
+                                    int32_t* R, int32_t* r_tail) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t u = q[i];
+        if (atomicExch(r_stamp + u, phase) != phase) R[atomicAdd(r_tail, 1)] = u;
+    }
+}
+
 __global__ void fill_i32(int32_t* p, int64_t count, int32_t value) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
          i += (int64_t)gridDim.x * blockDim.x)
@@ -354,6 +409,201 @@ int sssp_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t*
         unsigned long long* acc = reinterpret_cast<unsigned long long*>(ws->dev_small);
         GHB_CUDA_TRY(cudaMemsetAsync(acc, 0, 2 * sizeof(unsigned long long), st));
         GHB_TRY(launch(ws, reached_edges_kernel, dim3(g), dim3(256), 0, n, rowptr, (const double*)dist_out, inf, acc));
+        GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, acc, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaEventSynchronize(ws->ev_stop));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        float ms = 0.f;
+        GHB_CUDA_TRY(cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop));
+        const unsigned long long* ha = reinterpret_cast<const unsigned long long*>(ws->host_pinned);
+        stats->levels = (int32_t)rounds;
+        stats->pull_levels = phase;
+        stats->edges_reached = (int64_t)ha[0];
+        stats->reached = (int64_t)ha[1];
+        stats->edges_examined = examined;
+        stats->device_ms = ms;
+    }
+    return GHB_OK;
+}
+
+// Weight-sorted copy of a resident graph's rows (once per handle).
+int graph_weight_sorted(ghb_workspace* ws, ghb_graph* g) {
+    if (g->sw_col || g->m == 0) return GHB_OK;
+    const int64_t m = g->m;
+    size_t sort_tmp = 0;
+    {
+        cub::DoubleBuffer<uint64_t> dk(nullptr, nullptr);
+        cub::DoubleBuffer<uint32_t> dv(nullptr, nullptr);
+        cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp, dk, dv, m, 0, 64);
+    }
+    Carver sizing(nullptr);
+    sizing.take<uint64_t>(m);
+    sizing.take<uint64_t>(m);
+    sizing.take<uint32_t>(m);
+    sizing.take<uint32_t>(m);
+    sizing.take<char>(sort_tmp);
+    GHB_TRY(ws_reserve(ws, sizing.off));
+    Carver c(ws->scratch);
+    uint64_t* k0 = c.take<uint64_t>(m);
+    uint64_t* k1 = c.take<uint64_t>(m);
+    uint32_t* v0 = c.take<uint32_t>(m);
+    uint32_t* v1 = c.take<uint32_t>(m);
+    void* tmp = c.take<char>(sort_tmp);
+    GHB_CUDA_TRY(cudaMalloc(&g->sw_col, sizeof(int32_t) * m));
+    GHB_CUDA_TRY(cudaMalloc(&g->sw_w, sizeof(double) * m));
+    g->device_bytes += (int64_t)(12 * m);
+    const unsigned gr = ws->num_sms * 8;
+    GHB_TRY(launch(ws, weight_key_kernel, dim3(gr), dim3(256), 0, g->n, (const int32_t*)g->rowptr,
+                   (const double*)g->w, k0, v0));
+    cub::DoubleBuffer<uint64_t> dk(k0, k1);
+    cub::DoubleBuffer<uint32_t> dv(v0, v1);
+    size_t tb = sort_tmp;
+    GHB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tb, dk, dv, m, 0, 64, ws->stream));
+    ws->launches++;
+    return launch(ws, weight_gather_kernel, dim3(gr), dim3(256), 0, m, (const uint32_t*)dv.Current(),
+                  (const int32_t*)g->col, (const double*)g->w, g->sw_col, g->sw_w);
+}
+
+// Delta-stepping on a resident graph: each bucket's rounds relax only the
+// light entries (w < delta) of its near queue; once the bucket is empty the
+// heavy entries of every vertex it settled are relaxed once.  Rows are read
+// from the weight-sorted copy, so a light pass reads only a row prefix.
+int sssp_delta_run(ghb_workspace* ws, ghb_graph* g, int32_t src, double inf, double delta, double* dist_out,
+                   ghb_traversal_stats* stats) {
+    const int32_t n = g->n;
+    cudaStream_t st = ws->stream;
+    GHB_TRY(graph_weight_sorted(ws, g));
+    // Clear the mantissa bits below the sort key's precision.
+    {
+        uint64_t b;
+        std::memcpy(&b, &delta, sizeof(b));
+        b &= ~((1ull << 25) - 1);
+        std::memcpy(&delta, &b, sizeof(b));
+        if (!(delta > 0)) delta = 1.0;
+    }
+    auto carve = [&](Carver& c, WalkBuffers* wb, int32_t** qa, int32_t** qb, int32_t** fa, int32_t** fb, int32_t** ns,
+                     int32_t** fs, int32_t** rs, int32_t** R, int32_t** le, SsspCounters** cnt, double** minfar,
+                     int32_t** rtail) {
+        *wb = WalkBuffers::carve(c, n);
+        *qa = c.take<int32_t>(n);
+        *qb = c.take<int32_t>(n);
+        *fa = c.take<int32_t>(n);
+        *fb = c.take<int32_t>(n);
+        *ns = c.take<int32_t>(n);
+        *fs = c.take<int32_t>(n);
+        *rs = c.take<int32_t>(n);
+        *R = c.take<int32_t>(n);
+        *le = c.take<int32_t>(n);
+        *cnt = c.take<SsspCounters>(1);
+        *minfar = c.take<double>(1);
+        *rtail = c.take<int32_t>(8);
+    };
+    WalkBuffers wb;
+    int32_t *qa, *qb, *fa, *fb, *ns, *fs, *rs, *R, *le, *rtail;
+    SsspCounters* cnt;
+    double* minfar;
+    Carver sizing(nullptr);
+    carve(sizing, &wb, &qa, &qb, &fa, &fb, &ns, &fs, &rs, &R, &le, &cnt, &minfar, &rtail);
+    GHB_TRY(ws_reserve(ws, sizing.off));
+    Carver c(ws->scratch);
+    carve(c, &wb, &qa, &qb, &fa, &fb, &ns, &fs, &rs, &R, &le, &cnt, &minfar, &rtail);
+
+    unsigned long long* dist = reinterpret_cast<unsigned long long*>(dist_out);
+    const unsigned gsz = grid_for(n, 256, ws->num_sms * 8);
+    if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
+    GHB_TRY(launch(ws, sssp_init_kernel, dim3(gsz), dim3(256), 0, n, src, inf, dist, ns, fs, qa));
+    GHB_TRY(launch(ws, fill_i32, dim3(gsz), dim3(256), 0, rs, (int64_t)n, (int32_t)-1));
+    GHB_TRY(launch(ws, light_end_kernel, dim3(gsz), dim3(256), 0, n, (const int32_t*)g->rowptr,
+                   (const double*)g->sw_w, delta, le));
+    GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(SsspCounters), st));
+    const int32_t* rp = g->rowptr;
+    const int32_t* rp1 = g->rowptr + 1;
+    int64_t near_count = 1, far_count = 0, examined = 0, rounds = 0;
+    int32_t round = 0, phase = 0;
+    double thr = delta;
+    const SsspCounters* hc = reinterpret_cast<const SsspCounters*>(ws->host_pinned);
+    const int64_t round_budget = 64ll * n + 1024;
+    while (true) {
+        int32_t r_count = 0;
+        GHB_CUDA_TRY(cudaMemsetAsync(rtail, 0, sizeof(int32_t), st));
+        while (true) {
+            while (near_count > 0) {
+                if (++rounds > round_budget) {
+                    set_error("SSSP round budget exhausted");
+                    return GHB_ERR_LIMIT;
+                }
+                ++round;
+                GHB_TRY(launch(ws, mark_settled_kernel, dim3(grid_for(near_count, 256, ws->num_sms * 8)), dim3(256), 0,
+                               (const int32_t*)qa, (int32_t)near_count, rs, phase, R, rtail));
+                GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, offsetof(SsspCounters, far_tail), st));
+                GHB_CUDA_TRY(cudaMemsetAsync(&cnt->examined, 0, sizeof(unsigned long long), st));
+                RelaxVisitor f{g->sw_w, dist, thr, qb, ns, round, fa, fs, phase, cnt, 0ull};
+                GHB_TRY(walk_range(ws, rp, (const int32_t*)le, g->sw_col, (const int32_t*)qa, (const int32_t*)nullptr,
+                                   near_count, near_count, wb, f));
+                GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, cnt, sizeof(SsspCounters), cudaMemcpyDeviceToHost, st));
+                GHB_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(ws->host_pinned) + 128, rtail, sizeof(int32_t),
+                                             cudaMemcpyDeviceToHost, st));
+                GHB_CUDA_TRY(cudaStreamSynchronize(st));
+                near_count = hc->near_tail;
+                far_count = hc->far_tail;
+                r_count = *reinterpret_cast<const int32_t*>(reinterpret_cast<const char*>(ws->host_pinned) + 128);
+                examined += (int64_t)hc->examined;
+                std::swap(qa, qb);
+            }
+            if (r_count == 0) break;
+            // Heavy entries of the vertices this bucket settled, once.
+            ++round;
+            GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, offsetof(SsspCounters, far_tail), st));
+            GHB_CUDA_TRY(cudaMemsetAsync(&cnt->examined, 0, sizeof(unsigned long long), st));
+            RelaxVisitor f{g->sw_w, dist, thr, qa, ns, round, fa, fs, phase, cnt, 0ull};
+            GHB_TRY(walk_range(ws, (const int32_t*)le, rp1, g->sw_col, (const int32_t*)R, (const int32_t*)nullptr,
+                               r_count, r_count, wb, f));
+            GHB_CUDA_TRY(cudaMemsetAsync(rtail, 0, sizeof(int32_t), st));
+            GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, cnt, sizeof(SsspCounters), cudaMemcpyDeviceToHost, st));
+            GHB_CUDA_TRY(cudaStreamSynchronize(st));
+            near_count = hc->near_tail;  // heavy entries landing in this bucket (rounding)
+            far_count = hc->far_tail;
+            examined += (int64_t)hc->examined;
+            r_count = 0;
+            if (near_count == 0) break;
+        }
+        if (far_count == 0) break;
+        ++phase;
+        ++round;
+        const double old_thr = thr;
+        GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(SsspCounters), st));
+        const double big = INFINITY;
+        GHB_CUDA_TRY(cudaMemcpyAsync(minfar, &big, sizeof(double), cudaMemcpyHostToDevice, st));
+        GHB_TRY(launch(ws, sssp_split_kernel, dim3(grid_for(far_count, 256, ws->num_sms * 8)), dim3(256), 0,
+                       (const int32_t*)fa, (int32_t)far_count, (const unsigned long long*)dist, old_thr, old_thr, qa, ns,
+                       round, fb, fs, phase, cnt, minfar));
+        GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, cnt, sizeof(SsspCounters), cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(ws->host_pinned) + 256, minfar, sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        const int64_t kept = hc->far_tail;
+        const double mn = *reinterpret_cast<const double*>(reinterpret_cast<const char*>(ws->host_pinned) + 256);
+        if (kept == 0) break;
+        double nthr = old_thr + delta;
+        if (mn >= nthr) nthr = old_thr + delta * std::floor((mn - old_thr) / delta + 1.0);
+        if (!(nthr > mn)) nthr = mn + delta;
+        ++phase;
+        ++round;
+        GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(SsspCounters), st));
+        GHB_TRY(launch(ws, sssp_split_kernel, dim3(grid_for(kept, 256, ws->num_sms * 8)), dim3(256), 0,
+                       (const int32_t*)fb, (int32_t)kept, (const unsigned long long*)dist, old_thr, nthr, qa, ns, round,
+                       fa, fs, phase, cnt, minfar));
+        GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, cnt, sizeof(SsspCounters), cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        near_count = hc->split_near;
+        far_count = hc->far_tail;
+        thr = nthr;
+    }
+    if (stats) {
+        GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
+        unsigned long long* acc = reinterpret_cast<unsigned long long*>(ws->dev_small);
+        GHB_CUDA_TRY(cudaMemsetAsync(acc, 0, 2 * sizeof(unsigned long long), st));
+        GHB_TRY(launch(ws, reached_edges_kernel, dim3(gsz), dim3(256), 0, n, (const int32_t*)g->rowptr,
+                       (const double*)dist_out, inf, acc));
         GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, acc, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         GHB_CUDA_TRY(cudaEventSynchronize(ws->ev_stop));
         GHB_CUDA_TRY(cudaStreamSynchronize(st));

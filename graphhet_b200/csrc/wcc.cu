@@ -97,3 +97,4 @@ extern "C" int ghb_wcc(ghb_workspace* ws, int32_t n, const int32_t* rowptr, cons
     GHB_REQUIRE(rowptr && label, "NULL argument");
     return wcc_run(ws, n, rowptr, col, label);
 }
+

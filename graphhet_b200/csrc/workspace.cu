@@ -30,6 +30,20 @@ int ws_reserve(ghb_workspace* ws, size_t bytes) {
     return GHB_OK;
 }
 
+int ws_reserve_stage(ghb_workspace* ws, size_t bytes) {
+    if (bytes <= ws->stage_cap) return GHB_OK;
+    if (ws->stage) {
+        GHB_CUDA_TRY(cudaStreamSynchronize(ws->stream));
+        GHB_CUDA_TRY(cudaFree(ws->stage));
+        ws->stage = nullptr;
+        ws->stage_cap = 0;
+    }
+    size_t cap = (bytes + (16ull << 20) - 1) & ~((16ull << 20) - 1);
+    GHB_CUDA_TRY(cudaMalloc(&ws->stage, cap));
+    ws->stage_cap = cap;
+    return GHB_OK;
+}
+
 int ws_read_small(ghb_workspace* ws, int words) {
     GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, ws->dev_small, sizeof(int64_t) * words,
                                  cudaMemcpyDeviceToHost, ws->stream));
@@ -88,6 +102,7 @@ int ghb_workspace_destroy(ghb_workspace* ws) {
     if (!ws) return GHB_OK;
     if (ws->stream || ws->scratch) cudaStreamSynchronize(ws->stream);
     if (ws->scratch) cudaFree(ws->scratch);
+    if (ws->stage) cudaFree(ws->stage);
     if (ws->host_pinned) cudaFreeHost(ws->host_pinned);
     if (ws->dev_small) cudaFree(ws->dev_small);
     if (ws->ev_start) cudaEventDestroy(ws->ev_start);
@@ -119,6 +134,9 @@ int ghb_workspace_trim(ghb_workspace* ws) {
     }
     ws->scratch = nullptr;
     ws->scratch_cap = 0;
+    if (ws->stage) GHB_CUDA_TRY(cudaFree(ws->stage));
+    ws->stage = nullptr;
+    ws->stage_cap = 0;
     return GHB_OK;
 }
 
@@ -126,7 +144,7 @@ int ghb_workspace_counters(ghb_workspace* ws, int64_t* kernel_launches, int64_t*
     ws = ws_resolve(ws);
     GHB_REQUIRE(ws != nullptr, "no workspace");
     if (kernel_launches) *kernel_launches = ws->launches;
-    if (scratch_bytes) *scratch_bytes = static_cast<int64_t>(ws->scratch_cap);
+    if (scratch_bytes) *scratch_bytes = static_cast<int64_t>(ws->scratch_cap + ws->stage_cap);
     return GHB_OK;
 }
 

@@ -112,7 +112,7 @@ int ghb_csr_merge_in_out(ghb_workspace* ws, int32_t n, const int32_t* in_rowptr,
 
 typedef struct {
     int32_t policy;
-    float alpha;             /* switch to pull when m_f > m_u / alpha (0: 14) */
+    float alpha;             /* switch to pull when m_f > m_u / alpha (0: 256) */
     float beta;              /* back to push when n_f < n / beta (0: 24)      */
     const int8_t* schedule;  /* host array for GHB_POLICY_SCHEDULE            */
     int32_t schedule_len;
@@ -236,6 +236,48 @@ int ghb_cdlp(ghb_workspace* ws, int32_t n, const int32_t* all_rowptr, const int3
  * NULL; *total receives sum(counts64) / 3 (may be NULL). */
 int ghb_tc(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col,
            int64_t* counts64, int32_t* counts32, int64_t* total);
+
+/* ---------------------------------------------------- resident graphs */
+/* A graph handle: the caller's CSR (device arrays, only read during the
+ * call) relabelled once on the GPU by total degree, descending, so hubs get
+ * the smallest ids, sorted rows list hubs first and vertices without entries
+ * form a tail the kernels skip.  This is the one-time preparation the
+ * reference does in toCSR (GPU_csr.hpp:282-339); every ghb_graph_* call then
+ * returns exactly what the raw-CSR entry point of the same name returns, in
+ * the caller's vertex ids (BFS/SSSP predecessors: a valid parent, not
+ * necessarily the smallest id).  in_* == NULL or == out_*: undirected.  The
+ * handle owns its device memory; calls on one handle may share a workspace
+ * but must not overlap. */
+typedef struct ghb_graph ghb_graph;
+
+int ghb_graph_create(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr,
+                     const int32_t* out_col, const double* out_w,
+                     const int32_t* in_rowptr, const int32_t* in_col, const double* in_w,
+                     ghb_graph** out);
+int ghb_graph_destroy(ghb_graph* g);
+int ghb_graph_info(const ghb_graph* g, int64_t* m, int32_t* n_active, int64_t* device_bytes,
+                   float* build_ms);
+/* Device arrays perm[old] = new and iperm[new] = old (owned by the handle). */
+int ghb_graph_perm(const ghb_graph* g, const int32_t** perm, const int32_t** iperm);
+
+int ghb_graph_bfs(ghb_workspace* ws, const ghb_graph* g, int32_t src, int32_t max_depth,
+                  int32_t* depth, const ghb_bfs_options* options, ghb_traversal_stats* stats);
+int ghb_graph_bfs_pred(ghb_workspace* ws, const ghb_graph* g, int32_t src, int32_t max_depth,
+                       int32_t* depth, int32_t* pred, const ghb_bfs_options* options,
+                       ghb_traversal_stats* stats);
+int ghb_graph_msbfs(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
+                    int32_t* depth, ghb_traversal_stats* stats);
+int ghb_graph_sssp(ghb_workspace* ws, const ghb_graph* g, int32_t src, double inf, double* dist,
+                   const ghb_sssp_options* options, ghb_traversal_stats* stats);
+int ghb_graph_sssp_pred(ghb_workspace* ws, const ghb_graph* g, int32_t src, double inf,
+                        double* dist, int32_t* pred, const ghb_sssp_options* options,
+                        ghb_traversal_stats* stats);
+int ghb_graph_wcc(ghb_workspace* ws, const ghb_graph* g, int32_t* label);
+int ghb_graph_pagerank(ghb_workspace* ws, const ghb_graph* g, const ghb_pr_options* options,
+                       double* rank, int32_t* iterations_run);
+int ghb_graph_cdlp(ghb_workspace* ws, const ghb_graph* g, int32_t iterations, int32_t* labels);
+int ghb_graph_tc(ghb_workspace* ws, const ghb_graph* g, int64_t* counts64, int32_t* counts32,
+                 int64_t* total);
 
 /* ------------------------------------------------------ batched graphs */
 /* Many independent graphs packed back to back.  vbase / ebase are HOST

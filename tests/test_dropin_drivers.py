@@ -33,6 +33,8 @@ def sections(text):
         if line.endswith("result:"):
             cur = line[: -len(" result:")]
             out[cur] = {}
+        elif line.startswith("Running"):
+            cur = None
         elif cur and len(line.split()) == 2:
             k, v = line.split()
             out[cur][k] = v
@@ -63,7 +65,7 @@ def write_dataset(tmp, name, og: O.Graph, directed: bool, names, src):
     with open(os.path.join(tmp, name + ".e"), "w") as f:
         for u, v, w in zip(rows, og.col, og.w):
             if directed or u < v:
-                f.write(f"{names[u]} {names[v]} {w!r}\n")
+                f.write(f"{names[u]} {names[v]} {float(w)!r}\n")
     m = og.m if directed else og.m // 2
     props = {
         "vertex-file": name + ".v", "edge-file": name + ".e", "vertices": n, "edges": m,
