@@ -11,6 +11,9 @@
 // The label array is the union-find forest (int32[n], L2 resident at
 // n = 2^24); parent reads bypass L1 (ld.cg) so updates from other SMs are
 // seen without going through stale lines.
+#include <mutex>
+#include <string>
+
 #include "common.cuh"
 #include "edge_walk.cuh"
 
@@ -98,3 +101,94 @@ extern "C" int ghb_wcc(ghb_workspace* ws, int32_t n, const int32_t* rowptr, cons
     return wcc_run(ws, n, rowptr, col, label);
 }
 
+// ---------------------------------------------------------------------------
+// WCC that allocates nothing.
+//
+// Some callers of this library must not allocate device memory while it
+// runs: an application that owns the GPU's memory through its own pool
+// allocator (the library loaded as a plugin inside a database or a serving
+// process, where a cudaMalloc behind the pool's back can fail or fragment
+// it), and latency-critical callers for which cudaMalloc / cudaFree would
+// synchronise the device.  Such a caller cannot create a ghb_workspace
+// either, since a workspace allocates its scratch and pinned counters.
+//
+// ghb_wcc_noalloc takes a stream instead of a workspace.  Its only scratch
+// is the row walker's deferred long-row list, kept in the fixed file-scope
+// device array below, which every GPU that loads libghb.so holds until the
+// process exits.  Limit: at most kNoAllocMaxEntries CSR entries, which bounds
+// the rows of kWalkBig or more entries by the list's capacity.
+namespace ghb {
+namespace {
+
+constexpr int64_t kNoAllocMaxEntries = 1ll << 28;                  // 268,435,456 entries
+constexpr int64_t kNoAllocBigRows = kNoAllocMaxEntries / kWalkBig;  // 65,536 long rows
+constexpr size_t kNoAllocScratchBytes = 800 * 1024;
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+}  // namespace
+}  // namespace ghb
+
+// Device-side scratch of ghb_wcc_noalloc.  In host code this name is only a
+// host-side stand-in for the symbol, not a device address: the device
+// address is looked up per device with cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_wcc_noalloc_scratch[ghb::kNoAllocScratchBytes];
+
+namespace ghb {
+
+// Device address of the scratch array on the current device, looked up once
+// per device (with that device current) and cached.
+static int noalloc_scratch_address(void** out) {
+    int dev = 0;
+    GHB_CUDA_TRY(cudaGetDevice(&dev));
+    GHB_REQUIRE(dev >= 0 && dev < 64, "device index outside [0, 64)");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        GHB_CUDA_TRY(cudaGetSymbolAddress(&p, g_wcc_noalloc_scratch));
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return GHB_OK;
+}
+
+}  // namespace ghb
+
+extern "C" int ghb_wcc_noalloc(int32_t n, const int32_t* rowptr, const int32_t* col, int32_t* label,
+                               void* stream) {
+    GHB_REQUIRE(n >= 1, "n must be >= 1");
+    GHB_REQUIRE(rowptr && label, "NULL argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // Entry count, for the size limit (one small read-back on `stream`).
+    int32_t m = 0;
+    GHB_CUDA_TRY(cudaMemcpyAsync(&m, rowptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (m < 0 || (int64_t)m > kNoAllocMaxEntries) {
+        set_error("invalid argument: ghb_wcc_noalloc handles at most 268435456 CSR entries (its scratch is a "
+                  "fixed 800 KiB device array); this graph has " + std::to_string(m) + ", use ghb_wcc");
+        return GHB_ERR_INVALID_ARGUMENT;
+    }
+    void* base = nullptr;
+    GHB_TRY(noalloc_scratch_address(&base));
+    Carver c(base);
+    WalkBuffers wb = WalkBuffers::carve(c, kNoAllocBigRows);
+    if (c.off > kNoAllocScratchBytes) {
+        set_error("internal: ghb_wcc_noalloc scratch layout exceeds its array");
+        return GHB_ERR_UNSUPPORTED;
+    }
+    // A stack workspace carries only the stream and SM count to the launch
+    // helpers; it owns no memory.
+    ghb_workspace tmp;
+    tmp.stream = st;
+    int dev = 0;
+    GHB_CUDA_TRY(cudaGetDevice(&dev));
+    GHB_CUDA_TRY(cudaDeviceGetAttribute(&tmp.num_sms, cudaDevAttrMultiProcessorCount, dev));
+    const unsigned g = grid_for(n, 256, tmp.num_sms * 8);
+    GHB_TRY(launch(&tmp, iota_kernel, dim3(g), dim3(256), 0, label, n));
+    // walk() zeroes the list's counter first: the array keeps the previous
+    // call's contents.
+    GHB_TRY(walk(&tmp, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
+                 UniteVisitor{label}));
+    return launch(&tmp, wcc_compress_kernel, dim3(g), dim3(256), 0, label, n);
+}

@@ -197,6 +197,22 @@ int ghb_mssssp(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_
 int ghb_wcc(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col,
             int32_t* label);
 
+/* The same WCC without any device allocation, for callers that must not
+ * allocate while the library runs: an application that owns the GPU's memory
+ * through its own pool (the library as a plugin inside a database or a
+ * serving process) or a latency-critical caller for which cudaMalloc would
+ * synchronise the device.  No counterpart in the reference.  It takes a
+ * cudaStream_t instead of a workspace; its scratch is a fixed 800 KiB device
+ * array inside libghb.so, held by every GPU that loads the library until the
+ * process exits.  Limit: at most 268,435,456 (2^28) CSR entries; larger
+ * graphs are rejected with GHB_ERR_INVALID_ARGUMENT.  The first call on a
+ * device looks up the array's address (cudaGetSymbolAddress): make that first
+ * call before any stream capture.  Every call shares the array, so calls that
+ * overlap on the GPU race: serialise them.  Reads rowptr[n] back once and
+ * synchronises `stream`. */
+int ghb_wcc_noalloc(int32_t n, const int32_t* rowptr, const int32_t* col, int32_t* label,
+                    void* stream);
+
 /* -------------------------------------------------------------- PageRank */
 #define GHB_PR_FP64 0
 #define GHB_PR_FP32_KAHAN 1
