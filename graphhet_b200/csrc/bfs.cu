@@ -17,6 +17,21 @@
 
 namespace ghb {
 
+bool bfs_persistent_available(ghb_workspace* ws, int* blocks);
+
+// The whole traversal runs in one cooperative launch unless the caller asks
+// for per-level traces (training data) or the learned policy (host-side for
+// now), or the device cannot launch cooperatively.
+bool bfs_use_persistent(ghb_workspace* ws, const ghb_bfs_options* opt) {
+    int blocks = 0;
+    if (!bfs_persistent_available(ws, &blocks)) return false;
+    if (!opt) return true;
+    if (opt->oracle_timing) return false;
+    if (opt->record_trace && opt->trace_cap < 0) return false;
+    return opt->policy == GHB_POLICY_HEURISTIC || opt->policy == GHB_POLICY_PUSH || opt->policy == GHB_POLICY_PULL ||
+           opt->policy == GHB_POLICY_SCHEDULE;
+}
+
 // n_active: vertices [n_active, n) have no entries at all (a relabelled
 // graph puts them last); bottom-up levels skip them.
 int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_rowptr, const int32_t* out_col,
@@ -252,6 +267,15 @@ int ghb_bfs(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32
             int32_t* depth, const ghb_bfs_options* options, ghb_traversal_stats* stats) {
     ws = ws_resolve(ws);
     GHB_REQUIRE(ws, "no workspace");
+    if (bfs_use_persistent(ws, options)) {
+        GHB_REQUIRE(n >= 1, "n must be >= 1");
+        GHB_REQUIRE(out_rowptr && depth, "NULL graph or output");
+        GHB_REQUIRE(src >= 0 && src < n, "source outside [0, n)");
+        GHB_REQUIRE(max_depth >= 0, "max_depth < 0");
+        const bool can_pull = in_rowptr != nullptr && in_col != nullptr;
+        return bfs_persistent_run(ws, n, n, out_rowptr, out_col, can_pull ? in_rowptr : nullptr,
+                                  can_pull ? in_col : nullptr, src, max_depth, depth, nullptr, nullptr, options, stats);
+    }
     return bfs_run(ws, n, n, out_rowptr, out_col, in_rowptr, in_col, src, max_depth, depth, options,
                    stats);
 }

@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(1024) bfs_big_scan_kernel(const int32_t* __res
 }
 
 // Edge-parallel expansion of the deferred lists.  Each warp takes 128
-// consecutive entries; since every list holds >= kBigList > 128 entries, a
+// consecutive entries; since every list holds >= kBigList >= 128 entries, a
 // chunk crosses at most one list boundary.
 __global__ void __launch_bounds__(256) bfs_big_kernel(
     const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,

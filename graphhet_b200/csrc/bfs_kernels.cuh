@@ -6,8 +6,12 @@
 namespace ghb {
 
 // Lists at least this long are expanded edge-parallel across the whole grid
-// instead of by one warp.
-constexpr int32_t kBigList = 4096;
+// instead of by one warp (a warp walking a long list is a chain of dependent
+// claims, 32 entries per step).
+constexpr int32_t kBigList = 256;
+// In the persistent kernel, deferred lists at least this long are walked by
+// every thread of the grid; shorter deferred lists by one block each.
+constexpr int32_t kHugeList = 1 << 16;
 
 struct BfsCounters {
     int32_t tail;       // next-queue length
@@ -121,5 +125,11 @@ __global__ void bfs_push_persistent_kernel(const int32_t* __restrict__ rowptr, c
                                            int64_t m_total, int64_t m_r_start, float alpha, BfsPersistState* ps);
 
 __global__ void bfs_bitmap_from_queue_kernel(const int32_t* __restrict__ q, int32_t count, uint32_t* f);
+
+bool bfs_use_persistent(ghb_workspace* ws, const ghb_bfs_options* opt);
+int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_rp, const int32_t* out_col,
+                       const int32_t* in_rp, const int32_t* in_col, int32_t src, int32_t max_depth, int32_t* depth,
+                       const int32_t* perm, int32_t* depth_out, const ghb_bfs_options* opt,
+                       ghb_traversal_stats* stats);
 
 }  // namespace ghb

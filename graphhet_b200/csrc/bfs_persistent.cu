@@ -1,0 +1,549 @@
+// Whole-traversal BFS in one cooperative launch.
+//
+// The host-driven BFS (bfs.cu) pays a host round trip per level; on an RMAT
+// scale-24 graph that is most of a traversal's time, and on a 4096x4096 grid
+// (4097 levels) it is all of it.  Here every level runs inside one launch:
+//
+//   level L:  expand   top-down (queue) or bottom-up (bitmap), claims write
+//                      depth, the next frontier bitmap and level counters
+//             barrier
+//             [top-down only, if the frontier held rows of >= kBigList
+//              entries: those rows, entry-parallel over the whole grid;
+//              barrier]
+//             block 0 decides the next level (direction rule, stop test)
+//             barrier
+//
+// Frontier bitmaps and counters are triple-buffered by level: level L reads
+// slot L%3, writes slot (L+1)%3 and clears slot (L+2)%3, which no block reads
+// or writes during level L, so the clears need no extra barrier.  Queues are
+// double-buffered (level L reads queue L%2, appends to queue (L+1)%2).
+// Every grid barrier is bounded (grid_barrier): on timeout all blocks leave
+// and the host reports GHB_ERR_TIMEOUT.
+#include <algorithm>
+#include <vector>
+
+#include "bfs_kernels.cuh"
+#include "common.cuh"
+
+namespace ghb {
+
+struct BfsRunState {
+    unsigned bar_count;            // barrier arrivals (own cache line)
+    unsigned pad_a[31];
+    unsigned bar_release;          // barrier epochs (own cache line)
+    unsigned pad_b[31];
+    int32_t status;
+    int32_t level;       // current level
+    int32_t dir;         // 0 top-down, 1 bottom-up
+    int32_t done;
+    int32_t append;      // top-down level appends to the queue (small frontier)
+    int32_t queue_ok;    // the current queue holds the current frontier
+    int32_t nf[3];       // frontier sizes by slot
+    int32_t big[3];      // deferred long rows by slot
+    unsigned dmax[3];
+    unsigned pad;
+    unsigned long long mf[3];
+    unsigned long long examined;
+    unsigned long long m_r;
+    long long reached;
+    int32_t pull_levels;
+    int32_t levels;
+    int32_t qcount;      // queue compaction cursor (zero at every level start)
+    int32_t pad2;
+    unsigned long long t_prev;       // global timer at the previous decision
+    int8_t lvl_dir[64];              // per-level record (first 64 levels)
+    float lvl_ms[64];
+    int32_t lvl_nf[64];
+    unsigned long long lvl_mf[64];
+};
+
+namespace {
+
+struct PAcc {
+    unsigned long long mf = 0, ex = 0;
+    unsigned int dm = 0, nf = 0;
+};
+
+// Block totals, one atomic per counter per block.  Contains __syncthreads.
+__device__ __forceinline__ void p_flush(PAcc a, BfsRunState* st, int slot, bool count_nf) {
+    __shared__ unsigned long long s_mf[32], s_ex[32];
+    __shared__ unsigned s_dm[32], s_nf[32];
+    a.mf = warp_sum(a.mf);
+    a.ex = warp_sum(a.ex);
+    a.nf = warp_sum(a.nf);
+    a.dm = warp_max(a.dm);
+    if (lane_id() == 0) {
+        s_mf[threadIdx.x >> 5] = a.mf;
+        s_ex[threadIdx.x >> 5] = a.ex;
+        s_dm[threadIdx.x >> 5] = a.dm;
+        s_nf[threadIdx.x >> 5] = a.nf;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long mf = 0, ex = 0;
+        unsigned dm = 0, nf = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+            mf += s_mf[i];
+            ex += s_ex[i];
+            nf += s_nf[i];
+            dm = s_dm[i] > dm ? s_dm[i] : dm;
+        }
+        if (mf) atomicAdd(&st->mf[slot], mf);
+        if (ex) atomicAdd(&st->examined, ex);
+        if (dm) atomicMax(&st->dmax[slot], dm);
+        if (count_nf && nf) atomicAdd(&st->nf[slot], (int32_t)nf);
+    }
+    __syncthreads();
+}
+
+// Claim v for level `next_depth`.
+__device__ __forceinline__ void p_visit(int32_t v, uint32_t* visited, uint32_t* f_next, int32_t* depth,
+                                        int32_t next_depth, int32_t* q_next, int32_t* tail, bool append,
+                                        const int32_t* __restrict__ rowptr, PAcc& acc) {
+    const uint32_t bit = 1u << (v & 31);
+    uint32_t* wp = visited + (v >> 5);
+    if (*wp & bit) return;
+    if (atomicOr(wp, bit) & bit) return;
+    depth[v] = next_depth;
+    atomicOr(f_next + (v >> 5), bit);
+    if (append) q_next[warp_append_active(tail)] = v;
+    else acc.nf += 1;
+    const unsigned dv = (unsigned)(rowptr[v + 1] - rowptr[v]);
+    acc.mf += dv;
+    acc.dm = dv > acc.dm ? dv : acc.dm;
+}
+
+__device__ __forceinline__ bool p_barrier(BfsRunState* st) {
+    return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, NoLeader());
+}
+template <class F>
+__device__ __forceinline__ bool p_barrier(BfsRunState* st, const F& leader) {
+    return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, leader);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(512) bfs_persistent_kernel(
+    int32_t n, int32_t n_active, const int32_t* __restrict__ out_rp, const int32_t* __restrict__ out_col,
+    const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col, int32_t src, int32_t max_depth,
+    int32_t* depth, uint32_t* visited, uint32_t* f0, uint32_t* f1, uint32_t* f2, int32_t* qa, int32_t* qb,
+    int32_t* big, int policy, float alpha, float beta, int64_t m_total, const int8_t* __restrict__ schedule,
+    int32_t schedule_len, const int32_t* __restrict__ perm, int32_t* depth_out, BfsRunState* st) {
+    const int lane = lane_id();
+    const int64_t gtid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t gsize = (int64_t)gridDim.x * blockDim.x;
+    const int64_t warp = gtid >> 5;
+    const int64_t nwarps = gsize >> 5;
+    const int64_t words = ((int64_t)n + 31) / 32;
+    const int64_t words_active = ((int64_t)n_active + 31) / 32;
+
+    // ---- init
+    for (int64_t v = gtid; v < n; v += gsize) depth[v] = (v == src) ? 0 : kInfDepth;
+    for (int64_t w = gtid; w < words; w += gsize) {
+        const uint32_t bit = (w == (src >> 5)) ? (1u << (src & 31)) : 0u;
+        visited[w] = bit;
+        f0[w] = bit;
+        f1[w] = 0u;
+        f2[w] = 0u;
+    }
+    if (gtid == 0) {
+        qa[0] = src;
+        const unsigned ds = (unsigned)(out_rp[src + 1] - out_rp[src]);
+        st->nf[0] = 1;
+        st->mf[0] = ds;
+        st->dmax[0] = ds;
+        st->append = ds < (unsigned)kAppendMaxEdges ? 1 : 0;
+        st->queue_ok = 1;
+        st->level = 0;
+        st->dir = (policy == GHB_POLICY_SCHEDULE && in_rp && schedule && schedule_len > 0 && schedule[0]) ? 1 : 0;
+        st->done = max_depth <= 0 ? 1 : 0;
+        st->t_prev = global_timer_ns();
+    }
+    if (!p_barrier(st)) return;
+
+    __shared__ int32_t s_state[6];
+    volatile BfsRunState* vs = st;
+    while (true) {
+        // Settled by the previous barrier: every block reads the same values.
+        // Thread 0 reads them and shares them (all threads reading the same
+        // L2 line would serialise thousands of requests per level).
+        if (threadIdx.x == 0) {
+            const int32_t lv = vs->level;
+            s_state[0] = vs->done;
+            s_state[1] = lv;
+            s_state[2] = vs->dir;
+            s_state[3] = vs->append;
+            s_state[4] = vs->nf[lv % 3];
+            s_state[5] = vs->queue_ok;
+        }
+        __syncthreads();
+        if (s_state[0]) break;
+        const int32_t L = s_state[1];
+        const int dir = s_state[2];
+        const int slot = L % 3, nslot = (L + 1) % 3, cslot = (L + 2) % 3;
+        const bool append = s_state[3] != 0;
+        const int32_t n_f = s_state[4];
+        const bool queue_ok = s_state[5] != 0;
+        // (selects, not an indexed array: an array would live in local memory)
+        uint32_t* f_cur = slot == 0 ? f0 : (slot == 1 ? f1 : f2);
+        uint32_t* f_next = nslot == 0 ? f0 : (nslot == 1 ? f1 : f2);
+        uint32_t* f_clear = cslot == 0 ? f0 : (cslot == 1 ? f1 : f2);
+        int32_t* q_cur = (L & 1) ? qb : qa;
+        int32_t* q_next = (L & 1) ? qa : qb;
+        const int32_t next_depth = L + 1;
+        PAcc acc;
+        // Level decision, run by the last block to reach the level's final
+        // barrier (all counters are settled then).
+        auto decide = [&]() {
+            volatile BfsRunState* vd = st;
+            const int32_t nf_next = vd->nf[nslot];
+            const unsigned long long mf_next = vd->mf[nslot];
+            const unsigned long long m_r_prev = vd->m_r;
+            const uint64_t now = global_timer_ns();
+            const uint64_t tp = vd->t_prev;
+            if (L < 64) {
+                st->lvl_dir[L] = (int8_t)dir;
+                st->lvl_ms[L] = (float)((double)(now - tp) * 1e-6);
+                st->lvl_nf[L] = nf_next;
+                st->lvl_mf[L] = mf_next;
+            }
+            st->t_prev = now;
+            st->m_r = m_r_prev + mf_next;
+            st->reached = vd->reached + nf_next;
+            st->levels = L + 1;
+            if (dir == 1) st->pull_levels = vd->pull_levels + 1;
+            int nd = dir;
+            const bool can_pull = in_rp != nullptr;
+            if (policy == GHB_POLICY_PUSH || !can_pull) {
+                nd = 0;
+            } else if (policy == GHB_POLICY_PULL) {
+                nd = 1;
+            } else if (policy == GHB_POLICY_SCHEDULE) {
+                nd = (schedule && L + 1 < schedule_len) ? (schedule[L + 1] ? 1 : 0) : dir;
+            } else {
+                const double m_u = (double)(m_total - (long long)(m_r_prev + mf_next));
+                if (dir == 0 && (double)mf_next > m_u / alpha) nd = 1;
+                else if (dir == 1 && (double)nf_next < (double)n / beta) nd = 0;
+            }
+            st->dir = nd;
+            // Top-down levels append to the queue only for small frontiers;
+            // the next queue holds the next frontier only if this level was
+            // top-down and appended.
+            st->append = (nd == 0 && mf_next < (unsigned long long)kAppendMaxEdges) ? 1 : 0;
+            st->queue_ok = (dir == 0 && append) ? 1 : 0;
+            st->qcount = 0;
+            st->level = L + 1;
+            st->done = (nf_next == 0 || L + 1 >= max_depth) ? 1 : 0;
+            st->nf[cslot] = 0;
+            st->mf[cslot] = 0;
+            st->dmax[cslot] = 0;
+            st->big[cslot] = 0;
+        };
+
+        if (dir == 0) {
+            if (!queue_ok) {
+                // Queue from the frontier bitmap (after a bottom-up level).
+                for (int64_t w0 = warp * 32; w0 < words_active; w0 += nwarps * 32) {
+                    const int64_t w = w0 + lane;
+                    uint32_t bits = w < words_active ? f_cur[w] : 0u;
+                    const int32_t c = __popc(bits);
+                    int32_t incl = c;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += x;
+                    }
+                    const int32_t total = __shfl_sync(0xffffffffu, incl, 31);
+                    if (total == 0) continue;
+                    int32_t base = 0;
+                    if (lane == 0) base = atomicAdd(&st->qcount, total);
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    int32_t pos = base + incl - c;
+                    while (bits) {
+                        const int b = __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        q_cur[pos++] = (int32_t)(w * 32 + b);
+                    }
+                }
+                if (!p_barrier(st)) return;
+            }
+            // Short and medium rows; rows of >= kBigList entries deferred.
+            for (int64_t base = warp * 32; base < n_f; base += nwarps * 32) {
+                const int64_t i = base + lane;
+                int32_t b = 0, e = 0;
+                if (i < n_f) {
+                    const int32_t u = q_cur[i];
+                    b = out_rp[u];
+                    e = out_rp[u + 1];
+                    if (e - b >= kBigList) {
+                        big[warp_append_active(&st->big[slot])] = u;
+                        e = b;
+                    }
+                }
+                acc.ex += (unsigned long long)(e - b);
+                unsigned med = __ballot_sync(0xffffffffu, e - b >= 32);
+                while (med) {
+                    const int leader = __ffs(med) - 1;
+                    med &= med - 1;
+                    const int32_t lb = __shfl_sync(0xffffffffu, b, leader);
+                    const int32_t le = __shfl_sync(0xffffffffu, e, leader);
+                    for (int32_t j = lb + lane; j < le; j += 32)
+                        p_visit(out_col[j], visited, f_next, depth, next_depth, q_next, &st->nf[nslot], append,
+                                out_rp, acc);
+                }
+                if (e - b >= 32) e = b;
+                const int32_t d = e - b;
+                int32_t incl = d;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += x;
+                }
+                const int32_t excl = incl - d;
+                const int32_t total = __shfl_sync(0xffffffffu, incl, 31);
+                for (int32_t k0 = 0; k0 < total; k0 += 32) {
+                    const int32_t k = k0 + lane;
+                    int owner = 0;
+#pragma unroll
+                    for (int sft = 16; sft >= 1; sft >>= 1) {
+                        const int cand = owner + sft;
+                        const int32_t ev = __shfl_sync(0xffffffffu, excl, cand);
+                        if (ev <= k) owner = cand;
+                    }
+                    const int32_t ob = __shfl_sync(0xffffffffu, b, owner);
+                    const int32_t oe = __shfl_sync(0xffffffffu, excl, owner);
+                    if (k < total)
+                        p_visit(out_col[ob + (k - oe)], visited, f_next, depth, next_depth, q_next, &st->nf[nslot],
+                                append, out_rp, acc);
+                }
+            }
+            for (int64_t w = gtid; w < words; w += gsize) f_clear[w] = 0u;
+            p_flush(acc, st, nslot, !append);
+            acc = PAcc();
+            // Decide now unless long rows were deferred (then after them).
+            if (!p_barrier(st, [&]() {
+                    if (((volatile BfsRunState*)st)->big[slot] == 0) decide();
+                }))
+                return;
+            __shared__ int32_t s_nbig;
+            if (threadIdx.x == 0) s_nbig = vs->big[slot];
+            __syncthreads();
+            const int32_t nbig = s_nbig;
+            if (nbig > 0) {
+                // Deferred rows: one block per row (round robin), except rows
+                // of kHugeList or more, which every thread of the grid strides.
+                for (int32_t r = blockIdx.x; r < nbig; r += gridDim.x) {
+                    const int32_t u = big[r];
+                    const int32_t rb = out_rp[u], re = out_rp[u + 1];
+                    if (re - rb >= kHugeList) continue;
+                    for (int32_t j = rb + threadIdx.x; j < re; j += blockDim.x)
+                        p_visit(out_col[j], visited, f_next, depth, next_depth, q_next, &st->nf[nslot], append, out_rp,
+                                acc);
+                    if (threadIdx.x == 0) acc.ex += (unsigned long long)(re - rb);
+                }
+                for (int32_t r = 0; r < nbig; ++r) {
+                    const int32_t u = big[r];
+                    const int32_t rb = out_rp[u], re = out_rp[u + 1];
+                    if (re - rb < kHugeList) continue;
+                    for (int64_t j = rb + gtid; j < re; j += gsize)
+                        p_visit(out_col[j], visited, f_next, depth, next_depth, q_next, &st->nf[nslot], append, out_rp,
+                                acc);
+                    if (gtid == 0) acc.ex += (unsigned long long)(re - rb);
+                }
+                p_flush(acc, st, nslot, !append);
+                if (!p_barrier(st, decide)) return;
+            }
+        } else {
+            // Bottom-up over the active vertices: a warp owns a bitmap word.
+            for (int64_t w = warp; w < words_active; w += nwarps) {
+                const uint32_t vis = visited[w];
+                if (vis == 0xffffffffu) continue;
+                const int64_t v = w * 32 + lane;
+                const bool todo = v < n_active && !((vis >> lane) & 1u);
+                bool found = false;
+                int32_t j = 0, e = 0;
+                if (todo) {
+                    j = in_rp[v];
+                    e = in_rp[v + 1];
+                    const int32_t b = j;
+                    const int32_t lim = min(e, b + 32);
+                    while (j < lim && !found) {
+                        int32_t u[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) u[k] = (j + k < lim) ? in_col[j + k] : -1;
+                        bool h[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) h[k] = u[k] >= 0 && ((f_cur[u[k] >> 5] >> (u[k] & 31)) & 1u);
+                        const int hit = h[0] ? 0 : h[1] ? 1 : h[2] ? 2 : h[3] ? 3 : -1;
+                        if (hit >= 0) {
+                            found = true;
+                            j += hit + 1;
+                        } else {
+                            j = min(j + 4, lim);
+                        }
+                    }
+                    acc.ex += (unsigned long long)(j - b);
+                }
+                unsigned rest = __ballot_sync(0xffffffffu, todo && !found && j < e);
+                while (rest) {
+                    const int leader = __ffs(rest) - 1;
+                    const int32_t lj = __shfl_sync(0xffffffffu, j, leader);
+                    const int32_t le = __shfl_sync(0xffffffffu, e, leader);
+                    bool hit = false;
+                    int32_t scanned = 0;
+                    for (int32_t k0 = lj; k0 < le; k0 += 32) {
+                        const int32_t k = k0 + lane;
+                        bool h = false;
+                        if (k < le) {
+                            const int32_t u = in_col[k];
+                            h = (f_cur[u >> 5] >> (u & 31)) & 1u;
+                        }
+                        const unsigned hm = __ballot_sync(0xffffffffu, h);
+                        scanned += min(32, le - k0);
+                        if (hm) {
+                            hit = true;
+                            break;
+                        }
+                    }
+                    if (lane == leader) {
+                        found = hit;
+                        acc.ex += (unsigned long long)scanned;
+                    }
+                    rest &= rest - 1;
+                }
+                const unsigned fm = __ballot_sync(0xffffffffu, found);
+                if (fm) {
+                    if (lane == 0) {
+                        visited[w] = vis | fm;
+                        f_next[w] = fm;
+                    }
+                    if (found) {
+                        depth[v] = next_depth;
+                        const unsigned dv = (unsigned)(out_rp[v + 1] - out_rp[v]);
+                        acc.mf += dv;
+                        acc.dm = dv > acc.dm ? dv : acc.dm;
+                        acc.nf += 1;
+                    }
+                }
+            }
+            for (int64_t w = gtid; w < words; w += gsize) f_clear[w] = 0u;
+            p_flush(acc, st, nslot, true);
+            if (!p_barrier(st, decide)) return;
+        }
+
+    }
+
+    // ---- results in the caller's ids
+    if (perm) {
+        for (int64_t v = gtid; v < n; v += gsize) depth_out[v] = depth[perm[v]];
+    }
+}
+
+}  // namespace ghb
+
+namespace ghb {
+
+bool bfs_persistent_available(ghb_workspace* ws, int* blocks) {
+    static int cached[64] = {0};
+    static bool known[64] = {false};
+    const int dev = ws->device;
+    if (dev < 0 || dev >= 64) return false;
+    if (!known[dev]) {
+        int coop = 0, per_sm = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent_kernel, 512, 0) == cudaSuccess)
+            cached[dev] = std::min(per_sm, 2) * ws->num_sms;
+        known[dev] = true;
+    }
+    *blocks = cached[dev];
+    return cached[dev] > 0;
+}
+
+// One cooperative launch for the whole traversal.  depth: per-vertex output
+// in the graph's ids; with perm, depth_out[v] = depth[perm[v]] as well.
+int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_rp, const int32_t* out_col,
+                       const int32_t* in_rp, const int32_t* in_col, int32_t src, int32_t max_depth, int32_t* depth,
+                       const int32_t* perm, int32_t* depth_out, const ghb_bfs_options* opt,
+                       ghb_traversal_stats* stats) {
+    int blocks = 0;
+    if (!bfs_persistent_available(ws, &blocks)) {
+        set_error("cooperative launch unavailable");
+        return GHB_ERR_UNSUPPORTED;
+    }
+    cudaStream_t st = ws->stream;
+    const int64_t words = ((int64_t)n + 31) / 32;
+    Carver sizing(nullptr);
+    auto carve = [&](Carver& c, uint32_t** vis, uint32_t** f0, uint32_t** f1, uint32_t** f2, int32_t** qa,
+                     int32_t** qb, int32_t** big, BfsRunState** rs, int8_t** sched) {
+        *vis = c.take<uint32_t>(words);
+        *f0 = c.take<uint32_t>(words);
+        *f1 = c.take<uint32_t>(words);
+        *f2 = c.take<uint32_t>(words);
+        *qa = c.take<int32_t>(n);
+        *qb = c.take<int32_t>(n);
+        *big = c.take<int32_t>(n);
+        *rs = c.take<BfsRunState>(1);
+        *sched = c.take<int8_t>(4096);
+    };
+    uint32_t *vis, *f0, *f1, *f2;
+    int32_t *qa, *qb, *big;
+    BfsRunState* rs;
+    int8_t* sched;
+    carve(sizing, &vis, &f0, &f1, &f2, &qa, &qb, &big, &rs, &sched);
+    GHB_TRY(ws_reserve(ws, sizing.off));
+    Carver c(ws->scratch);
+    carve(c, &vis, &f0, &f1, &f2, &qa, &qb, &big, &rs, &sched);
+
+    int policy = opt ? opt->policy : GHB_POLICY_HEURISTIC;
+    float alpha = (opt && opt->alpha > 0) ? opt->alpha : 256.0f;
+    float beta = (opt && opt->beta > 0) ? opt->beta : 24.0f;
+    int32_t sched_len = 0;
+    if (policy == GHB_POLICY_SCHEDULE && opt && opt->schedule && opt->schedule_len > 0) {
+        sched_len = std::min<int32_t>(opt->schedule_len, 4096);
+        GHB_CUDA_TRY(cudaMemcpyAsync(sched, opt->schedule, sched_len, cudaMemcpyHostToDevice, st));
+    }
+    int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
+    GHB_CUDA_TRY(cudaMemcpyAsync(hp, out_rp + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaMemcpyAsync(hp + 1, out_rp + src, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaMemsetAsync(rs, 0, sizeof(BfsRunState), st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    const int64_t m_total = hp[0];
+    const int64_t deg_src = (int64_t)hp[2] - hp[1];
+    if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
+    GHB_TRY(launch_coop(ws, bfs_persistent_kernel, dim3(blocks), dim3(512), 0, n, n_active, out_rp, out_col, in_rp,
+                        in_col, src, max_depth, depth, vis, f0, f1, f2, qa, qb, big, policy, alpha, beta, m_total,
+                        (const int8_t*)(sched_len ? sched : nullptr), sched_len, perm, depth_out, rs));
+    if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
+    GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, rs, sizeof(BfsRunState), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    const BfsRunState* h = reinterpret_cast<const BfsRunState*>(ws->host_pinned);
+    if (h->status != kDevOk) {
+        set_error("BFS: grid barrier timed out");
+        return GHB_ERR_TIMEOUT;
+    }
+    if (opt && opt->record_trace && opt->trace) {
+        // Coarse per-level record of the persistent run: frontier size and
+        // out-entries produced by the level, direction, level time.
+        for (int l = 0; l < std::min<int>(std::min(h->levels, 64), opt->trace_cap); ++l) {
+            float* row = opt->trace + (size_t)l * GHB_TRACE_COLS;
+            for (int k = 0; k < GHB_TRACE_COLS; ++k) row[k] = -1.f;
+            row[12] = (float)h->lvl_dir[l];
+            row[13] = h->lvl_ms[l];
+            row[17] = (float)h->lvl_nf[l];
+            row[16] = (float)h->lvl_mf[l];
+        }
+    }
+    if (stats) {
+        float ms = 0.f;
+        GHB_CUDA_TRY(cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop));
+        stats->levels = h->levels;
+        stats->pull_levels = h->pull_levels;
+        stats->reached = 1 + h->reached;
+        stats->edges_reached = deg_src + (int64_t)h->m_r;
+        stats->edges_examined = (int64_t)h->examined;
+        stats->device_ms = ms;
+    }
+    return GHB_OK;
+}
+
+}  // namespace ghb

@@ -227,6 +227,56 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, int
     return s_ok != 0;
 }
 
+// Grid barrier with leader work, for cooperatively launched kernels.
+// *count (arrivals) and *release (epochs) must sit on different cache lines
+// and start at zero.  A block's thread 0 adds one arrival; the last block to
+// arrive runs leader() (every other block is waiting and has published its
+// writes), then publishes the epoch on *release, for which the others wait.
+// Bounded like grid_barrier: a wait that exceeds limit_ns raises *status and
+// returns false, and the caller must leave the kernel.
+struct NoLeader {
+    __device__ void operator()() const {}
+};
+
+template <class Leader>
+__device__ __forceinline__ bool grid_sync_leader(unsigned* count, unsigned* release, int32_t* status,
+                                                 const Leader& leader, uint64_t limit_ns = 2000000000ull) {
+    __shared__ int s_ok2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+        __threadfence();
+        const unsigned old = atomicAdd(count, 1u);
+        const unsigned epoch = old / nblocks + 1u;
+        if (old % nblocks == nblocks - 1u) {
+            __threadfence();
+            leader();
+            __threadfence();
+            atomicExch(release, epoch);
+        } else {
+            unsigned spins = 0;
+            uint64_t t0 = 0;
+            while ((int)(ld_acquire_u32(release) - epoch) < 0) {
+                if ((++spins & 127u) == 0) {
+                    if (*(volatile int32_t*)status != 0) { ok = 0; break; }
+                    const uint64_t t = global_timer_ns();
+                    if (t0 == 0) t0 = t;
+                    else if (t - t0 > limit_ns) {
+                        atomicExch(status, (int32_t)kDevBarrierTimeout);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        __threadfence();
+        s_ok2 = ok;
+    }
+    __syncthreads();
+    return s_ok2 != 0;
+}
+
 template <class T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

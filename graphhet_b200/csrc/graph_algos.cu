@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "bfs_kernels.cuh"
 #include "graph.cuh"
 
 namespace ghb {
@@ -112,6 +113,9 @@ int ghb_graph_bfs(ghb_workspace* ws, const ghb_graph* g, int32_t src, int32_t ma
     GHB_REQUIRE(src >= 0 && src < g->n, "source outside [0, n)");
     GHB_TRY(ws_reserve_stage(ws, sizeof(int32_t) * (size_t)g->n));
     int32_t* dnew = static_cast<int32_t*>(ws->stage);
+    if (bfs_use_persistent(ws, options))
+        return bfs_persistent_run(ws, g->n, g->n_active, g->rowptr, g->col, g->in_rowptr, g->in_col,
+                                  g->perm_host[src], max_depth, dnew, g->perm, depth, options, stats);
     GHB_TRY(bfs_run(ws, g->n, g->n_active, g->rowptr, g->col, g->in_rowptr, g->in_col, g->perm_host[src], max_depth,
                     dnew, options, stats));
     return map_back_i32(ws, g, dnew, depth);
