@@ -399,6 +399,33 @@ def extras(args, G, g, rg, srcs, ws):
     ex["msbfs64_gteps"] = round(mr_sum / (ms / 1e3) / 1e9, 3)
     del out
     torch.cuda.empty_cache()
+    # Learned schedule policy (trained on the 400-graph family; this graph is
+    # held out): GTEPS over the same sources, and regret of each policy
+    # against the replayed per-level oracle schedule.
+    from graphhet_b200 import policy as P
+    if os.path.exists(P.WEIGHTS_PATH):
+        P.install()
+
+        def bfs_sum(**kw):
+            t = 0.0
+            for s in srcs:
+                t += rg.bfs(s, out=lab, **kw)[1]["device_ms"]
+            return t
+        bfs_sum(policy=G.POLICY_LEARNED)
+        t_h, t_l = bfs_sum(policy=G.POLICY_HEURISTIC), bfs_sum(policy=G.POLICY_LEARNED)
+        ex["learned_bfs_gteps"] = round(mr_sum / (t_l / 1e3) / 1e9, 3)
+        ex["heuristic_bfs_gteps_same_run"] = round(mr_sum / (t_h / 1e3) / 1e9, 3)
+        r = P.regret(rg, srcs[:8])
+        ex["regret_rmat"] = {k: (round(v, 4) if isinstance(v, float) else {a: round(b, 3) for a, b in v.items()})
+                             for k, v in r.items()}
+        t_rule = t_net = 0.0
+        for s in srcs[:4]:
+            t_rule += rg.sssp(s, out=dist)[1]["device_ms"]
+            t_net += rg.sssp(s, out=dist, policy=G.POLICY_LEARNED)[1]["device_ms"]
+        ex["sssp_learned_ms_per_source"] = round(t_net / 4, 3)
+        ex["sssp_rule_ms_per_source"] = round(t_rule / 4, 3)
+        ex["learned_vs_plain"] = round(t_h / t_l, 3)
+        ex["batched_vs_plain"] = round((mr_sum / (ms / 1e3)) / (mr_sum / (t_h / 1e3)), 3)
     # 4096 x 4096 grid: BFS and SSSP from its centre
     gg = G.ResidentGraph(G.grid_graph(4096, 4096, weight_seed=args.seed))
     c = 2048 * 4096 + 2048
@@ -412,6 +439,14 @@ def extras(args, G, g, rg, srcs, ws):
     ms, (_, st) = timed(lambda: gg.sssp(c, out=dgs))
     ex["grid_sssp_ms"] = round(ms, 2)
     ex["grid_sssp_gteps"] = round(st["edges_reached"] / (ms / 1e3) / 1e9, 3)
+    if G.policy_loaded():
+        ms, _ = timed(lambda: gg.bfs(c, out=dg, policy=G.POLICY_LEARNED))
+        ex["grid_learned_bfs_ms"] = round(ms, 2)
+        ms, _ = timed(lambda: gg.sssp(c, out=dgs, policy=G.POLICY_LEARNED))
+        ex["grid_learned_sssp_ms"] = round(ms, 2)
+        r = P.regret(gg, [c], repeats=1)
+        ex["regret_grid"] = {k: (round(v, 4) if isinstance(v, float) else {a: round(b, 3) for a, b in v.items()})
+                             for k, v in r.items()}
     return ex
 
 

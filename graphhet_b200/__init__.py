@@ -30,7 +30,8 @@ POLICY_HEURISTIC, POLICY_LEARNED, POLICY_PUSH, POLICY_PULL, POLICY_SCHEDULE = 0,
 PR_FP64, PR_FP32_KAHAN = 0, 1
 BUILD_SYMMETRIZE, BUILD_DROP_SELF_LOOPS, BUILD_TRANSPOSE = 1, 2, 4
 WEIGHT_NONE, WEIGHT_UNIFORM01, WEIGHT_INT100 = 0, 1, 2
-TRACE_FEATURES, TRACE_COLS = 12, 20
+TRACE_FEATURES, TRACE_COLS = 12, 24
+POLICY_PARAMS, POLICY_OUT = 6292, 20
 
 _p = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -78,6 +79,7 @@ _SIGS = {
     "ghb_gen_rmat": (ctypes.c_int, [_p, _i32, _i64, _u64, _f64, _f64, _f64, _i32, _p, _p]),
     "ghb_gen_grid": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
     "ghb_gen_er": (ctypes.c_int, [_p, _i32, _i64, _u64, _p, _p]),
+    "ghb_gen_powerlaw": (ctypes.c_int, [_p, _i32, _i64, _f64, _u64, _p, _p]),
     "ghb_csr_build": (ctypes.c_int, [_p, _i32, _p, _p, _p, _i64, _i32, _i32, _u64, _p, _p, _p,
                                      ctypes.POINTER(_i64)]),
     "ghb_csr_transpose": (ctypes.c_int, [_p, _i32, _i64, _p, _p, _p, _p, _p, _p]),
@@ -108,6 +110,11 @@ _SIGS = {
     "ghb_graph_pagerank": (ctypes.c_int, [_p, _p, _p, _p, _p]),
     "ghb_graph_cdlp": (ctypes.c_int, [_p, _p, _i32, _p]),
     "ghb_graph_tc": (ctypes.c_int, [_p, _p, _p, _p, _p]),
+    "ghb_policy_load": (ctypes.c_int, [_p, _p]),
+    "ghb_policy_loaded": (ctypes.c_int, []),
+    "ghb_mlp_forward": (ctypes.c_int, [_p, _p, _p, _p, _i32, _p]),
+    "ghb_mlp_grad": (ctypes.c_int, [_p, _p, _p, _p, _p, _i32, _p, ctypes.POINTER(ctypes.c_float)]),
+    "ghb_mlp_train": (ctypes.c_int, [_p, _p, _p, _p, _p, _i32, _i32, ctypes.c_float, _p]),
 }
 
 _lib = None
@@ -268,6 +275,15 @@ def gen_er(n: int, n_edges: int, seed: int, device=None, ws=None):
     dst = torch.empty(max(1, n_edges), dtype=torch.int32, device=d)
     _check(lib().ghb_gen_er(_ws(ws), n, n_edges, seed, _ptr(src), _ptr(dst)), "ghb_gen_er")
     return src[:n_edges], dst[:n_edges]
+
+
+def gen_powerlaw(scale: int, n_edges: int, exponent: float, seed: int, device=None, ws=None):
+    dev = _dev(device)
+    src = torch.empty(n_edges, dtype=torch.int32, device=dev)
+    dst = torch.empty(n_edges, dtype=torch.int32, device=dev)
+    _check(lib().ghb_gen_powerlaw(_ws(ws), scale, n_edges, exponent, seed, _ptr(src), _ptr(dst)),
+           "ghb_gen_powerlaw")
+    return src, dst
 
 
 def build_csr(n: int, src: torch.Tensor, dst: torch.Tensor, w: Optional[torch.Tensor] = None,
@@ -482,9 +498,9 @@ class ResidentGraph:
         return torch.empty(self.n * k, dtype=torch.int32, device=self._dev)
 
     def bfs(self, src, max_depth=INT32_MAX, policy=POLICY_HEURISTIC, schedule=None, trace_cap=0,
-            oracle_timing=False, out=None, ws=None):
+            oracle_timing=False, alpha=0.0, beta=0.0, out=None, ws=None):
         depth = out if out is not None else self._i32()
-        opt = BfsOptions(policy=policy)
+        opt = BfsOptions(policy=policy, alpha=alpha, beta=beta)
         keep = None
         if schedule is not None:
             keep = (ctypes.c_int8 * len(schedule))(*[int(x) for x in schedule])
@@ -519,12 +535,21 @@ class ResidentGraph:
                "ghb_graph_msbfs")
         return depth.view(len(sd), self.n), st.as_dict()
 
-    def sssp(self, src, inf=DBL_MAX, delta=0.0, out=None, ws=None):
+    def sssp(self, src, inf=DBL_MAX, delta=0.0, policy=POLICY_HEURISTIC, trace=False, out=None, ws=None):
+        """Distances and stats; with trace=True also the width-choice row
+        (features, width used, rule's width, chosen by the network)."""
         dist = out if out is not None else torch.empty(self.n, dtype=torch.float64, device=self._dev)
-        opt = SsspOptions(delta=delta)
+        opt = SsspOptions(delta=delta, policy=policy)
+        row = None
+        if trace:
+            row = (ctypes.c_float * TRACE_COLS)()
+            opt.record_trace, opt.trace, opt.trace_cap = 1, ctypes.cast(row, _p), 1
         st = TraversalStats()
         _check(lib().ghb_graph_sssp(_ws(ws), self._h, src, inf, _ptr(dist), ctypes.byref(opt), ctypes.byref(st)),
                "ghb_graph_sssp")
+        if row is not None:
+            import numpy as np
+            return dist, st.as_dict(), np.frombuffer(row, dtype=np.float32).copy()
         return dist, st.as_dict()
 
     def sssp_pred(self, src, inf=DBL_MAX, ws=None):
@@ -562,3 +587,47 @@ class ResidentGraph:
         total = _i64()
         _check(lib().ghb_graph_tc(_ws(ws), self._h, _ptr(c64), _ptr(c32), ctypes.byref(total)), "ghb_graph_tc")
         return c64, c32, total.value
+
+
+# ------------------------------------------------------------ schedule policy
+def mlp_forward(params: torch.Tensor, norm: torch.Tensor, x: torch.Tensor, ws=None) -> torch.Tensor:
+    """logits[B][20] of the policy network (device tensors, float32)."""
+    logits = torch.empty(x.shape[0], POLICY_OUT, dtype=torch.float32, device=x.device)
+    _check(lib().ghb_mlp_forward(_ws(ws), _ptr(params), _ptr(norm), _ptr(x.contiguous()), x.shape[0], _ptr(logits)),
+           "ghb_mlp_forward")
+    return logits
+
+
+def mlp_grad(params: torch.Tensor, norm: torch.Tensor, x: torch.Tensor, y: torch.Tensor, ws=None):
+    """(gradient[6292], loss) of the summed per-head mean cross-entropy."""
+    grad = torch.empty(POLICY_PARAMS, dtype=torch.float32, device=x.device)
+    loss = ctypes.c_float()
+    _check(lib().ghb_mlp_grad(_ws(ws), _ptr(params), _ptr(norm), _ptr(x.contiguous()), _ptr(y.contiguous()),
+                              x.shape[0], _ptr(grad), ctypes.byref(loss)), "ghb_mlp_grad")
+    return grad, loss.value
+
+
+def mlp_train(params: torch.Tensor, norm: torch.Tensor, x: torch.Tensor, y: torch.Tensor, epochs: int,
+              lr: float = 3e-3, ws=None):
+    """Full-batch Adam on the device; updates params in place, returns the loss per epoch."""
+    hist = (ctypes.c_float * max(1, epochs))()
+    _check(lib().ghb_mlp_train(_ws(ws), _ptr(params), _ptr(norm), _ptr(x.contiguous()), _ptr(y.contiguous()),
+                               x.shape[0], epochs, lr, ctypes.cast(hist, _p)), "ghb_mlp_train")
+    return list(hist)[:epochs]
+
+
+def policy_load(params, norm) -> None:
+    """Install a network for POLICY_LEARNED (host or device float32 arrays);
+    policy_load(None, None) uninstalls it."""
+    if params is None and norm is None:
+        _check(lib().ghb_policy_load(None, None), "ghb_policy_load")
+        return
+    p = torch.as_tensor(params, dtype=torch.float32).cpu().contiguous()
+    q = torch.as_tensor(norm, dtype=torch.float32).cpu().contiguous()
+    if p.numel() != POLICY_PARAMS or q.numel() != 2 * TRACE_FEATURES:
+        raise ValueError("policy needs %d parameters and %d norm values" % (POLICY_PARAMS, 2 * TRACE_FEATURES))
+    _check(lib().ghb_policy_load(ctypes.c_void_p(p.data_ptr()), ctypes.c_void_p(q.data_ptr())), "ghb_policy_load")
+
+
+def policy_loaded() -> bool:
+    return bool(lib().ghb_policy_loaded())

@@ -19,9 +19,9 @@ namespace ghb {
 
 bool bfs_persistent_available(ghb_workspace* ws, int* blocks);
 
-// The whole traversal runs in one cooperative launch unless the caller asks
-// for per-level traces (training data) or the learned policy (host-side for
-// now), or the device cannot launch cooperatively.
+// The whole traversal runs in one cooperative launch (the learned policy's
+// network included) unless the caller asks for per-level push/pull timings
+// (oracle_timing), or the device cannot launch cooperatively.
 bool bfs_use_persistent(ghb_workspace* ws, const ghb_bfs_options* opt) {
     int blocks = 0;
     if (!bfs_persistent_available(ws, &blocks)) return false;
@@ -29,7 +29,7 @@ bool bfs_use_persistent(ghb_workspace* ws, const ghb_bfs_options* opt) {
     if (opt->oracle_timing) return false;
     if (opt->record_trace && opt->trace_cap < 0) return false;
     return opt->policy == GHB_POLICY_HEURISTIC || opt->policy == GHB_POLICY_PUSH || opt->policy == GHB_POLICY_PULL ||
-           opt->policy == GHB_POLICY_SCHEDULE;
+           opt->policy == GHB_POLICY_SCHEDULE || opt->policy == GHB_POLICY_LEARNED;
 }
 
 // n_active: vertices [n_active, n) have no entries at all (a relabelled
@@ -109,14 +109,19 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
     };
 
     while (n_f > 0 && level < max_depth) {
-        // ---- direction for this level
+        // ---- direction for this level; fmt_req: output of a top-down level
+        // (0 by frontier size, 1 queue, 2 bitmap only)
         const int64_t m_u = m_total - m_r;
+        int fmt_req = 0;
+        bool by_net = false;
         if (policy == GHB_POLICY_PUSH) {
             dir = 0;
         } else if (policy == GHB_POLICY_PULL) {
             dir = level == 0 ? 0 : 1;
         } else if (policy == GHB_POLICY_SCHEDULE) {
-            dir = (opt->schedule && level < opt->schedule_len) ? (opt->schedule[level] ? 1 : 0) : dir;
+            const bool has = opt->schedule && level < opt->schedule_len;
+            dir = has ? (opt->schedule[level] & 1) : dir;
+            fmt_req = has ? ((opt->schedule[level] >> 1) & 3) : 0;
         } else {
             int heur = dir;
             if (dir == 0 && (double)m_f > (double)m_u / alpha) heur = 1;
@@ -125,14 +130,18 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
             if (policy == GHB_POLICY_LEARNED) {
                 float feat[GHB_TRACE_FEATURES];
                 bfs_features(feat, n, m_total, n_f, m_f, m_u, level, deg2_f, degmax_f, prev_dir, prev_ms);
-                int d = policy_pick_direction(feat);
-                if (d >= 0) dir = d;
+                int d = 0, f = 0;
+                if (policy_pick_level(feat, &d, &f)) {
+                    dir = d;
+                    fmt_req = f ? 2 : 1;
+                    by_net = true;
+                }
             }
         }
         float row[GHB_TRACE_COLS];
         if (opt->record_trace && level < opt->trace_cap) {
             bfs_features(row, n, m_total, n_f, m_f, m_u, level, deg2_f, degmax_f, prev_dir, prev_ms);
-            row[13] = row[14] = row[15] = -1.f;
+            for (int k = GHB_TRACE_FEATURES; k < GHB_TRACE_COLS; ++k) row[k] = -1.f;
         }
 
         float t_push = -1.f, t_pull = -1.f;
@@ -188,8 +197,8 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
         GHB_CUDA_TRY(cudaMemsetAsync(B.counters, 0, sizeof(BfsCounters), st));
         GHB_CUDA_TRY(cudaMemsetAsync(f_next, 0, words * sizeof(uint32_t), st));
         if (opt->record_trace) GHB_CUDA_TRY(cudaEventRecord(ws->ev_a, st));
+        const bool append = fmt_req == 1 || (fmt_req == 0 && m_f < kAppendMaxEdges);
         if (dir == 0) {
-            const bool append = m_f < kAppendMaxEdges;
             GHB_TRY(bfs_push_level(ws, B, n, out_rowptr, out_col, q_cur, n_f, level + 1, depth,
                                    append ? q_next : (int32_t*)nullptr, f_next));
             if (!append)
@@ -224,6 +233,8 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
             // examined and write 4 B of depth per vertex reached.
             row[19] = (float)(4.0 * (dir ? unvisited : (double)n_f) + 4.0 * (double)hc->examined +
                               4.0 * (double)hc->tail);
+            row[20] = dir == 0 ? (append ? 0.f : 1.f) : -1.f;
+            row[22] = by_net ? 1.f : 0.f;
             for (int k = 0; k < GHB_TRACE_COLS; ++k) opt->trace[(size_t)level * GHB_TRACE_COLS + k] = row[k];
         }
         prev_dir = dir;

@@ -24,6 +24,7 @@
 
 #include "bfs_kernels.cuh"
 #include "common.cuh"
+#include "policy.cuh"
 
 namespace ghb {
 
@@ -41,55 +42,58 @@ struct BfsRunState {
     int32_t nf[3];       // frontier sizes by slot
     int32_t big[3];      // deferred long rows by slot
     unsigned dmax[3];
-    unsigned pad;
+    int32_t by_net;      // the network chose the current level's direction
     unsigned long long mf[3];
+    unsigned long long d2[3];        // sum of squared out-degrees by slot
     unsigned long long examined;
-    unsigned long long m_r;
-    long long reached;
+    unsigned long long ex_prev;      // examined at the previous decision
+    unsigned long long m_r;          // entries out of reached vertices (source included)
+    long long reached;               // vertices reached (source excluded)
     int32_t pull_levels;
     int32_t levels;
     int32_t qcount;      // queue compaction cursor (zero at every level start)
     int32_t pad2;
     unsigned long long t_prev;       // global timer at the previous decision
-    int8_t lvl_dir[64];              // per-level record (first 64 levels)
-    float lvl_ms[64];
-    int32_t lvl_nf[64];
-    unsigned long long lvl_mf[64];
+    unsigned long long t_comp;       // global timer after this level's compaction
 };
 
 namespace {
 
 struct PAcc {
-    unsigned long long mf = 0, ex = 0;
+    unsigned long long mf = 0, ex = 0, d2 = 0;
     unsigned int dm = 0, nf = 0;
 };
 
 // Block totals, one atomic per counter per block.  Contains __syncthreads.
 __device__ __forceinline__ void p_flush(PAcc a, BfsRunState* st, int slot, bool count_nf) {
-    __shared__ unsigned long long s_mf[32], s_ex[32];
+    __shared__ unsigned long long s_mf[32], s_ex[32], s_d2[32];
     __shared__ unsigned s_dm[32], s_nf[32];
     a.mf = warp_sum(a.mf);
     a.ex = warp_sum(a.ex);
+    a.d2 = warp_sum(a.d2);
     a.nf = warp_sum(a.nf);
     a.dm = warp_max(a.dm);
     if (lane_id() == 0) {
         s_mf[threadIdx.x >> 5] = a.mf;
         s_ex[threadIdx.x >> 5] = a.ex;
+        s_d2[threadIdx.x >> 5] = a.d2;
         s_dm[threadIdx.x >> 5] = a.dm;
         s_nf[threadIdx.x >> 5] = a.nf;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned long long mf = 0, ex = 0;
+        unsigned long long mf = 0, ex = 0, d2 = 0;
         unsigned dm = 0, nf = 0;
         for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
             mf += s_mf[i];
             ex += s_ex[i];
+            d2 += s_d2[i];
             nf += s_nf[i];
             dm = s_dm[i] > dm ? s_dm[i] : dm;
         }
         if (mf) atomicAdd(&st->mf[slot], mf);
         if (ex) atomicAdd(&st->examined, ex);
+        if (d2) atomicAdd(&st->d2[slot], d2);
         if (dm) atomicMax(&st->dmax[slot], dm);
         if (count_nf && nf) atomicAdd(&st->nf[slot], (int32_t)nf);
     }
@@ -110,6 +114,7 @@ __device__ __forceinline__ void p_visit(int32_t v, uint32_t* visited, uint32_t* 
     else acc.nf += 1;
     const unsigned dv = (unsigned)(rowptr[v + 1] - rowptr[v]);
     acc.mf += dv;
+    acc.d2 += (unsigned long long)dv * dv;
     acc.dm = dv > acc.dm ? dv : acc.dm;
 }
 
@@ -120,6 +125,17 @@ template <class F>
 __device__ __forceinline__ bool p_barrier(BfsRunState* st, const F& leader) {
     return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, leader);
 }
+// Barrier whose decision runs on every thread of the last block to arrive.
+template <class F>
+__device__ __forceinline__ bool p_barrier_block(BfsRunState* st, const F& leader) {
+    return grid_sync_block_leader(&st->bar_count, &st->bar_release, &st->status, leader);
+}
+
+// Output format of a top-down level: fmt 1 queue, 2 bitmap only, 0 by the
+// frontier's out-entries.
+__device__ __forceinline__ int32_t p_append(int nd, int fmt, unsigned long long mf) {
+    return (nd == 0 && (fmt == 1 || (fmt == 0 && mf < (unsigned long long)kAppendMaxEdges))) ? 1 : 0;
+}
 
 }  // namespace
 
@@ -128,7 +144,8 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
     const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col, int32_t src, int32_t max_depth,
     int32_t* depth, uint32_t* visited, uint32_t* f0, uint32_t* f1, uint32_t* f2, int32_t* qa, int32_t* qb,
     int32_t* big, int policy, float alpha, float beta, int64_t m_total, const int8_t* __restrict__ schedule,
-    int32_t schedule_len, const int32_t* __restrict__ perm, int32_t* depth_out, BfsRunState* st) {
+    int32_t schedule_len, const int32_t* __restrict__ perm, int32_t* depth_out, BfsRunState* st,
+    const float* __restrict__ pol, float* trace, int32_t trace_cap) {
     const int lane = lane_id();
     const int64_t gtid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t gsize = (int64_t)gridDim.x * blockDim.x;
@@ -146,20 +163,41 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
         f1[w] = 0u;
         f2[w] = 0u;
     }
+    // The network (parameters + normalisation) in shared memory, when the
+    // learned policy is on: every block may be the one that decides.
+    extern __shared__ float s_pol[];
+    const bool net = pol != nullptr;
+    if (net)
+        for (int i = threadIdx.x; i < kPolTotal; i += blockDim.x) s_pol[i] = pol[i];
+    const bool can_pull = in_rp != nullptr;
     if (gtid == 0) {
         qa[0] = src;
         const unsigned ds = (unsigned)(out_rp[src + 1] - out_rp[src]);
         st->nf[0] = 1;
         st->mf[0] = ds;
+        st->d2[0] = (unsigned long long)ds * ds;
         st->dmax[0] = ds;
-        st->append = ds < (unsigned)kAppendMaxEdges ? 1 : 0;
+        st->m_r = ds;
+        int d0 = 0, f0req = 0;
+        if (policy == GHB_POLICY_SCHEDULE && schedule && schedule_len > 0) {
+            d0 = can_pull ? (schedule[0] & 1) : 0;
+            f0req = (schedule[0] >> 1) & 3;
+        }
+        st->append = p_append(d0, f0req, ds);
         st->queue_ok = 1;
         st->level = 0;
-        st->dir = (policy == GHB_POLICY_SCHEDULE && in_rp && schedule && schedule_len > 0 && schedule[0]) ? 1 : 0;
+        st->dir = d0;
         st->done = max_depth <= 0 ? 1 : 0;
         st->t_prev = global_timer_ns();
+        if (trace && trace_cap > 0)
+            bfs_features(trace, (double)n, (double)m_total, 1.0, (double)ds, (double)(m_total - (int64_t)ds), 0,
+                         (double)ds * ds, (double)ds, 0, 0.f);
     }
     if (!p_barrier(st)) return;
+
+    __shared__ float s_feat[kPolIn], s_h1[kPolH], s_h2[kPolH], s_logit[kPolOut];
+    __shared__ int32_t s_dec[2];
+    __shared__ int32_t s_flag;
 
     __shared__ int32_t s_state[6];
     volatile BfsRunState* vs = st;
@@ -192,52 +230,93 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
         int32_t* q_next = (L & 1) ? qa : qb;
         const int32_t next_depth = L + 1;
         PAcc acc;
-        // Level decision, run by the last block to reach the level's final
-        // barrier (all counters are settled then).
+        // Level decision, run by every thread of the last block to reach the
+        // level's final barrier (all counters are settled then).  Thread 0
+        // does the bookkeeping and the fixed rules; the block evaluates the
+        // network when the learned policy is on.
         auto decide = [&]() {
-            volatile BfsRunState* vd = st;
-            const int32_t nf_next = vd->nf[nslot];
-            const unsigned long long mf_next = vd->mf[nslot];
-            const unsigned long long m_r_prev = vd->m_r;
-            const uint64_t now = global_timer_ns();
-            const uint64_t tp = vd->t_prev;
-            if (L < 64) {
-                st->lvl_dir[L] = (int8_t)dir;
-                st->lvl_ms[L] = (float)((double)(now - tp) * 1e-6);
-                st->lvl_nf[L] = nf_next;
-                st->lvl_mf[L] = mf_next;
-            }
-            st->t_prev = now;
-            st->m_r = m_r_prev + mf_next;
-            st->reached = vd->reached + nf_next;
-            st->levels = L + 1;
-            if (dir == 1) st->pull_levels = vd->pull_levels + 1;
-            int nd = dir;
-            const bool can_pull = in_rp != nullptr;
-            if (policy == GHB_POLICY_PUSH || !can_pull) {
-                nd = 0;
-            } else if (policy == GHB_POLICY_PULL) {
-                nd = 1;
-            } else if (policy == GHB_POLICY_SCHEDULE) {
-                nd = (schedule && L + 1 < schedule_len) ? (schedule[L + 1] ? 1 : 0) : dir;
-            } else {
+            int32_t nf_next = 0;
+            unsigned long long mf_next = 0;
+            if (threadIdx.x == 0) {
+                volatile BfsRunState* vd = st;
+                nf_next = vd->nf[nslot];
+                mf_next = vd->mf[nslot];
+                const unsigned long long m_r_prev = vd->m_r;
+                const unsigned long long ex_now = vd->examined;
+                const long long reached_prev = vd->reached;
+                const uint64_t now = global_timer_ns();
+                const uint64_t tp = vd->t_prev;
+                const float ms = (float)((double)(now - tp) * 1e-6);
+                if (trace && L < trace_cap) {
+                    float* row = trace + (size_t)L * GHB_TRACE_COLS;
+                    const double unvisited = (double)n - 1.0 - (double)reached_prev;
+                    const double ex = (double)(ex_now - vd->ex_prev);
+                    row[12] = (float)dir;
+                    row[13] = ms;
+                    row[14] = -1.f;
+                    row[15] = -1.f;
+                    row[16] = (float)ex;
+                    row[17] = (float)nf_next;
+                    row[18] = (float)unvisited;
+                    row[19] = (float)(4.0 * (dir ? unvisited : (double)n_f) + 4.0 * ex + 4.0 * (double)nf_next);
+                    row[20] = dir == 0 ? (append ? 0.f : 1.f) : -1.f;
+                    row[21] = (dir == 0 && !queue_ok) ? (float)((double)(vd->t_comp - tp) * 1e-6) : -1.f;
+                    row[22] = (float)vd->by_net;
+                    row[23] = -1.f;
+                }
+                st->ex_prev = ex_now;
+                st->t_prev = now;
+                st->m_r = m_r_prev + mf_next;
+                st->reached = reached_prev + nf_next;
+                st->levels = L + 1;
+                if (dir == 1) st->pull_levels = vd->pull_levels + 1;
+                int nd = dir, fmt = 0;
                 const double m_u = (double)(m_total - (long long)(m_r_prev + mf_next));
-                if (dir == 0 && (double)mf_next > m_u / alpha) nd = 1;
-                else if (dir == 1 && (double)nf_next < (double)n / beta) nd = 0;
+                if (policy == GHB_POLICY_PUSH || !can_pull) {
+                    nd = 0;
+                } else if (policy == GHB_POLICY_PULL) {
+                    nd = 1;
+                } else if (policy == GHB_POLICY_SCHEDULE) {
+                    if (schedule && L + 1 < schedule_len) {
+                        nd = schedule[L + 1] & 1;
+                        fmt = (schedule[L + 1] >> 1) & 3;
+                    }
+                } else {
+                    if (dir == 0 && (double)mf_next > m_u / alpha) nd = 1;
+                    else if (dir == 1 && (double)nf_next < (double)n / beta) nd = 0;
+                }
+                bfs_features(s_feat, (double)n, (double)m_total, (double)nf_next, (double)mf_next, m_u, L + 1,
+                             (double)vd->d2[nslot], (double)vd->dmax[nslot], dir, ms);
+                if (trace && L + 1 < trace_cap)
+                    for (int k = 0; k < kPolIn; ++k) trace[(size_t)(L + 1) * GHB_TRACE_COLS + k] = s_feat[k];
+                s_dec[0] = nd;
+                s_dec[1] = fmt;
             }
-            st->dir = nd;
-            // Top-down levels append to the queue only for small frontiers;
-            // the next queue holds the next frontier only if this level was
-            // top-down and appended.
-            st->append = (nd == 0 && mf_next < (unsigned long long)kAppendMaxEdges) ? 1 : 0;
-            st->queue_ok = (dir == 0 && append) ? 1 : 0;
-            st->qcount = 0;
-            st->level = L + 1;
-            st->done = (nf_next == 0 || L + 1 >= max_depth) ? 1 : 0;
-            st->nf[cslot] = 0;
-            st->mf[cslot] = 0;
-            st->dmax[cslot] = 0;
-            st->big[cslot] = 0;
+            if (net) {
+                __syncthreads();
+                policy_eval_block(s_pol, s_feat, s_h1, s_h2, s_logit);
+            }
+            if (threadIdx.x == 0) {
+                int nd = s_dec[0], fmt = s_dec[1];
+                if (net) {
+                    nd = (can_pull && s_logit[kHeadDir + 1] > s_logit[kHeadDir]) ? 1 : 0;
+                    fmt = s_logit[kHeadFmt + 1] > s_logit[kHeadFmt] ? 2 : 1;
+                }
+                st->by_net = net ? 1 : 0;
+                st->dir = nd;
+                // The next queue holds the next frontier only if this level
+                // was top-down and appended.
+                st->append = p_append(nd, fmt, mf_next);
+                st->queue_ok = (dir == 0 && append) ? 1 : 0;
+                st->qcount = 0;
+                st->level = L + 1;
+                st->done = (nf_next == 0 || L + 1 >= max_depth) ? 1 : 0;
+                st->nf[cslot] = 0;
+                st->mf[cslot] = 0;
+                st->d2[cslot] = 0;
+                st->dmax[cslot] = 0;
+                st->big[cslot] = 0;
+            }
         };
 
         if (dir == 0) {
@@ -265,7 +344,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                         q_cur[pos++] = (int32_t)(w * 32 + b);
                     }
                 }
-                if (!p_barrier(st)) return;
+                if (!p_barrier(st, [&]() { st->t_comp = global_timer_ns(); })) return;
             }
             // Short and medium rows; rows of >= kBigList entries deferred.
             for (int64_t base = warp * 32; base < n_f; base += nwarps * 32) {
@@ -321,8 +400,10 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
             p_flush(acc, st, nslot, !append);
             acc = PAcc();
             // Decide now unless long rows were deferred (then after them).
-            if (!p_barrier(st, [&]() {
-                    if (((volatile BfsRunState*)st)->big[slot] == 0) decide();
+            if (!p_barrier_block(st, [&]() {
+                    if (threadIdx.x == 0) s_flag = ((volatile BfsRunState*)st)->big[slot] == 0 ? 1 : 0;
+                    __syncthreads();
+                    if (s_flag) decide();
                 }))
                 return;
             __shared__ int32_t s_nbig;
@@ -351,7 +432,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                     if (gtid == 0) acc.ex += (unsigned long long)(re - rb);
                 }
                 p_flush(acc, st, nslot, !append);
-                if (!p_barrier(st, decide)) return;
+                if (!p_barrier_block(st, decide)) return;
             }
         } else {
             // Bottom-up over the active vertices: a warp owns a bitmap word.
@@ -421,6 +502,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                         depth[v] = next_depth;
                         const unsigned dv = (unsigned)(out_rp[v + 1] - out_rp[v]);
                         acc.mf += dv;
+                        acc.d2 += (unsigned long long)dv * dv;
                         acc.dm = dv > acc.dm ? dv : acc.dm;
                         acc.nf += 1;
                     }
@@ -428,7 +510,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
             }
             for (int64_t w = gtid; w < words; w += gsize) f_clear[w] = 0u;
             p_flush(acc, st, nslot, true);
-            if (!p_barrier(st, decide)) return;
+            if (!p_barrier_block(st, decide)) return;
         }
 
     }
@@ -451,7 +533,9 @@ bool bfs_persistent_available(ghb_workspace* ws, int* blocks) {
     if (!known[dev]) {
         int coop = 0, per_sm = 0;
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent_kernel, 512, 0) == cudaSuccess)
+        // Sized with the network in shared memory, so both variants fit.
+        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent_kernel, 512,
+                                                                  sizeof(float) * kPolTotal) == cudaSuccess)
             cached[dev] = std::min(per_sm, 2) * ws->num_sms;
         known[dev] = true;
     }
@@ -473,8 +557,10 @@ int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int
     cudaStream_t st = ws->stream;
     const int64_t words = ((int64_t)n + 31) / 32;
     Carver sizing(nullptr);
+    const bool want_trace = opt && opt->record_trace && opt->trace && opt->trace_cap > 0;
+    const int32_t tcap = want_trace ? std::min<int32_t>(opt->trace_cap, 1 << 16) : 0;
     auto carve = [&](Carver& c, uint32_t** vis, uint32_t** f0, uint32_t** f1, uint32_t** f2, int32_t** qa,
-                     int32_t** qb, int32_t** big, BfsRunState** rs, int8_t** sched) {
+                     int32_t** qb, int32_t** big, BfsRunState** rs, int8_t** sched, float** tr) {
         *vis = c.take<uint32_t>(words);
         *f0 = c.take<uint32_t>(words);
         *f1 = c.take<uint32_t>(words);
@@ -484,15 +570,17 @@ int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int
         *big = c.take<int32_t>(n);
         *rs = c.take<BfsRunState>(1);
         *sched = c.take<int8_t>(4096);
+        *tr = c.take<float>((size_t)(tcap > 0 ? tcap : 1) * GHB_TRACE_COLS);
     };
     uint32_t *vis, *f0, *f1, *f2;
     int32_t *qa, *qb, *big;
     BfsRunState* rs;
     int8_t* sched;
-    carve(sizing, &vis, &f0, &f1, &f2, &qa, &qb, &big, &rs, &sched);
+    float* tr;
+    carve(sizing, &vis, &f0, &f1, &f2, &qa, &qb, &big, &rs, &sched, &tr);
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
-    carve(c, &vis, &f0, &f1, &f2, &qa, &qb, &big, &rs, &sched);
+    carve(c, &vis, &f0, &f1, &f2, &qa, &qb, &big, &rs, &sched, &tr);
 
     int policy = opt ? opt->policy : GHB_POLICY_HEURISTIC;
     float alpha = (opt && opt->alpha > 0) ? opt->alpha : 256.0f;
@@ -502,17 +590,23 @@ int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int
         sched_len = std::min<int32_t>(opt->schedule_len, 4096);
         GHB_CUDA_TRY(cudaMemcpyAsync(sched, opt->schedule, sched_len, cudaMemcpyHostToDevice, st));
     }
+    // The learned policy runs in the kernel when a network is installed;
+    // otherwise GHB_POLICY_LEARNED falls back to the heuristic.
+    const float* pol = nullptr;
+    if (policy == GHB_POLICY_LEARNED) {
+        pol = policy_device_params();
+        if (!pol) policy = GHB_POLICY_HEURISTIC;
+    }
     int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
     GHB_CUDA_TRY(cudaMemcpyAsync(hp, out_rp + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    GHB_CUDA_TRY(cudaMemcpyAsync(hp + 1, out_rp + src, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     GHB_CUDA_TRY(cudaMemsetAsync(rs, 0, sizeof(BfsRunState), st));
     GHB_CUDA_TRY(cudaStreamSynchronize(st));
     const int64_t m_total = hp[0];
-    const int64_t deg_src = (int64_t)hp[2] - hp[1];
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
-    GHB_TRY(launch_coop(ws, bfs_persistent_kernel, dim3(blocks), dim3(512), 0, n, n_active, out_rp, out_col, in_rp,
-                        in_col, src, max_depth, depth, vis, f0, f1, f2, qa, qb, big, policy, alpha, beta, m_total,
-                        (const int8_t*)(sched_len ? sched : nullptr), sched_len, perm, depth_out, rs));
+    GHB_TRY(launch_coop(ws, bfs_persistent_kernel, dim3(blocks), dim3(512), pol ? sizeof(float) * kPolTotal : 0, n,
+                        n_active, out_rp, out_col, in_rp, in_col, src, max_depth, depth, vis, f0, f1, f2, qa, qb, big,
+                        policy, alpha, beta, m_total, (const int8_t*)(sched_len ? sched : nullptr), sched_len, perm,
+                        depth_out, rs, pol, tcap > 0 ? tr : (float*)nullptr, tcap));
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
     GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, rs, sizeof(BfsRunState), cudaMemcpyDeviceToHost, st));
     GHB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -521,26 +615,27 @@ int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int
         set_error("BFS: grid barrier timed out");
         return GHB_ERR_TIMEOUT;
     }
-    if (opt && opt->record_trace && opt->trace) {
-        // Coarse per-level record of the persistent run: frontier size and
-        // out-entries produced by the level, direction, level time.
-        for (int l = 0; l < std::min<int>(std::min(h->levels, 64), opt->trace_cap); ++l) {
-            float* row = opt->trace + (size_t)l * GHB_TRACE_COLS;
-            for (int k = 0; k < GHB_TRACE_COLS; ++k) row[k] = -1.f;
-            row[12] = (float)h->lvl_dir[l];
-            row[13] = h->lvl_ms[l];
-            row[17] = (float)h->lvl_nf[l];
-            row[16] = (float)h->lvl_mf[l];
+    const int32_t levels = h->levels;
+    const int32_t pull_levels = h->pull_levels;
+    const int64_t reached = 1 + h->reached;
+    const int64_t m_r = (int64_t)h->m_r;
+    const int64_t examined = (int64_t)h->examined;
+    if (tcap > 0) {
+        const int32_t rows = std::min(levels, tcap);
+        if (rows > 0) {
+            GHB_CUDA_TRY(cudaMemcpyAsync(opt->trace, tr, sizeof(float) * rows * GHB_TRACE_COLS, cudaMemcpyDeviceToHost,
+                                         st));
+            GHB_CUDA_TRY(cudaStreamSynchronize(st));
         }
     }
     if (stats) {
         float ms = 0.f;
         GHB_CUDA_TRY(cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop));
-        stats->levels = h->levels;
-        stats->pull_levels = h->pull_levels;
-        stats->reached = 1 + h->reached;
-        stats->edges_reached = deg_src + (int64_t)h->m_r;
-        stats->edges_examined = (int64_t)h->examined;
+        stats->levels = levels;
+        stats->pull_levels = pull_levels;
+        stats->reached = reached;
+        stats->edges_reached = m_r;
+        stats->edges_examined = examined;
         stats->device_ms = ms;
     }
     return GHB_OK;

@@ -277,6 +277,54 @@ __device__ __forceinline__ bool grid_sync_leader(unsigned* count, unsigned* rele
     return s_ok2 != 0;
 }
 
+// As grid_sync_leader, but every thread of the last block to arrive runs
+// leader() (which may contain __syncthreads) before the release, so a
+// decision can use the whole block (the policy network's layers).
+template <class Leader>
+__device__ __forceinline__ bool grid_sync_block_leader(unsigned* count, unsigned* release, int32_t* status,
+                                                       const Leader& leader, uint64_t limit_ns = 2000000000ull) {
+    __shared__ int s_ok3, s_last3;
+    __shared__ unsigned s_epoch3;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+        __threadfence();
+        const unsigned old = atomicAdd(count, 1u);
+        s_epoch3 = old / nblocks + 1u;
+        s_last3 = (old % nblocks == nblocks - 1u) ? 1 : 0;
+        s_ok3 = 1;
+    }
+    __syncthreads();
+    if (s_last3) {
+        __threadfence();
+        leader();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicExch(release, s_epoch3);
+        }
+    } else if (threadIdx.x == 0) {
+        const unsigned epoch = s_epoch3;
+        unsigned spins = 0;
+        uint64_t t0 = 0;
+        while ((int)(ld_acquire_u32(release) - epoch) < 0) {
+            if ((++spins & 127u) == 0) {
+                if (*(volatile int32_t*)status != 0) { s_ok3 = 0; break; }
+                const uint64_t t = global_timer_ns();
+                if (t0 == 0) t0 = t;
+                else if (t - t0 > limit_ns) {
+                    atomicExch(status, (int32_t)kDevBarrierTimeout);
+                    s_ok3 = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return s_ok3 != 0;
+}
+
 template <class T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

@@ -56,6 +56,30 @@ __global__ void er_kernel(uint32_t n, int64_t n_edges, uint64_t stream, int32_t*
     }
 }
 
+// Chung-Lu power-law graph: both endpoints drawn with probability
+// proportional to (i+1)^-theta, theta = 1/(gamma-1), through the inverse of
+// the continuous cumulative weight, then scattered by the seed's permutation.
+__global__ void powerlaw_kernel(int scale, int64_t n_edges, double theta, uint64_t stream, ghb_perm perm,
+                                int32_t* __restrict__ src, int32_t* __restrict__ dst) {
+    const double n = (double)(1u << scale);
+    const double q = 1.0 - theta;
+    const double span = pow(n + 1.0, q) - 1.0;
+    const uint32_t last = (1u << scale) - 1u;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_edges;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t id[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const double u = (double)(ghb_draw(stream, 2 * (uint64_t)e + k) >> 11) * 0x1.0p-53;
+            const double x = pow(1.0 + u * span, 1.0 / q) - 1.0;
+            uint32_t i = x <= 0.0 ? 0u : (x >= (double)last ? last : (uint32_t)x);
+            id[k] = ghb_perm_apply(&perm, i);
+        }
+        src[e] = (int32_t)id[0];
+        dst[e] = (int32_t)id[1];
+    }
+}
+
 }  // namespace
 }  // namespace ghb
 
@@ -102,6 +126,20 @@ int ghb_gen_er(ghb_workspace* ws, int32_t n, int64_t n_edges, uint64_t seed, int
     unsigned g = grid_for(n_edges, 256, ws->num_sms * 16);
     return launch(ws, er_kernel, dim3(g), dim3(256), 0, (uint32_t)n, n_edges,
                   ghb_stream(seed, GHB_PURPOSE_ER), src, dst);
+}
+
+int ghb_gen_powerlaw(ghb_workspace* ws, int32_t scale, int64_t n_edges, double exponent, uint64_t seed,
+                     int32_t* src, int32_t* dst) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    GHB_REQUIRE(scale >= 1 && scale <= 30, "scale must be in [1, 30]");
+    GHB_REQUIRE(n_edges >= 0, "n_edges < 0");
+    GHB_REQUIRE(exponent > 2.0 && exponent < 10.0, "exponent must be in (2, 10)");
+    if (n_edges == 0) return GHB_OK;
+    GHB_REQUIRE(src && dst, "NULL output");
+    unsigned g = grid_for(n_edges, 256, ws->num_sms * 16);
+    return launch(ws, powerlaw_kernel, dim3(g), dim3(256), 0, (int)scale, n_edges, 1.0 / (exponent - 1.0),
+                  ghb_stream(seed, GHB_PURPOSE_POWERLAW), ghb_perm_make(seed, scale), src, dst);
 }
 
 }  // extern "C"

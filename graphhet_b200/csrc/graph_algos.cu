@@ -20,15 +20,16 @@ int sssp_pred_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
                   const double* dist, int32_t* pred);
 int sssp_delta_run(ghb_workspace* ws, ghb_graph* g, int32_t src, double inf, double delta, double* dist_out,
                    ghb_traversal_stats* stats);
-int sssp_pick_delta(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const double* w, double* delta);
+int sssp_choose_delta(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const double* w, int32_t src,
+                      const ghb_sssp_options* opt, double* delta);
 
 // Resident SSSP: delta-stepping with the light/heavy split when the rows fit
 // the weight-sorted copy's key (n <= 2^25), else the near/far form.
 static int graph_sssp_dispatch(ghb_workspace* ws, const ghb_graph* g, int32_t src_new, double inf, double* dnew,
                                const ghb_sssp_options* options, ghb_traversal_stats* stats) {
     if (g->m > 0 && g->n <= (1 << 25)) {
-        double delta = options ? options->delta : 0.0;
-        if (!(delta > 0)) GHB_TRY(sssp_pick_delta(ws, g->n, g->rowptr, g->w, &delta));
+        double delta = 0.0;
+        GHB_TRY(sssp_choose_delta(ws, g->n, g->rowptr, g->w, src_new, options, &delta));
         return sssp_delta_run(ws, const_cast<ghb_graph*>(g), src_new, inf, delta, dnew, stats);
     }
     return sssp_run(ws, g->n, g->rowptr, g->col, g->w, src_new, inf, dnew, options, stats);

@@ -1,5 +1,5 @@
-// Learned schedule policy: features of a traversal level and the decision
-// hooks used by the BFS / SSSP drivers.
+// Learned schedule policy: the features of a traversal level, the network's
+// parameter layout, and its block-wide evaluation inside a kernel.
 #pragma once
 
 #include <cmath>
@@ -7,6 +7,16 @@
 #include "common.cuh"
 
 namespace ghb {
+
+// Network 12 -> 64 -> 64 (ReLU) -> 20, row-major x @ W, then the
+// normalisation (mean[12], 1/std[12]) after the parameters.
+constexpr int kPolIn = 12, kPolH = 64, kPolOut = 20;
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kPolIn * kPolH, kOffW2 = kOffB1 + kPolH, kOffB2 = kOffW2 + kPolH * kPolH,
+              kOffW3 = kOffB2 + kPolH, kOffB3 = kOffW3 + kPolH * kPolOut, kPolParams = kOffB3 + kPolOut;
+constexpr int kOffNorm = kPolParams;            // mean[12], inv_std[12]
+constexpr int kPolTotal = kPolParams + 2 * kPolIn;  // floats on the device
+// Heads: [0,2) direction, [2,4) top-down output format, [4,20) SSSP width bin.
+constexpr int kHeadDir = 0, kHeadFmt = 2, kHeadDelta = 4, kDeltaBins = 16, kDeltaBinZero = 6;
 
 // The 12 policy features of one BFS level (also the first 12 trace columns):
 //  0 log2(1+n_f)      frontier vertices
@@ -21,32 +31,105 @@ namespace ghb {
 //  9 previous direction (0 push, 1 pull)
 // 10 log2(1+1000*previous level ms)
 // 11 log2(1+n_f) - log2(n)
-inline void bfs_features(float* f, int64_t n, int64_t m, int64_t n_f, int64_t m_f, int64_t m_u,
-                         int level, double deg2, double degmax, int prev_dir, float prev_ms) {
-    const double nf = (double)n_f > 0 ? (double)n_f : 0.0;
-    const double mean = nf > 0 ? (double)m_f / nf : 0.0;
+// One definition for the host-driven loop and the persistent kernel.
+__host__ __device__ inline void bfs_features(float* f, double n, double m, double n_f, double m_f, double m_u,
+                                             int level, double deg2, double degmax, int prev_dir, float prev_ms) {
+    const double nf = n_f > 0 ? n_f : 0.0;
+    const double mean = nf > 0 ? m_f / nf : 0.0;
     double var = nf > 0 ? deg2 / nf - mean * mean : 0.0;
     if (var < 0) var = 0;
-    f[0] = (float)std::log2(1.0 + nf);
-    f[1] = (float)std::log2(1.0 + (double)m_f);
-    f[2] = (float)std::log2(1.0 + (double)(m_u > 0 ? m_u : 0));
+    f[0] = log2f((float)(1.0 + nf));
+    f[1] = log2f((float)(1.0 + m_f));
+    f[2] = log2f((float)(1.0 + (m_u > 0 ? m_u : 0.0)));
     f[3] = (float)level;
-    f[4] = (float)std::log2(1.0 + mean);
-    f[5] = (float)std::log2(1.0 + var);
-    f[6] = (float)std::log2(1.0 + degmax);
-    f[7] = (float)std::log2((double)(n > 0 ? n : 1));
-    f[8] = (float)std::log2(1.0 + (double)m);
+    f[4] = log2f((float)(1.0 + mean));
+    f[5] = log2f((float)(1.0 + var));
+    f[6] = log2f((float)(1.0 + degmax));
+    f[7] = log2f((float)(n > 0 ? n : 1.0));
+    f[8] = log2f((float)(1.0 + m));
     f[9] = (float)prev_dir;
-    f[10] = (float)std::log2(1.0 + 1000.0 * (double)prev_ms);
+    f[10] = log2f(1.0f + 1000.0f * prev_ms);
     f[11] = f[0] - f[7];
 }
 
-// Direction from the loaded policy network (0 push, 1 pull), or -1 when no
-// network is loaded (the caller keeps the heuristic's choice).
-int policy_pick_direction(const float* features);
+// The features of one SSSP call (one width decision per traversal); level is
+// -1 to tell them from BFS levels:
+//  0 log2(1+deg(src))  1 log2(1+mean degree)  2 log2(1+degree variance)
+//  3 -1                4 log2(1+max degree)   5 log2(n)
+//  6 log2(1+m)         7 log2(mean weight / base width)
+//  8 log2(max weight / mean weight)   9 log2(mean weight / min weight)
+// 10 log2(1 + vertices with entries)   11 log2(1+mean degree) - log2(n)
+__host__ __device__ inline void sssp_features(float* f, double n, double m, double n_active, double deg_src,
+                                              double deg2_sum, double degmax, double w_mean, double w_min,
+                                              double w_max, double base_delta) {
+    const double na = n_active > 0 ? n_active : 1.0;
+    const double mean = m / na;
+    double var = deg2_sum / na - mean * mean;
+    if (var < 0) var = 0;
+    const double tiny = 1e-300;
+    f[0] = log2f((float)(1.0 + deg_src));
+    f[1] = log2f((float)(1.0 + mean));
+    f[2] = log2f((float)(1.0 + var));
+    f[3] = -1.0f;
+    f[4] = log2f((float)(1.0 + degmax));
+    f[5] = log2f((float)(n > 0 ? n : 1.0));
+    f[6] = log2f((float)(1.0 + m));
+    f[7] = (float)log2((w_mean + tiny) / (base_delta + tiny));
+    f[8] = (float)log2((w_max + tiny) / (w_mean + tiny));
+    f[9] = (float)log2((w_mean + tiny) / (w_min + tiny));
+    f[10] = log2f((float)(1.0 + n_active));
+    f[11] = f[1] - f[5];
+}
 
-// SSSP bucket width from the loaded network, or a negative value when no
-// network is loaded.
+// Block-wide evaluation for one feature row.  P: kPolTotal floats (shared or
+// global); feat: 12 floats, h1/h2: 64, logits: 20, all in shared memory.
+// Needs blockDim.x >= 512; every thread of the block must call it.
+__device__ __forceinline__ void policy_eval_block(const float* P, const float* feat, float* h1, float* h2,
+                                                  float* logits) {
+    const int t = threadIdx.x;
+    if (t < kPolH) {
+        float z = P[kOffB1 + t];
+#pragma unroll
+        for (int i = 0; i < kPolIn; ++i)
+            z = fmaf((feat[i] - P[kOffNorm + i]) * P[kOffNorm + kPolIn + i], P[kOffW1 + i * kPolH + t], z);
+        h1[t] = fmaxf(z, 0.f);
+    }
+    __syncthreads();
+    if (t < 512) {
+        // 8 threads per output, 8 inputs each, reduced across the 8 lanes.
+        const int o = t >> 3, part = t & 7;
+        float z = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) z = fmaf(h1[part * 8 + k], P[kOffW2 + (part * 8 + k) * kPolH + o], z);
+        z += __shfl_xor_sync(0xffffffffu, z, 1);
+        z += __shfl_xor_sync(0xffffffffu, z, 2);
+        z += __shfl_xor_sync(0xffffffffu, z, 4);
+        if (part == 0) h2[o] = fmaxf(z + P[kOffB2 + o], 0.f);
+    }
+    __syncthreads();
+    if (t < kPolOut * 8) {
+        const int o = t >> 3, part = t & 7;
+        float z = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) z = fmaf(h2[part * 8 + k], P[kOffW3 + (part * 8 + k) * kPolOut + o], z);
+        z += __shfl_xor_sync(0xffffffffu, z, 1);
+        z += __shfl_xor_sync(0xffffffffu, z, 2);
+        z += __shfl_xor_sync(0xffffffffu, z, 4);
+        if (part == 0) logits[o] = z + P[kOffB3 + o];
+    }
+    __syncthreads();
+}
+
+// Device copy of the installed network for the current device (kPolTotal
+// floats), or nullptr when none is installed.
+const float* policy_device_params();
+
+// Host evaluation of the installed network: direction (0 push, 1 pull) and
+// top-down output format (0 queue, 1 bitmap).  False when none is installed.
+bool policy_pick_level(const float* features, int* dir, int* fmt);
+
+// SSSP bucket width from the installed network (base_delta * 2^(bin-6)), or
+// a negative value when none is installed.
 double policy_pick_delta(const float* features, double base_delta);
 
 }  // namespace ghb

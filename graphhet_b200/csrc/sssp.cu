@@ -143,6 +143,53 @@ __global__ void mean_weight_kernel(const double* __restrict__ w, int64_t m, int6
     }
 }
 
+// Graph statistics for the width choice: degree sum of squares, maximum and
+// vertices with entries (all rows); weight sum, count, min, max (every
+// stride-th entry).  out: [0] deg2 sum, [1] w sum, [2] w count,
+// [3] degmax (as u64), [4] active (u64), [5] w min bits, [6] w max bits.
+__global__ void sssp_stats_kernel(int32_t n, const int32_t* __restrict__ rp, const double* __restrict__ w, int64_t m,
+                                  int64_t stride, double* out) {
+    unsigned long long* u = reinterpret_cast<unsigned long long*>(out);
+    double d2 = 0.0, ws = 0.0, wc = 0.0;
+    unsigned long long dmax = 0, act = 0;
+    long long wmin = 0x7fefffffffffffffll, wmax = 0;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, nt = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = tid; v < n; v += nt) {
+        const unsigned long long d = (unsigned long long)(rp[v + 1] - rp[v]);
+        d2 += (double)d * (double)d;
+        dmax = d > dmax ? d : dmax;
+        act += d > 0 ? 1 : 0;
+    }
+    for (int64_t i = tid * stride; i < m; i += nt * stride) {
+        const double x = w[i];
+        ws += x;
+        wc += 1.0;
+        const long long b = __double_as_longlong(x);  // weights are >= 0: bits order as values
+        wmin = b < wmin ? b : wmin;
+        wmax = b > wmax ? b : wmax;
+    }
+    d2 = warp_sum(d2);
+    ws = warp_sum(ws);
+    wc = warp_sum(wc);
+    act = warp_sum(act);
+    dmax = warp_max(dmax);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const long long a = __shfl_xor_sync(0xffffffffu, wmin, o), b = __shfl_xor_sync(0xffffffffu, wmax, o);
+        wmin = a < wmin ? a : wmin;
+        wmax = b > wmax ? b : wmax;
+    }
+    if (lane_id() == 0) {
+        atomicAdd(out, d2);
+        atomicAdd(out + 1, ws);
+        atomicAdd(out + 2, wc);
+        atomicMax(u + 3, dmax);
+        atomicAdd(u + 4, act);
+        atomicMin(reinterpret_cast<long long*>(u + 5), wmin);
+        atomicMax(reinterpret_cast<long long*>(u + 6), wmax);
+    }
+}
+
 // Predecessors after the distances are final: the smallest-id u in v's
 // in-row with dist[u] + w(u, v) == dist[v] exactly.
 __global__ void sssp_pred_pull_kernel(int32_t n, int32_t src, const int32_t* __restrict__ in_rp,
@@ -303,6 +350,73 @@ int sssp_pick_delta(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const d
     return GHB_OK;
 }
 
+// The width for one SSSP call: the caller's, else the weight rule above,
+// scaled by the policy network's bin when the learned policy is asked for
+// and a network is installed.  With record_trace, trace row 0 gets the
+// features, then 12 the width used, 13 -1, 14 the rule's width, 15 1 when
+// the network chose it; the caller's driver fills 13 (device ms).
+int sssp_choose_delta(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const double* w, int32_t src,
+                      const ghb_sssp_options* opt, double* delta) {
+    if (opt && opt->delta > 0) {
+        *delta = opt->delta;
+        return GHB_OK;
+    }
+    GHB_TRY(sssp_pick_delta(ws, n, rowptr, w, delta));
+    const bool learned = opt && opt->policy == GHB_POLICY_LEARNED;
+    const bool tracing = opt && opt->record_trace && opt->trace && opt->trace_cap > 0;
+    if (!learned && !tracing) return GHB_OK;
+    cudaStream_t st = ws->stream;
+    int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
+    GHB_CUDA_TRY(cudaMemcpyAsync(hp, rowptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaMemcpyAsync(hp + 1, rowptr + src, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    const int64_t m = hp[0];
+    const double deg_src = (double)(hp[2] - hp[1]);
+    double* acc = reinterpret_cast<double*>(ws->dev_small);
+    double init[7] = {0, 0, 0, 0, 0, 0, 0};
+    const long long big = 0x7fefffffffffffffll;
+    std::memcpy(&init[5], &big, sizeof(double));
+    std::memcpy(ws->host_pinned, init, sizeof(init));
+    GHB_CUDA_TRY(cudaMemcpyAsync(acc, ws->host_pinned, sizeof(init), cudaMemcpyHostToDevice, st));
+    const int64_t stride = std::max<int64_t>(1, m / (1 << 20));
+    GHB_TRY(launch(ws, sssp_stats_kernel, dim3(grid_for(n, 256, ws->num_sms * 4)), dim3(256), 0, n, rowptr, w, m,
+                   stride, acc));
+    GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, acc, sizeof(init), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    double h[7];
+    std::memcpy(h, ws->host_pinned, sizeof(h));
+    unsigned long long dmax, act;
+    long long bmin, bmax;
+    std::memcpy(&dmax, &h[3], 8);
+    std::memcpy(&act, &h[4], 8);
+    std::memcpy(&bmin, &h[5], 8);
+    std::memcpy(&bmax, &h[6], 8);
+    double wmin, wmax;
+    std::memcpy(&wmin, &bmin, 8);
+    std::memcpy(&wmax, &bmax, 8);
+    const double wmean = h[2] > 0 ? h[1] / h[2] : 1.0;
+    float f[GHB_TRACE_FEATURES];
+    sssp_features(f, (double)n, (double)m, (double)act, deg_src, h[0], (double)dmax, wmean, wmin, wmax, *delta);
+    const double base = *delta;
+    bool by_net = false;
+    if (learned) {
+        const double d = policy_pick_delta(f, base);
+        if (d > 0) {
+            *delta = d;
+            by_net = true;
+        }
+    }
+    if (tracing) {
+        float* row = opt->trace;
+        for (int k = 0; k < GHB_TRACE_COLS; ++k) row[k] = -1.f;
+        for (int k = 0; k < GHB_TRACE_FEATURES; ++k) row[k] = f[k];
+        row[12] = (float)*delta;
+        row[14] = (float)base;
+        row[15] = by_net ? 1.f : 0.f;
+    }
+    return GHB_OK;
+}
+
 int sssp_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, const double* w,
              int32_t src, double inf, double* dist_out, const ghb_sssp_options* opt,
              ghb_traversal_stats* stats) {
@@ -313,8 +427,8 @@ int sssp_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t*
     ghb_sssp_options defaults = {};
     if (!opt) opt = &defaults;
     cudaStream_t st = ws->stream;
-    double delta = opt->delta;
-    if (!(delta > 0)) GHB_TRY(sssp_pick_delta(ws, n, rowptr, w, &delta));
+    double delta = 0.0;
+    GHB_TRY(sssp_choose_delta(ws, n, rowptr, w, src, opt, &delta));
 
     Carver sizing(nullptr);
     auto carve = [&](Carver& c, WalkBuffers* wb, int32_t** qa, int32_t** qb, int32_t** fa, int32_t** fb,

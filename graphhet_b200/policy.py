@@ -1,0 +1,407 @@
+"""Learned schedule policy for the CSR traversals: training data, training,
+evaluation.
+
+The network (12 -> 64 -> 64 -> 20 logits in three heads: BFS direction,
+top-down output format, SSSP bucket-width bin) is trained by libghb's own
+kernels (``ghb_mlp_train``) and runs inside the persistent BFS kernel, where
+the block that closes a level evaluates it before releasing the grid, and in
+the SSSP width choice.  The reference has no counterpart: its BFS is
+top-down only (GPU_BFS_csr.cuh:15-249), its BFS_pre switches direction at a
+fixed n/100 frontier (GPU_BFS_pre_csr.cuh:104-118), and its SSSP has no
+buckets (GPU_SSSP_csr.cuh:253-319).
+
+Labels come from measurement.  The vertex set of BFS level L does not depend
+on the directions taken before it, so one traversal can be replayed under
+forced schedules (GHB_POLICY_SCHEDULE) and timed level by level inside the
+persistent kernel:
+
+  A  every level top-down, next frontier written as a queue
+  B  every level top-down, next frontier written as a bitmap only (the next
+     top-down level first turns it into a queue; that time is recorded apart)
+  C  every level after the first bottom-up (at most PULL_LEVEL_CAP levels)
+
+From those times a dynamic program over the frontier's form (queue or bitmap
+only) gives the cheapest schedule (`oracle_schedule`); its decisions are the
+labels, and the schedule itself, replayed, is the per-level oracle against
+which a policy's regret is measured.  SSSP labels are the fastest of the
+bucket widths 2^(k-6) x the weight rule's width, k = 0..15, timed per graph.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import time
+from dataclasses import asdict, dataclass
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+WEIGHTS_PATH = os.path.join(_HERE, "policy_net.npz")
+
+N_FEATURES, N_OUT, N_PARAMS = 12, 20, 6292
+DELTA_BINS, DELTA_BIN_ZERO = 16, 6
+# Schedule bytes: bit 0 direction, bits 1-2 top-down output (1 queue, 2 bitmap).
+PUSH_QUEUE, PUSH_BITMAP, PULL = 2, 4, 1
+PULL_LEVEL_CAP = 96
+# Trace columns (include/ghb.h).
+T_DIR, T_MS, T_FMT, T_COMP, T_NET = 12, 13, 20, 21, 22
+
+
+# ------------------------------------------------------------ graph family
+@dataclass
+class GraphSpec:
+    kind: str          # rmat | er | grid | powerlaw
+    scale: int         # log2 of the vertex count
+    param: float       # rmat: a; er: mean degree; grid: aspect log2; powerlaw: exponent
+    edge_factor: int   # generated edges per vertex (rmat, powerlaw)
+    seed: int
+
+
+def training_specs(count: int = 400, seed: int = 4) -> List[GraphSpec]:
+    """The training family: RMAT with a in [.45, .65], Erdos-Renyi, grids and
+    Chung-Lu power-law graphs with exponent in [2.1, 2.8], scales 16-22,
+    cycled in that order.  Held out: the scale-24 RMAT and the 4096x4096 grid."""
+    rng = np.random.default_rng(seed)
+    kinds = ["rmat", "er", "grid", "powerlaw"]
+    out = []
+    for i in range(count):
+        kind = kinds[i % 4]
+        scale = int(rng.integers(16, 23))
+        if kind == "rmat":
+            param, ef = float(rng.uniform(0.45, 0.65)), int(rng.choice([4, 8, 16, 32]))
+        elif kind == "er":
+            param, ef = float(rng.uniform(2.0, 32.0)), 0
+        elif kind == "grid":
+            param, ef = float(rng.integers(0, 3)), 0
+        else:
+            param, ef = float(rng.uniform(2.1, 2.8)), int(rng.choice([2, 4, 8, 16]))
+        out.append(GraphSpec(kind, scale, param, ef, int(rng.integers(1, 2**31))))
+    return out
+
+
+def build_graph(spec: GraphSpec, weighted: bool = True):
+    """CSRGraph of a spec on the current CUDA device (undirected, weights
+    U(0,1] except grids, which get integers in [1, 100])."""
+    import graphhet_b200 as G
+    wm = G.WEIGHT_UNIFORM01 if weighted else G.WEIGHT_NONE
+    n = 1 << spec.scale
+    if spec.kind == "rmat":
+        a = spec.param
+        b = c = (1.0 - a - 0.05) / 2.0
+        return G.rmat_graph(spec.scale, spec.edge_factor, spec.seed, a=a, b=b, c=c, weight_mode=wm)
+    if spec.kind == "er":
+        src, dst = G.gen_er(n, int(n * spec.param / 2), spec.seed)
+        return G.make_graph(n, src, dst, False, weight_mode=wm, weight_seed=spec.seed)
+    if spec.kind == "grid":
+        r = spec.scale // 2 - int(spec.param)
+        return G.grid_graph(1 << r, 1 << (spec.scale - r), weight_seed=spec.seed)
+    src, dst = G.gen_powerlaw(spec.scale, n * spec.edge_factor, spec.param, spec.seed)
+    return G.make_graph(n, src, dst, False, weight_mode=wm, weight_seed=spec.seed)
+
+
+def pick_sources(g, k: int, seed: int) -> List[int]:
+    """k distinct vertices with at least one entry, seeded."""
+    import torch
+    deg = (g.rowptr[1:] - g.rowptr[:-1]).cpu().numpy()
+    cand = np.nonzero(deg > 0)[0]
+    if cand.size == 0:
+        return []
+    rng = np.random.default_rng(seed)
+    return [int(x) for x in rng.choice(cand, size=min(k, cand.size), replace=False)]
+
+
+# ------------------------------------------------------ per-level oracle
+def oracle_schedule(t_queue: Sequence[float], t_bitmap: Sequence[float], t_comp: Sequence[float],
+                    t_pull: Sequence[float]) -> Tuple[List[int], List[float], float]:
+    """Cheapest schedule for one traversal from per-level costs.
+
+    t_queue[L]   top-down level L writing the next frontier as a queue
+    t_bitmap[L]  top-down level L writing it as a bitmap only (expansion)
+    t_comp[L]    turning frontier L from a bitmap into a queue
+    t_pull[L]    bottom-up level L (inf where not timed)
+    Level 0's frontier is a queue.  A top-down level needs a queue (paying
+    t_comp if the frontier is a bitmap); a bottom-up level reads the bitmap,
+    which always exists, and leaves a bitmap.  Returns the schedule bytes, the
+    chosen cost of each level (compaction included) and the total."""
+    L = len(t_queue)
+    INF = float("inf")
+    # V[l][s]: cheapest cost of levels l.. with frontier l in form s (0 queue, 1 bitmap).
+    V = [[0.0, 0.0] for _ in range(L + 1)]
+    act = [[None, None] for _ in range(L)]
+    for l in range(L - 1, -1, -1):
+        for s in (0, 1):
+            comp = 0.0 if s == 0 else (t_comp[l] if t_comp[l] >= 0 else 0.0)
+            opts = [(comp + t_queue[l] + V[l + 1][0], PUSH_QUEUE),
+                    (comp + t_bitmap[l] + V[l + 1][1], PUSH_BITMAP),
+                    ((t_pull[l] if l > 0 else INF) + V[l + 1][1], PULL)]
+            best = min(opts, key=lambda x: x[0])
+            V[l][s], act[l][s] = best
+    sched, cost, s = [], [], 0
+    for l in range(L):
+        a = act[l][s]
+        comp = 0.0 if s == 0 else (t_comp[l] if t_comp[l] >= 0 else 0.0)
+        c = {PUSH_QUEUE: comp + t_queue[l], PUSH_BITMAP: comp + t_bitmap[l], PULL: t_pull[l]}[a]
+        sched.append(a)
+        cost.append(c)
+        s = 0 if a == PUSH_QUEUE else 1
+    return sched, cost, V[0][0]
+
+
+def level_rows(trace_a: np.ndarray, sched: Sequence[int], cost: Sequence[float],
+               max_rows: int = 48) -> Tuple[np.ndarray, np.ndarray]:
+    """Training rows of one traversal: the features of frontier L (the same in
+    every replay) with the history features (9 previous direction, 10
+    previous level time) taken from the oracle schedule, and the labels
+    (direction, top-down output format).  Level 0 is skipped: the kernel
+    decides it without the network.  A long traversal (a grid's thousands of
+    levels) gives its first max_rows/2 levels and evenly spaced others, so
+    that it does not outweigh the rest of the family."""
+    X, Y = [], []
+    levels = list(range(1, len(sched)))
+    if len(levels) > max_rows:
+        head = levels[: max_rows // 2]
+        rest = levels[max_rows // 2:]
+        pick = np.linspace(0, len(rest) - 1, max_rows - len(head)).round().astype(int)
+        levels = head + [rest[i] for i in sorted(set(pick.tolist()))]
+    for l in levels:
+        f = trace_a[l, :N_FEATURES].astype(np.float32).copy()
+        f[9] = 1.0 if sched[l - 1] == PULL else 0.0
+        f[10] = math.log2(1.0 + 1000.0 * max(cost[l - 1], 0.0))
+        d = 1 if sched[l] == PULL else 0
+        fm = -1 if d else (0 if sched[l] == PUSH_QUEUE else 1)
+        X.append(f)
+        Y.append([d, fm, -1])
+    if not X:
+        return np.zeros((0, N_FEATURES), np.float32), np.zeros((0, 3), np.int32)
+    return np.asarray(X, np.float32), np.asarray(Y, np.int32)
+
+
+def replay_costs(rg, src: int):
+    """Run schedules A, B, C on one source; per-level cost table and run A's
+    trace (features).  Returns None when the traversal has one level."""
+    import graphhet_b200 as G
+    cap = 1 << 15
+    _, st_a, ta = rg.bfs(src, policy=G.POLICY_SCHEDULE, schedule=[PUSH_QUEUE] * cap, trace_cap=cap)
+    levels = ta.shape[0]
+    if levels < 2:
+        return None
+    _, _, tb = rg.bfs(src, policy=G.POLICY_SCHEDULE, schedule=[PUSH_BITMAP] * levels, trace_cap=levels)
+    npull = min(levels, PULL_LEVEL_CAP)
+    sched_c = [PUSH_QUEUE] + [PULL] * (npull - 1) + [PUSH_QUEUE] * (levels - npull)
+    _, _, tc = rg.bfs(src, policy=G.POLICY_SCHEDULE, schedule=sched_c, trace_cap=levels)
+    t_q = ta[:, T_MS].astype(np.float64)
+    comp_b = np.where(tb[:, T_COMP] >= 0, tb[:, T_COMP], 0.0).astype(np.float64)
+    t_b = tb[:, T_MS].astype(np.float64) - comp_b
+    # Frontier l of run B is a bitmap for l >= 1, so run B timed every compaction.
+    t_comp = comp_b.copy()
+    t_p = np.full(levels, np.inf)
+    t_p[1:npull] = tc[1:npull, T_MS]
+    return dict(t_queue=t_q, t_bitmap=t_b, t_comp=t_comp, t_pull=t_p, trace=ta, levels=levels,
+                m_r=st_a["edges_reached"])
+
+
+# ------------------------------------------------------------ SSSP labels
+def sssp_rows(rg, src: int, max_buckets: float = 4096.0, max_ms: float = 2000.0):
+    """One row for the width head: the width rule's features and the fastest
+    of the 16 width bins (each timed once after a warm-up at the rule's width).
+    Bins whose width would give more than max_buckets buckets over the largest
+    finite distance are not run."""
+    import torch
+    import graphhet_b200 as G
+    d0, st0, row = rg.sssp(src, trace=True)
+    base = float(row[14])
+    fin = d0[d0 < 1e300]
+    dmax = float(fin.max().item()) if fin.numel() else 0.0
+    times = np.full(DELTA_BINS, np.inf)
+    for k in range(DELTA_BINS):
+        delta = base * 2.0 ** (k - DELTA_BIN_ZERO)
+        if dmax / delta > max_buckets:
+            continue
+        d, st = rg.sssp(src, delta=delta)
+        times[k] = st["device_ms"]
+        if not torch.equal(d, d0):
+            raise RuntimeError("SSSP distances changed with the bucket width")
+        if st["device_ms"] > max_ms:
+            break
+    if not np.isfinite(times).any():
+        return None
+    return row[:N_FEATURES].astype(np.float32), int(np.argmin(times)), times
+
+
+# ------------------------------------------------------------- collection
+def collect(specs: Sequence[GraphSpec], bfs_sources: int = 2, sssp_every: int = 2, sssp_max_scale: int = 20,
+            log=print) -> Dict[str, np.ndarray]:
+    """Training rows from every graph of `specs` (needs a GPU)."""
+    import torch
+    import graphhet_b200 as G
+    Xs, Ys, meta = [], [], []
+    t0 = time.time()
+    for gi, spec in enumerate(specs):
+        g = build_graph(spec)
+        rg = G.ResidentGraph(g)
+        srcs = pick_sources(g, bfs_sources, spec.seed)
+        nrows = 0
+        for s in srcs:
+            rg.bfs(s)  # warm-up (scratch, first-touch)
+            r = replay_costs(rg, s)
+            if r is None:
+                continue
+            sched, cost, total = oracle_schedule(r["t_queue"], r["t_bitmap"], r["t_comp"], r["t_pull"])
+            X, Y = level_rows(r["trace"], sched, cost)
+            Xs.append(X)
+            Ys.append(Y)
+            nrows += len(X)
+        if gi % sssp_every == 0 and spec.scale <= sssp_max_scale and srcs:
+            out = sssp_rows(rg, srcs[0])
+            if out is not None:
+                f, lab, _ = out
+                Xs.append(f[None, :])
+                Ys.append(np.array([[-1, -1, lab]], np.int32))
+                nrows += 1
+        meta.append(dict(asdict(spec), rows=nrows, n=g.n, m=int(g.m)))
+        rg.close()
+        del rg, g
+        torch.cuda.empty_cache()
+        if log and (gi % 20 == 0 or gi == len(specs) - 1):
+            log("graph %d/%d %s scale %d rows %d (%.0f s)" % (gi + 1, len(specs), spec.kind, spec.scale, nrows,
+                                                              time.time() - t0))
+    return dict(X=np.concatenate(Xs).astype(np.float32), Y=np.concatenate(Ys).astype(np.int32),
+                meta=np.array(json.dumps(meta)))
+
+
+# --------------------------------------------------------------- training
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-initialised weights, zero biases, in the kernels' layout."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for fan_in, fan_out in [(12, 64), (64, 64), (64, 20)]:
+        parts.append(rng.normal(0.0, math.sqrt(2.0 / fan_in), size=fan_in * fan_out))
+        parts.append(np.zeros(fan_out))
+    p = np.concatenate(parts).astype(np.float32)
+    assert p.size == N_PARAMS
+    return p
+
+
+def norm_of(X: np.ndarray) -> np.ndarray:
+    mu = X.mean(0)
+    sd = X.std(0)
+    return np.concatenate([mu, 1.0 / np.maximum(sd, 1e-3)]).astype(np.float32)
+
+
+def train(X: np.ndarray, Y: np.ndarray, epochs: int = 3000, lr: float = 3e-3, seed: int = 0):
+    """Full-batch Adam on the GPU with libghb's MLP kernels.  Returns
+    (params, norm, loss history)."""
+    import torch
+    import graphhet_b200 as G
+    norm = norm_of(X)
+    p = torch.from_numpy(init_params(seed)).cuda()
+    hist = G.mlp_train(p, torch.from_numpy(norm).cuda(), torch.from_numpy(X).cuda(), torch.from_numpy(Y).cuda(),
+                       epochs=epochs, lr=lr)
+    return p.cpu().numpy(), norm, np.asarray(hist, np.float32)
+
+
+def predict(params: np.ndarray, norm: np.ndarray, X: np.ndarray) -> np.ndarray:
+    """Logits through ghb_mlp_forward (GPU)."""
+    import torch
+    import graphhet_b200 as G
+    return G.mlp_forward(torch.from_numpy(params).cuda(), torch.from_numpy(norm).cuda(),
+                         torch.from_numpy(X.astype(np.float32)).cuda()).cpu().numpy()
+
+
+def accuracy(params, norm, X, Y) -> Dict[str, float]:
+    z = predict(params, norm, X)
+    out = {}
+    for h, (a, b), name in [(0, (0, 2), "dir"), (1, (2, 4), "fmt"), (2, (4, 20), "delta")]:
+        keep = Y[:, h] >= 0
+        if keep.any():
+            out[name] = float((z[keep, a:b].argmax(1) == Y[keep, h]).mean())
+    return out
+
+
+def save(path: str, params, norm, info: dict) -> None:
+    np.savez(path, params=params.astype(np.float32), norm=norm.astype(np.float32), info=np.array(json.dumps(info)))
+
+
+def load(path: str = WEIGHTS_PATH):
+    z = np.load(path)
+    return z["params"], z["norm"], json.loads(str(z["info"]))
+
+
+def install(path: str = WEIGHTS_PATH) -> dict:
+    """Install the trained network for POLICY_LEARNED (this process)."""
+    import graphhet_b200 as G
+    params, norm, info = load(path)
+    G.policy_load(params, norm)
+    return info
+
+
+# ------------------------------------------------------------- evaluation
+def regret(rg, sources: Sequence[int], repeats: int = 3) -> Dict[str, float]:
+    """Measured regret of the heuristic and the learned policy against the
+    per-level oracle schedule on `rg` (needs an installed network): each
+    policy's persistent BFS time over the sources (median of `repeats`) ÷ the
+    oracle schedule's time, minus one.  Also the oracle's own estimate from
+    the cost table."""
+    import graphhet_b200 as G
+
+    def timed(src, **kw):
+        ts = []
+        for _ in range(repeats):
+            _, st = rg.bfs(src, **kw)
+            ts.append(st["device_ms"])
+        return float(np.median(ts)), st
+
+    tot = dict(heuristic=0.0, learned=0.0, oracle=0.0, beamer14=0.0, table=0.0)
+    for s in sources:
+        rg.bfs(s)
+        r = replay_costs(rg, s)
+        if r is None:
+            continue
+        sched, cost, total = oracle_schedule(r["t_queue"], r["t_bitmap"], r["t_comp"], r["t_pull"])
+        tot["table"] += total
+        tot["oracle"] += timed(s, policy=G.POLICY_SCHEDULE, schedule=sched)[0]
+        tot["heuristic"] += timed(s, policy=G.POLICY_HEURISTIC)[0]
+        tot["beamer14"] += timed(s, policy=G.POLICY_HEURISTIC, alpha=14.0, beta=24.0)[0]
+        tot["learned"] += timed(s, policy=G.POLICY_LEARNED)[0]
+    o = tot["oracle"]
+    return dict(ms=tot, regret_heuristic=tot["heuristic"] / o - 1.0, regret_learned=tot["learned"] / o - 1.0,
+                regret_beamer14=tot["beamer14"] / o - 1.0)
+
+
+def main(argv=None) -> int:
+    import argparse
+    import torch
+    ap = argparse.ArgumentParser(description="collect traces, train the schedule policy, save it")
+    ap.add_argument("--graphs", type=int, default=400)
+    ap.add_argument("--epochs", type=int, default=3000)
+    ap.add_argument("--lr", type=float, default=3e-3)
+    ap.add_argument("--out", default=WEIGHTS_PATH)
+    ap.add_argument("--data", default=None, help="save / reuse the collected rows (.npz)")
+    a = ap.parse_args(argv)
+    if a.data and os.path.exists(a.data):
+        z = np.load(a.data)
+        data = dict(X=z["X"], Y=z["Y"], meta=z["meta"])
+    else:
+        data = collect(training_specs(a.graphs))
+        if a.data:
+            np.savez(a.data, **data)
+    X, Y = data["X"], data["Y"]
+    # Hold out every tenth BFS row block for validation accuracy.
+    idx = np.arange(len(X))
+    val = idx % 10 == 0
+    params, norm, hist = train(X[~val], Y[~val], epochs=a.epochs, lr=a.lr)
+    acc_tr, acc_val = accuracy(params, norm, X[~val], Y[~val]), accuracy(params, norm, X[val], Y[val])
+    params, norm, hist_all = train(X, Y, epochs=a.epochs, lr=a.lr)
+    info = dict(graphs=a.graphs, rows=int(len(X)), bfs_rows=int((Y[:, 0] >= 0).sum()),
+                sssp_rows=int((Y[:, 2] >= 0).sum()), pull_frac=float((Y[:, 0] == 1).sum() / max(1, (Y[:, 0] >= 0).sum())),
+                epochs=a.epochs, lr=a.lr, loss_first=float(hist_all[0]), loss_last=float(hist_all[-1]),
+                acc_train=acc_tr, acc_val=acc_val)
+    save(a.out, params, norm, info)
+    print(json.dumps(info))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

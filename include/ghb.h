@@ -75,6 +75,12 @@ int ghb_gen_rmat(ghb_workspace* ws, int32_t scale, int64_t n_edges, uint64_t see
 int ghb_gen_grid(ghb_workspace* ws, int32_t rows, int32_t cols, int32_t* src, int32_t* dst);
 int ghb_gen_er(ghb_workspace* ws, int32_t n, int64_t n_edges, uint64_t seed,
                int32_t* src, int32_t* dst);
+/* Chung-Lu power-law graph on 2^scale vertices: each endpoint is vertex i
+ * with probability proportional to (i+1)^(-1/(exponent-1)) (degree
+ * distribution ~ d^-exponent), ids scattered by the seed's permutation.
+ * exponent in (2, 10).  Training graphs for the schedule policy. */
+int ghb_gen_powerlaw(ghb_workspace* ws, int32_t scale, int64_t n_edges, double exponent,
+                     uint64_t seed, int32_t* src, int32_t* dst);
 
 /* ----------------------------------------------------------- CSR builder */
 /* Build a CSR from an edge list (replaces the host flattening in toCSR,
@@ -114,7 +120,10 @@ typedef struct {
     int32_t policy;
     float alpha;             /* switch to pull when m_f > m_u / alpha (0: 256) */
     float beta;              /* back to push when n_f < n / beta (0: 24)      */
-    const int8_t* schedule;  /* host array for GHB_POLICY_SCHEDULE            */
+    const int8_t* schedule;  /* host array for GHB_POLICY_SCHEDULE: per level
+                                bit 0 direction (0 push, 1 pull); bits 1-2 the
+                                output of a top-down level: 0 by frontier size,
+                                2 queue, 4 bitmap only                        */
     int32_t schedule_len;
     int32_t record_trace;    /* 1: fill trace[] with one row per level         */
     float* trace;            /* host, trace_cap x GHB_TRACE_COLS               */
@@ -122,12 +131,16 @@ typedef struct {
     int32_t oracle_timing;   /* 1: time push and pull at every level (slow)   */
 } ghb_bfs_options;
 
-/* Trace row: 12 policy features, then direction used, level time (ms),
- * push time (ms) and pull time (ms) when oracle_timing is set (else -1),
- * CSR entries read, vertices reached by the level, vertices unvisited
- * before it, and the level's algorithmic bytes (rowptr + col + depth). */
+/* Trace row (one per level): 12 policy features of the level's frontier,
+ * then 12 direction used, 13 level time (ms), 14 push time and 15 pull time
+ * (ms) when oracle_timing is set (else -1), 16 CSR entries read, 17 vertices
+ * reached by the level, 18 vertices unvisited before it, 19 the level's
+ * algorithmic bytes (rowptr + col + depth), 20 output format of a top-down
+ * level (0 queue, 1 bitmap), 21 time (ms) spent turning the frontier bitmap
+ * into a queue at the level's start (-1 none), 22 1 when the learned network
+ * chose the level's direction, 23 reserved (-1). */
 #define GHB_TRACE_FEATURES 12
-#define GHB_TRACE_COLS 20
+#define GHB_TRACE_COLS 24
 
 typedef struct {
     int32_t levels;          /* frontier expansions run                      */
@@ -311,6 +324,37 @@ int ghb_batch_wcc(ghb_workspace* ws, int32_t n_graphs, const int64_t* vbase,
 int ghb_batch_tc(ghb_workspace* ws, int32_t n_graphs, const int64_t* vbase,
                  const int64_t* ebase, const int32_t* rowptr, const int32_t* col,
                  int64_t* counts64, int64_t* totals);
+
+/* ------------------------------------------------------- schedule policy */
+/* The learned schedule policy: an MLP 12 -> 64 -> 64 (ReLU) -> 20 logits in
+ * three heads: [0,2) BFS direction (push, pull), [2,4) top-down frontier
+ * format (queue, bitmap), [4,20) SSSP bucket width (bin k: 2^(k-6) times the
+ * weight-derived base width).  No counterpart in the reference (its direction
+ * is fixed per kernel).  Parameters, row-major x @ W, FP32:
+ * W1[12][64] b1[64] W2[64][64] b2[64] W3[64][20] b3[20].  norm: mean[12]
+ * then 1/std[12], applied to the features first. */
+#define GHB_POLICY_PARAMS 6292
+#define GHB_POLICY_OUT 20
+
+/* Install a network (host arrays) for GHB_POLICY_LEARNED in every BFS and
+ * SSSP call of this process; it is copied to each device on first use.
+ * Both NULL: uninstall (GHB_POLICY_LEARNED then runs the heuristic). */
+int ghb_policy_load(const float* params, const float* norm);
+/* 1 when a network is installed. */
+int ghb_policy_loaded(void);
+
+/* Device arrays: logits[batch][20] = network(x[batch][12]). */
+int ghb_mlp_forward(ghb_workspace* ws, const float* params, const float* norm, const float* x,
+                    int32_t batch, float* logits);
+/* Device arrays: grad[GHB_POLICY_PARAMS] of the summed mean softmax
+ * cross-entropy of the three heads; y[batch][3] holds the class of each head
+ * (-1: no label).  loss (host, may be NULL) gets the loss. */
+int ghb_mlp_grad(ghb_workspace* ws, const float* params, const float* norm, const float* x,
+                 const int32_t* y, int32_t batch, float* grad, float* loss);
+/* `epochs` full-batch Adam steps on device params (in place); loss_history
+ * (host, may be NULL) gets the loss before each step. */
+int ghb_mlp_train(ghb_workspace* ws, float* params, const float* norm, const float* x,
+                  const int32_t* y, int32_t batch, int32_t epochs, float lr, float* loss_history);
 
 #ifdef __cplusplus
 }

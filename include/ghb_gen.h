@@ -51,6 +51,7 @@ GHB_HD uint64_t ghb_draw(uint64_t stream, uint64_t ctr) {
 #define GHB_PURPOSE_ER 4ULL
 #define GHB_PURPOSE_SOURCES 5ULL
 #define GHB_PURPOSE_DANGLING 6ULL
+#define GHB_PURPOSE_POWERLAW 7ULL
 
 /* RMAT quadrant thresholds as 32-bit integers, so CPU and GPU compare the
  * same integers: quadrant 0 if r < t0, 1 if r < t1, 2 if r < t2, else 3. */

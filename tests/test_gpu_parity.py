@@ -191,7 +191,7 @@ def test_bfs_schedule_and_trace(G):
     ref = O.bfs(og, 10)
     d, st, tr = G.bfs(g, 10, trace_cap=64, oracle_timing=True)
     assert np.array_equal(d.cpu().numpy(), ref)
-    assert tr.shape[0] == st["levels"] and tr.shape[1] == 20
+    assert tr.shape[0] == st["levels"] and tr.shape[1] == G.TRACE_COLS
     assert np.all(tr[:, 14] >= 0) and np.all(tr[:, 15] >= 0)
     sched = [0, 1, 0, 1, 1, 0, 0, 1, 0, 1, 1, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0]
     d2, _ = G.bfs(g, 10, policy=G.POLICY_SCHEDULE, schedule=sched)

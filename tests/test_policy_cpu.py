@@ -1,0 +1,86 @@
+"""Host logic of the learned schedule policy: the per-level oracle (dynamic
+program over the frontier's form) against brute force, the training rows,
+and the training family."""
+import itertools
+import math
+
+import numpy as np
+
+from graphhet_b200 import policy as P
+
+
+def brute_force(tq, tb, tc, tp):
+    best = (math.inf, None)
+    L = len(tq)
+    for acts in itertools.product([P.PUSH_QUEUE, P.PUSH_BITMAP, P.PULL], repeat=L):
+        if acts[0] == P.PULL:
+            continue
+        s, tot = 0, 0.0
+        for l, a in enumerate(acts):
+            comp = tc[l] if s == 1 else 0.0
+            if a == P.PULL:
+                tot += tp[l]
+                s = 1
+            else:
+                tot += comp + (tq[l] if a == P.PUSH_QUEUE else tb[l])
+                s = 0 if a == P.PUSH_QUEUE else 1
+        if tot < best[0]:
+            best = (tot, list(acts))
+    return best
+
+
+def test_oracle_schedule_matches_brute_force():
+    rng = np.random.default_rng(1)
+    for _ in range(200):
+        L = int(rng.integers(1, 7))
+        tq, tb, tc, tp = (rng.uniform(0.01, 1.0, L) for _ in range(4))
+        if rng.random() < 0.3:
+            tp[int(rng.integers(0, L))] = np.inf
+        sched, cost, total = P.oracle_schedule(tq, tb, tc, tp)
+        bt, bs = brute_force(tq, tb, tc, tp)
+        assert math.isclose(total, bt, rel_tol=1e-12)
+        assert math.isclose(sum(cost), total, rel_tol=1e-12)
+        assert sched[0] != P.PULL
+
+
+def test_level_rows_history_features_and_labels():
+    L = 5
+    trace = np.arange(L * 24, dtype=np.float32).reshape(L, 24)
+    sched = [P.PUSH_QUEUE, P.PULL, P.PUSH_BITMAP, P.PUSH_QUEUE, P.PULL]
+    cost = [0.1, 0.2, 0.3, 0.4, 0.5]
+    X, Y = P.level_rows(trace, sched, cost)
+    assert X.shape == (4, 12) and Y.shape == (4, 3)
+    assert Y.tolist() == [[1, -1, -1], [0, 1, -1], [0, 0, -1], [1, -1, -1]]
+    assert X[:, 9].tolist() == [0.0, 1.0, 0.0, 0.0]
+    assert np.allclose(X[:, 10], np.log2(1 + 1000 * np.array(cost[:4])))
+    assert np.array_equal(X[:, :9], trace[1:, :9])
+
+
+def test_level_rows_subsamples_long_traversals():
+    L = 3000
+    trace = np.zeros((L, 24), np.float32)
+    trace[:, 3] = np.arange(L)
+    sched = [P.PUSH_QUEUE] * L
+    X, Y = P.level_rows(trace, sched, [0.01] * L, max_rows=48)
+    assert len(X) <= 48
+    assert X[:24, 3].tolist() == list(range(1, 25))
+    assert X[-1, 3] == L - 1
+
+
+def test_training_family():
+    specs = P.training_specs(400)
+    assert len(specs) == 400
+    kinds = {k: [s for s in specs if s.kind == k] for k in ("rmat", "er", "grid", "powerlaw")}
+    assert all(len(v) == 100 for v in kinds.values())
+    assert all(16 <= s.scale <= 22 for s in specs)
+    assert all(0.45 <= s.param <= 0.65 for s in kinds["rmat"])
+    assert all(2.1 <= s.param <= 2.8 for s in kinds["powerlaw"])
+    assert P.training_specs(400) == specs  # seeded
+
+
+def test_init_params_layout():
+    p = P.init_params(0)
+    assert p.shape == (6292,) and p.dtype == np.float32
+    assert np.all(p[768:832] == 0) and np.all(p[6272:] == 0)
+    n = P.norm_of(np.random.default_rng(0).normal(size=(50, 12)).astype(np.float32))
+    assert n.shape == (24,)
