@@ -65,6 +65,21 @@ def measured_peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+def profiled_traffic(args):
+    """DRAM bytes (read + write) per BFS launch from the committed ncu summary
+    of this workload (RMAT scale 24, edge factor 16, seed 7), else None."""
+    if (args.scale, args.edge_factor, args.seed) != (24, 16, 7):
+        return None
+    path = os.path.join(ROOT, "profiles", "bfs_persistent_kernel_rmat24_dram.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def pick_sources(rowptr_host: np.ndarray, count: int, seed: int, salt: int = 0):
     """Seeded random non-isolated sources (splitmix64 draws, first hits)."""
     n = len(rowptr_host) - 1
@@ -261,7 +276,8 @@ def run_ours(args, world, rank, local):
     bytes_per = [4 * (n + 1) + 4 * mr[s] + 4 * n for _ in range(args.steps) for s in srcs]
     achieved = sum(bytes_per) / (sum(launch_ms) / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": "bfs_persistent_kernel", "achieved": round(achieved, 1), "peak": hbm,
-                "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": None,
+                "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": profiled_traffic(args),
+                "traffic_source": "profiles/bfs_persistent_kernel_rmat24_dram.md (ncu, 3 launches)",
                 "bytes_per_launch": int(sum(bytes_per) / len(bytes_per)),
                 "launch_ms_mean": round(sum(launch_ms) / len(launch_ms), 4), "launches": len(launch_ms),
                 "share_of_step": round(sum(launch_ms) / ms, 3) if world == 1 else None}
