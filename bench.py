@@ -442,6 +442,36 @@ def extras(args, G, g, rg, srcs, ws):
         ex["sssp_rule_ms_per_source"] = round(t_rule / 4, 3)
         ex["learned_vs_plain"] = round(t_h / t_l, 3)
         ex["batched_vs_plain"] = round((mr_sum / (ms / 1e3)) / (mr_sum / (t_h / 1e3)), 3)
+    # Batched sources (RMAT seed 3 scale 22, 256 sources): one 256-source
+    # pass (4 words per vertex) against 256 single-source traversals.
+    del rank, lab
+    torch.cuda.empty_cache()
+    g22 = G.rmat_graph(22, 16, 3)
+    bsrc = pick_sources(g22.rowptr.cpu().numpy(), 256, 3)
+    gb = G.ResidentGraph(g22)
+    del g22
+    lb = torch.empty(gb.n, dtype=torch.int32, device="cuda")
+    mr_b, t_single = 0, 0.0
+    for s in bsrc:
+        gb.bfs(s, out=lb)
+    for s in bsrc:
+        _, stb = gb.bfs(s, out=lb)
+        mr_b += stb["edges_reached"]
+        t_single += stb["device_ms"]
+    ob = torch.empty(256 * gb.n, dtype=torch.int32, device="cuda")
+    gb.msbfs(bsrc, out=ob)
+    ms256, _ = timed(lambda: gb.msbfs(bsrc, out=ob))
+    ms64, _ = timed(lambda: gb.msbfs(bsrc[:64], out=ob))
+    mr_64 = 0
+    for s in bsrc[:64]:
+        mr_64 += gb.bfs(s, out=lb)[1]["edges_reached"]
+    ex["batch256_rmat22_single_gteps"] = round(mr_b / (t_single / 1e3) / 1e9, 3)
+    ex["batch256_rmat22_msbfs_ms"] = round(ms256, 2)
+    ex["batch256_rmat22_msbfs_gteps"] = round(mr_b / (ms256 / 1e3) / 1e9, 3)
+    ex["batch64_rmat22_msbfs_gteps"] = round(mr_64 / (ms64 / 1e3) / 1e9, 3)
+    ex["batch256_vs_plain"] = round(t_single / ms256, 3)
+    del ob, gb
+    torch.cuda.empty_cache()
     # 4096 x 4096 grid: BFS and SSSP from its centre
     gg = G.ResidentGraph(G.grid_graph(4096, 4096, weight_seed=args.seed))
     c = 2048 * 4096 + 2048

@@ -45,6 +45,8 @@ void clear_error();
 // -------------------------------------------------------------- constants
 constexpr int kWarp = 32;
 constexpr int32_t kInfDepth = 0x7fffffff;
+// Sources per multi-source BFS pass (4 uint64 words of source bits per vertex).
+constexpr int32_t kMsPass = 256;
 
 // Device status word written by kernels whose waits gave up or whose budgets
 // ran out; read back by the host after the launch.

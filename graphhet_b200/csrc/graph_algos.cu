@@ -41,9 +41,9 @@ int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* c
            int32_t* counts32, int64_t* total);
 int pagerank_run(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int32_t* in_col, const int32_t* out_rp,
                  const ghb_pr_options* o, double* rank, int32_t* iters_run);
-int msbfs_batch(ghb_workspace* ws, int32_t n, const int32_t* out_rp, const int32_t* out_col, const int32_t* in_rp,
-                const int32_t* in_col, const int32_t* srcs_dev, int32_t k, int32_t* depth, int64_t* levels_out,
-                int64_t* examined_out);
+int msbfs_batch(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_rp, const int32_t* out_col,
+                const int32_t* in_rp, const int32_t* in_col, const int32_t* srcs_dev, int32_t k,
+                const int32_t* perm, int32_t* depth, int64_t* levels_out, int64_t* examined_out);
 
 namespace {
 
@@ -71,15 +71,6 @@ __global__ void pred_map_kernel(int32_t n, const int32_t* __restrict__ perm, con
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         const int32_t p = pred_new[perm[v]];
         out[v] = p < 0 ? p : iperm[p];
-    }
-}
-
-__global__ void map_rows_kernel(int32_t n, int32_t k, const int32_t* __restrict__ perm, const int32_t* __restrict__ src,
-                                int32_t* dst) {
-    const int64_t total = (int64_t)n * k;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t s = i / n, v = i - s * n;
-        dst[i] = src[s * n + perm[v]];
     }
 }
 
@@ -151,18 +142,16 @@ int ghb_graph_msbfs(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, 
         GHB_REQUIRE(hs[i] >= 0 && hs[i] < g->n, "source outside [0, n)");
         hs[i] = g->perm_host[hs[i]];
     }
-    const int32_t kmax = std::min<int32_t>(64, std::max<int32_t>(1, n_src));
-    GHB_TRY(ws_reserve_stage(ws, sizeof(int32_t) * ((size_t)g->n * kmax + 64 + 256)));
-    int32_t* dnew = static_cast<int32_t*>(ws->stage);
-    int32_t* snew = dnew + (size_t)g->n * kmax + 64;
+    // Sources in the graph's ids; depths go straight to the caller's rows.
+    GHB_TRY(ws_reserve_stage(ws, sizeof(int32_t) * kMsPass));
+    int32_t* snew = static_cast<int32_t*>(ws->stage);
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
     int64_t levels = 0, examined = 0;
-    for (int32_t s0 = 0; s0 < n_src; s0 += 64) {
-        const int32_t k = std::min<int32_t>(64, n_src - s0);
+    for (int32_t s0 = 0; s0 < n_src; s0 += kMsPass) {
+        const int32_t k = std::min<int32_t>(kMsPass, n_src - s0);
         GHB_CUDA_TRY(cudaMemcpyAsync(snew, hs.data() + s0, sizeof(int32_t) * k, cudaMemcpyHostToDevice, st));
-        GHB_TRY(msbfs_batch(ws, g->n, g->rowptr, g->col, g->in_rowptr, g->in_col, snew, k, dnew, &levels, &examined));
-        GHB_TRY(launch(ws, map_rows_kernel, dim3(grid_for((int64_t)g->n * k, 256, ws->num_sms * 16)), dim3(256), 0,
-                       g->n, k, (const int32_t*)g->perm, (const int32_t*)dnew, depth + (int64_t)s0 * g->n));
+        GHB_TRY(msbfs_batch(ws, g->n, g->n_active, g->rowptr, g->col, g->in_rowptr, g->in_col, snew, k,
+                            (const int32_t*)g->perm, depth + (int64_t)s0 * g->n, &levels, &examined));
     }
     GHB_CUDA_TRY(cudaStreamSynchronize(st));  // hs (host) is read by the copies above
     if (stats) {

@@ -167,8 +167,10 @@ int ghb_bfs_pred(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr,
                  int32_t src, int32_t max_depth, int32_t* depth, int32_t* pred,
                  const ghb_bfs_options* options, ghb_traversal_stats* stats);
 
-/* Many sources at once: 64 sources per uint64 bitmask word.  depth is
- * n_src x n, row s holding the depths from srcs[s]. */
+/* Many sources at once: one bit per source in 1, 2 or 4 uint64 words per
+ * vertex, so one traversal serves up to 256 sources (larger n_src runs in
+ * passes of 256).  depth is n_src x n, row s holding the depths from srcs[s]
+ * (the values of n_src ghb_bfs calls). */
 int ghb_msbfs(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, const int32_t* out_col,
               const int32_t* in_rowptr, const int32_t* in_col, const int32_t* srcs,
               int32_t n_src, int32_t* depth, ghb_traversal_stats* stats);

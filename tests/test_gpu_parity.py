@@ -278,3 +278,70 @@ def test_batch_wcc_and_tc(G):
         ref = O.tc(og)
         assert np.array_equal(c64[a:b].astype(np.int32), ref)
         assert totals[i] == int(ref.astype(np.int64).sum()) // 18
+
+
+@pytest.mark.parametrize("count", [1, 64, 65, 130, 256, 300])
+def test_msbfs_word_widths(G, count):
+    """Passes of 64, 128 and 256 sources (1, 2 and 4 words per vertex), a
+    second pass past 256, duplicates and isolated sources; raw CSR and the
+    relabelled handle, directed and undirected; a star hub so that pull rows
+    go to the block-per-row path."""
+    import ctypes
+    for directed in (False, True):
+        og = O.rmat_graph(11, 8, 13 + count, directed=directed)
+        if not directed:
+            # Add a hub adjacent to 1500 vertices (rows of > 256 entries).
+            s, d = O.rmat_edges(11, 8 << 11, 13 + count)
+            hub = np.full(1500, 5, np.int32)
+            leaves = np.arange(200, 1700, dtype=np.int32)
+            og = O.make_graph(1 << 11, np.concatenate([s, hub]), np.concatenate([d, leaves]), False)
+        g = to_gpu(G, og)
+        rng = np.random.default_rng(count)
+        srcs = rng.integers(0, og.n, count).astype(np.int32)
+        if count > 2:
+            srcs[1] = srcs[0]
+        deg = np.diff(og.rowptr) + (np.diff(og.in_rowptr) if directed else 0)
+        iso = np.nonzero(deg == 0)[0]
+        if iso.size and count > 3:
+            srcs[2] = iso[0]
+        d = torch.empty(count * og.n, dtype=torch.int32, device="cuda")
+        st = G.TraversalStats()
+        irp, icol = (g.in_rowptr, g.in_col) if directed else (g.rowptr, g.col)
+        G._check(G.lib().ghb_msbfs(G._ws(None), og.n, G._ptr(g.rowptr), G._ptr(g.col), G._ptr(irp), G._ptr(icol),
+                                   G._ptr(torch.from_numpy(srcs).cuda()), count, G._ptr(d), ctypes.byref(st)),
+                 "ghb_msbfs")
+        d = d.cpu().numpy().reshape(count, og.n)
+        rg = G.ResidentGraph(g)
+        dr, _ = rg.msbfs(srcs)
+        dr = dr.cpu().numpy()
+        check = set(range(0, count, 17)) | {0, 1, 2, count - 1}
+        if count > 255:
+            check |= {63, 64, 127, 128, 255, 256}
+        for i in sorted(check):
+            if i < count:
+                ref = O.bfs(og, int(srcs[i]))
+                assert np.array_equal(d[i], ref), (directed, i)
+                assert np.array_equal(dr[i], ref), (directed, i)
+        rg.close()
+
+
+@pytest.mark.parametrize("count", [3, 100, 200])
+def test_msbfs_long_diameter(G, count):
+    """A grid (about 70 levels): depths leave the kept level words in many
+    chunks, on the raw CSR and on the relabelled handle."""
+    import ctypes
+    og = O.grid_graph(30, 40, 1)
+    g = to_gpu(G, og)
+    srcs = np.random.default_rng(count).integers(0, og.n, count).astype(np.int32)
+    d = torch.empty(count * og.n, dtype=torch.int32, device="cuda")
+    st = G.TraversalStats()
+    G._check(G.lib().ghb_msbfs(G._ws(None), og.n, G._ptr(g.rowptr), G._ptr(g.col), G._ptr(g.rowptr), G._ptr(g.col),
+                               G._ptr(torch.from_numpy(srcs).cuda()), count, G._ptr(d), ctypes.byref(st)), "ghb_msbfs")
+    d = d.cpu().numpy().reshape(count, og.n)
+    rg = G.ResidentGraph(g)
+    dr = rg.msbfs(srcs)[0].cpu().numpy()
+    for i in sorted({0, count // 2, count - 1}):
+        ref = O.bfs(og, int(srcs[i]))
+        assert np.array_equal(d[i], ref)
+        assert np.array_equal(dr[i], ref)
+    rg.close()
