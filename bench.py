@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--sources", type=int, default=64)
     ap.add_argument("--extras", type=int, default=1, help="also measure the other algorithms")
     ap.add_argument("--cpu-sample", type=int, default=1, help="number of BFS sources in the CPU baseline")
+    ap.add_argument("--only", default=None,
+                    choices=["bfs", "sssp", "wcc", "pr", "pr64", "cdlp", "tc", "msbfs64", "msbfs256"],
+                    help="profiling driver: run one algorithm --warmup + --steps times on the RMAT graph of "
+                         "--scale and print its mean time (not a bench line)")
     return ap.parse_args()
 
 
@@ -552,8 +556,46 @@ def run_reference(args, world, rank):
     }
 
 
+def run_only(args):
+    """One algorithm on the seeded RMAT graph of --scale: the small cases that
+    the committed ncu summaries capture (kernel names are filtered by ncu)."""
+    import torch
+
+    import graphhet_b200 as G
+    g = G.rmat_graph(args.scale, args.edge_factor, args.seed)
+    rg = G.ResidentGraph(g)
+    srcs = pick_sources(g.rowptr.cpu().numpy(), 256, args.seed)
+    n = g.n
+    i32 = torch.empty(n, dtype=torch.int32, device="cuda")
+    f64 = torch.empty(n, dtype=torch.float64, device="cuda")
+    big = None
+    if args.only.startswith("msbfs"):
+        big = torch.empty(256 * n, dtype=torch.int32, device="cuda")
+    calls = {
+        "bfs": lambda i: rg.bfs(srcs[i % len(srcs)], out=i32),
+        "sssp": lambda i: rg.sssp(srcs[i % len(srcs)], out=f64),
+        "wcc": lambda i: rg.wcc(out=i32),
+        "pr": lambda i: rg.pagerank(10, 0.85, precision=G.PR_FP32_KAHAN, out=f64),
+        "pr64": lambda i: rg.pagerank(10, 0.85, precision=G.PR_FP64, out=f64),
+        "cdlp": lambda i: rg.cdlp(10, out=i32),
+        "tc": lambda i: rg.tc(),
+        "msbfs64": lambda i: rg.msbfs(srcs[:64], out=big),
+        "msbfs256": lambda i: rg.msbfs(srcs[:256], out=big),
+    }
+    fn = calls[args.only]
+    for i in range(args.warmup):
+        fn(i)
+    torch.cuda.synchronize()
+    ms, _ = timed(lambda: [fn(i) for i in range(args.steps)])
+    return {"only": args.only, "scale": args.scale, "n": n, "m": g.m, "steps": args.steps,
+            "ms_per_call": round(ms / max(1, args.steps), 4)}
+
+
 def main():
     args = parse()
+    if args.only:
+        print(json.dumps(run_only(args)), flush=True)
+        return
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         out = run_reference(args, world, rank)

@@ -533,7 +533,7 @@ class ResidentGraph:
         st = TraversalStats()
         _check(lib().ghb_graph_msbfs(_ws(ws), self._h, _ptr(sd), len(sd), _ptr(depth), ctypes.byref(st)),
                "ghb_graph_msbfs")
-        return depth.view(len(sd), self.n), st.as_dict()
+        return depth[: len(sd) * self.n].view(len(sd), self.n), st.as_dict()
 
     def sssp(self, src, inf=DBL_MAX, delta=0.0, policy=POLICY_HEURISTIC, trace=False, out=None, ws=None):
         """Distances and stats; with trace=True also the width-choice row

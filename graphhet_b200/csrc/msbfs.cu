@@ -17,8 +17,8 @@
 //         entries are finished by the whole warp, 32 entries a step; longer
 //         ones by a block each (ms_pull_hub_kernel), so the hubs that a
 //         degree-ordered graph puts side by side never serialise one warp.
-// Every level writes its new-bit words densely (front_new); the last
-// kMsChunk levels' words are kept, and every kMsChunk levels (and at the end)
+// Every level writes its new-bit words densely (front_new); the words of the
+// last chunk of levels are kept, and after every chunk (and at the end)
 // ms_flush_kernel turns them into depths, thread per output vertex in the
 // caller's ids, so a warp's stores to one source row cover 32 consecutive
 // vertices and a relabelled graph needs no separate mapping pass.  Each depth
@@ -41,7 +41,10 @@ struct MsCounters {
 };
 
 constexpr int32_t kMsWarpRest = 256;
-constexpr int kMsChunk = 8;  // levels of new-bit words kept between flushes
+// Levels of new-bit words kept between flushes: up to kMsChunkMax, fewer when
+// kMsMaskBudget bytes do not hold that many (n x W words each).
+constexpr int kMsChunkMax = 16;
+constexpr size_t kMsMaskBudget = size_t(8) << 30;
 
 __global__ void ms_init_kernel(int64_t words, uint64_t* seen, uint64_t* front, uint64_t* next) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < words; i += (int64_t)gridDim.x * blockDim.x) {
@@ -348,41 +351,44 @@ __global__ void __launch_bounds__(256) ms_pull_hub_kernel(const uint64_t* __rest
     }
 }
 
-// Depths of levels [l0, l1] (at most kMsChunk, kept in slot l % kMsChunk of
-// `masks`), thread per output vertex v in the caller's ids (internal id
-// p = perm[v], or v without perm).  The final flush also writes INT32_MAX
-// for every source bit that v never received.  Vertices p >= n_scan have no
-// entries: only level 0 (a source) can reach them.
+// Depths of levels [l0, l1] (at most `chunk`, level l kept in slot l % chunk
+// of `masks`), thread per output vertex v in the caller's ids (internal id
+// p = perm[v], or v without perm).  The level of each bit inside the chunk
+// is read from four bit-slices of the chunk's words (slice t ORs the levels
+// whose index has bit t).  The final flush also writes INT32_MAX for every
+// source bit that v never received.  Vertices p >= n_scan have no entries:
+// only level 0 (a source) can reach them.
 template <int W>
 __global__ void __launch_bounds__(256) ms_flush_kernel(int32_t n, int32_t n_scan, int32_t k,
                                                        const int32_t* __restrict__ perm,
-                                                       const uint64_t* __restrict__ masks, int32_t l0, int32_t l1,
-                                                       bool final_flush, const uint64_t* __restrict__ seen,
-                                                       int32_t* depth) {
+                                                       const uint64_t* __restrict__ masks, int32_t chunk, int32_t l0,
+                                                       int32_t l1, bool final_flush,
+                                                       const uint64_t* __restrict__ seen, int32_t* depth) {
     const int64_t slot = (int64_t)n * W;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         const int64_t p = perm ? perm[v] : v;
 #pragma unroll
         for (int w = 0; w < W; ++w) {
             if (w * 64 >= k) break;
-            uint64_t m[kMsChunk];
-            uint64_t any = 0;
-#pragma unroll
-            for (int i = 0; i < kMsChunk; ++i) {
-                const int32_t l = l0 + i;
-                m[i] = (l <= l1 && (p < n_scan || l == 0)) ? masks[(l % kMsChunk) * slot + p * W + w] : 0ull;
-                any |= m[i];
+            uint64_t any = 0, sl0 = 0, sl1 = 0, sl2 = 0, sl3 = 0;
+            for (int32_t l = l0; l <= l1; ++l) {
+                if (p >= n_scan && l > 0) break;
+                const uint64_t m = masks[(int64_t)(l % chunk) * slot + p * W + w];
+                const int i = l - l0;
+                any |= m;
+                sl0 |= (i & 1) ? m : 0ull;
+                sl1 |= (i & 2) ? m : 0ull;
+                sl2 |= (i & 4) ? m : 0ull;
+                sl3 |= (i & 8) ? m : 0ull;
             }
             const uint64_t unreached = final_flush ? ~seen[p * W + w] : 0ull;
             if (!(any | unreached)) continue;
             const int bmax = min(64, k - w * 64);
             for (int b = 0; b < bmax; ++b) {
-                int32_t d = -1;
-#pragma unroll
-                for (int i = 0; i < kMsChunk; ++i)
-                    if ((m[i] >> b) & 1ull) d = l0 + i;
-                if (d < 0 && ((unreached >> b) & 1ull)) d = kInfDepth;
-                if (d >= 0) depth[(int64_t)(w * 64 + b) * n + v] = d;
+                const int32_t d = l0 + (int32_t)((sl0 >> b) & 1ull) + 2 * (int32_t)((sl1 >> b) & 1ull) +
+                                  4 * (int32_t)((sl2 >> b) & 1ull) + 8 * (int32_t)((sl3 >> b) & 1ull);
+                if ((any >> b) & 1ull) depth[(int64_t)(w * 64 + b) * n + v] = d;
+                else if ((unreached >> b) & 1ull) depth[(int64_t)(w * 64 + b) * n + v] = kInfDepth;
             }
         }
     }
@@ -394,11 +400,13 @@ int msbfs_pass(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* ou
                const int32_t* perm, int32_t* depth, int64_t* levels_out, int64_t* examined_out) {
     cudaStream_t st = ws->stream;
     const int64_t words = (int64_t)n * W;
+    const int32_t chunk = (int32_t)std::max<int64_t>(
+        2, std::min<int64_t>(kMsChunkMax, (int64_t)(kMsMaskBudget / (size_t)(words * sizeof(uint64_t)))));
     Carver sizing(nullptr);
     auto carve = [&](Carver& c, uint64_t** seen, uint64_t** masks, uint64_t** next, int32_t** qa, int32_t** qb,
                      WalkBuffers* wb, MsCounters** cnt, uint64_t** all, int32_t** hubs) {
         *seen = c.take<uint64_t>(words);
-        *masks = c.take<uint64_t>(words * kMsChunk);
+        *masks = c.take<uint64_t>(words * chunk);
         *next = c.take<uint64_t>(words);
         *qa = c.take<int32_t>(n);
         *qb = c.take<int32_t>(n);
@@ -415,7 +423,7 @@ int msbfs_pass(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* ou
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
     carve(c, &seen, &masks, &next, &qa, &qb, &wb, &cnt, &all, &hubs);
-    auto slot = [&](int32_t l) { return masks + (int64_t)(l % kMsChunk) * words; };
+    auto slot = [&](int32_t l) { return masks + (int64_t)(l % chunk) * words; };
 
     const unsigned g = ws->num_sms * 8;
     // Source masks per word (built on the host: k is known here).
@@ -443,7 +451,7 @@ int msbfs_pass(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* ou
     int32_t *q_cur = qa, *q_new = qb;
     auto flush = [&](int32_t l1, bool final_flush) -> int {
         return launch(ws, ms_flush_kernel<W>, dim3(grid_for(n, 256, g)), dim3(256), 0, n, n_active, k, perm,
-                      (const uint64_t*)masks, flushed, l1, final_flush, (const uint64_t*)seen, depth);
+                      (const uint64_t*)masks, chunk, flushed, l1, final_flush, (const uint64_t*)seen, depth);
     };
     while (active > 0 && lvl < n) {
         ++lvl;
@@ -466,7 +474,7 @@ int msbfs_pass(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* ou
                            out_rp, seen, f_new, next, q_new, cnt));
         }
         // The next level overwrites slot lvl + 1: flush a full chunk first.
-        if ((lvl + 1) % kMsChunk == 0) {
+        if ((lvl + 1) % chunk == 0) {
             GHB_TRY(flush(lvl, false));
             flushed = lvl + 1;
         }
