@@ -446,10 +446,15 @@ def extras(args, G, g, rg, srcs, ws):
         ex["sssp_rule_ms_per_source"] = round(t_rule / 4, 3)
         ex["learned_vs_plain"] = round(t_h / t_l, 3)
         ex["batched_vs_plain"] = round((mr_sum / (ms / 1e3)) / (mr_sum / (t_h / 1e3)), 3)
-    # Batched sources (RMAT seed 3 scale 22, 256 sources): one 256-source
-    # pass (4 words per vertex) against 256 single-source traversals.
+    # PageRank precision: RMAT seed 11 scale 25 directed with ~10 % of the
+    # vertices dangling; FP32 ranks + Kahan rows (FP64 sink mass and L1)
+    # against the FP64 path, per iteration, and run to L1 change 1e-9.
     del rank, lab
     torch.cuda.empty_cache()
+    ex["pr_precision"] = pr_precision(G, hbm)
+    torch.cuda.empty_cache()
+    # Batched sources (RMAT seed 3 scale 22, 256 sources): one 256-source
+    # pass (4 words per vertex) against 256 single-source traversals.
     g22 = G.rmat_graph(22, 16, 3)
     bsrc = pick_sources(g22.rowptr.cpu().numpy(), 256, 3)
     gb = G.ResidentGraph(g22)
@@ -476,6 +481,12 @@ def extras(args, G, g, rg, srcs, ws):
     ex["batch256_vs_plain"] = round(t_single / ms256, 3)
     del ob, gb
     torch.cuda.empty_cache()
+    # Many small graphs (2,000 ER graphs, n log-uniform in [1k, 200k], mean
+    # degree uniform in [2, 32], seed 5) as one disjoint-union CSR: WCC + TC
+    # of all of them in one launch-only call, eager and replayed from a CUDA
+    # graph, against the per-graph entry points.
+    ex["batch_er2000"] = er_batch_section(G, ws)
+    torch.cuda.empty_cache()
     # 4096 x 4096 grid: BFS and SSSP from its centre
     gg = G.ResidentGraph(G.grid_graph(4096, 4096, weight_seed=args.seed))
     c = 2048 * 4096 + 2048
@@ -498,6 +509,100 @@ def extras(args, G, g, rg, srcs, ws):
         ex["regret_grid"] = {k: (round(v, 4) if isinstance(v, float) else {a: round(b, 3) for a, b in v.items()})
                              for k, v in r.items()}
     return ex
+
+
+def er_batch_section(G, ws, n_graphs=2000, seed=5):
+    import ctypes
+
+    import torch
+    t0 = time.time()
+    b = G.er_batch(n_graphs, seed)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    N, m = b.g.n, b.g.m
+    b.reserve(ws)
+    lab = torch.empty(N, dtype=torch.int32, device="cuda")
+    c64 = torch.empty(N, dtype=torch.int64, device="cuda")
+    tri = torch.empty(n_graphs, dtype=torch.int64, device="cuda")
+    b.wcc_tc(lab, c64, tri, ws=ws)
+    eager_ms, _ = timed(lambda: b.wcc_tc(lab, c64, tri, ws=ws), reps=3)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(graph, stream=side):
+            b.wcc_tc(lab, c64, tri, ws=ws)
+    graph.replay()
+    torch.cuda.synchronize()
+    graph_ms, _ = timed(lambda: graph.replay(), reps=3)
+    lab_u, tri_u = lab.clone(), tri.clone()
+    del graph
+    # Per-graph entry points (ghb_wcc, ghb_tc) on the same union arrays.
+    vb = b.vbase_host
+    rp_h = b.g.rowptr.cpu().numpy()
+    lab1 = torch.empty(N, dtype=torch.int32, device="cuda")
+    tot = ctypes.c_int64()
+    L = G.lib()
+    wsh = ws.handle
+
+    def per_graph():
+        tris = []
+        for g in range(n_graphs):
+            lo, hi = int(vb[g]), int(vb[g + 1])
+            rp_l = b.g.rowptr[lo:hi + 1] - int(rp_h[lo])
+            col_l = b.g.col[int(rp_h[lo]):int(rp_h[hi])] - lo
+            G._check(L.ghb_wcc(wsh, hi - lo, G._ptr(rp_l), G._ptr(col_l), G._ptr(lab1[lo:hi])), "ghb_wcc")
+            G._check(L.ghb_tc(wsh, hi - lo, G._ptr(rp_l), G._ptr(col_l), None, None, ctypes.byref(tot)), "ghb_tc")
+            tris.append(tot.value)
+        return tris
+    per_ms, tris = timed(per_graph)
+    same = bool(torch.equal(lab1, lab_u)) and tris == tri_u.cpu().tolist()
+    return {"workload": f"{n_graphs} Erdos-Renyi graphs, n log-uniform [1k, 200k], mean degree U[2, 32], seed {seed}",
+            "n_total": N, "m_total": m, "build_s": round(build_s, 2), "union_eager_ms": round(eager_ms, 2),
+            "union_cuda_graph_ms": round(graph_ms, 2), "per_graph_calls_ms": round(per_ms, 1),
+            "speedup_vs_per_graph": round(per_ms / graph_ms, 2), "identical_to_per_graph": same,
+            "edges_per_s_union": round(m / (graph_ms / 1e3) / 1e9, 3)}
+
+
+def pr_precision(G, hbm, scale=25, seed=11, fraction=0.1):
+    import torch
+    gp = G.rmat_dangling_graph(scale, 16, seed, fraction)
+    n, m = gp.n, gp.m
+    outdeg = gp.rowptr[1:] - gp.rowptr[:-1]
+    indeg = torch.bincount(gp.col.long(), minlength=n)
+    sinks = int(((outdeg == 0) & (indeg > 0)).sum())
+    touched = int(((outdeg > 0) | (indeg > 0)).sum())
+    rp = G.ResidentGraph(gp)
+    del gp, outdeg, indeg
+    torch.cuda.empty_cache()
+    r32 = torch.empty(n, dtype=torch.float64, device="cuda")
+    r64 = torch.empty(n, dtype=torch.float64, device="cuda")
+    rel, mx = [], []
+    for it in range(1, 21):
+        rp.pagerank(it, 0.85, precision=G.PR_FP32_KAHAN, out=r32)
+        rp.pagerank(it, 0.85, precision=G.PR_FP64, out=r64)
+        d = (r32 - r64).abs()
+        rel.append(float(d.sum() / r64.abs().sum()))
+        mx.append(float(d.max()))
+    out = {"workload": f"RMAT scale {scale} edge factor 16 seed {seed}, directed, out-edges of ~{fraction:.0%} of "
+                       f"the vertices dropped", "n": n, "m": m, "sinks_with_in_edges": sinks,
+           "vertices_with_edges": touched}
+    bytes_it = {"fp32_kahan": 4 * (n + 1) + 4 * m + 8 * n, "fp64": 4 * (n + 1) + 4 * m + 16 * n}
+    for prec, name in ((G.PR_FP32_KAHAN, "fp32_kahan"), (G.PR_FP64, "fp64")):
+        ms, _ = timed(lambda: rp.pagerank(20, 0.85, precision=prec, out=r32), reps=2)
+        out[f"{name}_ms_per_iter"] = round(ms / 20, 4)
+        out[f"{name}_gbs"] = round(bytes_it[name] / (ms / 20 / 1e3) / 1e9, 1)
+        out[f"{name}_frac_hbm"] = round(bytes_it[name] / (ms / 20 / 1e3) / 1e9 / hbm, 4)
+    out["rel_l1_vs_fp64_per_iter"] = [float("%.3e" % x) for x in rel]
+    out["max_abs_vs_fp64_per_iter"] = [float("%.3e" % x) for x in mx]
+    _, i32, h32 = rp.pagerank(1000, 0.85, precision=G.PR_FP32_KAHAN, tolerance=1e-9, l1_history=True, out=r32)
+    _, i64, h64 = rp.pagerank(1000, 0.85, precision=G.PR_FP64, tolerance=1e-9, l1_history=True, out=r64)
+    d = (r32 - r64).abs()
+    out["to_1e-9"] = {"fp32_kahan_iters": i32, "fp64_iters": i64, "rel_l1": float("%.3e" % float(d.sum() / r64.abs().sum())),
+                      "max_abs": float("%.3e" % float(d.max())), "fp32_kahan_last_l1": h32[-1] if h32 else None,
+                      "fp64_last_l1": h64[-1] if h64 else None}
+    rp.close()
+    return out
 
 
 def cpu_baseline_port(g, srcs):

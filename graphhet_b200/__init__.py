@@ -80,6 +80,7 @@ _SIGS = {
     "ghb_gen_grid": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
     "ghb_gen_er": (ctypes.c_int, [_p, _i32, _i64, _u64, _p, _p]),
     "ghb_gen_powerlaw": (ctypes.c_int, [_p, _i32, _i64, _f64, _u64, _p, _p]),
+    "ghb_gen_dangling_keep": (ctypes.c_int, [_p, _i64, _p, _u64, _f64, _p]),
     "ghb_csr_build": (ctypes.c_int, [_p, _i32, _p, _p, _p, _i64, _i32, _i32, _u64, _p, _p, _p,
                                      ctypes.POINTER(_i64)]),
     "ghb_csr_transpose": (ctypes.c_int, [_p, _i32, _i64, _p, _p, _p, _p, _p, _p]),
@@ -96,6 +97,8 @@ _SIGS = {
     "ghb_tc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p]),
     "ghb_batch_wcc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p]),
     "ghb_batch_tc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _p]),
+    "ghb_union_reserve": (ctypes.c_int, [_p, _i32, _i64]),
+    "ghb_union_wcc_tc": (ctypes.c_int, [_p, _i32, _p, _i32, _i64, _p, _p, _p, _p, _p]),
     "ghb_graph_create": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _p, ctypes.POINTER(_p)]),
     "ghb_graph_destroy": (ctypes.c_int, [_p]),
     "ghb_graph_info": (ctypes.c_int, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i32), ctypes.POINTER(_i64),
@@ -339,6 +342,65 @@ def rmat_graph(scale: int, edge_factor: int, seed: int, directed=False, a=0.57, 
     g = make_graph(1 << scale, src, dst, directed, weight_mode=weight_mode, weight_seed=seed, ws=ws)
     del src, dst
     return g
+
+
+def rmat_dangling_graph(scale: int, edge_factor: int, seed: int, fraction: float = 0.1, device=None,
+                        ws=None) -> CSRGraph:
+    """Directed RMAT(scale, edge_factor) whose seeded `fraction` of vertices
+    lose all out-edges (the PageRank precision workload), no weights."""
+    src, dst = gen_rmat(scale, edge_factor << scale, seed, 0.57, 0.19, 0.19, True, device=device, ws=ws)
+    keep = torch.empty(src.numel(), dtype=torch.uint8, device=src.device)
+    _check(lib().ghb_gen_dangling_keep(_ws(ws), src.numel(), _ptr(src), seed, fraction, _ptr(keep)),
+           "ghb_gen_dangling_keep")
+    k = keep.bool()
+    src, dst = src[k].contiguous(), dst[k].contiguous()
+    del keep, k
+    return make_graph(1 << scale, src, dst, True, weight_mode=WEIGHT_NONE, ws=ws)
+
+
+class UnionBatch:
+    """Many independent graphs as one disjoint-union CSR (ghb_union_*): graph
+    g owns global vertices [vbase[g], vbase[g+1])."""
+
+    def __init__(self, vbase, g: CSRGraph):
+        self.vbase = torch.as_tensor(vbase, dtype=torch.int64).to(g.rowptr.device)
+        self.vbase_host = self.vbase.cpu().numpy()
+        self.g = g
+        self.n_graphs = len(self.vbase_host) - 1
+
+    def reserve(self, ws=None):
+        _check(lib().ghb_union_reserve(_ws(ws), self.g.n, self.g.m), "ghb_union_reserve")
+
+    def wcc_tc(self, label=None, counts64=None, triangles=None, ws=None):
+        """Fills the given device tensors (label int32[n_total], counts64
+        int64[n_total], triangles int64[n_graphs]); launches only."""
+        _check(lib().ghb_union_wcc_tc(_ws(ws), self.n_graphs, _ptr(self.vbase), self.g.n, self.g.m,
+                                      _ptr(self.g.rowptr), _ptr(self.g.col) if self.g.m else None, _ptr(label),
+                                      _ptr(counts64), _ptr(triangles)), "ghb_union_wcc_tc")
+
+
+def er_batch(n_graphs: int, seed: int, n_lo: int = 1000, n_hi: int = 200000, deg_lo: float = 2.0,
+             deg_hi: float = 32.0, device=None, ws=None) -> UnionBatch:
+    """n_graphs Erdos-Renyi graphs, n log-uniform in [n_lo, n_hi], mean degree
+    uniform in [deg_lo, deg_hi] (edges = n * degree / 2, ghb_gen_er with seed
+    seed * 1000003 + g), symmetrised and deduplicated, as one union CSR."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), n_graphs)).astype(np.int64)
+    degs = rng.uniform(deg_lo, deg_hi, n_graphs)
+    es = (ns * degs / 2).astype(np.int64)
+    vbase = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+    ebase = np.concatenate([[0], np.cumsum(es)]).astype(np.int64)
+    d = _dev(device)
+    src = torch.empty(int(ebase[-1]), dtype=torch.int32, device=d)
+    dst = torch.empty(int(ebase[-1]), dtype=torch.int32, device=d)
+    for gi in range(n_graphs):
+        s, t = gen_er(int(ns[gi]), int(es[gi]), seed * 1000003 + gi, device=d, ws=ws)
+        src[ebase[gi]:ebase[gi + 1]] = s + int(vbase[gi])
+        dst[ebase[gi]:ebase[gi + 1]] = t + int(vbase[gi])
+    g = make_graph(int(vbase[-1]), src, dst, False, weight_mode=WEIGHT_NONE, ws=ws)
+    del src, dst
+    return UnionBatch(vbase, g)
 
 
 def grid_graph(rows: int, cols: int, weight_seed=0, device=None, ws=None) -> CSRGraph:

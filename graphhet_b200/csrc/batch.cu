@@ -16,6 +16,9 @@
 namespace ghb {
 
 int wcc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int32_t* label);
+size_t tc_oriented_bytes(int32_t n, int64_t m);
+int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* rowptr, const int32_t* col, void* base,
+                     unsigned long long* cnt, int64_t* counts64);
 int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
            int32_t* counts32, int64_t* total);
 int sssp_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, const double* w,
@@ -98,6 +101,49 @@ __global__ void bw_compress_local(int32_t ng, const int64_t* __restrict__ vbase,
     }
 }
 
+// Disjoint-union form: a warp per row of the union CSR (global ids).
+__global__ void __launch_bounds__(256) uw_link_kernel(int32_t n, const int32_t* __restrict__ rowptr,
+                                                      const int32_t* __restrict__ col, int32_t* parent) {
+    const int lane = lane_id();
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t u = warp; u < n; u += nwarps) {
+        const int32_t b = rowptr[u], e = rowptr[u + 1];
+        for (int32_t j = b + lane; j < e; j += 32) {
+            const int32_t v = col[j];
+            if (v > (int32_t)u) bw_unite(parent, (int32_t)u, v);  // symmetric: each edge once
+        }
+    }
+}
+
+// Triangles per graph: block per graph over its vertex range (fixed order).
+__global__ void __launch_bounds__(256) union_graph_totals_kernel(int32_t ng, const int64_t* __restrict__ vbase,
+                                                                 const unsigned long long* __restrict__ cnt,
+                                                                 int64_t* tri) {
+    __shared__ unsigned long long red[8];
+    for (int32_t g = blockIdx.x; g < ng; g += gridDim.x) {
+        unsigned long long s = 0;
+        for (int64_t v = vbase[g] + threadIdx.x; v < vbase[g + 1]; v += blockDim.x) s += cnt[v];
+        s = warp_sum(s);
+        if (lane_id() == 0) red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long t = 0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+            tri[g] = (int64_t)(t / 3);
+        }
+        __syncthreads();
+    }
+}
+
+size_t union_bytes(int32_t n, int64_t m) {
+    Carver c(nullptr);
+    c.take<int32_t>(n);                       // union-find forest
+    c.take<unsigned long long>((size_t)n + 1);  // triangles per vertex (+ total)
+    c.take<unsigned char>(tc_oriented_bytes(n, m));
+    return c.off;
+}
+
 }  // namespace
 }  // namespace ghb
 
@@ -157,6 +203,44 @@ int ghb_batch_tc(ghb_workspace* ws, int32_t n_graphs, const int64_t* vbase, cons
         GHB_TRY(tc_run(ws, (int32_t)ng, rowptr + vbase[g] + g, col ? col + ebase[g] : nullptr,
                        counts64 ? counts64 + vbase[g] : nullptr, nullptr, &t));
         if (totals) totals[g] = t;
+    }
+    return GHB_OK;
+}
+
+int ghb_union_reserve(ghb_workspace* ws, int32_t n_total, int64_t m) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    GHB_REQUIRE(n_total >= 1 && m >= 0 && m < (1ll << 31), "sizes out of range");
+    return ws_reserve(ws, union_bytes(n_total, m));
+}
+
+int ghb_union_wcc_tc(ghb_workspace* ws, int32_t n_graphs, const int64_t* vbase, int32_t n_total, int64_t m,
+                     const int32_t* rowptr, const int32_t* col, int32_t* label, int64_t* counts64,
+                     int64_t* triangles) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    GHB_REQUIRE(n_graphs >= 1 && n_total >= 1 && m >= 0 && m < (1ll << 31), "sizes out of range");
+    GHB_REQUIRE(vbase && rowptr && (m == 0 || col), "NULL argument");
+    GHB_REQUIRE(label || counts64 || triangles, "no output requested");
+    const size_t need = union_bytes(n_total, m);
+    GHB_REQUIRE(ws->scratch_cap >= need, "workspace scratch too small: call ghb_union_reserve first");
+    Carver c(ws->scratch);
+    int32_t* parent = c.take<int32_t>(n_total);
+    unsigned long long* cnt = c.take<unsigned long long>((size_t)n_total + 1);
+    void* tcbase = c.take<unsigned char>(tc_oriented_bytes(n_total, m));
+    const unsigned g = ws->num_sms * 8;
+    if (label) {
+        GHB_TRY(launch(ws, bw_iota, dim3(grid_for(n_total, 256, g)), dim3(256), 0, parent, (int64_t)n_total));
+        GHB_TRY(launch(ws, uw_link_kernel, dim3(grid_for((int64_t)n_total * 32, 256, g)), dim3(256), 0, n_total,
+                       rowptr, col, parent));
+        GHB_TRY(launch(ws, bw_compress_local, dim3(grid_for(n_total, 256, g)), dim3(256), 0, n_graphs, vbase,
+                       (int64_t)n_total, parent, label));
+    }
+    if (counts64 || triangles) {
+        GHB_TRY(tc_oriented_core(ws, n_total, m, rowptr, col, tcbase, cnt, counts64));
+        if (triangles)
+            GHB_TRY(launch(ws, union_graph_totals_kernel, dim3(std::min<int32_t>(n_graphs, ws->num_sms * 8)),
+                           dim3(256), 0, n_graphs, vbase, (const unsigned long long*)cnt, triangles));
     }
     return GHB_OK;
 }

@@ -80,6 +80,13 @@ __global__ void powerlaw_kernel(int scale, int64_t n_edges, double theta, uint64
     }
 }
 
+__global__ void keep_not_dangling_kernel(int64_t n_edges, const int32_t* __restrict__ src, uint64_t dstream,
+                                         uint32_t threshold, uint8_t* __restrict__ keep) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_edges;
+         e += (int64_t)gridDim.x * blockDim.x)
+        keep[e] = ghb_is_dangling(dstream, (uint32_t)src[e], threshold) ? 0 : 1;
+}
+
 }  // namespace
 }  // namespace ghb
 
@@ -126,6 +133,19 @@ int ghb_gen_er(ghb_workspace* ws, int32_t n, int64_t n_edges, uint64_t seed, int
     unsigned g = grid_for(n_edges, 256, ws->num_sms * 16);
     return launch(ws, er_kernel, dim3(g), dim3(256), 0, (uint32_t)n, n_edges,
                   ghb_stream(seed, GHB_PURPOSE_ER), src, dst);
+}
+
+int ghb_gen_dangling_keep(ghb_workspace* ws, int64_t n_edges, const int32_t* src, uint64_t seed, double fraction,
+                          uint8_t* keep) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    GHB_REQUIRE(n_edges >= 0, "n_edges < 0");
+    GHB_REQUIRE(fraction >= 0.0 && fraction <= 1.0, "fraction outside [0, 1]");
+    if (n_edges == 0) return GHB_OK;
+    GHB_REQUIRE(src && keep, "NULL argument");
+    const uint32_t threshold = fraction >= 1.0 ? 0xffffffffu : (uint32_t)(fraction * 4294967296.0);
+    return launch(ws, keep_not_dangling_kernel, dim3(grid_for(n_edges, 256, ws->num_sms * 16)), dim3(256), 0,
+                  n_edges, src, ghb_stream(seed, GHB_PURPOSE_DANGLING), threshold, keep);
 }
 
 int ghb_gen_powerlaw(ghb_workspace* ws, int32_t scale, int64_t n_edges, double exponent, uint64_t seed,

@@ -204,6 +204,49 @@ __global__ void tc_finish_kernel(int32_t n, const unsigned long long* __restrict
 
 }  // namespace
 
+// Oriented triangle counting with no host round trip and no allocation: the
+// caller guarantees a symmetric, loop-free CSR with strictly increasing rows
+// and m = rowptr[n] entries, and passes tc_oriented_bytes(n, m) bytes of
+// device scratch at `base`.  cnt (n + 1 entries, zeroed here) gets each
+// vertex's triangles and, with counts64, their sum in cnt[n]; counts64 (may
+// be NULL) gets the reference's 6x count.
+size_t tc_oriented_bytes(int32_t n, int64_t m) {
+    Carver c(nullptr);
+    WalkBuffers::carve(c, n);
+    c.take<int32_t>((size_t)n + 1);
+    c.take<int32_t>((size_t)n + 1);
+    c.take<int64_t>(scan_scratch_words(n));
+    c.take<int32_t>(m > 0 ? m : 1);
+    return c.off;
+}
+
+int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* rowptr, const int32_t* col, void* base,
+                     unsigned long long* cnt, int64_t* counts64) {
+    cudaStream_t st = ws->stream;
+    Carver c(base);
+    WalkBuffers wb = WalkBuffers::carve(c, n);
+    int32_t* keep = c.take<int32_t>((size_t)n + 1);
+    int32_t* orp = c.take<int32_t>((size_t)n + 1);
+    int64_t* bsums = c.take<int64_t>(scan_scratch_words(n));
+    int32_t* ocol = c.take<int32_t>(m > 0 ? m : 1);
+    GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * ((size_t)n + 1), st));
+    GHB_CUDA_TRY(cudaMemsetAsync(keep, 0, sizeof(int32_t) * n, st));
+    GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
+                 KeepCountVisitor{rowptr, keep}));
+    GHB_TRY(scan_exclusive_i32(ws, keep, orp, n, bsums));
+    GHB_TRY(launch(ws, orient_fill_kernel, dim3(grid_for((int64_t)n * 32, 256, ws->num_sms * 8)), dim3(256), 0, n,
+                   rowptr, col, (const int32_t*)orp, ocol));
+    GHB_TRY(launch(ws, orient_fill_long_kernel, dim3(ws->num_sms), dim3(1024), 0, n, rowptr, col, (const int32_t*)orp,
+                   ocol));
+    GHB_TRY(walk(ws, (const int32_t*)orp, (const int32_t*)ocol, (const int32_t*)nullptr, (const int32_t*)nullptr,
+                 (int64_t)n, (int64_t)n, wb, OrientedVisitor{orp, ocol, cnt}));
+    if (counts64)
+        GHB_TRY(launch(ws, tc_finish_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n,
+                       (const unsigned long long*)cnt, 6, counts64, (int32_t*)nullptr,
+                       (unsigned long long*)(cnt + n)));
+    return GHB_OK;
+}
+
 int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
            int32_t* counts32, int64_t* total) {
     cudaStream_t st = ws->stream;

@@ -81,6 +81,11 @@ int ghb_gen_er(ghb_workspace* ws, int32_t n, int64_t n_edges, uint64_t seed,
  * exponent in (2, 10).  Training graphs for the schedule policy. */
 int ghb_gen_powerlaw(ghb_workspace* ws, int32_t scale, int64_t n_edges, double exponent,
                      uint64_t seed, int32_t* src, int32_t* dst);
+/* keep[e] = 0 when src[e] is one of the seed's dangling vertices (about
+ * `fraction` of all ids, ghb_is_dangling), else 1: dropping those edges makes
+ * the PageRank precision workload's sinks. */
+int ghb_gen_dangling_keep(ghb_workspace* ws, int64_t n_edges, const int32_t* src, uint64_t seed,
+                          double fraction, uint8_t* keep);
 
 /* ----------------------------------------------------------- CSR builder */
 /* Build a CSR from an edge list (replaces the host flattening in toCSR,
@@ -326,6 +331,23 @@ int ghb_batch_wcc(ghb_workspace* ws, int32_t n_graphs, const int64_t* vbase,
 int ghb_batch_tc(ghb_workspace* ws, int32_t n_graphs, const int64_t* vbase,
                  const int64_t* ebase, const int32_t* rowptr, const int32_t* col,
                  int64_t* counts64, int64_t* totals);
+
+/* Disjoint-union batches: many graphs in one CSR whose graph g owns the
+ * global vertices [vbase[g], vbase[g+1]) (vbase: DEVICE int64, n_graphs + 1
+ * entries, vbase[0] = 0, vbase[n_graphs] = n_total), every row of it pointing
+ * into its own graph, symmetric, sorted, loop- and duplicate-free (what
+ * ghb_csr_build with SYMMETRIZE | DROP_SELF_LOOPS writes for an edge list of
+ * global ids), m = rowptr[n_total] < 2^31.  No counterpart in the reference
+ * (it runs one graph per call).
+ * ghb_union_reserve sizes the workspace once; ghb_union_wcc_tc then only
+ * launches kernels (no allocation, no host round trip), so a stream capture
+ * can record it.  label (local ids: smallest local id of the component),
+ * counts64 (the reference's 6x per-vertex triangle count) and triangles
+ * (per graph) are device arrays; any may be NULL. */
+int ghb_union_reserve(ghb_workspace* ws, int32_t n_total, int64_t m);
+int ghb_union_wcc_tc(ghb_workspace* ws, int32_t n_graphs, const int64_t* vbase, int32_t n_total,
+                     int64_t m, const int32_t* rowptr, const int32_t* col, int32_t* label,
+                     int64_t* counts64, int64_t* triangles);
 
 /* ------------------------------------------------------- schedule policy */
 /* The learned schedule policy: an MLP 12 -> 64 -> 64 (ReLU) -> 20 logits in

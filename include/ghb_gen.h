@@ -144,4 +144,10 @@ GHB_HD void ghb_er_edge(uint64_t stream, uint32_t n, uint64_t e, uint32_t* src, 
     *dst = (uint32_t)(((r & 0xFFFFFFFFULL) * (uint64_t)n) >> 32);
 }
 
+/* Dangling vertices for the PageRank precision workload: vertex v loses all
+ * its out-edges when a 32-bit draw of (seed, v) is below fraction * 2^32. */
+GHB_HD int ghb_is_dangling(uint64_t dstream, uint32_t v, uint32_t threshold) {
+    return (uint32_t)(ghb_draw(dstream, v) >> 32) < threshold;
+}
+
 #endif /* GHB_GEN_H */

@@ -48,6 +48,7 @@ def port() -> ctypes.CDLL:
             "orc_gen_rmat": (None, [ctypes.c_int, _i64, _u64, _f64, _f64, _f64, ctypes.c_int, _p, _p]),
             "orc_gen_grid": (None, [_i32, _i32, _p, _p]),
             "orc_gen_er": (None, [_i32, _i64, _u64, _p, _p]),
+            "orc_gen_dangling_keep": (None, [_i64, _p, _u64, ctypes.c_double, _p]),
             "orc_pair_weight": (_f64, [_u64, _i32, _i32, ctypes.c_int]),
             "orc_csr_build": (_i64, [_i32, _p, _p, _p, _i64, ctypes.c_int, ctypes.c_int, _u64, _p, _p, _p]),
             "orc_bfs": (None, [_i32, _p, _p, _i32, _i32, _p]),
@@ -90,6 +91,13 @@ def er_edges(n: int, n_edges: int, seed: int):
     dst = np.empty(max(1, n_edges), np.int32)
     port().orc_gen_er(n, n_edges, seed, _np_ptr(src), _np_ptr(dst))
     return src[:n_edges], dst[:n_edges]
+
+
+def dangling_keep(src, seed: int, fraction: float):
+    src = np.ascontiguousarray(src, np.int32)
+    keep = np.empty(max(1, src.size), np.uint8)
+    port().orc_gen_dangling_keep(src.size, _np_ptr(src), seed, fraction, _np_ptr(keep))
+    return keep[: src.size]
 
 
 def build_csr(n, src, dst, w=None, symmetrize=False, drop_self_loops=True, transpose=False,

@@ -72,6 +72,14 @@ ORC_API void orc_gen_er(int32_t n, int64_t n_edges, uint64_t seed, int32_t* src,
     }
 }
 
+/* keep[e] = 0 when src[e] is a dangling vertex of the seed (ghb_is_dangling). */
+ORC_API void orc_gen_dangling_keep(int64_t n_edges, const int32_t* src, uint64_t seed, double fraction,
+                                   uint8_t* keep) {
+    const uint32_t threshold = fraction >= 1.0 ? 0xffffffffu : (uint32_t)(fraction * 4294967296.0);
+    const uint64_t ds = ghb_stream(seed, GHB_PURPOSE_DANGLING);
+    for (int64_t e = 0; e < n_edges; ++e) keep[e] = ghb_is_dangling(ds, (uint32_t)src[e], threshold) ? 0 : 1;
+}
+
 ORC_API double orc_pair_weight(uint64_t seed, int32_t u, int32_t v, int mode) {
     return ghb_pair_weight(ghb_stream(seed, GHB_PURPOSE_WEIGHT), (uint32_t)u, (uint32_t)v, mode);
 }

@@ -345,3 +345,47 @@ def test_msbfs_long_diameter(G, count):
         assert np.array_equal(d[i], ref)
         assert np.array_equal(dr[i], ref)
     rg.close()
+
+
+def test_union_batch_wcc_tc_and_graph_capture(G):
+    """Many ER graphs as one disjoint-union CSR: WCC labels and triangle
+    counts equal the oracle's per graph; the launch-only call recorded in a
+    CUDA graph and replayed gives the same arrays."""
+    b = G.er_batch(25, 7, n_lo=50, n_hi=3000, deg_lo=1.0, deg_hi=12.0)
+    ws = G.Workspace()
+    b.reserve(ws)
+    N = b.g.n
+    lab = torch.empty(N, dtype=torch.int32, device="cuda")
+    c64 = torch.empty(N, dtype=torch.int64, device="cuda")
+    tri = torch.empty(b.n_graphs, dtype=torch.int64, device="cuda")
+    b.wcc_tc(lab, c64, tri, ws=ws)
+    torch.cuda.synchronize()
+    rp, col = b.g.rowptr.cpu().numpy(), b.g.col.cpu().numpy()
+    lab_h, c64_h, tri_h = lab.cpu().numpy(), c64.cpu().numpy(), tri.cpu().numpy()
+    vb = b.vbase_host
+    for g in range(b.n_graphs):
+        lo, hi = int(vb[g]), int(vb[g + 1])
+        lrp = (rp[lo:hi + 1] - rp[lo]).astype(np.int32)
+        lcol = (col[rp[lo]:rp[hi]] - lo).astype(np.int32)
+        og = O.Graph(n=hi - lo, rowptr=lrp, col=lcol, w=None, directed=False, in_rowptr=lrp, in_col=lcol, in_w=None)
+        assert np.array_equal(lab_h[lo:hi], O.wcc(og)), g
+        ref_tc = O.tc(og)
+        assert np.array_equal(c64_h[lo:hi].astype(np.int32), ref_tc), g
+        assert tri_h[g] * 18 == int(ref_tc.astype(np.int64).sum()), g
+    # Record the launch-only call in a CUDA graph and replay it twice.
+    lab2 = torch.full_like(lab, -1)
+    c642 = torch.full_like(c64, -1)
+    tri2 = torch.full_like(tri, -1)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(graph, stream=side):
+            b.wcc_tc(lab2, c642, tri2, ws=ws)
+    for _ in range(2):
+        lab2.fill_(-1)
+        graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(lab2, lab) and torch.equal(c642, c64) and torch.equal(tri2, tri)
+    del graph
+    ws.close()
