@@ -389,3 +389,24 @@ def test_union_batch_wcc_tc_and_graph_capture(G):
         assert torch.equal(lab2, lab) and torch.equal(c642, c64) and torch.equal(tri2, tri)
     del graph
     ws.close()
+
+
+def test_dangling_selection_matches_oracle_and_pagerank(G):
+    """The seeded dangling-vertex selection (PageRank precision workload) is
+    the same on the GPU and in the oracle, and PageRank on such a directed
+    graph meets the 1e-6 relative-L1 bar in both precisions."""
+    import ctypes
+    s, d = O.rmat_edges(12, 16 << 12, 11)
+    keep = torch.empty(len(s), dtype=torch.uint8, device="cuda")
+    G._check(G.lib().ghb_gen_dangling_keep(G._ws(None), len(s), G._ptr(torch.from_numpy(s).cuda()), 11, 0.1,
+                                           G._ptr(keep)), "ghb_gen_dangling_keep")
+    ref_keep = O.dangling_keep(s, 11, 0.1)
+    assert np.array_equal(keep.cpu().numpy(), ref_keep)
+    og = O.make_graph(1 << 12, s[ref_keep == 1], d[ref_keep == 1], True, weight_mode=0)
+    ref = O.pagerank(og, 20, 0.85)
+    g = G.rmat_dangling_graph(12, 16, 11, 0.1)
+    assert g.m == og.m
+    for prec in (G.PR_FP64, G.PR_FP32_KAHAN):
+        pr, _, _ = G.pagerank(g, 20, 0.85, precision=prec)
+        pr = pr.cpu().numpy()
+        assert np.abs(pr - ref).sum() / np.abs(ref).sum() <= 1e-6
