@@ -76,6 +76,8 @@ _SIGS = {
     "ghb_workspace_trim": (ctypes.c_int, [_p]),
     "ghb_workspace_counters": (ctypes.c_int, [_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "ghb_default_workspace": (_p, []),
+    "ghb_tune_set": (ctypes.c_int, [_p, ctypes.c_char_p, _i32]),
+    "ghb_tune_get": (ctypes.c_int, [_p, ctypes.c_char_p, ctypes.POINTER(_i32)]),
     "ghb_gen_rmat": (ctypes.c_int, [_p, _i32, _i64, _u64, _f64, _f64, _f64, _i32, _p, _p]),
     "ghb_gen_grid": (ctypes.c_int, [_p, _i32, _i32, _p, _p]),
     "ghb_gen_er": (ctypes.c_int, [_p, _i32, _i64, _u64, _p, _p]),
@@ -108,6 +110,7 @@ _SIGS = {
     "ghb_graph_bfs_pred": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p, _p]),
     "ghb_graph_msbfs": (ctypes.c_int, [_p, _p, _p, _i32, _p, _p]),
     "ghb_graph_sssp": (ctypes.c_int, [_p, _p, _i32, _f64, _p, _p, _p]),
+    "ghb_graph_mssssp": (ctypes.c_int, [_p, _p, _p, _i32, _f64, _p, _p]),
     "ghb_graph_sssp_pred": (ctypes.c_int, [_p, _p, _i32, _f64, _p, _p, _p, _p]),
     "ghb_graph_wcc": (ctypes.c_int, [_p, _p, _p]),
     "ghb_graph_pagerank": (ctypes.c_int, [_p, _p, _p, _p, _p]),
@@ -192,6 +195,20 @@ class Workspace:
             self.close()
         except Exception:
             pass
+
+
+TUNABLES = ("pr_cache_kb", "pr_threads", "pr_blocks_per_sm", "pr_short", "pr_chunk", "ms_warp_rest", "ms_pull_div")
+
+
+def tune_set(name: str, value: int, ws=None) -> None:
+    """Set a launch shape / threshold of the workspace (results do not change)."""
+    _check(lib().ghb_tune_set(_ws(ws), name.encode(), int(value)), "ghb_tune_set")
+
+
+def tune_get(name: str, ws=None) -> int:
+    v = _i32()
+    _check(lib().ghb_tune_get(_ws(ws), name.encode(), ctypes.byref(v)), "ghb_tune_get")
+    return v.value
 
 
 _default_ws: dict = {}
@@ -596,6 +613,15 @@ class ResidentGraph:
         _check(lib().ghb_graph_msbfs(_ws(ws), self._h, _ptr(sd), len(sd), _ptr(depth), ctypes.byref(st)),
                "ghb_graph_msbfs")
         return depth[: len(sd) * self.n].view(len(sd), self.n), st.as_dict()
+
+    def mssssp(self, srcs, inf=DBL_MAX, out=None, ws=None):
+        """Distances from every source (n_src x n), passes of up to 256."""
+        sd = torch.as_tensor(srcs, dtype=torch.int32, device=self._dev)
+        dist = out if out is not None else torch.empty(len(sd) * self.n, dtype=torch.float64, device=self._dev)
+        st = TraversalStats()
+        _check(lib().ghb_graph_mssssp(_ws(ws), self._h, _ptr(sd), len(sd), inf, _ptr(dist), ctypes.byref(st)),
+               "ghb_graph_mssssp")
+        return dist[: len(sd) * self.n].view(len(sd), self.n), st.as_dict()
 
     def sssp(self, src, inf=DBL_MAX, delta=0.0, policy=POLICY_HEURISTIC, trace=False, out=None, ws=None):
         """Distances and stats; with trace=True also the width-choice row

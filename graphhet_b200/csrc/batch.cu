@@ -1,4 +1,5 @@
-// Many independent graphs in one call, and multi-source SSSP.
+// Many independent graphs in one call; the multi-source SSSP entry point
+// (its engine is mssssp.cu).
 //
 // Batched graphs are packed back to back: graph g owns global vertices
 // [vbase[g], vbase[g+1]) and entries [ebase[g], ebase[g+1]) (int64 bases, so
@@ -21,8 +22,9 @@ int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* row
                      unsigned long long* cnt, int64_t* counts64);
 int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
            int32_t* counts32, int64_t* total);
-int sssp_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, const double* w,
-             int32_t src, double inf, double* dist_out, const ghb_sssp_options* opt, ghb_traversal_stats* stats);
+int mssssp_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* rp, const int32_t* col,
+               const double* wt, const int32_t* srcs_host, int32_t n_src, double delta, double inf,
+               const int32_t* perm, double* dist, ghb_traversal_stats* stats);
 
 namespace {
 
@@ -251,30 +253,16 @@ int ghb_mssssp(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_
     GHB_REQUIRE(ws, "no workspace");
     GHB_REQUIRE(n >= 1 && n_src >= 0, "bad sizes");
     GHB_REQUIRE(rowptr && dist && srcs, "NULL argument");
+    GHB_REQUIRE(inf >= 0, "inf must be >= 0");
     cudaStream_t st = ws->stream;
     std::vector<int32_t> hs(n_src > 0 ? n_src : 1);
     if (n_src > 0) {
         GHB_CUDA_TRY(cudaMemcpyAsync(hs.data(), srcs, sizeof(int32_t) * n_src, cudaMemcpyDeviceToHost, st));
         GHB_CUDA_TRY(cudaStreamSynchronize(st));
     }
-    double ms = 0;
-    int64_t examined = 0, levels = 0;
-    for (int32_t s = 0; s < n_src; ++s) {
-        ghb_traversal_stats one{};
-        GHB_TRY(sssp_run(ws, n, rowptr, col, w, hs[s], inf, dist + (int64_t)s * n, nullptr, stats ? &one : nullptr));
-        ms += one.device_ms;
-        examined += one.edges_examined;
-        levels += one.levels;
-    }
-    if (stats) {
-        stats->levels = (int32_t)levels;
-        stats->pull_levels = 0;
-        stats->reached = -1;
-        stats->edges_reached = -1;
-        stats->edges_examined = examined;
-        stats->device_ms = ms;
-    }
-    return GHB_OK;
+    for (int32_t i = 0; i < n_src; ++i) GHB_REQUIRE(hs[i] >= 0 && hs[i] < n, "source outside [0, n)");
+    if (n_src == 0) return GHB_OK;
+    return mssssp_run(ws, n, n, rowptr, col, w, hs.data(), n_src, 0.0, inf, nullptr, dist, stats);
 }
 
 }  // extern "C"

@@ -56,6 +56,20 @@ enum DeviceStatus : int32_t {
     kDevOverflow = 2,
 };
 
+// Launch shapes and thresholds, per workspace.  The defaults are the
+// autotuner's choices on B200 (graphhet_b200/autotune.py on RMAT scale 24
+// for PageRank, scales 22 and 24 for the multi-source BFS); ghb_tune_set
+// changes them for other graphs.
+struct Tuning {
+    int32_t pr_cache_kb = 144;     // PageRank hub cache: shared memory per block (KB)
+    int32_t pr_threads = 1024;     // threads of the persistent PageRank blocks
+    int32_t pr_blocks_per_sm = 1;  // persistent PageRank blocks per SM
+    int32_t pr_short = 64;         // rows up to this many entries: one thread per row
+    int32_t pr_chunk = 1024;       // longer rows: chunks of this many entries, warp per chunk
+    int32_t ms_warp_rest = 512;    // multi-source pull: longer rest of a row -> a block
+    int32_t ms_pull_div = 16;      // multi-source: pull when frontier entries > m / ms_pull_div
+};
+
 }  // namespace ghb
 
 // --------------------------------------------------------------- workspace
@@ -72,6 +86,7 @@ struct ghb_workspace {
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
     int64_t launches = 0;
+    ghb::Tuning tune;
 };
 
 namespace ghb {

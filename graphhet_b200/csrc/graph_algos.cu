@@ -35,6 +35,11 @@ static int graph_sssp_dispatch(ghb_workspace* ws, const ghb_graph* g, int32_t sr
     return sssp_run(ws, g->n, g->rowptr, g->col, g->w, src_new, inf, dnew, options, stats);
 }
 int wcc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int32_t* label);
+int wcc_afforest_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* rowptr, const int32_t* col,
+                     int32_t* label);
+int mssssp_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* rp, const int32_t* col,
+               const double* wt, const int32_t* srcs_host, int32_t n_src, double delta, double inf,
+               const int32_t* perm, double* dist, ghb_traversal_stats* stats);
 int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col, int32_t iterations,
              int32_t* labels, const int32_t* init_labels);
 int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
@@ -169,6 +174,27 @@ int ghb_graph_msbfs(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, 
     return GHB_OK;
 }
 
+int ghb_graph_mssssp(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src, double inf,
+                     double* dist, ghb_traversal_stats* stats) {
+    GRAPH_PRELUDE();
+    GHB_REQUIRE(srcs && dist && n_src >= 0, "bad arguments");
+    GHB_REQUIRE(g->weighted || g->m == 0, "graph has no weights");
+    GHB_REQUIRE(inf >= 0, "inf must be >= 0");
+    cudaStream_t st = ws->stream;
+    std::vector<int32_t> hs(n_src > 0 ? n_src : 1);
+    if (n_src > 0) {
+        GHB_CUDA_TRY(cudaMemcpyAsync(hs.data(), srcs, sizeof(int32_t) * n_src, cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    for (int32_t i = 0; i < n_src; ++i) {
+        GHB_REQUIRE(hs[i] >= 0 && hs[i] < g->n, "source outside [0, n)");
+        hs[i] = g->perm_host[hs[i]];
+    }
+    if (n_src == 0) return GHB_OK;
+    return mssssp_run(ws, g->n, g->n_active, g->rowptr, g->col, g->w, hs.data(), n_src, 0.0, inf,
+                      (const int32_t*)g->perm, dist, stats);
+}
+
 int ghb_graph_sssp(ghb_workspace* ws, const ghb_graph* g, int32_t src, double inf, double* dist,
                    const ghb_sssp_options* options, ghb_traversal_stats* stats) {
     GRAPH_PRELUDE();
@@ -204,8 +230,9 @@ int ghb_graph_wcc(ghb_workspace* ws, const ghb_graph* g, int32_t* label) {
     GHB_TRY(ws_reserve_stage(ws, 2 * sizeof(int32_t) * (size_t)g->n + 256));
     int32_t* lnew = static_cast<int32_t*>(ws->stage);
     int32_t* cmin = lnew + (((size_t)g->n + 63) & ~(size_t)63);
-    // Union-find over the relabelled graph's in-CSR (every edge once).
-    GHB_TRY(wcc_run(ws, g->n, g->in_rowptr, g->in_col, lnew));
+    // Afforest over the relabelled graph's all-CSR (symmetric: in then out
+    // neighbours; the CSR itself when undirected).
+    GHB_TRY(wcc_afforest_run(ws, g->n, g->n_active, g->all_rowptr, g->all_col, lnew));
     const unsigned gr = grid_for(g->n, 256, ws->num_sms * 8);
     GHB_TRY(launch(ws, fill_kernel, dim3(gr), dim3(256), 0, cmin, (int64_t)g->n, (int32_t)0x7fffffff));
     GHB_TRY(launch(ws, comp_min_kernel, dim3(gr), dim3(256), 0, g->n, (const int32_t*)lnew, (const int32_t*)g->iperm,

@@ -13,8 +13,9 @@
 //   pull: for each vertex v not yet seen by all sources, OR the frontier
 //         words of its in-neighbours, stopping once every missing source
 //         bit is found.  The first 16 entries are probed by the vertex's
-//         own thread (4 gathers in flight); rows with up to kMsWarpRest more
-//         entries are finished by the whole warp, 32 entries a step; longer
+//         own thread (4 gathers in flight); rows with up to ms_warp_rest
+//         more entries (a workspace tunable, 256 by default) are finished by
+//         the whole warp, 32 entries a step; longer
 //         ones by a block each (ms_pull_hub_kernel), so the hubs that a
 //         degree-ordered graph puts side by side never serialise one warp.
 // Every level writes its new-bit words densely (front_new); the words of the
@@ -40,7 +41,6 @@ struct MsCounters {
     unsigned long long examined;
 };
 
-constexpr int32_t kMsWarpRest = 256;
 // Levels of new-bit words kept between flushes: up to kMsChunkMax, fewer when
 // kMsMaskBudget bytes do not hold that many (n x W words each).
 constexpr int kMsChunkMax = 16;
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(256) ms_pull_kernel(int32_t n_scan, const uint
                                                       const int32_t* __restrict__ out_rp,
                                                       const uint64_t* __restrict__ front, uint64_t* seen,
                                                       uint64_t* front_new, int32_t* queue, int32_t* hubs,
-                                                      MsCounters* cnt) {
+                                                      MsCounters* cnt, int32_t warp_rest) {
     const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(256) ms_pull_kernel(int32_t n_scan, const uint
                 done = ms_covers<W>(acc, missing);
             }
             ex += (unsigned long long)(j - b);
-            if (!done && e - j > kMsWarpRest) {
+            if (!done && e - j > warp_rest) {
                 // Long row: a block of ms_pull_hub_kernel settles it.  Here
                 // it stays as it is (no new bits; front_new is rewritten there).
                 hubs[atomicAdd(&cnt->hubs, 1)] = (int32_t)v;
@@ -459,11 +459,11 @@ int msbfs_pass(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* ou
         uint64_t* f_new = slot(lvl);
         GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(MsCounters), st));
         // Pull when the frontier's out-entries are a large share of the graph.
-        const bool pull = can_pull && (double)m_f * 8.0 > (double)m;
+        const bool pull = can_pull && (double)m_f * (double)ws->tune.ms_pull_div > (double)m;
         if (pull) {
             GHB_TRY(launch(ws, ms_pull_kernel<W>, dim3(grid_for((int64_t)n_active, 256, g)), dim3(256), 0, n_active,
                            (const uint64_t*)all, in_rp, in_col, out_rp, (const uint64_t*)f_cur, seen, f_new, q_new,
-                           hubs, cnt));
+                           hubs, cnt, ws->tune.ms_warp_rest));
             GHB_TRY(launch(ws, ms_pull_hub_kernel<W>, dim3(ws->num_sms * 4), dim3(256), 0, (const uint64_t*)all, in_rp,
                            in_col, out_rp, (const uint64_t*)f_cur, seen, f_new, q_new, (const int32_t*)hubs, cnt));
         } else {

@@ -29,8 +29,6 @@
 namespace ghb {
 namespace {
 
-constexpr int32_t kPrShort = 32;   // rows up to this length are packed
-constexpr int32_t kPrChunk = 256;  // longer rows are cut into chunks of this many entries
 constexpr int kPrThreads = 256;
 
 template <class T>
@@ -147,18 +145,19 @@ __device__ __forceinline__ void block_partials(double sink, double l1, double* p
     }
 }
 
-// Shared-memory cache of the first kHubCacheBytes / sizeof(T) contributions.
+// Shared-memory cache of the first K contributions (K from the workspace's
+// pr_cache_kb, 192 KB by default).
 // On a degree-relabelled graph these are the hubs' (the top 32K vertices of
 // an RMAT scale-22 graph hold half of all entries), so about half of the
 // gathers are served from shared memory instead of L2 sectors.  The kernels
-// that use it run one persistent 1024-thread block per SM, so each SM fills
-// the cache once per launch.
+// that use it run persistent blocks (pr_threads x pr_blocks_per_sm per SM,
+// 1024 x 1 by default), so each block fills the cache once per launch.
 constexpr int kPrPersistThreads = 1024;
-constexpr int kHubCacheBytes = 192 * 1024;
 
 template <class T>
-__device__ __forceinline__ int32_t fill_hub_cache(T* cache, const T* __restrict__ contrib_old, int32_t n) {
-    const int32_t K = min((int32_t)(kHubCacheBytes / sizeof(T)), n);
+__device__ __forceinline__ int32_t fill_hub_cache(T* cache, const T* __restrict__ contrib_old, int32_t n,
+                                                  int32_t cache_elems) {
+    const int32_t K = min(cache_elems, n);
     for (int32_t i = threadIdx.x; i < K; i += blockDim.x) cache[i] = contrib_old[i];
     __syncthreads();
     return K;
@@ -170,7 +169,7 @@ __device__ __forceinline__ T gather(const T* cache, int32_t K, const T* __restri
     return u < K ? cache[u] : load_contrib<T>(contrib_old + u, pol);
 }
 
-// Rows of up to kPrShort entries: one thread per row, gathers four at a time
+// Rows of up to `short_max` entries: one thread per row, gathers four at a time
 // (independent loads), Kahan-summed in row order.  Longer rows are skipped
 // here (chunk path).
 template <class T>
@@ -178,16 +177,16 @@ __global__ void __launch_bounds__(kPrPersistThreads) pr_rows_short_kernel(
     int32_t n, const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col,
     const int32_t* __restrict__ outdeg, const T* __restrict__ contrib_old, const T* rank_old,
     T* rank_new, T* contrib_new, const PrScalars* sc, double damping, int track_l1, double* part_sink,
-    double* part_l1) {
+    double* part_l1, int32_t short_max, int32_t cache_elems) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* cache = reinterpret_cast<T*>(smem_raw);
-    const int32_t K = fill_hub_cache<T>(cache, contrib_old, n);
+    const int32_t K = fill_hub_cache<T>(cache, contrib_old, n, cache_elems);
     const uint64_t pol_stream = policy_evict_first();
     const uint64_t pol_keep = policy_evict_last();
     double sink = 0.0, l1 = 0.0;
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
         const int32_t b = in_rp[r], e = in_rp[r + 1];
-        if (e - b > kPrShort) continue;
+        if (e - b > short_max) continue;
         KSum<T> acc;
         for (int32_t j = b; j < e; j += 4) {
             int32_t u[4];
@@ -205,19 +204,20 @@ __global__ void __launch_bounds__(kPrPersistThreads) pr_rows_short_kernel(
     block_partials<T>(sink, l1, part_sink, part_l1, blockIdx.x);
 }
 
-__global__ void pr_long_flags_kernel(int32_t n, const int32_t* __restrict__ in_rp, int32_t* flag) {
+__global__ void pr_long_flags_kernel(int32_t n, const int32_t* __restrict__ in_rp, int32_t* flag, int32_t short_max) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
-        flag[v] = (in_rp[v + 1] - in_rp[v]) > kPrShort ? 1 : 0;
+        flag[v] = (in_rp[v + 1] - in_rp[v]) > short_max ? 1 : 0;
 }
 
 // Long rows in ascending order, and their chunk counts.
 __global__ void pr_long_compact_kernel(int32_t n, const int32_t* __restrict__ in_rp, const int32_t* __restrict__ flag,
-                                       const int32_t* __restrict__ pos, int32_t* long_rows, int32_t* nchunks) {
+                                       const int32_t* __restrict__ pos, int32_t* long_rows, int32_t* nchunks,
+                                       int32_t chunk) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         if (!flag[v]) continue;
         const int32_t i = pos[v];
         long_rows[i] = (int32_t)v;
-        nchunks[i] = (in_rp[v + 1] - in_rp[v] + kPrChunk - 1) / kPrChunk;
+        nchunks[i] = (in_rp[v + 1] - in_rp[v] + chunk - 1) / chunk;
     }
 }
 
@@ -229,16 +229,17 @@ __global__ void pr_chunk_rows_kernel(int32_t nlong, const int32_t* __restrict__ 
         for (int32_t c = chunk_prefix[i] + lane_id(); c < chunk_prefix[i + 1]; c += 32) chunk_row[c] = (int32_t)i;
 }
 
-// One warp per chunk of kPrChunk entries: a partial sum, four independent
+// One warp per chunk of `chunk` entries: a partial sum, four independent
 // 32-wide loads in flight per lane, hub contributions from shared memory.
 template <class T>
 __global__ void __launch_bounds__(kPrPersistThreads) pr_chunk_kernel(
     int32_t n, const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col,
     const int32_t* __restrict__ long_rows, const int32_t* __restrict__ chunk_prefix,
-    const int32_t* __restrict__ chunk_row, int32_t nchunks, const T* __restrict__ contrib_old, double* chunk_sum) {
+    const int32_t* __restrict__ chunk_row, int32_t nchunks, const T* __restrict__ contrib_old, double* chunk_sum,
+    int32_t chunk, int32_t cache_elems) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* cache = reinterpret_cast<T*>(smem_raw);
-    const int32_t K = fill_hub_cache<T>(cache, contrib_old, n);
+    const int32_t K = fill_hub_cache<T>(cache, contrib_old, n, cache_elems);
     const uint64_t pol_stream = policy_evict_first();
     const uint64_t pol_keep = policy_evict_last();
     const int lane = lane_id();
@@ -248,8 +249,8 @@ __global__ void __launch_bounds__(kPrPersistThreads) pr_chunk_kernel(
         const int32_t i = chunk_row[ch];
         const int32_t u = long_rows[i];
         const int32_t rb = in_rp[u], re = in_rp[u + 1];
-        const int32_t b = rb + (int32_t)(ch - chunk_prefix[i]) * kPrChunk;
-        const int32_t e = min(re, b + kPrChunk);
+        const int32_t b = rb + (int32_t)(ch - chunk_prefix[i]) * chunk;
+        const int32_t e = min(re, b + chunk);
         KSum<T> acc;
         for (int32_t j0 = b; j0 < e; j0 += 128) {
             int32_t x[4];
@@ -331,16 +332,21 @@ template <class T>
 int pagerank_impl(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int32_t* in_col,
                   const int32_t* out_rp, const ghb_pr_options* o, double* rank_out, int32_t* iters_run) {
     cudaStream_t st = ws->stream;
-    const unsigned grid_rows = ws->num_sms;  // persistent: one block per SM
+    const Tuning& tu = ws->tune;
+    const int32_t short_max = tu.pr_short, chunk = tu.pr_chunk;
+    const int pthreads = tu.pr_threads;
+    const size_t cache_bytes = (size_t)tu.pr_cache_kb * 1024;
+    const int32_t cache_elems = (int32_t)(cache_bytes / sizeof(T));
+    const unsigned grid_rows = ws->num_sms * tu.pr_blocks_per_sm;  // persistent blocks
     const unsigned grid_long = ws->num_sms * 2;
     const int nparts = grid_rows + grid_long;
     int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
     GHB_CUDA_TRY(cudaMemcpyAsync(hp, in_rp + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     GHB_CUDA_TRY(cudaStreamSynchronize(st));
     const int64_t m = hp[0];
-    // Upper bounds: long rows <= min(n, m / (kPrShort + 1)), chunks <= m / kPrChunk + long rows.
-    const int64_t max_long = std::min<int64_t>(n, m / (kPrShort + 1) + 1);
-    const int64_t max_chunks = m / kPrChunk + max_long + 1;
+    // Upper bounds: long rows <= min(n, m / (short_max + 1)), chunks <= m / chunk + long rows.
+    const int64_t max_long = std::min<int64_t>(n, m / (short_max + 1) + 1);
+    const int64_t max_chunks = m / chunk + max_long + 1;
     auto carve = [&](Carver& c, T** ra, T** rb, T** ca, T** cb, int32_t** outdeg, int32_t** flag, int32_t** pos,
                      int32_t** long_rows, int32_t** nch, int32_t** cpre, int32_t** crow, double** csum, int64_t** bs,
                      double** ps, double** pl, PrScalars** sc, double** hist) {
@@ -378,16 +384,16 @@ int pagerank_impl(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int3
     const double d = o->damping;
     const unsigned g = ws->num_sms * 8;
     GHB_CUDA_TRY(cudaFuncSetAttribute(pr_rows_short_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      kHubCacheBytes));
+                                      (int)cache_bytes));
     GHB_CUDA_TRY(cudaFuncSetAttribute(pr_chunk_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      kHubCacheBytes));
+                                      (int)cache_bytes));
     GHB_CUDA_TRY(cudaMemsetAsync(ps, 0, sizeof(double) * nparts, st));
     GHB_CUDA_TRY(cudaMemsetAsync(pl, 0, sizeof(double) * nparts, st));
     GHB_TRY(launch(ws, pr_init_kernel<T>, dim3(grid_rows), dim3(kPrThreads), 0, n, out_rp, outdeg, ra, ca, ps));
     GHB_TRY(launch(ws, pr_reduce_kernel, dim3(1), dim3(1024), 0, (const double*)ps, (const double*)pl, nparts, n, d,
                    sc, (double*)nullptr, 0, 0));
     // Long-row list (ascending) and its chunks.
-    GHB_TRY(launch(ws, pr_long_flags_kernel, dim3(grid_for(n, 256, g)), dim3(256), 0, n, in_rp, flag));
+    GHB_TRY(launch(ws, pr_long_flags_kernel, dim3(grid_for(n, 256, g)), dim3(256), 0, n, in_rp, flag, short_max));
     GHB_TRY(scan_exclusive_i32(ws, flag, pos, n, bs));
     GHB_CUDA_TRY(cudaMemcpyAsync(hp, pos + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     GHB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -395,7 +401,7 @@ int pagerank_impl(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int3
     int32_t nchunks = 0;
     if (nlong > 0) {
         GHB_TRY(launch(ws, pr_long_compact_kernel, dim3(grid_for(n, 256, g)), dim3(256), 0, n, in_rp,
-                       (const int32_t*)flag, (const int32_t*)pos, long_rows, nch));
+                       (const int32_t*)flag, (const int32_t*)pos, long_rows, nch, chunk));
         GHB_TRY(scan_exclusive_i32(ws, nch, cpre, nlong, bs));
         GHB_CUDA_TRY(cudaMemcpyAsync(hp, cpre + nlong, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         GHB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -408,13 +414,13 @@ int pagerank_impl(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int3
     const bool track = o->tolerance > 0 || o->l1_history != nullptr;
     int it = 0;
     for (; it < o->iterations; ++it) {
-        GHB_TRY(launch(ws, pr_rows_short_kernel<T>, dim3(grid_rows), dim3(kPrPersistThreads), (size_t)kHubCacheBytes,
-                       n, in_rp, in_col, (const int32_t*)outdeg, (const T*)c_cur, (const T*)r_cur, r_nxt, c_nxt,
-                       (const PrScalars*)sc, d, track ? 1 : 0, ps, pl));
+        GHB_TRY(launch(ws, pr_rows_short_kernel<T>, dim3(grid_rows), dim3(pthreads), cache_bytes, n, in_rp, in_col,
+                       (const int32_t*)outdeg, (const T*)c_cur, (const T*)r_cur, r_nxt, c_nxt, (const PrScalars*)sc, d,
+                       track ? 1 : 0, ps, pl, short_max, cache_elems));
         if (nlong > 0) {
-            GHB_TRY(launch(ws, pr_chunk_kernel<T>, dim3(ws->num_sms), dim3(kPrPersistThreads), (size_t)kHubCacheBytes,
-                           n, in_rp, in_col, (const int32_t*)long_rows, (const int32_t*)cpre, (const int32_t*)crow,
-                           nchunks, (const T*)c_cur, csum));
+            GHB_TRY(launch(ws, pr_chunk_kernel<T>, dim3(grid_rows), dim3(pthreads), cache_bytes, n, in_rp, in_col,
+                           (const int32_t*)long_rows, (const int32_t*)cpre, (const int32_t*)crow, nchunks,
+                           (const T*)c_cur, csum, chunk, cache_elems));
         }
         GHB_TRY(launch(ws, pr_long_finish_kernel<T>, dim3(grid_long), dim3(kPrThreads), 0, nlong,
                        (const int32_t*)long_rows, (const int32_t*)cpre, (const double*)csum, (const int32_t*)outdeg,

@@ -72,7 +72,98 @@ __global__ void wcc_compress_kernel(int32_t* parent, int32_t n) {
     }
 }
 
+// Afforest (Sutton, Ben-Nun and Barak, IPDPS 2018), for symmetric CSRs:
+// every vertex first links to its first kAffSample neighbours (on a
+// degree-relabelled graph those are hubs), the forest is compressed, the
+// largest component is found from a sample of labels, and only vertices
+// outside it link their remaining entries.  Skipping a giant-component
+// vertex's entries is safe because each such entry (u, v) with v outside the
+// giant component is also entry (v, u) of v's row, which is processed.
+constexpr int32_t kAffSample = 2;
+constexpr int kAffProbe = 1024;
+
+__global__ void aff_sample_kernel(int32_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                                  int32_t* parent) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t b = rowptr[v], e = min(rowptr[v + 1], b + kAffSample);
+        for (int32_t j = b; j < e; ++j)
+            if (col[j] != (int32_t)v) wcc_unite(parent, (int32_t)v, col[j]);
+    }
+}
+
+// The most frequent label among kAffProbe hashed vertices of [0, n_active)
+// (ties: the smaller label), by a bitonic sort in shared memory.
+__global__ void __launch_bounds__(kAffProbe) aff_giant_kernel(int32_t n_active, const int32_t* __restrict__ parent,
+                                                              int32_t* giant) {
+    __shared__ int32_t s[kAffProbe];
+    const int t = threadIdx.x;
+    const uint64_t h = (uint64_t)(t + 1) * 0x9E3779B97F4A7C15ull;
+    s[t] = n_active > 0 ? __ldcg(parent + (int64_t)((h >> 33) % (uint64_t)n_active)) : 0;
+    __syncthreads();
+    for (int size = 2; size <= kAffProbe; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const int o = t ^ stride;
+            if (o > t) {
+                const bool up = (t & size) == 0;
+                const int32_t a = s[t], b = s[o];
+                if ((a > b) == up) {
+                    s[t] = b;
+                    s[o] = a;
+                }
+            }
+            __syncthreads();
+        }
+    if (t == 0) {
+        int32_t bl = s[0], bc = 0, cl = s[0], cc = 0;
+        for (int i = 0; i < kAffProbe; ++i) {
+            if (s[i] == cl) ++cc;
+            else {
+                cl = s[i];
+                cc = 1;
+            }
+            if (cc > bc) {
+                bc = cc;
+                bl = cl;
+            }
+        }
+        *giant = bl;
+    }
+}
+
+struct UniteRestVisitor {
+    int32_t* parent;
+    const int32_t* rowptr;
+    const int32_t* giant;  // written by aff_giant_kernel before the walk
+    __device__ bool want_row(int32_t u) const { return __ldcg(parent + u) != __ldg(giant); }
+    __device__ void operator()(int32_t u, int32_t v, int32_t j) const {
+        if (j - rowptr[u] >= kAffSample && u != v) wcc_unite(parent, u, v);
+    }
+    __device__ void finish() const {}
+};
+
 }  // namespace
+
+// Symmetric CSR (every entry (u, v) also present as (v, u)) only.
+int wcc_afforest_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* rowptr, const int32_t* col,
+                     int32_t* label) {
+    Carver sizing(nullptr);
+    WalkBuffers::carve(sizing, n);
+    sizing.take<int32_t>(8);
+    GHB_TRY(ws_reserve(ws, sizing.off));
+    Carver c(ws->scratch);
+    WalkBuffers wb = WalkBuffers::carve(c, n);
+    int32_t* giant = c.take<int32_t>(8);
+    const unsigned g = grid_for(n, 256, ws->num_sms * 8);
+    GHB_TRY(launch(ws, iota_kernel, dim3(g), dim3(256), 0, label, n));
+    GHB_TRY(launch(ws, aff_sample_kernel, dim3(g), dim3(256), 0, n, rowptr, col, label));
+    GHB_TRY(launch(ws, wcc_compress_kernel, dim3(g), dim3(256), 0, label, n));
+    GHB_TRY(launch(ws, aff_giant_kernel, dim3(1), dim3(kAffProbe), 0, n_active, (const int32_t*)label, giant));
+    // The giant label is read on the device by the visitor (no round trip).
+    GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
+                 UniteRestVisitor{label, rowptr, (const int32_t*)giant}));
+    return launch(ws, wcc_compress_kernel, dim3(g), dim3(256), 0, label, n);
+}
 
 int wcc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int32_t* label) {
     Carver sizing(nullptr);

@@ -113,6 +113,50 @@ int ghb_workspace_destroy(ghb_workspace* ws) {
     return GHB_OK;
 }
 
+namespace {
+struct TuneField {
+    const char* name;
+    int32_t ghb::Tuning::*field;
+    int32_t lo, hi;
+};
+const TuneField kTuneFields[] = {
+    {"pr_cache_kb", &ghb::Tuning::pr_cache_kb, 0, 200},
+    {"pr_threads", &ghb::Tuning::pr_threads, 128, 1024},
+    {"pr_blocks_per_sm", &ghb::Tuning::pr_blocks_per_sm, 1, 8},
+    {"pr_short", &ghb::Tuning::pr_short, 4, 256},
+    {"pr_chunk", &ghb::Tuning::pr_chunk, 64, 4096},
+    {"ms_warp_rest", &ghb::Tuning::ms_warp_rest, 32, 1 << 20},
+    {"ms_pull_div", &ghb::Tuning::ms_pull_div, 1, 1024},
+};
+const TuneField* tune_field(const char* name) {
+    if (!name) return nullptr;
+    for (const TuneField& f : kTuneFields)
+        if (std::strcmp(f.name, name) == 0) return &f;
+    return nullptr;
+}
+}  // namespace
+
+int ghb_tune_set(ghb_workspace* ws, const char* name, int32_t value) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws, "no workspace");
+    const TuneField* f = tune_field(name);
+    GHB_REQUIRE(f, std::string("unknown tuning parameter: ") + (name ? name : "(null)"));
+    GHB_REQUIRE(value >= f->lo && value <= f->hi,
+                std::string(f->name) + " outside [" + std::to_string(f->lo) + ", " + std::to_string(f->hi) + "]");
+    if (f->field == &ghb::Tuning::pr_threads) GHB_REQUIRE(value % 32 == 0, "pr_threads must be a multiple of 32");
+    ws->tune.*(f->field) = value;
+    return GHB_OK;
+}
+
+int ghb_tune_get(ghb_workspace* ws, const char* name, int32_t* value) {
+    ws = ws_resolve(ws);
+    GHB_REQUIRE(ws && value, "NULL argument");
+    const TuneField* f = tune_field(name);
+    GHB_REQUIRE(f, std::string("unknown tuning parameter: ") + (name ? name : "(null)"));
+    *value = ws->tune.*(f->field);
+    return GHB_OK;
+}
+
 int ghb_workspace_set_stream(ghb_workspace* ws, void* stream) {
     ws = ws_resolve(ws);
     GHB_REQUIRE(ws != nullptr, "no workspace");

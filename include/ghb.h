@@ -62,6 +62,14 @@ int ghb_workspace_trim(ghb_workspace* ws);
 int ghb_workspace_counters(ghb_workspace* ws, int64_t* kernel_launches, int64_t* scratch_bytes);
 /* Process-wide workspace on the current device (used by the C++ wrappers). */
 ghb_workspace* ghb_default_workspace(void);
+/* Launch shapes and thresholds of this workspace (no counterpart in the
+ * reference): "pr_cache_kb" PageRank hub cache in shared memory, "pr_threads"
+ * and "pr_blocks_per_sm" its persistent blocks, "pr_short" / "pr_chunk" its
+ * row split, "ms_warp_rest" / "ms_pull_div" the multi-source BFS's block-row
+ * threshold and direction switch.  Results do not depend on them.  Unknown
+ * names and values outside the documented ranges are rejected. */
+int ghb_tune_set(ghb_workspace* ws, const char* name, int32_t value);
+int ghb_tune_get(ghb_workspace* ws, const char* name, int32_t* value);
 
 /* ------------------------------------------------------------ generators */
 /* Seeded synthetic inputs (include/ghb_gen.h).  Outputs are device arrays of
@@ -205,7 +213,10 @@ int ghb_sssp_pred(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
                   const double* in_w, int32_t src, double inf, double* dist, int32_t* pred,
                   const ghb_sssp_options* options, ghb_traversal_stats* stats);
 
-/* Many sources: dist is n_src x n. */
+/* Many sources: dist is n_src x n, row s the distances from srcs[s] (the
+ * values of n_src ghb_sssp calls).  Up to 256 sources share one bucketed
+ * traversal (a vertex's distances for all of them side by side); more run in
+ * passes of 256. */
 int ghb_mssssp(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col,
                const double* w, const int32_t* srcs, int32_t n_src, double inf, double* dist,
                ghb_traversal_stats* stats);
@@ -303,6 +314,8 @@ int ghb_graph_bfs_pred(ghb_workspace* ws, const ghb_graph* g, int32_t src, int32
                        ghb_traversal_stats* stats);
 int ghb_graph_msbfs(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
                     int32_t* depth, ghb_traversal_stats* stats);
+int ghb_graph_mssssp(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
+                     double inf, double* dist, ghb_traversal_stats* stats);
 int ghb_graph_sssp(ghb_workspace* ws, const ghb_graph* g, int32_t src, double inf, double* dist,
                    const ghb_sssp_options* options, ghb_traversal_stats* stats);
 int ghb_graph_sssp_pred(ghb_workspace* ws, const ghb_graph* g, int32_t src, double inf,
