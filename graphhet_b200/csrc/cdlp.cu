@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "edge_walk.cuh"
 
 namespace ghb {
 namespace {
@@ -54,6 +55,48 @@ __device__ __forceinline__ int32_t unpack_label(unsigned long long k) {
     return (int32_t)(0x7FFFFFFFu - (uint32_t)(k & 0xFFFFFFFFull));
 }
 
+// Insert label x (valid lanes) into an open-addressing table of `slots`
+// (power of two) entries, K = labels, C = counts.  Lanes of the warp holding
+// the same label are merged first (one atomic per distinct label per warp),
+// which matters once labels converge and a hub's row repeats a few labels.
+// Every lane of the warp must call it.
+__device__ __forceinline__ void table_insert_merged(int32_t* K, int32_t* C, uint32_t slots, int32_t x, bool valid) {
+    const unsigned act = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    const unsigned same = __match_any_sync(act, x);
+    if (lane_id() != __ffs(same) - 1) return;
+    uint32_t h = hash_label(x) & (slots - 1);
+    while (true) {
+        const int32_t k = atomicCAS(&K[h], kEmpty, x);
+        if (k == kEmpty || k == x) {
+            atomicAdd(&C[h], __popc(same));
+            return;
+        }
+        h = (h + 1) & (slots - 1);
+    }
+}
+
+// First iteration over labels that are all distinct, on rows without
+// repeated entries: every count is 1, so the new label is the smallest
+// neighbour label.  Lanes that share a row merge their minimum first.
+struct MinLabelVisitor {
+    const int32_t* lab;
+    int32_t* out;
+    __device__ bool want_row(int32_t) const { return true; }
+    __device__ void operator()(int32_t u, int32_t v, int32_t) const {
+        const int32_t x = lab[v];
+        const unsigned same = __match_any_sync(__activemask(), u);
+        const int32_t m = __reduce_min_sync(same, x);
+        if (lane_id() == __ffs(same) - 1) atomicMin(out + u, m);
+    }
+    __device__ void finish() const {}
+};
+
+__global__ void cdlp_fill_max_kernel(int32_t* p, int32_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = 0x7FFFFFFF;
+}
+
 __global__ void cdlp_count_classes_kernel(int32_t n, const int32_t* __restrict__ rp, int32_t* counts) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
          v += (int64_t)gridDim.x * blockDim.x) {
@@ -62,7 +105,7 @@ __global__ void cdlp_count_classes_kernel(int32_t n, const int32_t* __restrict__
         const unsigned same = __match_any_sync(__activemask(), c);
         const int leader = __ffs(same) - 1;
         if (lane_id() == leader) atomicAdd(&counts[c], __popc(same));
-        if (c == 8) atomicMax(&counts[15], d);
+        if (c == 8) atomicAdd(&counts[14], d);
     }
 }
 
@@ -168,17 +211,9 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_warp_kernel(
             C[s] = 0;
         }
         __syncwarp();
-        for (int32_t j = b + lane; j < e; j += 32) {
-            const int32_t x = lab[col[j]];
-            uint32_t h = hash_label(x) & (kWarpSlots - 1);
-            while (true) {
-                const int32_t k = atomicCAS(&K[h], kEmpty, x);
-                if (k == kEmpty || k == x) {
-                    atomicAdd(&C[h], 1);
-                    break;
-                }
-                h = (h + 1) & (kWarpSlots - 1);
-            }
+        for (int32_t j0 = b; j0 < e; j0 += 32) {
+            const int32_t j = j0 + lane;
+            table_insert_merged(K, C, kWarpSlots, j < e ? lab[col[j]] : 0, j < e);
         }
         __syncwarp();
         unsigned long long best = 0;
@@ -221,26 +256,21 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_block_kernel(
     for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
         const int32_t v = rows[i];
         const int32_t b = rp[v], e = rp[v + 1];
-        for (int s = threadIdx.x; s < kBlockSlots; s += blockDim.x) {
+        // Table of the next power of two >= 2 x the row (at most kBlockSlots).
+        uint32_t cap = 512;
+        while (cap < 2u * (uint32_t)(e - b) && cap < (uint32_t)kBlockSlots) cap <<= 1;
+        for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
             K[s] = kEmpty;
             C[s] = 0;
         }
         __syncthreads();
-        for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
-            const int32_t x = lab[col[j]];
-            uint32_t h = hash_label(x) & (kBlockSlots - 1);
-            while (true) {
-                const int32_t k = atomicCAS(&K[h], kEmpty, x);
-                if (k == kEmpty || k == x) {
-                    atomicAdd(&C[h], 1);
-                    break;
-                }
-                h = (h + 1) & (kBlockSlots - 1);
-            }
+        for (int32_t j0 = b; j0 < e; j0 += blockDim.x) {
+            const int32_t j = j0 + threadIdx.x;
+            table_insert_merged(K, C, cap, j < e ? lab[col[j]] : 0, j < e);
         }
         __syncthreads();
         unsigned long long best = 0;
-        for (int s = threadIdx.x; s < kBlockSlots; s += blockDim.x) {
+        for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
             const int32_t k = K[s];
             if (k != kEmpty) {
                 const unsigned long long key = pack_best((uint32_t)C[s], k);
@@ -252,36 +282,23 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_block_kernel(
     }
 }
 
-// One block per row of > 4096 entries; table in global memory, one region
-// of `region` slots per block, sized per row to the next power of two >= 2d.
+// One block per row of > 4096 entries (many blocks, round robin); each row
+// owns a table in global scratch at tab_off[i] (the next power of two >= 2 x
+// the row), left empty after use, so only the first call clears the pool.
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_global_kernel(
     const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
     const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out,
-    int32_t* table, int64_t region) {
+    int32_t* pool, const int64_t* __restrict__ tab_off) {
     __shared__ unsigned long long red[32];
-    int32_t* K = table + (int64_t)blockIdx.x * 2 * region;
-    int32_t* C = K + region;
     for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
         const int32_t v = rows[i];
         const int32_t b = rp[v], e = rp[v + 1];
-        uint32_t cap = 1;
-        while (cap < 2u * (uint32_t)(e - b)) cap <<= 1;
-        for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
-            K[s] = kEmpty;
-            C[s] = 0;
-        }
-        __syncthreads();
-        for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
-            const int32_t x = lab[col[j]];
-            uint32_t h = hash_label(x) & (cap - 1);
-            while (true) {
-                const int32_t k = atomicCAS(&K[h], kEmpty, x);
-                if (k == kEmpty || k == x) {
-                    atomicAdd(&C[h], 1);
-                    break;
-                }
-                h = (h + 1) & (cap - 1);
-            }
+        const uint32_t cap = (uint32_t)((tab_off[i + 1] - tab_off[i]) / 2);
+        int32_t* K = pool + tab_off[i];
+        int32_t* C = K + cap;
+        for (int32_t j0 = b; j0 < e; j0 += blockDim.x) {
+            const int32_t j = j0 + threadIdx.x;
+            table_insert_merged(K, C, cap, j < e ? lab[col[j]] : 0, j < e);
         }
         __syncthreads();
         unsigned long long best = 0;
@@ -290,6 +307,8 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_global_kernel(
             if (k != kEmpty) {
                 const unsigned long long key = pack_best((uint32_t)__ldcg(&C[s]), k);
                 best = key > best ? key : best;
+                K[s] = kEmpty;  // leave the table empty for the next iteration
+                C[s] = 0;
             }
         }
         best = block_max_u64(best, red);
@@ -297,14 +316,37 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_global_kernel(
     }
 }
 
+// Block per row: keys kEmpty, counts 0.
+__global__ void cdlp_pool_clear_kernel(int32_t* pool, const int64_t* __restrict__ tab_off, int32_t count) {
+    for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
+        const int64_t b = tab_off[i], half = (tab_off[i + 1] - b) / 2;
+        for (int64_t s = threadIdx.x; s < half; s += blockDim.x) {
+            pool[b + s] = kEmpty;
+            pool[b + half + s] = 0;
+        }
+    }
+}
+
+// Table sizes of the global-class rows: 2 x (next power of two >= 2 d) ints each.
+__global__ void cdlp_table_sizes_kernel(const int32_t* __restrict__ rows, int32_t count,
+                                        const int32_t* __restrict__ rp, int64_t* sizes) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = rows[i];
+        int64_t cap = 1;
+        while (cap < 2 * (int64_t)(rp[v + 1] - rp[v])) cap <<= 1;
+        sizes[i] = 2 * cap;
+    }
+}
+
 }  // namespace
 
 // init_labels (device, may be NULL = vertex ids): starting label values.
+// first_min: the rows repeat no entry and the starting labels are distinct,
+// so the first iteration is a minimum over each row's labels.
 int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col, int32_t iterations,
-             int32_t* labels, const int32_t* init_labels) {
+             int32_t* labels, const int32_t* init_labels, bool first_min) {
     cudaStream_t st = ws->stream;
-    // Largest row, for the global table region.
-    const unsigned grid_global = ws->num_sms;
+    const unsigned grid_global = ws->num_sms * 8;
     int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
 
     // Pass 1: class sizes.
@@ -323,30 +365,53 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
         cls[k] = hp[k];
         off[k + 1] = off[k] + cls[k];
     }
-    // Global-table region per block: the next power of two >= 2 * longest row.
-    int64_t region = 0;
-    if (cls[8] > 0) {
-        region = 1;
-        while (region < 2 * (int64_t)hp[15]) region <<= 1;
-    }
+    // Global-class tables: 2 x (next power of two >= 2 d) ints per row, so
+    // fewer than 8 ints per entry of those rows.
+    const int64_t pool_bound = cls[8] > 0 ? 8 * (int64_t)hp[14] + 16 : 1;
     Carver sizing(nullptr);
     sizing.take<int32_t>(16);
     sizing.take<int32_t>(16);
     sizing.take<int32_t>(n);
     sizing.take<int32_t>(n);
-    sizing.take<int32_t>(region > 0 ? 2 * region * grid_global : 1);
+    sizing.take<int32_t>(pool_bound);
+    sizing.take<int64_t>((size_t)cls[8] + 1);
+    WalkBuffers::carve(sizing, n);
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
     counts = c.take<int32_t>(16);
     int32_t* cursor = c.take<int32_t>(16);
     int32_t* rows = c.take<int32_t>(n);
     int32_t* other = c.take<int32_t>(n);
-    int32_t* table = c.take<int32_t>(region > 0 ? 2 * region * grid_global : 1);
+    int32_t* pool = c.take<int32_t>(pool_bound);
+    int64_t* tab_off = c.take<int64_t>((size_t)cls[8] + 1);
+    WalkBuffers wb = WalkBuffers::carve(c, n);
 
     for (int k = 0; k < kCdlpClasses; ++k) hp[k] = off[k];
     GHB_CUDA_TRY(cudaMemcpyAsync(cursor, hp, kCdlpClasses * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     GHB_TRY(launch(ws, cdlp_fill_classes_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n, rp,
                    cursor, rows));
+    if (cls[8] > 0) {
+        // Table offsets on the host (a few thousand rows), then an empty pool.
+        GHB_TRY(launch(ws, cdlp_table_sizes_kernel, dim3(grid_for(cls[8], 256, ws->num_sms)), dim3(256), 0,
+                       (const int32_t*)(rows + off[8]), cls[8], rp, tab_off));
+        std::vector<int64_t> sz((size_t)cls[8] + 1);
+        GHB_CUDA_TRY(cudaMemcpyAsync(sz.data(), tab_off, sizeof(int64_t) * cls[8], cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        int64_t acc = 0;
+        for (int32_t i = 0; i < cls[8]; ++i) {
+            const int64_t x = sz[i];
+            sz[i] = acc;
+            acc += x;
+        }
+        sz[cls[8]] = acc;
+        GHB_REQUIRE(acc <= pool_bound, "CDLP table pool bound");
+        GHB_CUDA_TRY(cudaMemcpyAsync(tab_off, sz.data(), sizeof(int64_t) * (cls[8] + 1), cudaMemcpyHostToDevice, st));
+        // Empty = kEmpty keys (0xffffffff) and zero counts; the offsets are
+        // even, so keys and counts are the two halves of each row's table.
+        GHB_TRY(launch(ws, cdlp_pool_clear_kernel, dim3(grid_for(cls[8], 1, grid_global)), dim3(256), 0, pool,
+                       (const int64_t*)tab_off, cls[8]));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));  // sz is read by the copy above
+    }
     if (init_labels)
         GHB_CUDA_TRY(cudaMemcpyAsync(labels, init_labels, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
     else
@@ -359,6 +424,14 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
     const unsigned g = ws->num_sms * 8;
     for (int it = 0; it < iterations; ++it) {
         const int32_t* R = rows;
+        if (it == 0 && first_min) {
+            GHB_TRY(launch(ws, cdlp_fill_max_kernel, dim3(grid_for(n, 256, g)), dim3(256), 0, nxt, n));
+            GHB_TRY(walk(ws, rp, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
+                         MinLabelVisitor{(const int32_t*)cur, nxt}));
+            if (cls[0]) GHB_TRY(launch(ws, cdlp_copy_kernel, dim3(grid_for(cls[0], 256, g)), dim3(256), 0, R + off[0], cls[0], (const int32_t*)cur, nxt));
+            std::swap(cur, nxt);
+            continue;
+        }
         if (cls[0]) GHB_TRY(launch(ws, cdlp_copy_kernel, dim3(grid_for(cls[0], 256, g)), dim3(256), 0, R + off[0], cls[0], (const int32_t*)cur, nxt));
         if (cls[1]) GHB_TRY(launch(ws, cdlp_small_kernel<2>, dim3(grid_for((int64_t)cls[1] * 2, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[1], cls[1], rp, col, (const int32_t*)cur, nxt));
         if (cls[2]) GHB_TRY(launch(ws, cdlp_small_kernel<4>, dim3(grid_for((int64_t)cls[2] * 4, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[2], cls[2], rp, col, (const int32_t*)cur, nxt));
@@ -367,7 +440,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
         if (cls[5]) GHB_TRY(launch(ws, cdlp_small_kernel<32>, dim3(grid_for((int64_t)cls[5] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[5], cls[5], rp, col, (const int32_t*)cur, nxt));
         if (cls[6]) GHB_TRY(launch(ws, cdlp_warp_kernel, dim3(grid_for((int64_t)cls[6] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[6], cls[6], rp, col, (const int32_t*)cur, nxt));
         if (cls[7]) GHB_TRY(launch(ws, cdlp_block_kernel, dim3(grid_for(cls[7], 1, ws->num_sms * 2)), dim3(kCdlpThreads), (size_t)(2 * kBlockSlots * sizeof(int32_t)), R + off[7], cls[7], rp, col, (const int32_t*)cur, nxt));
-        if (cls[8]) GHB_TRY(launch(ws, cdlp_global_kernel, dim3(grid_for(cls[8], 1, grid_global)), dim3(kCdlpThreads), 0, R + off[8], cls[8], rp, col, (const int32_t*)cur, nxt, table, region));
+        if (cls[8]) GHB_TRY(launch(ws, cdlp_global_kernel, dim3(grid_for(cls[8], 1, grid_global)), dim3(kCdlpThreads), 0, R + off[8], cls[8], rp, col, (const int32_t*)cur, nxt, pool, (const int64_t*)tab_off));
         std::swap(cur, nxt);
     }
     if (cur != labels)
@@ -386,5 +459,5 @@ extern "C" int ghb_cdlp(ghb_workspace* ws, int32_t n, const int32_t* all_rowptr,
     GHB_REQUIRE(n >= 1, "n must be >= 1");
     GHB_REQUIRE(all_rowptr && labels, "NULL argument");
     GHB_REQUIRE(iterations >= 0, "iterations < 0");
-    return cdlp_run(ws, n, all_rowptr, all_col, iterations, labels, nullptr);
+    return cdlp_run(ws, n, all_rowptr, all_col, iterations, labels, nullptr, false);
 }

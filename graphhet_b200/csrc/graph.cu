@@ -101,6 +101,18 @@ int dalloc(T** p, size_t count, int64_t* total) {
 
 // Relabel one CSR (rows and columns through perm), rows sorted, weights
 // carried along.
+// Sets *flag when a sorted row holds an entry twice (warp per row).
+__global__ void repeat_check_kernel(int32_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                                    int32_t* flag) {
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t v = warp; v < n; v += nwarps) {
+        const int32_t b = rp[v], e = rp[v + 1];
+        for (int32_t j = b + 1 + lane_id(); j < e; j += 32)
+            if (col[j] == col[j - 1]) *flag = 1;
+    }
+}
+
 int relabel_csr(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* rp, const int32_t* col, const double* w,
                 const int32_t* perm, int32_t* rp_out, int32_t* col_out, double* w_out) {
     if (m == 0) {
@@ -285,6 +297,16 @@ int ghb_graph_create(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr, co
     if (directed) GG_TRY(relabel_csr(ws, n, g->m_in, in_rowptr, in_col, in_w, g->perm, g->in_rowptr, g->in_col, g->in_w));
     GG_TRY(launch(ws, outdeg_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n,
                   (const int32_t*)g->rowptr, g->outdeg));
+    {
+        int32_t* flag = reinterpret_cast<int32_t*>(ws->dev_small);
+        GG_TRY(cudaMemsetAsync(flag, 0, sizeof(int32_t), st) == cudaSuccess ? GHB_OK : GHB_ERR_CUDA);
+        GG_TRY(launch(ws, repeat_check_kernel, dim3(grid_for((int64_t)n * 32, 256, ws->num_sms * 8)), dim3(256), 0, n,
+                      (const int32_t*)g->rowptr, (const int32_t*)g->col, flag));
+        GG_TRY(cudaMemcpyAsync(hp + 2, flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st) == cudaSuccess ? GHB_OK
+                                                                                                      : GHB_ERR_CUDA);
+        GG_TRY(cudaStreamSynchronize(st) == cudaSuccess ? GHB_OK : GHB_ERR_CUDA);
+        g->repeats = hp[2] != 0;
+    }
     if (directed) {
         GG_TRY(dalloc(&g->all_rowptr, (size_t)n + 1, &g->device_bytes));
         GG_TRY(dalloc(&g->all_col, (size_t)(g->m + g->m_in), &g->device_bytes));

@@ -13,6 +13,7 @@ struct ghb_graph {
     int32_t n_active = 0;    // vertices with at least one entry: new ids [0, n_active)
     bool directed = false;
     bool weighted = false;
+    bool repeats = false;    // some out-row holds an entry twice
     int device = 0;
     // perm[old] = new, iperm[new] = old.  New ids are ranked by total degree,
     // descending, ties by old id.

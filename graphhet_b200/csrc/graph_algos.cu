@@ -41,7 +41,7 @@ int mssssp_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* rp
                const double* wt, const int32_t* srcs_host, int32_t n_src, double delta, double inf,
                const int32_t* perm, double* dist, ghb_traversal_stats* stats);
 int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col, int32_t iterations,
-             int32_t* labels, const int32_t* init_labels);
+             int32_t* labels, const int32_t* init_labels, bool first_min);
 int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
            int32_t* counts32, int64_t* total);
 int pagerank_run(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int32_t* in_col, const int32_t* out_rp,
@@ -260,7 +260,9 @@ int ghb_graph_cdlp(ghb_workspace* ws, const ghb_graph* g, int32_t iterations, in
     int32_t* lnew = static_cast<int32_t*>(ws->stage);
     // Label values stay caller ids (iperm), so the smallest-label tie-break is
     // the caller's.
-    GHB_TRY(cdlp_run(ws, g->n, g->all_rowptr, g->all_col, iterations, lnew, g->iperm));
+    // Undirected without repeated entries: iperm is a permutation, so the
+    // first iteration is a row minimum.
+    GHB_TRY(cdlp_run(ws, g->n, g->all_rowptr, g->all_col, iterations, lnew, g->iperm, !g->directed && !g->repeats));
     return map_back_i32(ws, g, lnew, labels);
 }
 

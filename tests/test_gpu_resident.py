@@ -113,3 +113,47 @@ def test_resident_sssp_light_heavy_deltas(G):
     rg = G.ResidentGraph(to_gpu(G, og))
     for delta in (1.0, 37.0, 150.0, 5000.0):
         assert np.array_equal(rg.sssp(77, delta=delta)[0].cpu().numpy(), O.sssp(og, 77))
+
+
+def test_resident_cdlp_and_wcc_with_repeated_entries(G):
+    """A symmetric CSR whose rows repeat some entries (so label counts of 2
+    occur in the first CDLP iteration) and a directed graph: CDLP and WCC on
+    the handle equal the oracle's."""
+    rng = np.random.default_rng(4)
+    n = 300
+    s = rng.integers(0, n, 1200)
+    d = rng.integers(0, n, 1200)
+    keep = s != d
+    s, d = s[keep], d[keep]
+    # Symmetric rows with repeats: each undirected pair listed 1 or 2 times.
+    rows = [[] for _ in range(n)]
+    for a, b in zip(s, d):
+        k = 2 if (a + b) % 5 == 0 else 1
+        rows[a] += [b] * k
+        rows[b] += [a] * k
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    col = np.concatenate([np.sort(np.array(r, np.int32)) for r in rows if r]).astype(np.int32)
+    og = O.Graph(n=n, rowptr=rp, col=col, w=None, directed=False, in_rowptr=rp, in_col=col, in_w=None)
+    rg = G.ResidentGraph(to_gpu(G, og))
+    assert np.array_equal(rg.cdlp(10).cpu().numpy(), O.cdlp(og, 10))
+    assert np.array_equal(rg.wcc().cpu().numpy(), O.wcc(og))
+    og2 = O.rmat_graph(10, 8, 77, directed=True)
+    rg2 = G.ResidentGraph(to_gpu(G, og2))
+    assert np.array_equal(rg2.cdlp(10).cpu().numpy(), O.cdlp(og2, 10))
+    assert np.array_equal(rg2.wcc().cpu().numpy(), O.wcc(og2))
+
+
+def test_cdlp_rows_beyond_4096_entries(G):
+    """Rows of the global-table class (> 4096 entries): two star hubs of 6,000
+    and 9,000 leaves on an RMAT graph, raw CSR and handle, 10 iterations."""
+    s, d = O.rmat_edges(14, 8 << 14, 31)
+    s = np.concatenate([s, np.zeros(6000, np.int32), np.full(9000, 7, np.int32)])
+    d = np.concatenate([d, np.arange(100, 6100, dtype=np.int32), np.arange(3000, 12000, dtype=np.int32)])
+    og = O.make_graph(1 << 14, s, d, False, weight_mode=0)
+    assert np.diff(og.rowptr).max() > 4096
+    ref = O.cdlp(og, 10)
+    assert np.array_equal(G.cdlp(to_gpu(G, og), 10).cpu().numpy(), ref)
+    rg = G.ResidentGraph(to_gpu(G, og))
+    assert np.array_equal(rg.cdlp(10).cpu().numpy(), ref)
+    assert np.array_equal(rg.cdlp(3).cpu().numpy(), O.cdlp(og, 3))
