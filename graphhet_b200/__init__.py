@@ -119,8 +119,8 @@ _SIGS = {
     "ghb_policy_load": (ctypes.c_int, [_p, _p]),
     "ghb_policy_loaded": (ctypes.c_int, []),
     "ghb_mlp_forward": (ctypes.c_int, [_p, _p, _p, _p, _i32, _p]),
-    "ghb_mlp_grad": (ctypes.c_int, [_p, _p, _p, _p, _p, _i32, _p, ctypes.POINTER(ctypes.c_float)]),
-    "ghb_mlp_train": (ctypes.c_int, [_p, _p, _p, _p, _p, _i32, _i32, ctypes.c_float, _p]),
+    "ghb_mlp_grad": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _i32, _p, ctypes.POINTER(ctypes.c_float)]),
+    "ghb_mlp_train": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _i32, _i32, ctypes.c_float, _p]),
 }
 
 _lib = None
@@ -686,21 +686,23 @@ def mlp_forward(params: torch.Tensor, norm: torch.Tensor, x: torch.Tensor, ws=No
     return logits
 
 
-def mlp_grad(params: torch.Tensor, norm: torch.Tensor, x: torch.Tensor, y: torch.Tensor, ws=None):
-    """(gradient[6292], loss) of the summed per-head mean cross-entropy."""
+def mlp_grad(params: torch.Tensor, norm: torch.Tensor, x: torch.Tensor, y: torch.Tensor, weight=None, ws=None):
+    """(gradient[6292], loss) of the summed per-head weighted mean cross-entropy."""
     grad = torch.empty(POLICY_PARAMS, dtype=torch.float32, device=x.device)
     loss = ctypes.c_float()
     _check(lib().ghb_mlp_grad(_ws(ws), _ptr(params), _ptr(norm), _ptr(x.contiguous()), _ptr(y.contiguous()),
-                              x.shape[0], _ptr(grad), ctypes.byref(loss)), "ghb_mlp_grad")
+                              _ptr(weight.contiguous()) if weight is not None else None, x.shape[0], _ptr(grad),
+                              ctypes.byref(loss)), "ghb_mlp_grad")
     return grad, loss.value
 
 
 def mlp_train(params: torch.Tensor, norm: torch.Tensor, x: torch.Tensor, y: torch.Tensor, epochs: int,
-              lr: float = 3e-3, ws=None):
+              lr: float = 3e-3, weight=None, ws=None):
     """Full-batch Adam on the device; updates params in place, returns the loss per epoch."""
     hist = (ctypes.c_float * max(1, epochs))()
     _check(lib().ghb_mlp_train(_ws(ws), _ptr(params), _ptr(norm), _ptr(x.contiguous()), _ptr(y.contiguous()),
-                               x.shape[0], epochs, lr, ctypes.cast(hist, _p)), "ghb_mlp_train")
+                               _ptr(weight.contiguous()) if weight is not None else None, x.shape[0], epochs, lr,
+                               ctypes.cast(hist, _p)), "ghb_mlp_train")
     return list(hist)[:epochs]
 
 

@@ -81,7 +81,7 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
     int64_t n_f = 1, m_f = deg_src, m_r = deg_src, examined = 0, reached = 1;
     double deg2_f = (double)deg_src * deg_src, degmax_f = (double)deg_src;
     int level = 0, pull_levels = 0, dir = 0 /* 0 push, 1 pull */, prev_dir = 0;
-    float prev_ms = 0.f;
+    double nf_prev = 1.0;  // frontier size of the previous level (growth feature)
     int32_t *q_cur = B.queue_a, *q_next = B.queue_b;
     uint32_t *f_cur = B.front_a, *f_next = B.front_b;
     const int threads = 256;
@@ -129,7 +129,8 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
             dir = heur;
             if (policy == GHB_POLICY_LEARNED) {
                 float feat[GHB_TRACE_FEATURES];
-                bfs_features(feat, n, m_total, n_f, m_f, m_u, level, deg2_f, degmax_f, prev_dir, prev_ms);
+                bfs_features(feat, n, m_total, n_f, m_f, m_u, level, deg2_f, degmax_f, prev_dir, nf_prev,
+                             (double)(n - reached));
                 int d = 0, f = 0;
                 if (policy_pick_level(feat, &d, &f)) {
                     dir = d;
@@ -140,7 +141,8 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
         }
         float row[GHB_TRACE_COLS];
         if (opt->record_trace && level < opt->trace_cap) {
-            bfs_features(row, n, m_total, n_f, m_f, m_u, level, deg2_f, degmax_f, prev_dir, prev_ms);
+            bfs_features(row, n, m_total, n_f, m_f, m_u, level, deg2_f, degmax_f, prev_dir, nf_prev,
+                         (double)(n - reached));
             for (int k = GHB_TRACE_FEATURES; k < GHB_TRACE_COLS; ++k) row[k] = -1.f;
         }
 
@@ -171,6 +173,7 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
             m_f = (int64_t)hs->mf[L % 3];
             deg2_f = 0.0;
             degmax_f = (double)hs->dmax[L % 3];
+            nf_prev = (double)hs->tail[(L + 2) % 3];
             examined += (int64_t)hs->examined;
             m_r += (int64_t)hs->m_r;
             reached += (int64_t)hs->reached;
@@ -238,7 +241,7 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
             for (int k = 0; k < GHB_TRACE_COLS; ++k) opt->trace[(size_t)level * GHB_TRACE_COLS + k] = row[k];
         }
         prev_dir = dir;
-        prev_ms = ms;
+        nf_prev = (double)n_f;
         n_f = hc->tail;
         m_f = (int64_t)hc->m_f;
         deg2_f = (double)hc->deg2;

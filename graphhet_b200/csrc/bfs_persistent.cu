@@ -28,6 +28,11 @@
 
 namespace ghb {
 
+// Deferred top-down rows (>= kBigList entries): up to kBigChunkRows of them
+// are cut into kBigChunk-entry chunks spread over every warp of the grid.
+constexpr int32_t kBigChunkRows = 2047;  // 4 per thread of a 512-thread block, plus the total
+constexpr int32_t kBigChunk = 256;
+
 struct BfsRunState {
     unsigned bar_count;            // barrier arrivals (own cache line)
     unsigned pad_a[31];
@@ -191,7 +196,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
         st->t_prev = global_timer_ns();
         if (trace && trace_cap > 0)
             bfs_features(trace, (double)n, (double)m_total, 1.0, (double)ds, (double)(m_total - (int64_t)ds), 0,
-                         (double)ds * ds, (double)ds, 0, 0.f);
+                         (double)ds * ds, (double)ds, 0, 1.0, (double)n - 1.0);
     }
     if (!p_barrier(st)) return;
 
@@ -286,7 +291,8 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                     else if (dir == 1 && (double)nf_next < (double)n / beta) nd = 0;
                 }
                 bfs_features(s_feat, (double)n, (double)m_total, (double)nf_next, (double)mf_next, m_u, L + 1,
-                             (double)vd->d2[nslot], (double)vd->dmax[nslot], dir, ms);
+                             (double)vd->d2[nslot], (double)vd->dmax[nslot], dir, (double)n_f,
+                             (double)n - 1.0 - (double)(reached_prev + nf_next));
                 if (trace && L + 1 < trace_cap)
                     for (int k = 0; k < kPolIn; ++k) trace[(size_t)(L + 1) * GHB_TRACE_COLS + k] = s_feat[k];
                 s_dec[0] = nd;
@@ -411,25 +417,83 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
             __syncthreads();
             const int32_t nbig = s_nbig;
             if (nbig > 0) {
-                // Deferred rows: one block per row (round robin), except rows
-                // of kHugeList or more, which every thread of the grid strides.
-                for (int32_t r = blockIdx.x; r < nbig; r += gridDim.x) {
-                    const int32_t u = big[r];
-                    const int32_t rb = out_rp[u], re = out_rp[u + 1];
-                    if (re - rb >= kHugeList) continue;
-                    for (int32_t j = rb + threadIdx.x; j < re; j += blockDim.x)
-                        p_visit(out_col[j], visited, f_next, depth, next_depth, q_next, &st->nf[nslot], append, out_rp,
-                                acc);
-                    if (threadIdx.x == 0) acc.ex += (unsigned long long)(re - rb);
-                }
-                for (int32_t r = 0; r < nbig; ++r) {
-                    const int32_t u = big[r];
-                    const int32_t rb = out_rp[u], re = out_rp[u + 1];
-                    if (re - rb < kHugeList) continue;
-                    for (int64_t j = rb + gtid; j < re; j += gsize)
-                        p_visit(out_col[j], visited, f_next, depth, next_depth, q_next, &st->nf[nslot], append, out_rp,
-                                acc);
-                    if (gtid == 0) acc.ex += (unsigned long long)(re - rb);
+                if (nbig <= kBigChunkRows) {
+                    // Deferred rows cut into kBigChunk-entry chunks shared by
+                    // every warp of the grid: each block builds the chunk
+                    // prefix of the (few) rows in shared memory, a warp takes
+                    // chunks round robin and finds the row by binary search.
+                    __shared__ int32_t s_cpre[kBigChunkRows + 1];  // indices 0..nbig <= 2047
+                    __shared__ int32_t s_wsum[16];
+                    const int t = threadIdx.x;
+                    int32_t cnt4[4];
+                    int32_t tsum = 0;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int32_t r = 4 * t + q;
+                        int32_t c = 0;
+                        if (r < nbig) {
+                            const int32_t u = big[r];
+                            c = (out_rp[u + 1] - out_rp[u] + kBigChunk - 1) / kBigChunk;
+                        }
+                        cnt4[q] = c;
+                        tsum += c;
+                    }
+                    int32_t incl = tsum;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += x;
+                    }
+                    if (lane == 31) s_wsum[t >> 5] = incl;
+                    __syncthreads();
+                    int32_t wbase = 0;
+                    for (int i = 0; i < (t >> 5); ++i) wbase += s_wsum[i];
+                    int32_t run = wbase + incl - tsum;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int32_t r = 4 * t + q;
+                        if (r <= nbig) s_cpre[r] = run;
+                        run += cnt4[q];
+                    }
+                    __syncthreads();
+                    const int32_t nchunks = s_cpre[nbig];
+                    for (int64_t ch = warp; ch < nchunks; ch += nwarps) {
+                        int32_t lo = 0, hi = nbig - 1;
+                        while (lo < hi) {
+                            const int32_t mid = (lo + hi + 1) >> 1;
+                            if (s_cpre[mid] <= ch) lo = mid;
+                            else hi = mid - 1;
+                        }
+                        const int32_t u = big[lo];
+                        const int32_t rb = out_rp[u] + (int32_t)(ch - s_cpre[lo]) * kBigChunk;
+                        const int32_t re = min(out_rp[u + 1], rb + kBigChunk);
+                        for (int32_t j = rb + lane; j < re; j += 32)
+                            p_visit(out_col[j], visited, f_next, depth, next_depth, q_next, &st->nf[nslot], append,
+                                    out_rp, acc);
+                        if (lane == 0) acc.ex += (unsigned long long)(re - rb);
+                    }
+                } else {
+                    // Many deferred rows: one block per row (round robin),
+                    // except rows of kHugeList or more, which every thread of
+                    // the grid strides.
+                    for (int32_t r = blockIdx.x; r < nbig; r += gridDim.x) {
+                        const int32_t u = big[r];
+                        const int32_t rb = out_rp[u], re = out_rp[u + 1];
+                        if (re - rb >= kHugeList) continue;
+                        for (int32_t j = rb + threadIdx.x; j < re; j += blockDim.x)
+                            p_visit(out_col[j], visited, f_next, depth, next_depth, q_next, &st->nf[nslot], append,
+                                    out_rp, acc);
+                        if (threadIdx.x == 0) acc.ex += (unsigned long long)(re - rb);
+                    }
+                    for (int32_t r = 0; r < nbig; ++r) {
+                        const int32_t u = big[r];
+                        const int32_t rb = out_rp[u], re = out_rp[u + 1];
+                        if (re - rb < kHugeList) continue;
+                        for (int64_t j = rb + gtid; j < re; j += gsize)
+                            p_visit(out_col[j], visited, f_next, depth, next_depth, q_next, &st->nf[nslot], append,
+                                    out_rp, acc);
+                        if (gtid == 0) acc.ex += (unsigned long long)(re - rb);
+                    }
                 }
                 p_flush(acc, st, nslot, !append);
                 if (!p_barrier_block(st, decide)) return;

@@ -43,9 +43,11 @@ __global__ void dense_fwd_kernel(const float* __restrict__ A, int in, const floa
     }
 }
 
-// Softmax cross-entropy per head; dZ = (softmax - onehot) / count(head).
-__global__ void loss_kernel(const float* __restrict__ logits, const int32_t* __restrict__ y, int B,
-                            const float* __restrict__ head_count, float* __restrict__ dZ, float* __restrict__ loss) {
+// Softmax cross-entropy per head, weighted mean over the labelled rows:
+// dZ = w_b (softmax - onehot) / sum_w(head); wt NULL = weight 1.
+__global__ void loss_kernel(const float* __restrict__ logits, const int32_t* __restrict__ y,
+                            const float* __restrict__ wt, int B, const float* __restrict__ head_count,
+                            float* __restrict__ dZ, float* __restrict__ loss) {
     const int heads[4] = {0, 2, 4, 20};
     for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < B; b += (int64_t)gridDim.x * blockDim.x) {
         float l = 0.f;
@@ -60,7 +62,7 @@ __global__ void loss_kernel(const float* __restrict__ logits, const int32_t* __r
             for (int k = s; k < e; ++k) mx = fmaxf(mx, logits[b * kOut + k]);
             float den = 0.f;
             for (int k = s; k < e; ++k) den += expf(logits[b * kOut + k] - mx);
-            const float inv_n = 1.f / head_count[h];
+            const float inv_n = (wt ? wt[b] : 1.f) / head_count[h];
             for (int k = s; k < e; ++k) {
                 const float p = expf(logits[b * kOut + k] - mx) / den;
                 dZ[b * kOut + k] = (p - (k - s == lab ? 1.f : 0.f)) * inv_n;
@@ -131,11 +133,11 @@ __global__ void sum_kernel(const float* __restrict__ x, int n, float* out) {
     }
 }
 
-// Labelled samples per head (for the mean cross-entropy).
-__global__ void head_count_kernel(const int32_t* __restrict__ y, int B, float* count) {
+// Summed weight of the labelled rows per head (for the weighted mean).
+__global__ void head_count_kernel(const int32_t* __restrict__ y, const float* __restrict__ wt, int B, float* count) {
     if (threadIdx.x < 3 && blockIdx.x == 0) {
         float c = 0.f;
-        for (int b = 0; b < B; ++b) c += y[b * 3 + threadIdx.x] >= 0 ? 1.f : 0.f;
+        for (int b = 0; b < B; ++b) c += y[b * 3 + threadIdx.x] >= 0 ? (wt ? wt[b] : 1.f) : 0.f;
         count[threadIdx.x] = c;
     }
 }
@@ -172,11 +174,11 @@ int mlp_forward(ghb_workspace* ws, const MlpBuffers& m, const float* P, const fl
 
 // Forward + loss + backward into m.grad; loss total into m.lsum[0].
 int mlp_grad(ghb_workspace* ws, const MlpBuffers& m, const float* P, const float* norm, const float* x,
-             const int32_t* y, int B) {
+             const int32_t* y, const float* wt, int B) {
     const unsigned g = ws->num_sms * 4;
     GHB_TRY(mlp_forward(ws, m, P, norm, x, B));
-    GHB_TRY(launch(ws, head_count_kernel, dim3(1), dim3(32), 0, y, B, m.hc));
-    GHB_TRY(launch(ws, loss_kernel, dim3(grid_for(B, 256, g)), dim3(256), 0, (const float*)m.z3, y, B,
+    GHB_TRY(launch(ws, head_count_kernel, dim3(1), dim3(32), 0, y, wt, B, m.hc));
+    GHB_TRY(launch(ws, loss_kernel, dim3(grid_for(B, 256, g)), dim3(256), 0, (const float*)m.z3, y, wt, B,
                    (const float*)m.hc, m.dz3, m.loss));
     GHB_TRY(launch(ws, sum_kernel, dim3(1), dim3(1024), 0, (const float*)m.loss, B, m.lsum));
     GHB_TRY(launch(ws, dense_wgrad_kernel, dim3(grid_for((kH + 1) * kOut, 256, g)), dim3(256), 0, (const float*)m.h2,
@@ -311,7 +313,7 @@ int ghb_mlp_forward(ghb_workspace* ws, const float* params, const float* norm, c
 }
 
 int ghb_mlp_grad(ghb_workspace* ws, const float* params, const float* norm, const float* x, const int32_t* y,
-                 int32_t batch, float* grad, float* loss) {
+                 const float* sample_weight, int32_t batch, float* grad, float* loss) {
     ws = ws_resolve(ws);
     GHB_REQUIRE(ws && params && norm && x && y && grad, "NULL argument");
     GHB_REQUIRE(batch >= 1, "batch < 1");
@@ -320,7 +322,7 @@ int ghb_mlp_grad(ghb_workspace* ws, const float* params, const float* norm, cons
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
     MlpBuffers m = MlpBuffers::carve(c, batch);
-    GHB_TRY(mlp_grad(ws, m, params, norm, x, y, batch));
+    GHB_TRY(mlp_grad(ws, m, params, norm, x, y, sample_weight, batch));
     GHB_CUDA_TRY(cudaMemcpyAsync(grad, m.grad, sizeof(float) * kParams, cudaMemcpyDeviceToDevice, ws->stream));
     if (loss) {
         GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, m.lsum, sizeof(float), cudaMemcpyDeviceToHost, ws->stream));
@@ -331,7 +333,7 @@ int ghb_mlp_grad(ghb_workspace* ws, const float* params, const float* norm, cons
 }
 
 int ghb_mlp_train(ghb_workspace* ws, float* params, const float* norm, const float* x, const int32_t* y,
-                  int32_t batch, int32_t epochs, float lr, float* loss_history) {
+                  const float* sample_weight, int32_t batch, int32_t epochs, float lr, float* loss_history) {
     ws = ws_resolve(ws);
     GHB_REQUIRE(ws && params && norm && x && y, "NULL argument");
     GHB_REQUIRE(batch >= 1 && epochs >= 0, "bad sizes");
@@ -351,7 +353,7 @@ int ghb_mlp_train(ghb_workspace* ws, float* params, const float* norm, const flo
     const float b1 = 0.9f, b2 = 0.999f;
     double p1 = 1.0, p2 = 1.0;
     for (int e = 0; e < epochs; ++e) {
-        GHB_TRY(mlp_grad(ws, m, params, norm, x, y, batch));
+        GHB_TRY(mlp_grad(ws, m, params, norm, x, y, sample_weight, batch));
         GHB_CUDA_TRY(cudaMemcpyAsync(hist + e, m.lsum, sizeof(float), cudaMemcpyDeviceToDevice, ws->stream));
         p1 *= b1;
         p2 *= b2;

@@ -18,38 +18,49 @@ constexpr int kPolTotal = kPolParams + 2 * kPolIn;  // floats on the device
 // Heads: [0,2) direction, [2,4) top-down output format, [4,20) SSSP width bin.
 constexpr int kHeadDir = 0, kHeadFmt = 2, kHeadDelta = 4, kDeltaBins = 16, kDeltaBinZero = 6;
 
-// The 12 policy features of one BFS level (also the first 12 trace columns):
-//  0 log2(1+n_f)      frontier vertices
-//  1 log2(1+m_f)      frontier out-edges
-//  2 log2(1+m_u)      edges of unvisited vertices
-//  3 level index
-//  4 log2(1+mean frontier degree)
-//  5 log2(1+frontier degree variance)
-//  6 log2(1+max frontier degree)
-//  7 log2(n)
-//  8 log2(1+m)
+// The 12 policy features of one BFS level (also the first 12 trace
+// columns), scale-free so that a network trained on scales 16-22 reads a
+// scale-24 graph's levels in the same ranges:
+//  0 log2(1+n_f) - log2(n)          frontier share of the vertices
+//  1 log2(1+m_f) - log2(1+m)        frontier share of the entries
+//  2 log2(1+m_u) - log2(1+m)        unexplored share of the entries
+//  3 log2(1+m_f) - log2(1+m_u)      the direction rule's ratio
+//  4 log2(1+mean frontier degree) - log2(1+m/n)
+//  5 log2(1+std of frontier degree) - log2(1+mean frontier degree)
+//  6 log2(1+max frontier degree) - log2(1+m/n)
+//  7 log2(1+level)
+//  8 log2(1+m/n)                    mean degree of the graph
 //  9 previous direction (0 push, 1 pull)
-// 10 log2(1+1000*previous level ms)
-// 11 log2(1+n_f) - log2(n)
+// 10 log2(1+n_f) - log2(1+n_f of the previous level)   frontier growth
+// 11 log2(1+unvisited) - log2(n)    unvisited share of the vertices
 // One definition for the host-driven loop and the persistent kernel.
 __host__ __device__ inline void bfs_features(float* f, double n, double m, double n_f, double m_f, double m_u,
-                                             int level, double deg2, double degmax, int prev_dir, float prev_ms) {
+                                             int level, double deg2, double degmax, int prev_dir, double n_f_prev,
+                                             double unvisited) {
     const double nf = n_f > 0 ? n_f : 0.0;
     const double mean = nf > 0 ? m_f / nf : 0.0;
     double var = nf > 0 ? deg2 / nf - mean * mean : 0.0;
     if (var < 0) var = 0;
-    f[0] = log2f((float)(1.0 + nf));
-    f[1] = log2f((float)(1.0 + m_f));
-    f[2] = log2f((float)(1.0 + (m_u > 0 ? m_u : 0.0)));
-    f[3] = (float)level;
-    f[4] = log2f((float)(1.0 + mean));
-    f[5] = log2f((float)(1.0 + var));
-    f[6] = log2f((float)(1.0 + degmax));
-    f[7] = log2f((float)(n > 0 ? n : 1.0));
-    f[8] = log2f((float)(1.0 + m));
+    const double nn = n > 0 ? n : 1.0;
+    const float lm = log2f((float)(1.0 + m));
+    const float ln = log2f((float)nn);
+    const float lmean_g = log2f((float)(1.0 + m / nn));
+    const float lnf = log2f((float)(1.0 + nf));
+    const float lmf = log2f((float)(1.0 + m_f));
+    const float lmu = log2f((float)(1.0 + (m_u > 0 ? m_u : 0.0)));
+    const float lmean = log2f((float)(1.0 + mean));
+    f[0] = lnf - ln;
+    f[1] = lmf - lm;
+    f[2] = lmu - lm;
+    f[3] = lmf - lmu;
+    f[4] = lmean - lmean_g;
+    f[5] = log2f((float)(1.0 + sqrt(var))) - lmean;
+    f[6] = log2f((float)(1.0 + degmax)) - lmean_g;
+    f[7] = log2f((float)(1 + (level > 0 ? level : 0)));
+    f[8] = lmean_g;
     f[9] = (float)prev_dir;
-    f[10] = log2f(1.0f + 1000.0f * prev_ms);
-    f[11] = f[0] - f[7];
+    f[10] = lnf - log2f((float)(1.0 + (n_f_prev > 0 ? n_f_prev : 0.0)));
+    f[11] = log2f((float)(1.0 + (unvisited > 0 ? unvisited : 0.0))) - ln;
 }
 
 // The features of one SSSP call (one width decision per traversal); level is

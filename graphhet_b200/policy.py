@@ -149,11 +149,27 @@ def oracle_schedule(t_queue: Sequence[float], t_bitmap: Sequence[float], t_comp:
     return sched, cost, V[0][0]
 
 
+def level_weights(r: dict, sched: Sequence[int], total: float) -> np.ndarray:
+    """Importance of each level's decision: what a wrong direction or format
+    costs at that level (from the replayed times), as a share of the whole
+    traversal's oracle time, times the number of levels (mean 1 when every
+    level matters equally)."""
+    L = len(sched)
+    w = np.zeros(L)
+    for l in range(L):
+        push = min(r["t_queue"][l], r["t_bitmap"][l] + (r["t_comp"][l + 1] if l + 1 < L else 0.0))
+        pull = r["t_pull"][l]
+        gap_dir = abs(pull - push) if np.isfinite(pull) else 0.0
+        gap_fmt = abs(r["t_queue"][l] - (r["t_bitmap"][l] + (r["t_comp"][l + 1] if l + 1 < L else 0.0)))
+        w[l] = (gap_dir + gap_fmt) / max(total, 1e-9) * L
+    return w
+
+
 def level_rows(trace_a: np.ndarray, sched: Sequence[int], cost: Sequence[float],
-               max_rows: int = 48) -> Tuple[np.ndarray, np.ndarray]:
+               max_rows: int = 48, weights: Optional[np.ndarray] = None):
     """Training rows of one traversal: the features of frontier L (the same in
-    every replay) with the history features (9 previous direction, 10
-    previous level time) taken from the oracle schedule, and the labels
+    every replay) with the history feature (9, previous direction) taken from
+    the oracle schedule, and the labels
     (direction, top-down output format).  Level 0 is skipped: the kernel
     decides it without the network.  A long traversal (a grid's thousands of
     levels) gives its first max_rows/2 levels and evenly spaced others, so
@@ -165,17 +181,22 @@ def level_rows(trace_a: np.ndarray, sched: Sequence[int], cost: Sequence[float],
         rest = levels[max_rows // 2:]
         pick = np.linspace(0, len(rest) - 1, max_rows - len(head)).round().astype(int)
         levels = head + [rest[i] for i in sorted(set(pick.tolist()))]
+    W = []
     for l in levels:
+        W.append(1.0 if weights is None else float(weights[l]))
         f = trace_a[l, :N_FEATURES].astype(np.float32).copy()
         f[9] = 1.0 if sched[l - 1] == PULL else 0.0
-        f[10] = math.log2(1.0 + 1000.0 * max(cost[l - 1], 0.0))
         d = 1 if sched[l] == PULL else 0
         fm = -1 if d else (0 if sched[l] == PUSH_QUEUE else 1)
         X.append(f)
         Y.append([d, fm, -1])
     if not X:
-        return np.zeros((0, N_FEATURES), np.float32), np.zeros((0, 3), np.int32)
-    return np.asarray(X, np.float32), np.asarray(Y, np.int32)
+        if weights is None:
+            return np.zeros((0, N_FEATURES), np.float32), np.zeros((0, 3), np.int32)
+        return np.zeros((0, N_FEATURES), np.float32), np.zeros((0, 3), np.int32), np.zeros(0, np.float32)
+    if weights is None:
+        return np.asarray(X, np.float32), np.asarray(Y, np.int32)
+    return np.asarray(X, np.float32), np.asarray(Y, np.int32), np.asarray(W, np.float32)
 
 
 def replay_costs(rg, src: int):
@@ -231,17 +252,19 @@ def sssp_rows(rg, src: int, max_buckets: float = 4096.0, max_ms: float = 2000.0)
 
 
 # ------------------------------------------------------------- collection
-def collect(specs: Sequence[GraphSpec], bfs_sources: int = 2, sssp_every: int = 2, sssp_max_scale: int = 20,
+def collect(specs: Sequence[GraphSpec], bfs_sources: int = 6, grid_sources: int = 2, sssp_every: int = 1,
+            sssp_max_scale: int = 20,
             log=print) -> Dict[str, np.ndarray]:
     """Training rows from every graph of `specs` (needs a GPU)."""
     import torch
     import graphhet_b200 as G
-    Xs, Ys, meta = [], [], []
+    Xs, Ys, Ws, meta = [], [], [], []
     t0 = time.time()
     for gi, spec in enumerate(specs):
         g = build_graph(spec)
         rg = G.ResidentGraph(g)
-        srcs = pick_sources(g, bfs_sources, spec.seed)
+        # Grids give many near-identical levels per source: fewer sources.
+        srcs = pick_sources(g, grid_sources if spec.kind == "grid" else bfs_sources, spec.seed)
         nrows = 0
         for s in srcs:
             rg.bfs(s)  # warm-up (scratch, first-touch)
@@ -249,16 +272,21 @@ def collect(specs: Sequence[GraphSpec], bfs_sources: int = 2, sssp_every: int = 
             if r is None:
                 continue
             sched, cost, total = oracle_schedule(r["t_queue"], r["t_bitmap"], r["t_comp"], r["t_pull"])
-            X, Y = level_rows(r["trace"], sched, cost)
+            X, Y, W = level_rows(r["trace"], sched, cost, weights=level_weights(r, sched, total))
             Xs.append(X)
             Ys.append(Y)
+            Ws.append(W)
             nrows += len(X)
         if gi % sssp_every == 0 and spec.scale <= sssp_max_scale and srcs:
             out = sssp_rows(rg, srcs[0])
             if out is not None:
-                f, lab, _ = out
+                f, lab, times = out
                 Xs.append(f[None, :])
                 Ys.append(np.array([[-1, -1, lab]], np.int32))
+                # Weight: the rule's width's excess time over the best width.
+                base = times[DELTA_BIN_ZERO] if np.isfinite(times[DELTA_BIN_ZERO]) else np.nanmax(
+                    np.where(np.isfinite(times), times, np.nan))
+                Ws.append(np.array([float(np.clip(base / times[lab] - 1.0, 0.05, 10.0))], np.float32))
                 nrows += 1
         meta.append(dict(asdict(spec), rows=nrows, n=g.n, m=int(g.m)))
         rg.close()
@@ -267,7 +295,12 @@ def collect(specs: Sequence[GraphSpec], bfs_sources: int = 2, sssp_every: int = 
         if log and (gi % 20 == 0 or gi == len(specs) - 1):
             log("graph %d/%d %s scale %d rows %d (%.0f s)" % (gi + 1, len(specs), spec.kind, spec.scale, nrows,
                                                               time.time() - t0))
-    return dict(X=np.concatenate(Xs).astype(np.float32), Y=np.concatenate(Ys).astype(np.int32),
+    W = np.concatenate(Ws).astype(np.float32)
+    bfs = np.concatenate(Ys)[:, 0] >= 0
+    # Normalise the BFS rows' weights to mean 1 and bound them.
+    if bfs.any():
+        W[bfs] = np.clip(W[bfs] / max(W[bfs].mean(), 1e-12), 0.02, 50.0)
+    return dict(X=np.concatenate(Xs).astype(np.float32), Y=np.concatenate(Ys).astype(np.int32), W=W,
                 meta=np.array(json.dumps(meta)))
 
 
@@ -290,15 +323,18 @@ def norm_of(X: np.ndarray) -> np.ndarray:
     return np.concatenate([mu, 1.0 / np.maximum(sd, 1e-3)]).astype(np.float32)
 
 
-def train(X: np.ndarray, Y: np.ndarray, epochs: int = 3000, lr: float = 3e-3, seed: int = 0):
-    """Full-batch Adam on the GPU with libghb's MLP kernels.  Returns
-    (params, norm, loss history)."""
+def train(X: np.ndarray, Y: np.ndarray, epochs: int = 3000, lr: float = 3e-3, seed: int = 0,
+          W: Optional[np.ndarray] = None):
+    """Full-batch Adam on the GPU with libghb's MLP kernels, rows weighted by
+    W (what a wrong decision there costs).  Returns (params, norm, loss
+    history)."""
     import torch
     import graphhet_b200 as G
     norm = norm_of(X)
     p = torch.from_numpy(init_params(seed)).cuda()
+    w = torch.from_numpy(W.astype(np.float32)).cuda() if W is not None else None
     hist = G.mlp_train(p, torch.from_numpy(norm).cuda(), torch.from_numpy(X).cuda(), torch.from_numpy(Y).cuda(),
-                       epochs=epochs, lr=lr)
+                       epochs=epochs, lr=lr, weight=w)
     return p.cpu().numpy(), norm, np.asarray(hist, np.float32)
 
 
@@ -382,18 +418,18 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     if a.data and os.path.exists(a.data):
         z = np.load(a.data)
-        data = dict(X=z["X"], Y=z["Y"], meta=z["meta"])
+        data = dict(X=z["X"], Y=z["Y"], W=z["W"] if "W" in z else None, meta=z["meta"])
     else:
         data = collect(training_specs(a.graphs))
         if a.data:
             np.savez(a.data, **data)
-    X, Y = data["X"], data["Y"]
-    # Hold out every tenth BFS row block for validation accuracy.
+    X, Y, W = data["X"], data["Y"], data.get("W")
+    # Hold out every tenth row for validation accuracy.
     idx = np.arange(len(X))
     val = idx % 10 == 0
-    params, norm, hist = train(X[~val], Y[~val], epochs=a.epochs, lr=a.lr)
+    params, norm, hist = train(X[~val], Y[~val], epochs=a.epochs, lr=a.lr, W=W[~val] if W is not None else None)
     acc_tr, acc_val = accuracy(params, norm, X[~val], Y[~val]), accuracy(params, norm, X[val], Y[val])
-    params, norm, hist_all = train(X, Y, epochs=a.epochs, lr=a.lr)
+    params, norm, hist_all = train(X, Y, epochs=a.epochs, lr=a.lr, W=W)
     info = dict(graphs=a.graphs, rows=int(len(X)), bfs_rows=int((Y[:, 0] >= 0).sum()),
                 sssp_rows=int((Y[:, 2] >= 0).sum()), pull_frac=float((Y[:, 0] == 1).sum() / max(1, (Y[:, 0] >= 0).sum())),
                 epochs=a.epochs, lr=a.lr, loss_first=float(hist_all[0]), loss_last=float(hist_all[-1]),

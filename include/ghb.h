@@ -383,15 +383,18 @@ int ghb_policy_loaded(void);
 /* Device arrays: logits[batch][20] = network(x[batch][12]). */
 int ghb_mlp_forward(ghb_workspace* ws, const float* params, const float* norm, const float* x,
                     int32_t batch, float* logits);
-/* Device arrays: grad[GHB_POLICY_PARAMS] of the summed mean softmax
- * cross-entropy of the three heads; y[batch][3] holds the class of each head
- * (-1: no label).  loss (host, may be NULL) gets the loss. */
+/* Device arrays: grad[GHB_POLICY_PARAMS] of the sum over the three heads of
+ * the weighted mean softmax cross-entropy; y[batch][3] holds the class of
+ * each head (-1: no label); sample_weight[batch] (may be NULL: all 1) weighs
+ * the rows.  loss (host, may be NULL) gets the loss. */
 int ghb_mlp_grad(ghb_workspace* ws, const float* params, const float* norm, const float* x,
-                 const int32_t* y, int32_t batch, float* grad, float* loss);
+                 const int32_t* y, const float* sample_weight, int32_t batch, float* grad,
+                 float* loss);
 /* `epochs` full-batch Adam steps on device params (in place); loss_history
  * (host, may be NULL) gets the loss before each step. */
 int ghb_mlp_train(ghb_workspace* ws, float* params, const float* norm, const float* x,
-                  const int32_t* y, int32_t batch, int32_t epochs, float lr, float* loss_history);
+                  const int32_t* y, const float* sample_weight, int32_t batch, int32_t epochs,
+                  float lr, float* loss_history);
 
 #ifdef __cplusplus
 }

@@ -443,3 +443,21 @@ def test_mssssp_matches_single_source(G, count):
                 assert np.array_equal(d[i], ref), i
                 assert np.array_equal(dr[i], ref), i
         rg.close()
+
+
+def test_tc_complete_graph_long_oriented_rows(G):
+    """K_1060: the oriented rows of the first vertices exceed the warp hash
+    kernel's 1,024 entries (binary-search path), the rest take the hash
+    path; every vertex is in C(1059, 2) triangles (the reference counts 6x)."""
+    n = 1060
+    iu = torch.triu_indices(n, n, 1)
+    src, dst = iu[0].int().cuda(), iu[1].int().cuda()
+    g = G.make_graph(n, src, dst, False, weight_mode=G.WEIGHT_NONE)
+    per_vertex = 6 * (n - 1) * (n - 2) // 2
+    triangles = n * (n - 1) * (n - 2) // 6
+    c64, c32, total = G.tc(g)
+    assert total == triangles
+    assert bool((c32 == per_vertex).all())
+    rg = G.ResidentGraph(g)
+    c64, c32, total = rg.tc()
+    assert total == triangles and bool((c32 == per_vertex).all())

@@ -21,7 +21,7 @@ def unpack(p):
     return out
 
 
-def ref_loss(p, norm, x, y):
+def ref_loss(p, norm, x, y, wt=None):
     W1, b1, W2, b2, W3, b3 = unpack(p)
     a = (x - norm[:12]) * norm[12:]
     h1 = torch.relu(a @ W1 + b1)
@@ -34,7 +34,12 @@ def ref_loss(p, norm, x, y):
         if keep.sum() == 0:
             continue
         lp = torch.log_softmax(z[keep, s:e], dim=1)
-        loss = loss - lp[torch.arange(int(keep.sum())), lab[keep].long()].mean()
+        picked = lp[torch.arange(int(keep.sum())), lab[keep].long()]
+        if wt is None:
+            loss = loss - picked.mean()
+        else:
+            w = wt[keep].to(p.dtype)
+            loss = loss - (w * picked).sum() / w.sum()
     return z, loss
 
 
@@ -49,15 +54,17 @@ def make_case(B, seed):
 
 
 @pytest.mark.parametrize("B", [1, 37, 1000])
-def test_mlp_forward_and_grad_match_autograd(B):
+@pytest.mark.parametrize("weighted", [False, True])
+def test_mlp_forward_and_grad_match_autograd(B, weighted):
     import graphhet_b200 as G
     p, norm, x, y = make_case(B, 5 + B)
+    wt = (torch.rand(B, generator=torch.Generator().manual_seed(B)) * 3 + 0.1) if weighted else None
     p64 = p.double().requires_grad_(True)
-    z, loss = ref_loss(p64, norm.double(), x.double(), y)
+    z, loss = ref_loss(p64, norm.double(), x.double(), y, wt)
     loss.backward()
     logits = G.mlp_forward(p.cuda(), norm.cuda(), x.cuda()).cpu()
     torch.testing.assert_close(logits.double(), z.detach(), rtol=1e-4, atol=1e-4)
-    grad, l = G.mlp_grad(p.cuda(), norm.cuda(), x.cuda(), y.cuda())
+    grad, l = G.mlp_grad(p.cuda(), norm.cuda(), x.cuda(), y.cuda(), weight=wt.cuda() if wt is not None else None)
     assert abs(l - loss.item()) <= 1e-4 * max(1.0, abs(loss.item()))
     # FP32 sums over the batch against the FP64 gradient.
     torch.testing.assert_close(grad.cpu().double(), p64.grad, rtol=2e-3, atol=2e-5)

@@ -52,8 +52,8 @@ def test_level_rows_history_features_and_labels():
     assert X.shape == (4, 12) and Y.shape == (4, 3)
     assert Y.tolist() == [[1, -1, -1], [0, 1, -1], [0, 0, -1], [1, -1, -1]]
     assert X[:, 9].tolist() == [0.0, 1.0, 0.0, 0.0]
-    assert np.allclose(X[:, 10], np.log2(1 + 1000 * np.array(cost[:4])))
     assert np.array_equal(X[:, :9], trace[1:, :9])
+    assert np.array_equal(X[:, 10:], trace[1:, 10:12])
 
 
 def test_level_rows_subsamples_long_traversals():
@@ -84,3 +84,14 @@ def test_init_params_layout():
     assert np.all(p[768:832] == 0) and np.all(p[6272:] == 0)
     n = P.norm_of(np.random.default_rng(0).normal(size=(50, 12)).astype(np.float32))
     assert n.shape == (24,)
+
+
+def test_level_weights_follow_the_cost_gap():
+    r = dict(t_queue=np.array([1.0, 1.0, 1.0]), t_bitmap=np.array([1.0, 1.0, 1.0]),
+             t_comp=np.array([0.0, 0.1, 0.1]), t_pull=np.array([np.inf, 5.0, 1.05]))
+    sched, cost, total = P.oracle_schedule(r["t_queue"], r["t_bitmap"], r["t_comp"], r["t_pull"])
+    w = P.level_weights(r, sched, total)
+    assert w.shape == (3,) and np.all(w >= 0)
+    assert w[1] > w[2]  # a wrong direction at level 1 costs 4 ms, at level 2 0.05 ms
+    X, Y, W = P.level_rows(np.zeros((3, 24), np.float32), sched, cost, weights=w)
+    assert len(W) == 2 and W[0] == np.float32(w[1])
