@@ -43,7 +43,7 @@ _f64 = ctypes.c_double
 class BfsOptions(ctypes.Structure):
     _fields_ = [("policy", _i32), ("alpha", ctypes.c_float), ("beta", ctypes.c_float),
                 ("schedule", _p), ("schedule_len", _i32), ("record_trace", _i32),
-                ("trace", _p), ("trace_cap", _i32), ("oracle_timing", _i32)]
+                ("trace", _p), ("trace_cap", _i32), ("oracle_timing", _i32), ("gamma", ctypes.c_float)]
 
 
 class SsspOptions(ctypes.Structure):
@@ -100,6 +100,13 @@ _SIGS = {
     "ghb_batch_wcc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p]),
     "ghb_batch_tc": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _p]),
     "ghb_union_reserve": (ctypes.c_int, [_p, _i32, _i64]),
+    "ghb_ldbc_load": (ctypes.c_int, [_p, ctypes.c_char_p, ctypes.c_char_p, _i32, ctypes.POINTER(_p)]),
+    "ghb_ldbc_info": (ctypes.c_int, [_p, ctypes.POINTER(_i32), ctypes.POINTER(_i64), ctypes.POINTER(_i32)]),
+    "ghb_ldbc_csr": (ctypes.c_int, [_p] + [ctypes.POINTER(_p)] * 6),
+    "ghb_ldbc_copy": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _p, _p]),
+    "ghb_ldbc_name": (ctypes.c_int, [_p, _i32, ctypes.POINTER(ctypes.c_char_p)]),
+    "ghb_ldbc_id": (ctypes.c_int, [_p, ctypes.c_char_p, ctypes.POINTER(_i32)]),
+    "ghb_ldbc_free": (ctypes.c_int, [_p]),
     "ghb_union_wcc_tc": (ctypes.c_int, [_p, _i32, _p, _i32, _i64, _p, _p, _p, _p, _p]),
     "ghb_graph_create": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p, _p, _p, ctypes.POINTER(_p)]),
     "ghb_graph_destroy": (ctypes.c_int, [_p]),
@@ -375,6 +382,36 @@ def rmat_dangling_graph(scale: int, edge_factor: int, seed: int, fraction: float
     return make_graph(1 << scale, src, dst, True, weight_mode=WEIGHT_NONE, ws=ws)
 
 
+def load_ldbc(vertex_path: str, edge_path: str, directed: bool, ws=None):
+    """LDBC .v/.e files -> (CSRGraph on the device, vertex names by id).  The
+    library parses them with every host thread and builds the CSR on the GPU
+    (ghb_ldbc_load); the arrays are copied out of its handle."""
+    h = _p()
+    _check(lib().ghb_ldbc_load(_ws(ws), vertex_path.encode(), edge_path.encode(), int(directed), ctypes.byref(h)),
+           "ghb_ldbc_load")
+    try:
+        n, m, wt = _i32(), _i64(), _i32()
+        _check(lib().ghb_ldbc_info(h, ctypes.byref(n), ctypes.byref(m), ctypes.byref(wt)), "ghb_ldbc_info")
+        n, m = n.value, m.value
+        t = lambda k, dt: torch.empty(max(1, k), dtype=dt, device="cuda")
+        rp, col, w = t(n + 1, torch.int32), t(m, torch.int32), t(m, torch.float64)
+        irp, icol, iw = (t(n + 1, torch.int32), t(m, torch.int32), t(m, torch.float64)) if directed else (None,) * 3
+        _check(lib().ghb_ldbc_copy(_ws(ws), h, _ptr(rp), _ptr(col), _ptr(w), _ptr(irp), _ptr(icol), _ptr(iw)),
+               "ghb_ldbc_copy")
+        torch.cuda.synchronize()
+        g = CSRGraph(n=n, rowptr=rp, col=col[:m], w=w[:m], directed=directed)
+        if directed:
+            g.in_rowptr, g.in_col, g.in_w = irp, icol[:m], iw[:m]
+        names = []
+        nm = ctypes.c_char_p()
+        for i in range(n):
+            _check(lib().ghb_ldbc_name(h, i, ctypes.byref(nm)), "ghb_ldbc_name")
+            names.append(nm.value.decode())
+        return g, names
+    finally:
+        lib().ghb_ldbc_free(h)
+
+
 class UnionBatch:
     """Many independent graphs as one disjoint-union CSR (ghb_union_*): graph
     g owns global vertices [vbase[g], vbase[g+1])."""
@@ -577,9 +614,9 @@ class ResidentGraph:
         return torch.empty(self.n * k, dtype=torch.int32, device=self._dev)
 
     def bfs(self, src, max_depth=INT32_MAX, policy=POLICY_HEURISTIC, schedule=None, trace_cap=0,
-            oracle_timing=False, alpha=0.0, beta=0.0, out=None, ws=None):
+            oracle_timing=False, alpha=0.0, beta=0.0, gamma=0.0, out=None, ws=None):
         depth = out if out is not None else self._i32()
-        opt = BfsOptions(policy=policy, alpha=alpha, beta=beta)
+        opt = BfsOptions(policy=policy, alpha=alpha, beta=beta, gamma=gamma)
         keep = None
         if schedule is not None:
             keep = (ctypes.c_int8 * len(schedule))(*[int(x) for x in schedule])

@@ -57,6 +57,11 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
     // the frontier is under 1/24 of the vertices.
     const float alpha = opt->alpha > 0 ? opt->alpha : 256.0f;
     const float beta = opt->beta > 0 ? opt->beta : 24.0f;
+    // A frontier with fewer than m / gamma out-entries never goes bottom-up:
+    // a bottom-up level scans every unvisited vertex, which a thin frontier
+    // (a grid's late levels, whose ratio to the unexplored entries is large
+    // only because little is left) never repays.
+    const float gamma = opt->gamma > 0 ? opt->gamma : 1024.0f;
     static_assert(sizeof(BfsPersistState) <= 16 * sizeof(unsigned long long), "persist state slot");
 
     const int64_t words = ((int64_t)n + 31) / 32;
@@ -124,7 +129,7 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
             fmt_req = has ? ((opt->schedule[level] >> 1) & 3) : 0;
         } else {
             int heur = dir;
-            if (dir == 0 && (double)m_f > (double)m_u / alpha) heur = 1;
+            if (dir == 0 && (double)m_f > (double)m_u / alpha && (double)m_f > (double)m_total / gamma) heur = 1;
             else if (dir == 1 && (double)n_f < (double)n / beta) heur = 0;
             dir = heur;
             if (policy == GHB_POLICY_LEARNED) {

@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
     int32_t n, int32_t n_active, const int32_t* __restrict__ out_rp, const int32_t* __restrict__ out_col,
     const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col, int32_t src, int32_t max_depth,
     int32_t* depth, uint32_t* visited, uint32_t* f0, uint32_t* f1, uint32_t* f2, int32_t* qa, int32_t* qb,
-    int32_t* big, int policy, float alpha, float beta, int64_t m_total, const int8_t* __restrict__ schedule,
+    int32_t* big, int policy, float alpha, float beta, float gamma, int64_t m_total, const int8_t* __restrict__ schedule,
     int32_t schedule_len, const int32_t* __restrict__ perm, int32_t* depth_out, BfsRunState* st,
     const float* __restrict__ pol, float* trace, int32_t trace_cap) {
     const int lane = lane_id();
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                         fmt = (schedule[L + 1] >> 1) & 3;
                     }
                 } else {
-                    if (dir == 0 && (double)mf_next > m_u / alpha) nd = 1;
+                    if (dir == 0 && (double)mf_next > m_u / alpha && (double)mf_next > (double)m_total / gamma) nd = 1;
                     else if (dir == 1 && (double)nf_next < (double)n / beta) nd = 0;
                 }
                 bfs_features(s_feat, (double)n, (double)m_total, (double)nf_next, (double)mf_next, m_u, L + 1,
@@ -649,6 +649,7 @@ int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int
     int policy = opt ? opt->policy : GHB_POLICY_HEURISTIC;
     float alpha = (opt && opt->alpha > 0) ? opt->alpha : 256.0f;
     float beta = (opt && opt->beta > 0) ? opt->beta : 24.0f;
+    float gamma = (opt && opt->gamma > 0) ? opt->gamma : 1024.0f;
     int32_t sched_len = 0;
     if (policy == GHB_POLICY_SCHEDULE && opt && opt->schedule && opt->schedule_len > 0) {
         sched_len = std::min<int32_t>(opt->schedule_len, 4096);
@@ -669,7 +670,8 @@ int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
     GHB_TRY(launch_coop(ws, bfs_persistent_kernel, dim3(blocks), dim3(512), pol ? sizeof(float) * kPolTotal : 0, n,
                         n_active, out_rp, out_col, in_rp, in_col, src, max_depth, depth, vis, f0, f1, f2, qa, qb, big,
-                        policy, alpha, beta, m_total, (const int8_t*)(sched_len ? sched : nullptr), sched_len, perm,
+                        policy, alpha, beta, gamma, m_total, (const int8_t*)(sched_len ? sched : nullptr), sched_len,
+                        perm,
                         depth_out, rs, pol, tcap > 0 ? tr : (float*)nullptr, tcap));
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
     GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, rs, sizeof(BfsRunState), cudaMemcpyDeviceToHost, st));

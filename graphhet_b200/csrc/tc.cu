@@ -157,116 +157,14 @@ struct OrientedVisitor {
     __device__ void finish() const {}
 };
 
-// Oriented counting, warp per row u: N+(u) goes into a warp-private hash
-// set in shared memory, then the warp walks the wedges (u, v, w) for v in
-// N+(u), w in N+(v) 32 at a time (a shuffle scan of the |N+(v)| spreads them
-// over the lanes) and looks w up in the set.  Each triangle adds 1 to w
-// (atomic), to v (merged over the lanes that share v) and to u (once per
-// row).  Rows with more than kTcHashMax oriented entries go to `big` for the
-// binary-search visitor.
-constexpr int kTcWarpsPerBlock = 8;
-constexpr int kTcSlots = 2048;            // per warp
-constexpr int32_t kTcHashMax = kTcSlots / 2;
-
-__device__ __forceinline__ uint32_t tc_hash(int32_t x) {
-    uint32_t h = (uint32_t)x * 0x9E3779B1u;
-    return h ^ (h >> 15);
-}
-
-__global__ void __launch_bounds__(kTcWarpsPerBlock * 32) tc_warp_kernel(int32_t n, const int32_t* __restrict__ orp,
-                                                                      const int32_t* __restrict__ ocol,
-                                                                      unsigned long long* cnt, int32_t* big,
-                                                                      int32_t* big_count) {
-    extern __shared__ int32_t tc_smem[];
-    const int lane = lane_id();
-    int32_t* T = tc_smem + (threadIdx.x >> 5) * kTcSlots;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t uu = warp; uu < n; uu += nwarps) {
-        const int32_t u = (int32_t)uu;
-        const int32_t ub = orp[u], ue = orp[u + 1], du = ue - ub;
-        if (du == 0) continue;
-        if (du > kTcHashMax) {
-            if (lane == 0) big[atomicAdd(big_count, 1)] = u;
-            continue;
-        }
-        uint32_t cap = 64;
-        while (cap < 2u * (uint32_t)du) cap <<= 1;
-        for (uint32_t s = lane; s < cap; s += 32) T[s] = -1;
-        __syncwarp();
-        for (int32_t j = ub + lane; j < ue; j += 32) {
-            const int32_t x = ocol[j];
-            uint32_t h = tc_hash(x) & (cap - 1);
-            while (atomicCAS(&T[h], -1, x) != -1) h = (h + 1) & (cap - 1);
-        }
-        __syncwarp();
-        unsigned long long total_u = 0;
-        for (int32_t g0 = ub; g0 < ue; g0 += 32) {
-            const int32_t i = g0 + lane;
-            int32_t v = -1, vb = 0, len = 0;
-            if (i < ue) {
-                v = ocol[i];
-                vb = orp[v];
-                len = orp[v + 1] - vb;
-            }
-            int32_t incl = len;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int32_t x = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += x;
-            }
-            const int32_t excl = incl - len;
-            const int32_t total = __shfl_sync(0xffffffffu, incl, 31);
-            for (int32_t k0 = 0; k0 < total; k0 += 32) {
-                const int32_t k = k0 + lane;
-                int owner = 0;
-#pragma unroll
-                for (int st = 16; st >= 1; st >>= 1) {
-                    const int cand = owner + st;
-                    if (__shfl_sync(0xffffffffu, excl, cand) <= k) owner = cand;
-                }
-                const int32_t ov = __shfl_sync(0xffffffffu, v, owner);
-                const int32_t ob = __shfl_sync(0xffffffffu, vb, owner);
-                const int32_t oe = __shfl_sync(0xffffffffu, excl, owner);
-                bool found = false;
-                int32_t w = 0;
-                if (k < total) {
-                    w = ocol[ob + (k - oe)];
-                    uint32_t h = tc_hash(w) & (cap - 1);
-                    while (true) {
-                        const int32_t y = T[h];
-                        if (y == w) {
-                            found = true;
-                            break;
-                        }
-                        if (y == -1) break;
-                        h = (h + 1) & (cap - 1);
-                    }
-                }
-                const unsigned fm = __ballot_sync(0xffffffffu, found);
-                if (found) {
-                    atomicAdd(cnt + w, 1ull);
-                    const unsigned same = __match_any_sync(fm, ov);
-                    if (lane == __ffs(same) - 1) atomicAdd(cnt + ov, (unsigned long long)__popc(same));
-                }
-                total_u += __popc(fm);
-            }
-        }
-        if (lane == 0 && total_u) atomicAdd(cnt + u, total_u);
-        __syncwarp();
-    }
-}
-
-// Triangles of the oriented CSR into cnt (zeroed by the caller): the warp
-// kernel, then the binary-search visitor over the rows it handed on.
+// Triangles of the oriented CSR into cnt (zeroed by the caller): the
+// load-balanced walk over every oriented entry with the binary-search
+// visitor.  (A warp-per-row shared-memory hash variant measured 25 % slower
+// on RMAT scale 24: most oriented rows hold a few entries, so a warp per row
+// leaves most lanes idle, where the walker packs short rows warp-wide.)
 int tc_count_oriented(ghb_workspace* ws, int32_t n, const int32_t* orp, const int32_t* ocol, unsigned long long* cnt,
-                      int32_t* big, int32_t* big_count, const WalkBuffers& wb) {
-    const size_t smem = sizeof(int32_t) * kTcSlots * kTcWarpsPerBlock;
-    GHB_CUDA_TRY(cudaFuncSetAttribute(tc_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GHB_CUDA_TRY(cudaMemsetAsync(big_count, 0, sizeof(int32_t), ws->stream));
-    GHB_TRY(launch(ws, tc_warp_kernel, dim3(grid_for((int64_t)n * 32, kTcWarpsPerBlock * 32, ws->num_sms * 8)),
-                   dim3(kTcWarpsPerBlock * 32), smem, n, orp, ocol, cnt, big, big_count));
-    return walk(ws, orp, ocol, (const int32_t*)big, (const int32_t*)big_count, (int64_t)n, (int64_t)n, wb,
+                      const WalkBuffers& wb) {
+    return walk(ws, orp, ocol, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
                 OrientedVisitor{orp, ocol, cnt});
 }
 
@@ -330,7 +228,6 @@ size_t tc_oriented_bytes(int32_t n, int64_t m) {
     c.take<int32_t>((size_t)n + 1);
     c.take<int64_t>(scan_scratch_words(n));
     c.take<int32_t>(m > 0 ? m : 1);
-    c.take<int32_t>((size_t)n + 1);
     return c.off;
 }
 
@@ -343,7 +240,6 @@ int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* row
     int32_t* orp = c.take<int32_t>((size_t)n + 1);
     int64_t* bsums = c.take<int64_t>(scan_scratch_words(n));
     int32_t* ocol = c.take<int32_t>(m > 0 ? m : 1);
-    int32_t* big = c.take<int32_t>((size_t)n + 1);
     GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * ((size_t)n + 1), st));
     GHB_CUDA_TRY(cudaMemsetAsync(keep, 0, sizeof(int32_t) * n, st));
     GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
@@ -353,7 +249,7 @@ int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* row
                    rowptr, col, (const int32_t*)orp, ocol));
     GHB_TRY(launch(ws, orient_fill_long_kernel, dim3(ws->num_sms), dim3(1024), 0, n, rowptr, col, (const int32_t*)orp,
                    ocol));
-    GHB_TRY(tc_count_oriented(ws, n, orp, ocol, cnt, big, big + n, wb));
+    GHB_TRY(tc_count_oriented(ws, n, orp, ocol, cnt, wb));
     if (counts64)
         GHB_TRY(launch(ws, tc_finish_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n,
                        (const unsigned long long*)cnt, 6, counts64, (int32_t*)nullptr,
@@ -378,7 +274,6 @@ int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* c
     sizing.take<int32_t>((size_t)n + 1);
     sizing.take<int64_t>(scan_scratch_words(n));
     sizing.take<int32_t>(m > 0 ? m : 1);
-    sizing.take<int32_t>((size_t)n + 1);
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
     WalkBuffers wb = WalkBuffers::carve(c, n);
@@ -389,7 +284,6 @@ int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* c
     int32_t* orp = c.take<int32_t>((size_t)n + 1);
     int64_t* bsums = c.take<int64_t>(scan_scratch_words(n));
     int32_t* ocol = c.take<int32_t>(m > 0 ? m : 1);
-    int32_t* big = c.take<int32_t>((size_t)n + 1);
 
     GHB_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int32_t), st));
     GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * n, st));
@@ -408,7 +302,7 @@ int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* c
                        n, rowptr, col, (const int32_t*)orp, ocol));
         GHB_TRY(launch(ws, orient_fill_long_kernel, dim3(ws->num_sms), dim3(1024), 0, n, rowptr, col,
                        (const int32_t*)orp, ocol));
-        GHB_TRY(tc_count_oriented(ws, n, orp, ocol, cnt, big, big + n, wb));
+        GHB_TRY(tc_count_oriented(ws, n, orp, ocol, cnt, wb));
     } else {
         GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
                      MergeVisitor{rowptr, col, cnt}));

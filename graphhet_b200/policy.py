@@ -399,7 +399,8 @@ def regret(rg, sources: Sequence[int], repeats: int = 3) -> Dict[str, float]:
         tot["table"] += total
         tot["oracle"] += timed(s, policy=G.POLICY_SCHEDULE, schedule=sched)[0]
         tot["heuristic"] += timed(s, policy=G.POLICY_HEURISTIC)[0]
-        tot["beamer14"] += timed(s, policy=G.POLICY_HEURISTIC, alpha=14.0, beta=24.0)[0]
+        # The classic rule: alpha 14, beta 24, no frontier guard.
+        tot["beamer14"] += timed(s, policy=G.POLICY_HEURISTIC, alpha=14.0, beta=24.0, gamma=1e30)[0]
         tot["learned"] += timed(s, policy=G.POLICY_LEARNED)[0]
     o = tot["oracle"]
     return dict(ms=tot, regret_heuristic=tot["heuristic"] / o - 1.0, regret_learned=tot["learned"] / o - 1.0,

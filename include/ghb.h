@@ -95,6 +95,30 @@ int ghb_gen_powerlaw(ghb_workspace* ws, int32_t scale, int64_t n_edges, double e
 int ghb_gen_dangling_keep(ghb_workspace* ws, int64_t n_edges, const int32_t* src, uint64_t seed,
                           double fraction, uint8_t* keep);
 
+/* ----------------------------------------------------------- LDBC loader */
+/* LDBC .v / .e text files straight into device CSRs (replaces
+ * LDBC::load_graph, include/LDBC/ldbc.hpp:181-253, and toCSR's flattening of
+ * graph_structure): ids follow first appearance (.v lines, then names first
+ * seen in .e, a before b), weights are the third field (else 1), an
+ * undirected graph gets both directions, a repeated ordered pair keeps its
+ * last line's weight, self-loops are kept.  The handle owns the arrays; a
+ * directed graph also gets the in-CSR (undirected: in = out). */
+typedef struct ghb_ldbc_graph ghb_ldbc_graph;
+int ghb_ldbc_load(ghb_workspace* ws, const char* vertex_path, const char* edge_path,
+                  int32_t directed, ghb_ldbc_graph** out);
+int ghb_ldbc_info(const ghb_ldbc_graph* g, int32_t* n, int64_t* m, int32_t* weighted);
+int ghb_ldbc_csr(const ghb_ldbc_graph* g, const int32_t** rowptr, const int32_t** col,
+                 const double** w, const int32_t** in_rowptr, const int32_t** in_col,
+                 const double** in_w);
+/* Copies the handle's arrays into caller-owned device arrays (any may be
+ * NULL; in_* only for a directed graph), on the workspace's stream. */
+int ghb_ldbc_copy(ghb_workspace* ws, const ghb_ldbc_graph* g, int32_t* rowptr, int32_t* col,
+                  double* w, int32_t* in_rowptr, int32_t* in_col, double* in_w);
+/* Vertex name of an id (valid while the handle lives) and the id of a name. */
+int ghb_ldbc_name(const ghb_ldbc_graph* g, int32_t id, const char** name);
+int ghb_ldbc_id(const ghb_ldbc_graph* g, const char* name, int32_t* id);
+int ghb_ldbc_free(ghb_ldbc_graph* g);
+
 /* ----------------------------------------------------------- CSR builder */
 /* Build a CSR from an edge list (replaces the host flattening in toCSR,
  * GPU_csr.hpp:282-339, for edge-list inputs).  Flags: */
@@ -123,7 +147,7 @@ int ghb_csr_merge_in_out(ghb_workspace* ws, int32_t n, const int32_t* in_rowptr,
 
 /* ------------------------------------------------------------------- BFS */
 /* Direction policy per level. */
-#define GHB_POLICY_HEURISTIC 0 /* Beamer alpha/beta rule                      */
+#define GHB_POLICY_HEURISTIC 0 /* Beamer alpha/beta rule + frontier guard     */
 #define GHB_POLICY_LEARNED 1   /* the trained MLP (ghb_policy_*); falls back   */
 #define GHB_POLICY_PUSH 2      /* top-down every level                        */
 #define GHB_POLICY_PULL 3      /* bottom-up every level after the first       */
@@ -142,6 +166,7 @@ typedef struct {
     float* trace;            /* host, trace_cap x GHB_TRACE_COLS               */
     int32_t trace_cap;
     int32_t oracle_timing;   /* 1: time push and pull at every level (slow)   */
+    float gamma;             /* ... and only when m_f > m / gamma (0: 1024)   */
 } ghb_bfs_options;
 
 /* Trace row (one per level): 12 policy features of the level's frontier,
