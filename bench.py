@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--extras", type=int, default=1, help="also measure the other algorithms")
     ap.add_argument("--cpu-sample", type=int, default=1, help="number of BFS sources in the CPU baseline")
     ap.add_argument("--only", default=None,
-                    choices=["bfs", "sssp", "wcc", "pr", "pr64", "cdlp", "tc", "msbfs64", "msbfs256"],
+                    choices=["bfs", "sssp", "wcc", "pr", "pr64", "cdlp", "tc", "msbfs64", "msbfs256", "mssssp256"],
                     help="profiling driver: run one algorithm --warmup + --steps times on the RMAT graph of "
                          "--scale and print its mean time (not a bench line)")
     return ap.parse_args()
@@ -717,6 +717,8 @@ def run_only(args):
     big = None
     if args.only.startswith("msbfs"):
         big = torch.empty(256 * n, dtype=torch.int32, device="cuda")
+    if args.only.startswith("mssssp"):
+        big = torch.empty(256 * n, dtype=torch.float64, device="cuda")
     calls = {
         "bfs": lambda i: rg.bfs(srcs[i % len(srcs)], out=i32),
         "sssp": lambda i: rg.sssp(srcs[i % len(srcs)], out=f64),
@@ -727,6 +729,7 @@ def run_only(args):
         "tc": lambda i: rg.tc(),
         "msbfs64": lambda i: rg.msbfs(srcs[:64], out=big),
         "msbfs256": lambda i: rg.msbfs(srcs[:256], out=big),
+        "mssssp256": lambda i: rg.mssssp(srcs[:256], out=big),
     }
     fn = calls[args.only]
     for i in range(args.warmup):
