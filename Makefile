@@ -26,9 +26,10 @@ $(BUILD)/%.o: graphhet_b200/csrc/%.cu $(CU_HDR)
 oracle:
 	$(MAKE) -C oracle REF_ROOT=$(REF_ROOT)
 
-# The reference's own GPU-CSR drivers (GPU_csr_example.cu, LDBC_GPU_csr.cu),
-# compiled unchanged from where they lie against this repository's
-# include/GPU_csr headers and linked to libghb.so: the drop-in check.
+# The reference's own GPU drivers (GPU_csr_example.cu, LDBC_GPU_csr.cu,
+# GPU_gpma_example.cu, LDBC_GPU_gpma.cu), compiled unchanged from where they
+# lie against this repository's include/GPU_csr and include/GPU_gpma headers
+# and linked to libghb.so: the drop-in check.
 DROPIN    := build/dropin
 dropin: graphhet_b200/libghb.so
 	@if [ -f "$(REF_ROOT)/src/LDBC/LDBC_GPU_csr.cu" ]; then \
@@ -36,7 +37,11 @@ dropin: graphhet_b200/libghb.so
 	  $(NVCC) $(ARCH) -O2 -std=c++17 -Iinclude -I$(REF_ROOT)/include $(REF_ROOT)/src/GPU_csr/GPU_csr_example.cu \
 	    -o $(DROPIN)/GPU_csr_example -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' && \
 	  $(NVCC) $(ARCH) -O2 -std=c++17 -Iinclude -I$(REF_ROOT)/include $(REF_ROOT)/src/LDBC/LDBC_GPU_csr.cu \
-	    -o $(DROPIN)/LDBC_GPU_csr -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' ; \
+	    -o $(DROPIN)/LDBC_GPU_csr -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' && \
+	  $(NVCC) $(ARCH) -O2 -std=c++17 -Iinclude -I$(REF_ROOT)/include $(REF_ROOT)/src/GPU_gpma/GPU_gpma_example.cu \
+	    -o $(DROPIN)/GPU_gpma_example -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' && \
+	  $(NVCC) $(ARCH) -O2 -std=c++17 -Iinclude -I$(REF_ROOT)/include $(REF_ROOT)/src/LDBC/LDBC_GPU_gpma.cu \
+	    -o $(DROPIN)/LDBC_GPU_gpma -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' ; \
 	else echo "reference drivers not found under $(REF_ROOT): skipping the drop-in build"; fi
 
 clean:

@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--extras", type=int, default=1, help="also measure the other algorithms")
     ap.add_argument("--cpu-sample", type=int, default=1, help="number of BFS sources in the CPU baseline")
     ap.add_argument("--only", default=None,
-                    choices=["bfs", "sssp", "wcc", "pr", "pr64", "cdlp", "tc", "msbfs64", "msbfs256", "mssssp256"],
+                    choices=["bfs", "sssp", "wcc", "pr", "pr64", "cdlp", "tc", "msbfs64", "msbfs256", "mssssp256", "gpma"],
                     help="profiling driver: run one algorithm --warmup + --steps times on the RMAT graph of "
                          "--scale and print its mean time (not a bench line)")
     return ap.parse_args()
@@ -520,6 +520,9 @@ def extras(args, G, g, rg, srcs, ws):
     # graph, against the per-graph entry points.
     ex["batch_er2000"] = er_batch_section(G, ws)
     torch.cuda.empty_cache()
+    # Dynamic graph: batched edge updates on this RMAT graph.
+    ex["gpma_rmat"] = gpma_section(G, g)
+    torch.cuda.empty_cache()
     # 4096 x 4096 grid: BFS and SSSP from its centre
     gg = G.ResidentGraph(G.grid_graph(4096, 4096, weight_seed=args.seed))
     c = 2048 * 4096 + 2048
@@ -542,6 +545,77 @@ def extras(args, G, g, rg, srcs, ws):
         ex["regret_grid"] = {k: (round(v, 4) if isinstance(v, float) else {a: round(b, 3) for a, b in v.items()})
                              for k, v in r.items()}
     return ex
+
+
+def gpma_batch(g, size, gen):
+    """One mixed update batch on the device: half inserts of random (mostly
+    new) edges with weights in (0.25, 2), a quarter deletes of present edges,
+    a quarter weight changes of present edges."""
+    import torch
+    n, m = g.n, g.m
+    q = size // 4
+    k_new = size - 2 * q
+    src = torch.randint(0, n, (k_new,), device="cuda", generator=gen)
+    dst = torch.randint(0, n, (k_new,), device="cuda", generator=gen)
+    j = torch.randint(0, m, (2 * q,), device="cuda", generator=gen)
+    rows = torch.searchsorted(g.rowptr, j.to(torch.int32), right=True) - 1
+    keys = torch.cat([(src.to(torch.int64) << 32) | dst, (rows.to(torch.int64) << 32) | g.col[j].to(torch.int64)])
+    vals = torch.rand(size, device="cuda", dtype=torch.float64, generator=gen) * 1.75 + 0.25
+    vals[k_new: k_new + q] = 0.0
+    perm = torch.randperm(size, device="cuda", generator=gen)
+    return keys[perm].contiguous(), vals[perm].contiguous()
+
+
+def gpma_section(G, g, sizes=(1000, 100000, 10000000), reps=(20, 10, 3), seed=7):
+    """Dynamic graph (the reference's GPMA update path) on graph g: load from
+    its CSR, batches of mixed updates (1,000 is the reference LDBC driver's
+    batch, LDBC_GPU_gpma.cu:124-140), each timed with CUDA events around the
+    call (which returns after its kernels are queued behind one host sync),
+    then the compact-CSR rebuild a following analytic pays, and one BFS on it."""
+    import ctypes
+
+    import torch
+    out = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dg = G.DynamicGraph.from_csr(g.rowptr, g.col, g.w)
+    torch.cuda.synchronize()
+    out["load_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    for size, r in zip(sizes, reps):
+        batches = [gpma_batch(g, size, gen) for _ in range(r + 1)]
+        dg.update(*batches[0])
+        times = []
+        for k, v in batches[1:]:
+            ms, _ = timed(lambda: dg.update(k, v))
+            times.append(ms)
+        med = statistics.median(times)
+        out[f"batch{size}_ms"] = round(med, 4)
+        out[f"batch{size}_mupdates_per_s"] = round(size / (med / 1e3) / 1e6, 3)
+        del batches
+    k, v = gpma_batch(g, 1000, gen)
+    dg.update(k, v)
+    ms, _ = timed(lambda: dg.csr_view(weights=False))
+    out["csr_rebuild_ms"] = round(ms, 3)
+    nm = dg.m
+    out["csr_rebuild_gbs"] = round((8 * nm + 16 * g.n) / (ms / 1e3) / 1e9, 1)
+    dg.update(*gpma_batch(g, 1000, gen))
+    ms, _ = timed(lambda: dg.csr_view(weights=True))
+    out["csr_rebuild_weights_ms"] = round(ms, 3)
+    rp, col, _ = dg.csr_view(weights=False)
+    depth = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    src = int(torch.argmax(g.rowptr[1:] - g.rowptr[:-1]))
+    call = lambda: G._check(G.lib().ghb_bfs(None, g.n, ctypes.c_void_p(rp), ctypes.c_void_p(col), None, None, src,
+                                            2**31 - 1, G._ptr(depth), None, None), "ghb_bfs")
+    call()
+    ms, _ = timed(call)
+    out["bfs_on_snapshot_ms"] = round(ms, 3)
+    st = dg.stats()
+    out["stats"] = {k: st[k] for k in ("rows_moved", "repacks", "slots_used", "slots")}
+    out["m_after"] = nm
+    dg.close()
+    return out
 
 
 def er_batch_section(G, ws, n_graphs=2000, seed=5):
@@ -709,6 +783,8 @@ def run_only(args):
 
     import graphhet_b200 as G
     g = G.rmat_graph(args.scale, args.edge_factor, args.seed)
+    if args.only == "gpma":
+        return gpma_only(args, G, g)
     rg = G.ResidentGraph(g)
     srcs = pick_sources(g.rowptr.cpu().numpy(), 256, args.seed)
     n = g.n
@@ -738,6 +814,35 @@ def run_only(args):
     ms, _ = timed(lambda: [fn(i) for i in range(args.steps)])
     return {"only": args.only, "scale": args.scale, "n": n, "m": g.m, "steps": args.steps,
             "ms_per_call": round(ms / max(1, args.steps), 4)}
+
+
+def gpma_only(args, G, g):
+    """Dynamic-graph section alone, plus the reference's CPU edits
+    (graph_structure::add_edge / remove_edge, CPU_adj_list.hpp:110-128, from
+    oracle/_ref) applying the same 1,000- and 100,000-update batches on this
+    graph on one host thread, as the CPU baseline of the update path."""
+    import torch
+    out = {"only": "gpma", "scale": args.scale, "n": g.n, "m": g.m, "gpu": gpma_section(G, g)}
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import oracle as O
+    if O.ref_available():
+        og = O.Graph(g.n, g.rowptr.cpu().numpy(), g.col.cpu().numpy(), g.w.cpu().numpy(), False,
+                     g.rowptr.cpu().numpy(), g.col.cpu().numpy(), g.w.cpu().numpy())
+        r = O.Ref().load(og)
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(args.seed + 1)
+        cpu = {}
+        for size in (1000, 100000):
+            k, v = gpma_batch(g, size, gen)
+            k = k.cpu().numpy()
+            t0 = time.perf_counter()
+            r.apply_updates((k >> 32).astype(np.int32), (k & 0xFFFFFFFF).astype(np.int32), v.cpu().numpy())
+            dt = time.perf_counter() - t0
+            cpu[f"batch{size}_ms"] = round(dt * 1e3, 3)
+            cpu[f"batch{size}_mupdates_per_s"] = round(size / dt / 1e6, 3)
+        r.close()
+        out["cpu_reference_graph_structure"] = dict(cpu, cores=1, kind="reference")
+    return out
 
 
 def main():

@@ -128,6 +128,18 @@ _SIGS = {
     "ghb_mlp_forward": (ctypes.c_int, [_p, _p, _p, _p, _i32, _p]),
     "ghb_mlp_grad": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _i32, _p, ctypes.POINTER(ctypes.c_float)]),
     "ghb_mlp_train": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _i32, _i32, ctypes.c_float, _p]),
+    "ghb_gpma_create": (ctypes.c_int, [_p, _i32, ctypes.POINTER(_p)]),
+    "ghb_gpma_destroy": (ctypes.c_int, [_p]),
+    "ghb_gpma_clone": (ctypes.c_int, [_p, _p, ctypes.POINTER(_p)]),
+    "ghb_gpma_clear": (ctypes.c_int, [_p, _p]),
+    "ghb_gpma_load_csr": (ctypes.c_int, [_p, _p, _p, _p, _p]),
+    "ghb_gpma_update": (ctypes.c_int, [_p, _p, _p, _p, _i64, _p]),
+    "ghb_gpma_info": (ctypes.c_int, [_p, ctypes.POINTER(_i32), ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+                                     ctypes.POINTER(_i64)]),
+    "ghb_gpma_stats": (ctypes.c_int, [_p, _p]),
+    "ghb_gpma_csr": (ctypes.c_int, [_p, _p, _i32, ctypes.POINTER(_p), ctypes.POINTER(_p), ctypes.POINTER(_p)]),
+    "ghb_gpma_export": (ctypes.c_int, [_p, _p, _p, _p, _p]),
+    "ghb_gpma_find": (ctypes.c_int, [_p, _p, _p, _i64, _p]),
 }
 
 _lib = None
@@ -758,3 +770,6 @@ def policy_load(params, norm) -> None:
 
 def policy_loaded() -> bool:
     return bool(lib().ghb_policy_loaded())
+
+
+from .gpma import DynamicGraph, edge_keys  # noqa: E402

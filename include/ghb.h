@@ -387,6 +387,54 @@ int ghb_union_wcc_tc(ghb_workspace* ws, int32_t n_graphs, const int64_t* vbase, 
                      int64_t m, const int32_t* rowptr, const int32_t* col, int32_t* label,
                      int64_t* counts64, int64_t* triangles);
 
+/* ----------------------------------------------------- dynamic graph */
+/* A GPU-resident graph that takes batches of edge updates (the reference's
+ * GPMA, include/GPU_gpma/GPU_gpma.hpp).  Update semantics of update_gpma
+ * (GPU_gpma.hpp:756-824, handle_del_mod at :166-180): key = (row << 32) |
+ * col with row, col < n; value 0 deletes the entry if present (no-op when
+ * absent); any other value sets the weight of an existing entry or inserts
+ * it.  Repeated keys in one batch: the last occurrence wins.  Rows stay
+ * sorted by column.  keys / values are DEVICE arrays.  Analytics read the
+ * compact CSR of ghb_gpma_csr (rows sorted, m < 2^31), which is rebuilt on
+ * the first call after a change and then cached. */
+typedef struct ghb_gpma ghb_gpma;
+#define GHB_GPMA_STATS 8 /* batches, inserted, deleted, modified, rows moved,
+                            repacks, arena slots used, arena slots */
+/* Empty graph over n vertices (init_csr_gpma, GPU_gpma.hpp:911-928). */
+int ghb_gpma_create(ghb_workspace* ws, int32_t n, ghb_gpma** out);
+int ghb_gpma_destroy(ghb_gpma* g);
+/* Deep copy (GPMA's copy assignment, LDBC_GPU_gpma.cu:206). */
+int ghb_gpma_clone(ghb_workspace* ws, const ghb_gpma* src, ghb_gpma** out);
+/* Remove every edge. */
+int ghb_gpma_clear(ghb_workspace* ws, ghb_gpma* g);
+/* Replace the contents with a CSR (rowptr[0] = 0, rows strictly increasing,
+ * columns in [0, n)); w NULL means weight 1, a weight of 0 is refused
+ * (init_gpma_from_csr, GPU_gpma.hpp:851-909). */
+int ghb_gpma_load_csr(ghb_workspace* ws, ghb_gpma* g, const int32_t* rowptr, const int32_t* col,
+                      const double* w);
+/* Apply one batch (update_gpma).  totals (host, may be NULL) receives
+ * inserted, deleted, modified, ignored (repeats and deletes of absent keys).
+ * A key outside [0, n) x [0, n) fails the whole batch with
+ * GHB_ERR_INVALID_ARGUMENT before anything is applied (batches beyond 2^25
+ * updates are applied in passes of 2^25, in order: the final graph is the
+ * same, totals count each pass's own effects, and a failing pass leaves the
+ * earlier passes applied). */
+int ghb_gpma_update(ghb_workspace* ws, ghb_gpma* g, const uint64_t* keys, const double* values,
+                    int64_t count, int64_t* totals);
+/* n, live entries, arena slots, version (bumped by every change). */
+int ghb_gpma_info(const ghb_gpma* g, int32_t* n, int64_t* m, int64_t* slots, int64_t* version);
+int ghb_gpma_stats(const ghb_gpma* g, int64_t* stats /* GHB_GPMA_STATS */);
+/* Device pointers of the compact CSR (valid until the next change or
+ * destroy); weights != 0 also materialises w. */
+int ghb_gpma_csr(ghb_workspace* ws, ghb_gpma* g, int32_t weights, const int32_t** rowptr,
+                 const int32_t** col, const double** w);
+/* The compact CSR copied into caller buffers (rowptr n + 1, col / w m; w may
+ * be NULL). */
+int ghb_gpma_export(ghb_workspace* ws, ghb_gpma* g, int32_t* rowptr, int32_t* col, double* w);
+/* Weight of each key, 0 when the entry is absent. */
+int ghb_gpma_find(ghb_workspace* ws, const ghb_gpma* g, const uint64_t* keys, int64_t count,
+                  double* values);
+
 /* ------------------------------------------------------- schedule policy */
 /* The learned schedule policy: an MLP 12 -> 64 -> 64 (ReLU) -> 20 logits in
  * three heads: [0,2) BFS direction (push, pull), [2,4) top-down frontier

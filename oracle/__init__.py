@@ -196,6 +196,69 @@ def tc(g: Graph):
     return c
 
 
+# ------------------------------------------------------- dynamic graph
+def gpma_keys(src, dst) -> np.ndarray:
+    """KEY_TYPE (row << 32) | col (LDBC_GPU_gpma.cu:91-93) as int64."""
+    return (np.asarray(src, np.int64) << 32) | np.asarray(dst, np.int64)
+
+
+def gpma_update(keys: np.ndarray, vals: np.ndarray, bkeys, bvals):
+    """One update_gpma batch (GPU_gpma.hpp:756-824) on a graph held as sorted
+    unique int64 keys with their weights: for the last occurrence of every
+    batch key, value 0 removes a present key (handle_del_mod,
+    GPU_gpma.hpp:166-180), any other value overwrites a present key's weight
+    or inserts the key.  Returns the new (keys, vals) and the counts
+    (inserted, deleted, modified, ignored)."""
+    bkeys = np.asarray(bkeys, np.int64)
+    bvals = np.asarray(bvals, np.float64)
+    order = np.argsort(bkeys, kind="stable")
+    sk, sv = bkeys[order], bvals[order]
+    last = np.ones(len(sk), bool)
+    last[:-1] = sk[1:] != sk[:-1]
+    uk, uv = sk[last], sv[last]
+    pos = np.searchsorted(keys, uk)
+    found = pos < len(keys)
+    found[found] = keys[pos[found]] == uk[found]
+    vals = vals.copy()
+    mod = found & (uv != 0)
+    vals[pos[mod]] = uv[mod]
+    keep = np.ones(len(keys), bool)
+    dele = found & (uv == 0)
+    keep[pos[dele]] = False
+    ins = ~found & (uv != 0)
+    nk = np.concatenate([keys[keep], uk[ins]])
+    nv = np.concatenate([vals[keep], uv[ins]])
+    o = np.argsort(nk, kind="stable")
+    counts = (int(ins.sum()), int(dele.sum()), int(mod.sum()), len(bkeys) - int(ins.sum() + dele.sum() + mod.sum()))
+    return nk[o], nv[o], counts
+
+
+def gpma_update_sequential(state: dict, bkeys, bvals) -> dict:
+    """The same batch applied one update at a time, in batch order (small
+    cases; pins gpma_update)."""
+    for k, v in zip(np.asarray(bkeys, np.int64).tolist(), np.asarray(bvals, np.float64).tolist()):
+        if v == 0.0:
+            state.pop(k, None)
+        else:
+            state[k] = v
+    return state
+
+
+def gpma_from_csr(rowptr, col, w=None):
+    rowptr = np.asarray(rowptr, np.int64)
+    rows = np.repeat(np.arange(len(rowptr) - 1, dtype=np.int64), np.diff(rowptr))
+    keys = gpma_keys(rows, col)
+    vals = np.ones(len(keys)) if w is None else np.asarray(w, np.float64).copy()
+    return keys, vals
+
+
+def gpma_to_csr(n: int, keys: np.ndarray, vals: np.ndarray):
+    rows = (keys >> 32).astype(np.int64)
+    rowptr = np.zeros(n + 1, np.int32)
+    np.add.at(rowptr, rows + 1, 1)
+    return np.cumsum(rowptr).astype(np.int32), (keys & 0xFFFFFFFF).astype(np.int32), vals.copy()
+
+
 # ------------------------------------------------- the reference, compiled
 class Ref:
     """The reference's CPU algorithms (oracle/_ref/libref.so) on one loaded graph."""
@@ -216,6 +279,9 @@ class Ref:
             "ref_cdlp": (ctypes.c_int, [ctypes.c_int, _p]),
             "ref_tc": (ctypes.c_int, [_p]),
             "ref_hardware_threads": (ctypes.c_int, []),
+            "ref_apply_updates": (ctypes.c_int, [ctypes.c_longlong, _p, _p, _p]),
+            "ref_out_entries": (ctypes.c_longlong, []),
+            "ref_export_out": (ctypes.c_int, [_p, _p, _p]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)
@@ -272,6 +338,21 @@ class Ref:
         c = np.empty(self.n, np.int32)
         self.L.ref_tc(_np_ptr(c))
         return c
+
+    def apply_updates(self, src, dst, w):
+        """Edits in order through graph_structure::add_edge / remove_edge."""
+        src = np.ascontiguousarray(src, np.int32)
+        dst = np.ascontiguousarray(dst, np.int32)
+        w = np.ascontiguousarray(w, np.float64)
+        self.L.ref_apply_updates(len(src), _np_ptr(src), _np_ptr(dst), _np_ptr(w))
+
+    def export_out(self):
+        m = int(self.L.ref_out_entries())
+        rp = np.empty(self.n + 1, np.int32)
+        col = np.empty(max(1, m), np.int32)
+        w = np.empty(max(1, m), np.float64)
+        self.L.ref_export_out(_np_ptr(rp), _np_ptr(col), _np_ptr(w))
+        return rp, col[:m], w[:m]
 
     def hardware_threads(self):
         return int(self.L.ref_hardware_threads())

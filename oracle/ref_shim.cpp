@@ -108,6 +108,45 @@ int ref_tc(int* counts) {
     return 0;
 }
 
+// Apply edge updates in order through the reference's own graph_structure
+// edits (CPU_adj_list.hpp:110-128): weight 0 -> remove_edge(u, v), any other
+// weight -> add_edge(u, v, w), which inserts or overwrites the weight.  These
+// are the edits the reference's GPMA drivers mirror on the GPU
+// (batch_add_edge / batch_delete_edge, LDBC_GPU_gpma.cu:124-148).
+int ref_apply_updates(long long count, const int* src, const int* dst, const double* w) {
+    if (!g_graph) return -1;
+    for (long long i = 0; i < count; ++i) {
+        if (w[i] == 0.0) g_graph->remove_edge(src[i], dst[i]);
+        else g_graph->add_edge(src[i], dst[i], w[i]);
+    }
+    return 0;
+}
+
+// Entries of the current out-rows.
+long long ref_out_entries() {
+    long long m = 0;
+    if (g_graph)
+        for (const auto& row : g_graph->OUTs) m += (long long)row.size();
+    return m;
+}
+
+// The current out-rows as a CSR (rp n + 1, col / w ref_out_entries()).
+int ref_export_out(int* rp, int* col, double* w) {
+    if (!g_graph) return -1;
+    long long o = 0;
+    const int n = (int)g_graph->OUTs.size();
+    for (int v = 0; v < n; ++v) {
+        rp[v] = (int)o;
+        for (const auto& e : g_graph->OUTs[v]) {
+            col[o] = e.first;
+            w[o] = e.second;
+            ++o;
+        }
+    }
+    rp[n] = (int)o;
+    return 0;
+}
+
 int ref_hardware_threads() { return (int)std::thread::hardware_concurrency(); }
 
 }  // extern "C"

@@ -11,7 +11,8 @@ Each fixture stores the input edge list, the CSR built from it (the layout
 the reference's toCSR produces from graph_structure's sorted rows) and the
 reference outputs: BFS depths and SSSP distances from `src`, WCC labels,
 PageRank (10 iterations, d = 0.85), CDLP labels (10 iterations) and the
-per-vertex triangle counts.
+per-vertex triangle counts.  gpma/ holds dynamic-graph fixtures: a graph,
+update batches, and the reference's rows after each batch.
 """
 import os
 import sys
@@ -74,6 +75,55 @@ def main():
     s, d = O.er_edges(3000, 9000, 5)
     g = O.make_graph(3000, s, d, False, weight_mode=1, weight_seed=5)
     run_ref("er3000_seed5", g, 0, dict(er_n=np.int64(3000), er_m=np.int64(9000), seed=np.int64(5)))
+    gpma_fixture()
+
+
+def gpma_batches(rowptr, col, n, n_batches, size, seed):
+    """Seeded update batches over a graph: new edges, weight changes and
+    deletes of present edges, deletes of absent ones, self-loops, and repeats
+    of keys inside a batch (the later value must win)."""
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(n), np.diff(rowptr))
+    present = list(zip(rows.tolist(), np.asarray(col).tolist()))
+    out = []
+    for _ in range(n_batches):
+        q = size // 8
+        s, d, w = [], [], []
+        for _ in range(2 * q):  # inserts (or overwrites when present)
+            s.append(int(rng.integers(n))); d.append(int(rng.integers(n))); w.append(float(rng.uniform(0.25, 2.0)))
+        for i in rng.integers(len(present), size=2 * q):  # deletes of present edges
+            s.append(present[i][0]); d.append(present[i][1]); w.append(0.0)
+        for _ in range(q):  # deletes of (mostly) absent edges
+            s.append(int(rng.integers(n))); d.append(int(rng.integers(n))); w.append(0.0)
+        for i in rng.integers(len(present), size=q):  # weight changes
+            s.append(present[i][0]); d.append(present[i][1]); w.append(float(rng.uniform(0.25, 2.0)))
+        for _ in range(q // 4):  # self-loops
+            v = int(rng.integers(n)); s.append(v); d.append(v); w.append(1.5)
+        perm = rng.permutation(len(s))
+        s, d, w = np.array(s, np.int32)[perm], np.array(d, np.int32)[perm], np.array(w)[perm]
+        rep = rng.integers(len(s), size=q)  # repeats with a new value (a third of them deletes)
+        rw = np.where(rng.random(q) < 1 / 3, 0.0, rng.uniform(0.25, 2.0, q))
+        s = np.concatenate([s, s[rep]]); d = np.concatenate([d, d[rep]]); w = np.concatenate([w, rw])
+        out.append((s, d, w))
+    return out
+
+
+def gpma_fixture():
+    """Dynamic-graph updates: the directed RMAT-9 graph (seed 42) edited by
+    four seeded batches through the reference's graph_structure::add_edge /
+    remove_edge (the edits the GPMA drivers mirror, LDBC_GPU_gpma.cu:124-148),
+    with the reference's out-rows after every batch."""
+    g = O.rmat_graph(9, 16, 42, directed=True)
+    r = O.Ref().load(g)
+    batches = gpma_batches(g.rowptr, g.col, g.n, 4, 2048, 2024)
+    out = dict(n=np.int64(g.n), rowptr=g.rowptr, col=g.col, w=g.w)
+    for i, (s, d, w) in enumerate(batches):
+        r.apply_updates(s, d, w)
+        rp, c, ww = r.export_out()
+        out.update({f"b{i}_src": s, f"b{i}_dst": d, f"b{i}_w": w, f"a{i}_rowptr": rp, f"a{i}_col": c, f"a{i}_w": ww})
+    os.makedirs(os.path.join(HERE, "gpma"), exist_ok=True)
+    np.savez_compressed(os.path.join(HERE, "gpma", "rmat9_seed42_batches.npz"), **out)
+    print("gpma rmat9_seed42_batches", [int(out[f"a{i}_rowptr"][-1]) for i in range(4)])
 
 
 if __name__ == "__main__":

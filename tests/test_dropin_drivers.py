@@ -1,11 +1,15 @@
-"""The reference's own GPU-CSR drivers, compiled unchanged against this
-repository's include/GPU_csr headers and linked to libghb.so (make dropin):
+"""The reference's own GPU drivers, compiled unchanged against this
+repository's include/GPU_csr and include/GPU_gpma headers and linked to
+libghb.so (make dropin):
 
-* GPU_csr_example prints the known answers of its 6-vertex graph;
-* LDBC_GPU_csr loads an LDBC Graphalytics dataset written here, runs BFS,
-  SSSP (+ SSSP with predecessors), WCC, PageRank and CDLP through the
-  drop-in entry points and validates them with the reference's own checkers
-  (include/LDBC/checker.hpp) against expected outputs from the CPU oracle.
+* GPU_csr_example and GPU_gpma_example print the known answers of their
+  6-vertex graph;
+* LDBC_GPU_csr and LDBC_GPU_gpma load an LDBC Graphalytics dataset written
+  here, run BFS, SSSP (+ SSSP with predecessors on the CSR path), WCC,
+  PageRank and CDLP through the drop-in entry points and validate them with
+  the reference's own checkers (include/LDBC/checker.hpp) against expected
+  outputs from the CPU oracle.  The GPMA driver builds its graphs with
+  update_gpma, so this also runs the dynamic graph's batch path.
 """
 import os
 import re
@@ -22,6 +26,8 @@ pytestmark = pytest.mark.gpu
 DROPIN = os.path.join(ROOT, "build", "dropin")
 EXAMPLE = os.path.join(DROPIN, "GPU_csr_example")
 LDBC = os.path.join(DROPIN, "LDBC_GPU_csr")
+GPMA_EXAMPLE = os.path.join(DROPIN, "GPU_gpma_example")
+GPMA_LDBC = os.path.join(DROPIN, "LDBC_GPU_gpma")
 
 needs_example = pytest.mark.skipif(not os.path.exists(EXAMPLE), reason="drop-in drivers not built (make dropin)")
 needs_ldbc = pytest.mark.skipif(not os.path.exists(LDBC), reason="drop-in drivers not built (make dropin)")
@@ -41,9 +47,11 @@ def sections(text):
     return out
 
 
-@needs_example
-def test_gpu_csr_example_known_answers():
-    r = subprocess.run([EXAMPLE], capture_output=True, text=True, timeout=300)
+@pytest.mark.parametrize("binary", [EXAMPLE, GPMA_EXAMPLE], ids=["csr", "gpma"])
+def test_gpu_example_known_answers(binary):
+    if not os.path.exists(binary):
+        pytest.skip("drop-in drivers not built (make dropin)")
+    r = subprocess.run([binary], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     s = sections(r.stdout)
     assert s["BFS"] == {"one": "0", "two": "1", "three": "1", "four": "1", "five": "2", "six": "1"}
@@ -99,20 +107,23 @@ def write_dataset(tmp, name, og: O.Graph, directed: bool, names, src):
             f.write(f"{names[i]} {names[cd[i]]}\n")
 
 
-@needs_ldbc
+@pytest.mark.parametrize("binary,csv,n_results", [(LDBC, "result-gpu-csr.csv", 5),
+                                                   (GPMA_LDBC, "result-gpu-gpma.csv", 5)], ids=["csr", "gpma"])
 @pytest.mark.parametrize("directed", [True, False])
-def test_ldbc_driver_validates_with_reference_checkers(tmp_path, directed):
+def test_ldbc_driver_validates_with_reference_checkers(tmp_path, directed, binary, csv, n_results):
+    if not os.path.exists(binary):
+        pytest.skip("drop-in drivers not built (make dropin)")
     og = O.rmat_graph(10, 8, 13, directed=directed)
     n = og.n
     names = [str(1000003 + 7919 * i) for i in range(n)]
     src = int(np.argmax(np.diff(og.rowptr)))
     name = "rmat10" + ("d" if directed else "u")
     write_dataset(str(tmp_path), name, og, directed, names, src)
-    r = subprocess.run([LDBC], input=f"{tmp_path}/\n{name}\n", capture_output=True, text=True, timeout=600,
+    r = subprocess.run([binary], input=f"{tmp_path}/\n{name}\n", capture_output=True, text=True, timeout=600,
                        cwd=str(tmp_path))
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     for what in ["BFS", "SSSP", "WCC", "PageRank", "CDLP"]:
         assert f"{what} results are correct!" in r.stdout, r.stdout[-3000:]
     assert "Error: pre_v is wrong" not in r.stdout and "Not found!" not in r.stdout
-    row = open(os.path.join(str(tmp_path), "result-gpu-csr.csv")).read().strip().split(",")
-    assert len(row) == 5 and all(re.fullmatch(r"[0-9.]+", x) for x in row), row
+    row = open(os.path.join(str(tmp_path), csv)).read().strip().split(",")
+    assert len(row) == n_results and all(re.fullmatch(r"[0-9.]+", x) for x in row), row
