@@ -57,6 +57,8 @@ def parse():
                     choices=["bfs", "sssp", "wcc", "pr", "pr64", "cdlp", "tc", "msbfs64", "msbfs256", "mssssp256", "gpma"],
                     help="profiling driver: run one algorithm --warmup + --steps times on the RMAT graph of "
                          "--scale and print its mean time (not a bench line)")
+    ap.add_argument("--gpma-sizes", default="1000,100000,10000000",
+                    help="update batch sizes of the dynamic-graph section (--only gpma)")
     return ap.parse_args()
 
 
@@ -581,6 +583,8 @@ def gpma_section(G, g, sizes=(1000, 100000, 10000000), reps=(20, 10, 3), seed=7)
     dg = G.DynamicGraph.from_csr(g.rowptr, g.col, g.w)
     torch.cuda.synchronize()
     out["load_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+    ms, _ = timed(lambda: dg.csr_view(weights=False))
+    out["csr_rebuild_fresh_ms"] = round(ms, 3)
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
     for size, r in zip(sizes, reps):
@@ -600,14 +604,17 @@ def gpma_section(G, g, sizes=(1000, 100000, 10000000), reps=(20, 10, 3), seed=7)
     out["csr_rebuild_ms"] = round(ms, 3)
     nm = dg.m
     out["csr_rebuild_gbs"] = round((8 * nm + 16 * g.n) / (ms / 1e3) / 1e9, 1)
+    dg.csr_view(weights=True)  # the first weighted view allocates its arrays
     dg.update(*gpma_batch(g, 1000, gen))
     ms, _ = timed(lambda: dg.csr_view(weights=True))
     out["csr_rebuild_weights_ms"] = round(ms, 3)
     rp, col, _ = dg.csr_view(weights=False)
     depth = torch.empty(g.n, dtype=torch.int32, device="cuda")
     src = int(torch.argmax(g.rowptr[1:] - g.rowptr[:-1]))
-    call = lambda: G._check(G.lib().ghb_bfs(None, g.n, ctypes.c_void_p(rp), ctypes.c_void_p(col), None, None, src,
-                                            2**31 - 1, G._ptr(depth), None, None), "ghb_bfs")
+    # undirected: the snapshot is its own in-CSR, so bottom-up levels run too
+    call = lambda: G._check(G.lib().ghb_bfs(None, g.n, ctypes.c_void_p(rp), ctypes.c_void_p(col), ctypes.c_void_p(rp),
+                                            ctypes.c_void_p(col), src, 2**31 - 1, G._ptr(depth), None, None),
+                            "ghb_bfs")
     call()
     ms, _ = timed(call)
     out["bfs_on_snapshot_ms"] = round(ms, 3)
@@ -822,7 +829,9 @@ def gpma_only(args, G, g):
     oracle/_ref) applying the same 1,000- and 100,000-update batches on this
     graph on one host thread, as the CPU baseline of the update path."""
     import torch
-    out = {"only": "gpma", "scale": args.scale, "n": g.n, "m": g.m, "gpu": gpma_section(G, g)}
+    sizes = tuple(int(x) for x in args.gpma_sizes.split(","))
+    reps = tuple(20 if x <= 1000 else 10 if x <= 100000 else 3 for x in sizes)
+    out = {"only": "gpma", "scale": args.scale, "n": g.n, "m": g.m, "gpu": gpma_section(G, g, sizes, reps)}
     sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
     import oracle as O
     if O.ref_available():

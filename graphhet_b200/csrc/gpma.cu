@@ -66,8 +66,17 @@ constexpr int kNop = 0, kIns = 1, kDel = 2, kMod = 3;
 // Updates applied per pass; larger batches are applied in consecutive passes
 // of this size, which keeps "last occurrence wins" and bounds the scratch.
 constexpr int64_t kPassUpdates = 1ll << 25;
-// Snapshot / repack copies: rows of at least this many entries get a block.
-constexpr int32_t kCopyBig = 256;
+// Snapshot / repack copies: rows of at least this many entries are cut into
+// chunks of this size, one warp per chunk.
+constexpr int32_t kCopyChunk = 256;
+// Rows of the batch with at most row_warp_max existing entries + updates
+// are rebuilt by one warp (a launch argument: kRowWarpSmall for small
+// batches, where a long row on one warp would be the critical path,
+// kRowWarpLarge otherwise); longer rows by the grid-wide kernels.
+constexpr int32_t kRowWarpSmall = 256;
+constexpr int32_t kRowWarpLarge = 4096;
+// Batches up to this many updates scan their flags in one block.
+constexpr int64_t kSmallScan = 32768;
 // Live entries are bounded so the snapshot's int32 offsets hold them.
 constexpr int64_t kMaxEntries = (1ll << 31) - 1;
 
@@ -169,7 +178,8 @@ __global__ void upd_row_summary_kernel(const int32_t* __restrict__ row_id, const
                                        const int32_t* __restrict__ headX, const int32_t* __restrict__ insX,
                                        const int32_t* __restrict__ delX, const int32_t* __restrict__ deg,
                                        const int32_t* __restrict__ cap, int64_t b, int32_t* __restrict__ scrn,
-                                       int32_t* __restrict__ exn, int64_t* __restrict__ reln) {
+                                       int32_t* __restrict__ exn, int64_t* __restrict__ reln,
+                                       int32_t row_warp_max, unsigned long long* __restrict__ n_long) {
     const int64_t K = headX[b];
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < b; k += (int64_t)gridDim.x * blockDim.x) {
         int32_t s = 0, e = 0;
@@ -183,6 +193,7 @@ __global__ void upd_row_summary_kernel(const int32_t* __restrict__ row_id, const
                 s = d2;
                 e = d;
                 if (d2 > cap[r]) rl = slack_cap(d2);
+                if ((int64_t)d + (z - a) > row_warp_max) atomicAdd(n_long, 1ull);
             }
         }
         scrn[k] = s;
@@ -226,104 +237,256 @@ __device__ __forceinline__ int64_t seg_of(const T* __restrict__ X, int64_t len, 
     return lo - 1;
 }
 
-// Existing entries of the changed rows -> their rank in the new row:
-// j + (inserts before the column) - (deletes before the column).  Deleted
-// entries are dropped.
-__global__ void upd_scatter_old_kernel(const int32_t* __restrict__ row_id, const int32_t* __restrict__ row_first,
-                                       const int32_t* __restrict__ exX, const int32_t* __restrict__ scrX,
+// Rank of an existing entry (column c at index j of row k) in the rebuilt
+// row: j + (inserts before c) - (deletes before c); -1 when it is deleted.
+// Updates of row k are skey[a, z), sorted.
+__device__ __forceinline__ int32_t old_rank(const uint64_t* __restrict__ skey, const int8_t* __restrict__ typ,
+                                            const int32_t* __restrict__ insX, const int32_t* __restrict__ delX,
+                                            int32_t a, int32_t z, uint32_t r, int32_t c, int32_t j) {
+    const uint64_t key = ((uint64_t)r << 32) | (uint32_t)c;
+    int32_t lo = a, hi = z;
+    while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (skey[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo < z && skey[lo] == key) {
+        int32_t q = lo;
+        while (q + 1 < z && skey[q + 1] == key) ++q;
+        if (typ[q] == kDel) return -1;
+    }
+    return j + (insX[lo] - insX[a]) - (delX[lo] - delX[a]);
+}
+
+// Rank of insert i (its row's updates start at a): insertion point - deletes
+// before it + inserts before it.
+__device__ __forceinline__ int32_t new_rank(const int32_t* __restrict__ pos, const int32_t* __restrict__ insX,
+                                            const int32_t* __restrict__ delX, int32_t a, int32_t i) {
+    return pos[i] + (insX[i] - insX[a]) - (delX[i] - delX[a]);
+}
+
+// Rows of the batch with at most kRowWarpMax existing entries + updates, one
+// warp each: rank the surviving entries and the inserts into the row's
+// scratch range, then (after __syncwarp, which orders the warp's scratch
+// writes before its reads) copy the range to the row's slots, in place or
+// to fresh ones at base + relX[k], and finish deg / start / cap.  Longer rows
+// go to `big` (with their old and new lengths in big_d / big_d2, zero past
+// the list) for the flattened kernels; big_flag[k] tells them apart.
+__global__ void upd_rows_warp_kernel(const int32_t* __restrict__ row_id, const int32_t* __restrict__ row_first,
+                                     const int32_t* __restrict__ headX, const int32_t* __restrict__ scrX,
+                                     const int32_t* __restrict__ exX, const int64_t* __restrict__ relX,
+                                     const uint64_t* __restrict__ skey, const uint32_t* __restrict__ sidx,
+                                     const double* __restrict__ values, const int8_t* __restrict__ typ,
+                                     const int32_t* __restrict__ pos, const int32_t* __restrict__ insX,
+                                     const int32_t* __restrict__ delX, int64_t base, int64_t b,
+                                     int64_t* __restrict__ start, int32_t* __restrict__ deg,
+                                     int32_t* __restrict__ cap, int32_t* __restrict__ col, double* __restrict__ val,
+                                     int32_t* __restrict__ scol, double* __restrict__ sval,
+                                     int32_t* __restrict__ big, int32_t* __restrict__ big_tail,
+                                     int32_t* __restrict__ big_d, int32_t* __restrict__ big_d2,
+                                     int8_t* __restrict__ big_flag, int32_t row_warp_max,
+                                     unsigned long long* __restrict__ moved, unsigned long long* __restrict__ bad_rank) {
+    const int lane = lane_id();
+    const int64_t K = headX[b];
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t k = warp; k < K; k += nwarps) {
+        const int32_t d = exX[k + 1] - exX[k], d2 = scrX[k + 1] - scrX[k];
+        const int32_t a = row_first[k], z = row_first[k + 1];
+        const bool changed = d > 0 || d2 > 0;
+        const bool is_big = changed && (int64_t)d + (z - a) > row_warp_max;
+        if (lane == 0) {
+            big_flag[k] = is_big ? 1 : 0;
+            if (is_big) {
+                const int32_t i = atomicAdd(big_tail, 1);
+                big[i] = (int32_t)k;
+                big_d[i] = d;
+                big_d2[i] = d2;
+            }
+        }
+        if (!changed || is_big) continue;
+        const int32_t r = row_id[k];
+        const int64_t s = start[r];
+        const int32_t o = scrX[k];
+        unsigned long long bad = 0;
+        for (int32_t j = lane; j < d; j += 32) {
+            const int32_t c = col[s + j];
+            const int32_t rk = old_rank(skey, typ, insX, delX, a, z, (uint32_t)r, c, j);
+            if (rk < 0) continue;
+            if (rk >= d2) {
+                ++bad;
+                continue;
+            }
+            scol[o + rk] = c;
+            sval[o + rk] = val[s + j];
+        }
+        for (int32_t i = a + lane; i < z; i += 32) {
+            if (typ[i] != kIns) continue;
+            const int32_t rk = new_rank(pos, insX, delX, a, i);
+            if (rk < 0 || rk >= d2) {
+                ++bad;
+                continue;
+            }
+            scol[o + rk] = (int32_t)(uint32_t)skey[i];
+            sval[o + rk] = values[sidx[i]];
+        }
+        if (bad) atomicAdd(bad_rank, bad);
+        __syncwarp();
+        const int32_t cp = cap[r];
+        const int64_t dst = d2 <= cp ? s : base + relX[k];
+        for (int32_t j = lane; j < d2; j += 32) {
+            col[dst + j] = scol[o + j];
+            val[dst + j] = sval[o + j];
+        }
+        if (lane == 0) {
+            if (d2 > cp) {
+                start[r] = dst;
+                cap[r] = (int32_t)slack_cap(d2);
+                atomicAdd(moved, 1ull);
+            }
+            deg[r] = d2;
+        }
+    }
+}
+
+// Exclusive prefix sums of up to three arrays of `count` values in one block
+// of 1,024 threads (thread t sums its own contiguous run, one block scan of
+// the run totals, then each run is written); out[count] = total.  For the
+// small batches, where three kernels per scan would cost more than the data.
+template <class T, int NA>
+__global__ void small_scan_kernel(const T* __restrict__ in0, const T* __restrict__ in1, const T* __restrict__ in2,
+                                  T* __restrict__ out0, T* __restrict__ out1, T* __restrict__ out2, int64_t count) {
+    __shared__ T s_w[NA][32];
+    const T* in[3] = {in0, in1, in2};
+    T* out[3] = {out0, out1, out2};
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int64_t per = (count + blockDim.x - 1) / blockDim.x;
+    const int64_t lo = min(count, (int64_t)threadIdx.x * per), hi = min(count, lo + per);
+    T sum[NA], incl[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+        sum[a] = 0;
+        for (int64_t i = lo; i < hi; ++i) sum[a] += in[a][i];
+        incl[a] = sum[a];
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const T x = __shfl_up_sync(0xffffffffu, incl[a], off);
+            if (lane >= off) incl[a] += x;
+        }
+        if (lane == 31) s_w[a][wid] = incl[a];
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+            T w = lane < nw ? s_w[a][lane] : 0;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const T x = __shfl_up_sync(0xffffffffu, w, off);
+                if (lane >= off) w += x;
+            }
+            if (lane < nw) s_w[a][lane] = w;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+        T run = (wid ? s_w[a][wid - 1] : 0) + incl[a] - sum[a];
+        for (int64_t i = lo; i < hi; ++i) {
+            const T x = in[a][i];
+            out[a][i] = run;
+            run += x;
+        }
+        if (threadIdx.x == 0) out[a][count] = s_w[a][nw - 1];
+    }
+}
+
+// Existing entries of the long rows, flattened over every thread of the grid.
+__global__ void big_scatter_old_kernel(const int32_t* __restrict__ big, const int32_t* __restrict__ big_tail,
+                                       const int32_t* __restrict__ bex, const int32_t* __restrict__ row_id,
+                                       const int32_t* __restrict__ row_first, const int32_t* __restrict__ scrX,
                                        const uint64_t* __restrict__ skey, const int8_t* __restrict__ typ,
                                        const int32_t* __restrict__ insX, const int32_t* __restrict__ delX,
                                        const int64_t* __restrict__ start, const int32_t* __restrict__ col,
-                                       const double* __restrict__ val, int64_t b, int64_t E,
-                                       int32_t* __restrict__ scol, double* __restrict__ sval,
-                                       unsigned long long* __restrict__ bad_rank) {
+                                       const double* __restrict__ val, int32_t* __restrict__ scol,
+                                       double* __restrict__ sval, unsigned long long* __restrict__ bad_rank) {
+    const int32_t nb = *big_tail;
+    const int64_t E = bex[nb];
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < E; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k = seg_of(exX, b, t);
-        const int32_t j = (int32_t)(t - exX[k]);
+        const int64_t i = seg_of(bex, nb, t);
+        const int32_t k = big[i];
+        const int32_t j = (int32_t)(t - bex[i]);
         const int32_t r = row_id[k];
         const int64_t s = start[r];
         const int32_t c = col[s + j];
-        const double w = val[s + j];
-        const int32_t a = row_first[k], z = row_first[k + 1];
-        const uint64_t key = ((uint64_t)(uint32_t)r << 32) | (uint32_t)c;
-        int32_t lo = a, hi = z;
-        while (lo < hi) {
-            const int32_t mid = (lo + hi) >> 1;
-            if (skey[mid] < key) lo = mid + 1;
-            else hi = mid;
-        }
-        bool gone = false;
-        if (lo < z && skey[lo] == key) {
-            int32_t q = lo;
-            while (q + 1 < z && skey[q + 1] == key) ++q;
-            gone = typ[q] == kDel;
-        }
-        if (!gone) {
-            const int64_t o = scrX[k] + j + (insX[lo] - insX[a]) - (delX[lo] - delX[a]);
-            if (o < scrX[k] || o >= scrX[k + 1]) {  // cannot happen for a consistent row table
-                atomicAdd(bad_rank, 1ull);
-                continue;
-            }
-            scol[o] = c;
-            sval[o] = w;
-        }
-    }
-}
-
-// Inserts -> their rank: insertion point - deletes before it + inserts before
-// it in the same row.
-__global__ void upd_scatter_new_kernel(const uint64_t* __restrict__ skey, const uint32_t* __restrict__ sidx,
-                                       const double* __restrict__ values, const int8_t* __restrict__ typ,
-                                       const int32_t* __restrict__ pos, const int32_t* __restrict__ headX,
-                                       const int32_t* __restrict__ row_first, const int32_t* __restrict__ insX,
-                                       const int32_t* __restrict__ delX, const int32_t* __restrict__ scrX, int64_t b,
-                                       int32_t* __restrict__ scol, double* __restrict__ sval,
-                                       unsigned long long* __restrict__ bad_rank) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
-        if (typ[i] != kIns) continue;
-        const int32_t k = headX[i + 1] - 1;
-        const int32_t a = row_first[k];
-        const int64_t o = scrX[k] + pos[i] + (insX[i] - insX[a]) - (delX[i] - delX[a]);
-        if (o < scrX[k] || o >= scrX[k + 1]) {
+        const int32_t rk = old_rank(skey, typ, insX, delX, row_first[k], row_first[k + 1], (uint32_t)r, c, j);
+        if (rk < 0) continue;
+        if (rk >= scrX[k + 1] - scrX[k]) {
             atomicAdd(bad_rank, 1ull);
             continue;
         }
-        scol[o] = (int32_t)(uint32_t)skey[i];
-        sval[o] = values[sidx[i]];
+        scol[scrX[k] + rk] = c;
+        sval[scrX[k] + rk] = val[s + j];
     }
 }
 
-// Rebuilt rows -> the arena: in place when the row still fits its slots,
-// else at base + relX[k].
-__global__ void upd_copyback_kernel(const int32_t* __restrict__ row_id, const int32_t* __restrict__ scrX,
-                                    const int64_t* __restrict__ relX, const int64_t* __restrict__ start,
-                                    const int32_t* __restrict__ cap, int64_t base, int64_t b, int64_t S,
-                                    const int32_t* __restrict__ scol, const double* __restrict__ sval,
-                                    int32_t* __restrict__ col, double* __restrict__ val) {
+// Inserts into the long rows.
+__global__ void big_scatter_new_kernel(const uint64_t* __restrict__ skey, const uint32_t* __restrict__ sidx,
+                                       const double* __restrict__ values, const int8_t* __restrict__ typ,
+                                       const int32_t* __restrict__ pos, const int32_t* __restrict__ headX,
+                                       const int32_t* __restrict__ row_first, const int32_t* __restrict__ insX,
+                                       const int32_t* __restrict__ delX, const int32_t* __restrict__ scrX,
+                                       const int8_t* __restrict__ big_flag, int64_t b, int32_t* __restrict__ scol,
+                                       double* __restrict__ sval, unsigned long long* __restrict__ bad_rank) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
+        if (typ[i] != kIns) continue;
+        const int32_t k = headX[i + 1] - 1;
+        if (!big_flag[k]) continue;
+        const int32_t rk = new_rank(pos, insX, delX, row_first[k], (int32_t)i);
+        if (rk < 0 || rk >= scrX[k + 1] - scrX[k]) {
+            atomicAdd(bad_rank, 1ull);
+            continue;
+        }
+        scol[scrX[k] + rk] = (int32_t)(uint32_t)skey[i];
+        sval[scrX[k] + rk] = values[sidx[i]];
+    }
+}
+
+// Long rows: scratch -> their slots (in place when they fit, else fresh ones).
+__global__ void big_copy_kernel(const int32_t* __restrict__ big, const int32_t* __restrict__ big_tail,
+                                const int32_t* __restrict__ bsz, const int32_t* __restrict__ row_id,
+                                const int32_t* __restrict__ scrX, const int64_t* __restrict__ relX,
+                                const int64_t* __restrict__ start, const int32_t* __restrict__ cap, int64_t base,
+                                const int32_t* __restrict__ scol, const double* __restrict__ sval,
+                                int32_t* __restrict__ col, double* __restrict__ val) {
+    const int32_t nb = *big_tail;
+    const int64_t S = bsz[nb];
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < S; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k = seg_of(scrX, b, t);
+        const int64_t i = seg_of(bsz, nb, t);
+        const int32_t k = big[i];
         const int32_t r = row_id[k];
         const int32_t d2 = scrX[k + 1] - scrX[k];
-        const int64_t dst = (d2 <= cap[r] ? start[r] : base + relX[k]) + (t - scrX[k]);
-        col[dst] = scol[t];
-        val[dst] = sval[t];
+        const int64_t j = t - bsz[i];
+        const int64_t dst = (d2 <= cap[r] ? start[r] : base + relX[k]) + j;
+        col[dst] = scol[scrX[k] + j];
+        val[dst] = sval[scrX[k] + j];
     }
 }
 
-__global__ void upd_finalize_kernel(const int32_t* __restrict__ row_id, const int32_t* __restrict__ headX,
-                                    const int32_t* __restrict__ scrX, const int32_t* __restrict__ exX,
-                                    const int64_t* __restrict__ relX, int64_t base, int64_t b,
-                                    int64_t* __restrict__ start, int32_t* __restrict__ deg,
-                                    int32_t* __restrict__ cap, unsigned long long* __restrict__ n_moved) {
-    const int64_t K = headX[b];
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t d = exX[k + 1] - exX[k], d2 = scrX[k + 1] - scrX[k];
-        if (d == 0 && d2 == 0) continue;  // row without inserts or deletes
+__global__ void big_finalize_kernel(const int32_t* __restrict__ big, const int32_t* __restrict__ big_tail,
+                                    const int32_t* __restrict__ row_id, const int32_t* __restrict__ scrX,
+                                    const int64_t* __restrict__ relX, int64_t base, int64_t* __restrict__ start,
+                                    int32_t* __restrict__ deg, int32_t* __restrict__ cap,
+                                    unsigned long long* __restrict__ moved) {
+    const int32_t nb = *big_tail;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+        const int32_t k = big[i];
         const int32_t r = row_id[k];
+        const int32_t d2 = scrX[k + 1] - scrX[k];
         if (d2 > cap[r]) {
             start[r] = base + relX[k];
             cap[r] = (int32_t)slack_cap(d2);
-            atomicAdd(n_moved, 1ull);
+            atomicAdd(moved, 1ull);
         }
         deg[r] = d2;
     }
@@ -352,15 +515,17 @@ __global__ void set_caps_kernel(const int64_t* __restrict__ want, int32_t n, int
         cap[v] = (int32_t)want[v];
 }
 
-// Copy every row (src_start/deg in the arena) to dst_off[v].  A warp takes 32
-// consecutive rows, scans their lengths and copies the concatenation 32
-// entries per step (each lane finds its row by a 5-step shuffle search);
-// rows of kCopyBig or more entries are left to row_copy_big_kernel.
+// Copy every row shorter than kCopyChunk (sstart/deg in the arena) to
+// dst_off[v].  A warp takes 32 consecutive rows, scans their lengths and
+// copies the concatenation, four 32-entry steps per round (each lane finds
+// its row by a 5-step shuffle search; the loads of a round are issued before
+// its stores).  Longer rows only get their chunk count, cc[v], for
+// row_copy_chunk_kernel.
 template <class DstOff>
 __global__ void row_copy_kernel(int32_t n, const int64_t* __restrict__ sstart, const int32_t* __restrict__ deg,
                                 const int32_t* __restrict__ scol, const double* __restrict__ sval,
                                 const DstOff* __restrict__ dst_off, int32_t* __restrict__ dcol,
-                                double* __restrict__ dval, int32_t* __restrict__ big, int32_t* __restrict__ big_tail) {
+                                double* __restrict__ dval, int32_t* __restrict__ cc) {
     const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -372,10 +537,8 @@ __global__ void row_copy_kernel(int32_t n, const int64_t* __restrict__ sstart, c
             d = deg[v];
             s = sstart[v];
             o = (int64_t)dst_off[v];
-            if (d >= kCopyBig) {
-                big[warp_append_active(big_tail)] = (int32_t)v;
-                d = 0;
-            }
+            cc[v] = d >= kCopyChunk ? (d + kCopyChunk - 1) / kCopyChunk : 0;
+            if (d >= kCopyChunk) d = 0;
         }
         int32_t incl = d;
 #pragma unroll
@@ -385,40 +548,78 @@ __global__ void row_copy_kernel(int32_t n, const int64_t* __restrict__ sstart, c
         }
         const int32_t excl = incl - d;
         const int32_t tot = __shfl_sync(0xffffffffu, incl, 31);
-        for (int32_t q0 = 0; q0 < tot; q0 += 32) {
-            const int32_t q = q0 + lane;
-            int w = 0;
+        for (int32_t q0 = 0; q0 < tot; q0 += 128) {
+            int64_t src[4], dst[4];
+            int32_t cv[4];
+            double wv[4];
 #pragma unroll
-            for (int step = 16; step > 0; step >>= 1) {
-                const int32_t x = __shfl_sync(0xffffffffu, incl, w + step - 1);
-                if (x <= q) w += step;
+            for (int u = 0; u < 4; ++u) {
+                const int32_t q = q0 + 32 * u + lane;
+                int w = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int32_t x = __shfl_sync(0xffffffffu, incl, w + step - 1);
+                    if (x <= q) w += step;
+                }
+                const int64_t sw = __shfl_sync(0xffffffffu, s, w);
+                const int64_t ow = __shfl_sync(0xffffffffu, o, w);
+                const int32_t ew = __shfl_sync(0xffffffffu, excl, w);
+                src[u] = q < tot ? sw + (q - ew) : -1;
+                dst[u] = ow + (q - ew);
             }
-            const int64_t sw = __shfl_sync(0xffffffffu, s, w);
-            const int64_t ow = __shfl_sync(0xffffffffu, o, w);
-            const int32_t ew = __shfl_sync(0xffffffffu, excl, w);
-            if (q < tot) {
-                const int32_t j = q - ew;
-                dcol[ow + j] = scol[sw + j];
-                if (dval) dval[ow + j] = sval[sw + j];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (src[u] >= 0) {
+                    cv[u] = scol[src[u]];
+                    if (dval) wv[u] = sval[src[u]];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (src[u] >= 0) {
+                    dcol[dst[u]] = cv[u];
+                    if (dval) dval[dst[u]] = wv[u];
+                }
             }
         }
     }
 }
 
+// Chunks of the long rows, one warp each (8 entries per lane, loads first):
+// chunk c belongs to the row v with coff[v] <= c < coff[v + 1].
 template <class DstOff>
-__global__ void row_copy_big_kernel(const int32_t* __restrict__ big, const int32_t* __restrict__ big_tail,
-                                    const int64_t* __restrict__ sstart, const int32_t* __restrict__ deg,
-                                    const int32_t* __restrict__ scol, const double* __restrict__ sval,
-                                    const DstOff* __restrict__ dst_off, int32_t* __restrict__ dcol,
-                                    double* __restrict__ dval) {
-    const int32_t count = *big_tail;
-    for (int32_t i = blockIdx.x; i < count; i += gridDim.x) {
-        const int32_t v = big[i];
-        const int64_t s = sstart[v], o = (int64_t)dst_off[v];
+__global__ void row_copy_chunk_kernel(int32_t n, const int32_t* __restrict__ coff, const int64_t* __restrict__ sstart,
+                                      const int32_t* __restrict__ deg, const int32_t* __restrict__ scol,
+                                      const double* __restrict__ sval, const DstOff* __restrict__ dst_off,
+                                      int32_t* __restrict__ dcol, double* __restrict__ dval) {
+    const int lane = lane_id();
+    const int64_t C = coff[n];
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c = warp; c < C; c += nwarps) {
+        const int64_t v = seg_of(coff, n, c);
         const int32_t d = deg[v];
-        for (int32_t j = threadIdx.x; j < d; j += blockDim.x) {
-            dcol[o + j] = scol[s + j];
-            if (dval) dval[o + j] = sval[s + j];
+        const int32_t j0 = (int32_t)(c - coff[v]) * kCopyChunk;
+        const int64_t s = sstart[v] + j0, o = (int64_t)dst_off[v] + j0;
+        const int32_t len = min(kCopyChunk, d - j0);
+        constexpr int kPer = kCopyChunk / 32;
+        int32_t cv[kPer];
+        double wv[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int32_t j = u * 32 + lane;
+            if (j < len) {
+                cv[u] = scol[s + j];
+                if (dval) wv[u] = sval[s + j];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int32_t j = u * 32 + lane;
+            if (j < len) {
+                dcol[o + j] = cv[u];
+                if (dval) dval[o + j] = wv[u];
+            }
         }
     }
 }
@@ -491,18 +692,18 @@ unsigned grid_of(ghb_workspace* ws, int64_t items, int threads = 256) {
 }
 
 // Copy n rows (sstart/deg into scol/sval) to dst offsets (int32 CSR offsets
-// or int64 arena starts).  `big` holds n int32, `big_tail` one.
+// or int64 arena starts).  `list` holds n + 2 int32.
 template <class DstOff>
 int copy_rows(ghb_workspace* ws, int32_t n, const int64_t* sstart, const int32_t* deg, const int32_t* scol,
-              const double* sval, const DstOff* dst_off, int32_t* dcol, double* dval, int32_t* big,
-              int32_t* big_tail) {
-    GHB_CUDA_TRY(cudaMemsetAsync(big_tail, 0, sizeof(int32_t), ws->stream));
+              const double* sval, const DstOff* dst_off, int32_t* dcol, double* dval, int32_t* cc, int32_t* coff,
+              int64_t* block_sums) {
     const unsigned grid = grid_for(((int64_t)n + 31) / 32 * 32, 256, (int64_t)ws->num_sms * 8);
     const double* sv = dval ? sval : nullptr;
     GHB_TRY(launch(ws, row_copy_kernel<DstOff>, dim3(grid), dim3(256), 0, n, sstart, deg, scol, sv, dst_off, dcol,
-                   dval, big, big_tail));
-    GHB_TRY(launch(ws, row_copy_big_kernel<DstOff>, dim3(ws->num_sms * 4), dim3(256), 0, (const int32_t*)big,
-                   (const int32_t*)big_tail, sstart, deg, scol, sv, dst_off, dcol, dval));
+                   dval, cc));
+    GHB_TRY(scan_exclusive_i32(ws, cc, coff, n, block_sums));
+    GHB_TRY(launch(ws, row_copy_chunk_kernel<DstOff>, dim3(ws->num_sms * 8), dim3(256), 0, n, (const int32_t*)coff,
+                   sstart, deg, scol, sv, dst_off, dcol, dval));
     return GHB_OK;
 }
 
@@ -522,7 +723,8 @@ int repack(ghb_workspace* ws, ghb_gpma* g, const int64_t* src_start, const int32
     int st = GHB_OK;
     do {
         if ((st = dev_alloc(&nstart, (int64_t)n + 1))) break;
-        if ((st = dev_alloc(&big, (int64_t)n + 1))) break;
+        // cc, coff (n + 1 int32 each) and the scan's block sums
+        if ((st = dev_alloc(&big, 2 * ((int64_t)n + 1) + 2 * scan_scratch_words(n)))) break;
         // nstart = exclusive scan of want; nstart[n] = total slots.
         cudaError_t e = cudaMemsetAsync(want + n, 0, sizeof(int64_t), ws->stream);
         if (e == cudaSuccess)
@@ -548,7 +750,7 @@ int repack(ghb_workspace* ws, ghb_gpma* g, const int64_t* src_start, const int32
         if ((st = dev_alloc(&ncol, slots))) break;
         if ((st = dev_alloc(&nval, slots))) break;
         if ((st = copy_rows<int64_t>(ws, n, src_start, g->deg, src_col, src_val, nstart, ncol, nval, big,
-                                     big + n)))
+                                     big + n + 1, reinterpret_cast<int64_t*>(big + 2 * ((int64_t)n + 1)))))
             break;
         if ((st = launch(ws, set_caps_kernel, dim3(grid_of(ws, n)), dim3(256), 0, (const int64_t*)want, n, g->cap)))
             break;
@@ -596,6 +798,8 @@ struct PassArrays {
     int8_t* typ;
     int32_t *insX, *delX, *headX, *row_id, *row_first, *scrn, *exn, *scrX, *exX;
     int64_t *reln, *relX, *block_sums;
+    int32_t *big, *big_tail, *big_d, *big_d2, *bex, *bsz;
+    int8_t* big_flag;
     void* tmp;
     int32_t* scol;
     double* sval;
@@ -622,6 +826,13 @@ void carve_pass(Carver& c, int64_t b, size_t tmp_bytes, PassArrays& a) {
     a.reln = c.take<int64_t>(b + 1);
     a.relX = c.take<int64_t>(b + 1);
     a.block_sums = c.take<int64_t>(scan_scratch_words(b + 1));
+    a.bex = c.take<int32_t>(b + 1);
+    a.bsz = c.take<int32_t>(b + 1);
+    a.big = c.take<int32_t>(b);
+    a.big_d = c.take<int32_t>(b);
+    a.big_d2 = c.take<int32_t>(b);
+    a.big_tail = c.take<int32_t>(1);
+    a.big_flag = c.take<int8_t>(b);
     a.tmp = c.take<char>(tmp_bytes);
 }
 
@@ -643,12 +854,14 @@ int apply_pass(ghb_workspace* ws, ghb_gpma* g, const uint64_t* keys, const doubl
     carve_pass(c, b, tmp_bytes, a);
 
     // dev_small: [0..5] totals, [6] modified, [7] invalid keys, [8] ranks
-    // outside their row (a consistency check of the row table).
+    // outside their row (a consistency check of the row table), [9] rows for
+    // the grid-wide rebuild.
     int64_t* small = ws->dev_small;
     unsigned long long* n_mod = reinterpret_cast<unsigned long long*>(small + 6);
     unsigned long long* n_bad = reinterpret_cast<unsigned long long*>(small + 7);
     unsigned long long* bad_rank = reinterpret_cast<unsigned long long*>(small + 8);
-    GHB_CUDA_TRY(cudaMemsetAsync(small, 0, sizeof(int64_t) * 9, ws->stream));
+    unsigned long long* n_long = reinterpret_cast<unsigned long long*>(small + 9);
+    GHB_CUDA_TRY(cudaMemsetAsync(small, 0, sizeof(int64_t) * 10, ws->stream));
     const unsigned gr = grid_of(ws, b);
 
     GHB_TRY(launch(ws, upd_prep_kernel, dim3(gr), dim3(256), 0, keys, b, n, a.idx, n_bad));
@@ -659,31 +872,47 @@ int apply_pass(ghb_workspace* ws, ghb_gpma* g, const uint64_t* keys, const doubl
     GHB_TRY(launch(ws, upd_classify_kernel, dim3(gr), dim3(256), 0, (const int64_t*)g->start,
                    (const int32_t*)g->deg, (const int32_t*)g->col, (const uint64_t*)a.skey,
                    (const uint32_t*)a.sidx, values, b, n, a.ins, a.del, a.head, a.pos, a.typ, n_mod));
-    GHB_TRY(scan_exclusive_i32(ws, a.ins, a.insX, b, a.block_sums));
-    GHB_TRY(scan_exclusive_i32(ws, a.del, a.delX, b, a.block_sums));
-    GHB_TRY(scan_exclusive_i32(ws, a.head, a.headX, b, a.block_sums));
+    const bool small_b = b <= kSmallScan;
+    const int32_t row_warp_max = small_b ? kRowWarpSmall : kRowWarpLarge;
+    if (small_b) {
+        GHB_TRY(launch(ws, small_scan_kernel<int32_t, 3>, dim3(1), dim3(1024), 0, (const int32_t*)a.ins,
+                       (const int32_t*)a.del, (const int32_t*)a.head, a.insX, a.delX, a.headX, b));
+    } else {
+        GHB_TRY(scan_exclusive_i32(ws, a.ins, a.insX, b, a.block_sums));
+        GHB_TRY(scan_exclusive_i32(ws, a.del, a.delX, b, a.block_sums));
+        GHB_TRY(scan_exclusive_i32(ws, a.head, a.headX, b, a.block_sums));
+    }
     GHB_TRY(launch(ws, upd_rows_kernel, dim3(gr), dim3(256), 0, (const uint64_t*)a.skey, (const int32_t*)a.head,
                    (const int32_t*)a.headX, b, a.row_id, a.row_first));
     GHB_TRY(launch(ws, upd_row_summary_kernel, dim3(gr), dim3(256), 0, (const int32_t*)a.row_id,
                    (const int32_t*)a.row_first, (const int32_t*)a.headX, (const int32_t*)a.insX,
                    (const int32_t*)a.delX, (const int32_t*)g->deg, (const int32_t*)g->cap, b, a.scrn, a.exn,
-                   a.reln));
-    GHB_TRY(scan_exclusive_i32(ws, a.scrn, a.scrX, b, a.block_sums));
-    GHB_TRY(scan_exclusive_i32(ws, a.exn, a.exX, b, a.block_sums));
-    GHB_CUDA_TRY(cudaMemsetAsync(a.reln + b, 0, sizeof(int64_t), ws->stream));
-    size_t cb = scan_bytes;
-    GHB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(a.tmp, cb, a.reln, a.relX, b + 1, ws->stream));
-    ws->launches++;
+                   a.reln, row_warp_max, n_long));
+    if (small_b) {
+        GHB_TRY(launch(ws, small_scan_kernel<int32_t, 2>, dim3(1), dim3(1024), 0, (const int32_t*)a.scrn,
+                       (const int32_t*)a.exn, (const int32_t*)nullptr, a.scrX, a.exX, (int32_t*)nullptr, b));
+        GHB_TRY(launch(ws, small_scan_kernel<int64_t, 1>, dim3(1), dim3(1024), 0, (const int64_t*)a.reln,
+                       (const int64_t*)nullptr, (const int64_t*)nullptr, a.relX, (int64_t*)nullptr,
+                       (int64_t*)nullptr, b));
+    } else {
+        GHB_TRY(scan_exclusive_i32(ws, a.scrn, a.scrX, b, a.block_sums));
+        GHB_TRY(scan_exclusive_i32(ws, a.exn, a.exX, b, a.block_sums));
+        GHB_CUDA_TRY(cudaMemsetAsync(a.reln + b, 0, sizeof(int64_t), ws->stream));
+        size_t cb = scan_bytes;
+        GHB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(a.tmp, cb, a.reln, a.relX, b + 1, ws->stream));
+        ws->launches++;
+    }
     GHB_TRY(launch(ws, upd_totals_kernel, dim3(1), dim3(32), 0, (const int32_t*)a.insX, (const int32_t*)a.delX,
                    (const int32_t*)a.headX, (const int32_t*)a.scrX, (const int32_t*)a.exX, (const int64_t*)a.relX, b,
                    small));
-    GHB_TRY(ws_read_small(ws, 8));
+    GHB_TRY(ws_read_small(ws, 10));
     const int64_t* h = ws->host_pinned;
     if (h[7]) {
         set_error("invalid argument: update key with a row or column outside [0, n)");
         return GHB_ERR_INVALID_ARGUMENT;
     }
-    const int64_t n_ins = h[0], n_del = h[1], S = h[3], E = h[4], R = h[5], n_modified = h[6];
+    const int64_t n_ins = h[0], n_del = h[1], K = h[2], S = h[3], E = h[4], R = h[5], n_modified = h[6];
+    const int64_t n_long_rows = h[9];
     if (g->m + n_ins - n_del > kMaxEntries) {
         set_error("dynamic graph would exceed 2^31 - 1 entries");
         return GHB_ERR_LIMIT;
@@ -727,25 +956,50 @@ int apply_pass(ghb_workspace* ws, ghb_gpma* g, const uint64_t* keys, const doubl
                        (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
                        (const int64_t*)g->start, b, g->val));
     if (S > 0 || E > 0) {
-        if (E > 0)
-            GHB_TRY(launch(ws, upd_scatter_old_kernel, dim3(grid_of(ws, E)), dim3(256), 0, (const int32_t*)a.row_id,
-                           (const int32_t*)a.row_first, (const int32_t*)a.exX, (const int32_t*)a.scrX,
-                           (const uint64_t*)a.skey, (const int8_t*)a.typ, (const int32_t*)a.insX,
-                           (const int32_t*)a.delX, (const int64_t*)g->start, (const int32_t*)g->col,
-                           (const double*)g->val, b, E, scol, sval, bad_rank));
-        if (n_ins > 0)
-            GHB_TRY(launch(ws, upd_scatter_new_kernel, dim3(gr), dim3(256), 0, (const uint64_t*)a.skey,
-                           (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
-                           (const int32_t*)a.headX, (const int32_t*)a.row_first, (const int32_t*)a.insX,
-                           (const int32_t*)a.delX, (const int32_t*)a.scrX, b, scol, sval, bad_rank));
-        if (S > 0)
-            GHB_TRY(launch(ws, upd_copyback_kernel, dim3(grid_of(ws, S)), dim3(256), 0, (const int32_t*)a.row_id,
+        const unsigned wide = (unsigned)ws->num_sms * 16;
+        GHB_CUDA_TRY(cudaMemsetAsync(a.big_tail, 0, sizeof(int32_t), ws->stream));
+        if (n_long_rows > 0) {
+            GHB_CUDA_TRY(cudaMemsetAsync(a.big_d, 0, sizeof(int32_t) * (size_t)b, ws->stream));
+            GHB_CUDA_TRY(cudaMemsetAsync(a.big_d2, 0, sizeof(int32_t) * (size_t)b, ws->stream));
+        }
+        GHB_TRY(launch(ws, upd_rows_warp_kernel, dim3(grid_for(K * 32, 256, (int64_t)ws->num_sms * 8)), dim3(256), 0,
+                       (const int32_t*)a.row_id,
+                       (const int32_t*)a.row_first, (const int32_t*)a.headX, (const int32_t*)a.scrX,
+                       (const int32_t*)a.exX, (const int64_t*)a.relX, (const uint64_t*)a.skey,
+                       (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
+                       (const int32_t*)a.insX, (const int32_t*)a.delX, base, b, g->start, g->deg, g->cap, g->col,
+                       g->val, scol, sval, a.big, a.big_tail, a.big_d, a.big_d2, a.big_flag, row_warp_max, g->moved,
+                       bad_rank));
+        if (n_long_rows > 0) {
+            // Offsets of the long rows' entries, in list order (zeros past it).
+            if (small_b) {
+                GHB_TRY(launch(ws, small_scan_kernel<int32_t, 2>, dim3(1), dim3(1024), 0, (const int32_t*)a.big_d,
+                               (const int32_t*)a.big_d2, (const int32_t*)nullptr, a.bex, a.bsz, (int32_t*)nullptr,
+                               b));
+            } else {
+                GHB_TRY(scan_exclusive_i32(ws, a.big_d, a.bex, b, a.block_sums));
+                GHB_TRY(scan_exclusive_i32(ws, a.big_d2, a.bsz, b, a.block_sums));
+            }
+            GHB_TRY(launch(ws, big_scatter_old_kernel, dim3(wide), dim3(256), 0, (const int32_t*)a.big,
+                           (const int32_t*)a.big_tail, (const int32_t*)a.bex, (const int32_t*)a.row_id,
+                           (const int32_t*)a.row_first, (const int32_t*)a.scrX, (const uint64_t*)a.skey,
+                           (const int8_t*)a.typ, (const int32_t*)a.insX, (const int32_t*)a.delX,
+                           (const int64_t*)g->start, (const int32_t*)g->col, (const double*)g->val, scol, sval,
+                           bad_rank));
+            if (n_ins > 0)
+                GHB_TRY(launch(ws, big_scatter_new_kernel, dim3(gr), dim3(256), 0, (const uint64_t*)a.skey,
+                               (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
+                               (const int32_t*)a.headX, (const int32_t*)a.row_first, (const int32_t*)a.insX,
+                               (const int32_t*)a.delX, (const int32_t*)a.scrX, (const int8_t*)a.big_flag, b, scol,
+                               sval, bad_rank));
+            GHB_TRY(launch(ws, big_copy_kernel, dim3(wide), dim3(256), 0, (const int32_t*)a.big,
+                           (const int32_t*)a.big_tail, (const int32_t*)a.bsz, (const int32_t*)a.row_id,
                            (const int32_t*)a.scrX, (const int64_t*)a.relX, (const int64_t*)g->start,
-                           (const int32_t*)g->cap, base, b, S, (const int32_t*)scol, (const double*)sval, g->col,
-                           g->val));
-        GHB_TRY(launch(ws, upd_finalize_kernel, dim3(gr), dim3(256), 0, (const int32_t*)a.row_id,
-                       (const int32_t*)a.headX, (const int32_t*)a.scrX, (const int32_t*)a.exX,
-                       (const int64_t*)a.relX, base, b, g->start, g->deg, g->cap, g->moved));
+                           (const int32_t*)g->cap, base, (const int32_t*)scol, (const double*)sval, g->col, g->val));
+            GHB_TRY(launch(ws, big_finalize_kernel, dim3(ws->num_sms), dim3(256), 0, (const int32_t*)a.big,
+                           (const int32_t*)a.big_tail, (const int32_t*)a.row_id, (const int32_t*)a.scrX,
+                           (const int64_t*)a.relX, base, g->start, g->deg, g->cap, g->moved));
+        }
     }
     // Without a repack every row counted in R moved to its new slots.
     if (!repacked) g->used += R;
@@ -785,13 +1039,15 @@ int snapshot(ghb_workspace* ws, ghb_gpma* g, bool weights) {
     Carver sizing(nullptr);
     sizing.take<int64_t>(scan_scratch_words((int64_t)n));
     sizing.take<int32_t>((int64_t)n + 1);
+    sizing.take<int32_t>((int64_t)n + 1);
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
     int64_t* block_sums = c.take<int64_t>(scan_scratch_words((int64_t)n));
-    int32_t* big = c.take<int32_t>((int64_t)n + 1);
+    int32_t* cc = c.take<int32_t>((int64_t)n + 1);
+    int32_t* coff = c.take<int32_t>((int64_t)n + 1);
     GHB_TRY(scan_exclusive_i32(ws, g->deg, g->s_rowptr, n, block_sums));
     GHB_TRY(copy_rows<int32_t>(ws, n, g->start, g->deg, g->col, g->val, g->s_rowptr, g->s_col,
-                               weights ? g->s_val : nullptr, big, big + n));
+                               weights ? g->s_val : nullptr, cc, coff, block_sums));
     g->s_ok = true;
     g->s_val_ok = weights;
     return GHB_OK;

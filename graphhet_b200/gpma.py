@@ -121,12 +121,26 @@ class DynamicGraph:
                                   ctypes.byref(w)), "ghb_gpma_csr")
         return rp.value, col.value, w.value
 
-    def csr_graph(self, weights: bool = True, device=None) -> CSRGraph:
-        """A copy of the current graph as an (undirected-layout) CSRGraph."""
+    def csr_graph(self, weights: bool = True, directed: bool = False, in_graph: Optional["DynamicGraph"] = None,
+                  device=None) -> CSRGraph:
+        """A copy of the current graph as a CSRGraph.  Undirected (the
+        default): the rows hold both directions.  Directed: the in-rows come
+        from `in_graph` (the reference keeps an in-GPMA beside the out-GPMA,
+        LDBC_GPU_gpma.cu:155-211) or, without one, from a transpose."""
         n, m, _, _ = self.info()
         dev = device or torch.device("cuda", torch.cuda.current_device())
         rp = torch.empty(n + 1, dtype=torch.int32, device=dev)
         col = torch.empty(max(1, m), dtype=torch.int32, device=dev)
         w = torch.empty(max(1, m), dtype=torch.float64, device=dev) if weights else None
         _check(lib().ghb_gpma_export(_ws(self._ws), self._h, _ptr(rp), _ptr(col), _ptr(w)), "ghb_gpma_export")
-        return CSRGraph(n=n, rowptr=rp, col=col[:m], w=w[:m] if w is not None else None, directed=False)
+        g = CSRGraph(n=n, rowptr=rp, col=col[:m], w=w[:m] if w is not None else None, directed=directed)
+        if directed:
+            if in_graph is not None:
+                ig = in_graph.csr_graph(weights=weights, device=dev)
+                if ig.n != n:
+                    raise GhbError("in_graph has a different vertex count")
+                g.in_rowptr, g.in_col, g.in_w = ig.rowptr, ig.col, ig.w
+            else:
+                from . import transpose_csr
+                g.in_rowptr, g.in_col, g.in_w = transpose_csr(n, g.rowptr, g.col, g.w, ws=self._ws)
+        return g

@@ -210,3 +210,55 @@ def test_analytics_after_updates(G):
     assert np.array_equal(G.tc(g)[1].cpu().numpy(), O.tc(upd))
     rg = G.ResidentGraph(g)
     assert np.array_equal(rg.bfs(src)[0].cpu().numpy(), O.bfs(upd, src))
+
+
+def test_directed_out_and_in_graphs(G):
+    """The reference's pair of GPMAs for a directed graph (out rows keyed
+    (u, v), in rows keyed (v, u), LDBC_GPU_gpma.cu:155-211): both take the same
+    edits, and the analytics read them as one directed CSRGraph."""
+    og = O.rmat_graph(12, 16, 31, directed=True)
+    n = og.n
+    out_g = G.DynamicGraph.from_csr(t(og.rowptr), t(og.col), t(og.w))
+    in_g = G.DynamicGraph.from_csr(t(og.in_rowptr), t(og.in_col), t(og.in_w))
+    keys, vals = O.gpma_from_csr(og.rowptr, og.col, og.w)
+    rng = np.random.default_rng(17)
+    for _ in range(3):
+        bk, bv = random_batch(rng, n, keys, 8000)
+        keep = (bk >> 32) != (bk & 0xFFFFFFFF)  # no self-loops
+        bk, bv = bk[keep], bv[keep]
+        keys, vals = update(out_g, keys, vals, bk, bv)
+        rev = ((bk & 0xFFFFFFFF) << 32) | (bk >> 32)
+        in_g.update(t(rev), t(bv))
+    rp, col, w = O.gpma_to_csr(n, keys, vals)
+    rk = ((keys & 0xFFFFFFFF) << 32) | (keys >> 32)
+    o = np.argsort(rk)
+    irp, icol, iw = O.gpma_to_csr(n, rk[o], vals[o])
+    upd = O.Graph(n, rp, col, w, True, irp, icol, iw)
+    for g in (out_g.csr_graph(directed=True, in_graph=in_g), out_g.csr_graph(directed=True)):
+        assert np.array_equal(g.in_rowptr.cpu().numpy(), irp) and np.array_equal(g.in_col.cpu().numpy(), icol)
+        src = int(np.argmax(np.diff(rp)))
+        assert np.array_equal(G.bfs(g, src)[0].cpu().numpy(), O.bfs(upd, src))
+        assert np.array_equal(G.sssp(g, src)[0].cpu().numpy(), O.sssp(upd, src))
+        assert np.array_equal(G.wcc(g).cpu().numpy(), O.wcc(upd))
+        pr, _, _ = G.pagerank(g, 10, 0.85)
+        ref = O.pagerank(upd, 10, 0.85)
+        assert float(np.abs(pr.cpu().numpy() - ref).sum() / np.abs(ref).sum()) <= 1e-6
+        assert np.array_equal(G.cdlp(g, 10).cpu().numpy(), O.cdlp(upd, 10))
+
+
+def test_long_rows_take_the_flattened_path(G):
+    """Rows with more than 4,096 existing entries + updates are rebuilt by the
+    grid-wide kernels: a star whose centre row grows, shrinks and moves."""
+    n = 50000
+    hub_cols = np.arange(1, 30001)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = len(hub_cols)
+    dg = G.DynamicGraph.from_csr(t(rp), t(hub_cols.astype(np.int32)))
+    keys, vals = O.gpma_from_csr(rp, hub_cols)
+    rng = np.random.default_rng(4)
+    for _ in range(4):
+        c = rng.integers(n, size=20000)
+        bk = O.gpma_keys(np.zeros(len(c), np.int64), c)
+        bv = np.where(rng.random(len(c)) < 0.45, 0.0, rng.uniform(0.5, 1.5, len(c)))
+        keys, vals = update(dg, keys, vals, bk, bv)
+        assert_state(dg, n, keys, vals)
