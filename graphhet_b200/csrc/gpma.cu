@@ -75,6 +75,9 @@ constexpr int32_t kCopyChunk = 256;
 // kRowWarpLarge otherwise); longer rows by the grid-wide kernels.
 constexpr int32_t kRowWarpSmall = 256;
 constexpr int32_t kRowWarpLarge = 4096;
+// The grid-wide kernels give each warp a chunk of this many entries of a
+// long row (one search for the chunk's row, 8 entries per lane).
+constexpr int32_t kBigChunk = 256;
 // Batches up to this many updates scan their flags in one block.
 constexpr int64_t kSmallScan = 32768;
 // Live entries are bounded so the snapshot's int32 offsets hold them.
@@ -270,8 +273,9 @@ __device__ __forceinline__ int32_t new_rank(const int32_t* __restrict__ pos, con
 // scratch range, then (after __syncwarp, which orders the warp's scratch
 // writes before its reads) copy the range to the row's slots, in place or
 // to fresh ones at base + relX[k], and finish deg / start / cap.  Longer rows
-// go to `big` (with their old and new lengths in big_d / big_d2, zero past
-// the list) for the flattened kernels; big_flag[k] tells them apart.
+// go to `big` (with the chunk counts of their old and new entries in big_d /
+// big_d2, zero past the list) for the grid-wide kernels; big_flag[k] tells
+// them apart.
 __global__ void upd_rows_warp_kernel(const int32_t* __restrict__ row_id, const int32_t* __restrict__ row_first,
                                      const int32_t* __restrict__ headX, const int32_t* __restrict__ scrX,
                                      const int32_t* __restrict__ exX, const int64_t* __restrict__ relX,
@@ -300,8 +304,8 @@ __global__ void upd_rows_warp_kernel(const int32_t* __restrict__ row_id, const i
             if (is_big) {
                 const int32_t i = atomicAdd(big_tail, 1);
                 big[i] = (int32_t)k;
-                big_d[i] = d;
-                big_d2[i] = d2;
+                big_d[i] = (d + kBigChunk - 1) / kBigChunk;
+                big_d2[i] = (d2 + kBigChunk - 1) / kBigChunk;
             }
         }
         if (!changed || is_big) continue;
@@ -401,32 +405,47 @@ __global__ void small_scan_kernel(const T* __restrict__ in0, const T* __restrict
     }
 }
 
-// Existing entries of the long rows, flattened over every thread of the grid.
+// Existing entries of the long rows: warp per kBigChunk-entry chunk, chunk c
+// of row big[i] for bex[i] <= c < bex[i + 1].
 __global__ void big_scatter_old_kernel(const int32_t* __restrict__ big, const int32_t* __restrict__ big_tail,
                                        const int32_t* __restrict__ bex, const int32_t* __restrict__ row_id,
                                        const int32_t* __restrict__ row_first, const int32_t* __restrict__ scrX,
-                                       const uint64_t* __restrict__ skey, const int8_t* __restrict__ typ,
-                                       const int32_t* __restrict__ insX, const int32_t* __restrict__ delX,
-                                       const int64_t* __restrict__ start, const int32_t* __restrict__ col,
-                                       const double* __restrict__ val, int32_t* __restrict__ scol,
-                                       double* __restrict__ sval, unsigned long long* __restrict__ bad_rank) {
+                                       const int32_t* __restrict__ exX, const uint64_t* __restrict__ skey,
+                                       const int8_t* __restrict__ typ, const int32_t* __restrict__ insX,
+                                       const int32_t* __restrict__ delX, const int64_t* __restrict__ start,
+                                       const int32_t* __restrict__ col, const double* __restrict__ val,
+                                       int32_t* __restrict__ scol, double* __restrict__ sval,
+                                       unsigned long long* __restrict__ bad_rank) {
+    const int lane = lane_id();
     const int32_t nb = *big_tail;
-    const int64_t E = bex[nb];
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < E; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = seg_of(bex, nb, t);
+    const int64_t C = bex[nb];
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t ch = warp; ch < C; ch += nwarps) {
+        const int64_t i = seg_of(bex, nb, ch);
         const int32_t k = big[i];
-        const int32_t j = (int32_t)(t - bex[i]);
         const int32_t r = row_id[k];
+        const int32_t d = exX[k + 1] - exX[k], d2 = scrX[k + 1] - scrX[k];
+        const int32_t a = row_first[k], z = row_first[k + 1];
         const int64_t s = start[r];
-        const int32_t c = col[s + j];
-        const int32_t rk = old_rank(skey, typ, insX, delX, row_first[k], row_first[k + 1], (uint32_t)r, c, j);
-        if (rk < 0) continue;
-        if (rk >= scrX[k + 1] - scrX[k]) {
-            atomicAdd(bad_rank, 1ull);
-            continue;
+        const int32_t o = scrX[k];
+        const int32_t j0 = (int32_t)(ch - bex[i]) * kBigChunk;
+        unsigned long long bad = 0;
+#pragma unroll 2
+        for (int u = 0; u < kBigChunk / 32; ++u) {
+            const int32_t j = j0 + u * 32 + lane;
+            if (j >= d) break;
+            const int32_t c = col[s + j];
+            const int32_t rk = old_rank(skey, typ, insX, delX, a, z, (uint32_t)r, c, j);
+            if (rk < 0) continue;
+            if (rk >= d2) {
+                ++bad;
+                continue;
+            }
+            scol[o + rk] = c;
+            sval[o + rk] = val[s + j];
         }
-        scol[scrX[k] + rk] = c;
-        sval[scrX[k] + rk] = val[s + j];
+        if (bad) atomicAdd(bad_rank, bad);
     }
 }
 
@@ -452,24 +471,46 @@ __global__ void big_scatter_new_kernel(const uint64_t* __restrict__ skey, const 
     }
 }
 
-// Long rows: scratch -> their slots (in place when they fit, else fresh ones).
+// Long rows: scratch -> their slots (in place when they fit, else fresh
+// ones), warp per kBigChunk-entry chunk as above (chunks of the new rows).
 __global__ void big_copy_kernel(const int32_t* __restrict__ big, const int32_t* __restrict__ big_tail,
                                 const int32_t* __restrict__ bsz, const int32_t* __restrict__ row_id,
                                 const int32_t* __restrict__ scrX, const int64_t* __restrict__ relX,
                                 const int64_t* __restrict__ start, const int32_t* __restrict__ cap, int64_t base,
                                 const int32_t* __restrict__ scol, const double* __restrict__ sval,
                                 int32_t* __restrict__ col, double* __restrict__ val) {
+    const int lane = lane_id();
     const int32_t nb = *big_tail;
-    const int64_t S = bsz[nb];
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < S; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = seg_of(bsz, nb, t);
+    const int64_t C = bsz[nb];
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t ch = warp; ch < C; ch += nwarps) {
+        const int64_t i = seg_of(bsz, nb, ch);
         const int32_t k = big[i];
         const int32_t r = row_id[k];
         const int32_t d2 = scrX[k + 1] - scrX[k];
-        const int64_t j = t - bsz[i];
-        const int64_t dst = (d2 <= cap[r] ? start[r] : base + relX[k]) + j;
-        col[dst] = scol[scrX[k] + j];
-        val[dst] = sval[scrX[k] + j];
+        const int64_t dst = d2 <= cap[r] ? start[r] : base + relX[k];
+        const int32_t o = scrX[k];
+        const int32_t j0 = (int32_t)(ch - bsz[i]) * kBigChunk;
+        constexpr int kPer = kBigChunk / 32;
+        int32_t cv[kPer];
+        double wv[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int32_t j = j0 + u * 32 + lane;
+            if (j < d2) {
+                cv[u] = scol[o + j];
+                wv[u] = sval[o + j];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int32_t j = j0 + u * 32 + lane;
+            if (j < d2) {
+                col[dst + j] = cv[u];
+                val[dst + j] = wv[u];
+            }
+        }
     }
 }
 
@@ -971,7 +1012,7 @@ int apply_pass(ghb_workspace* ws, ghb_gpma* g, const uint64_t* keys, const doubl
                        g->val, scol, sval, a.big, a.big_tail, a.big_d, a.big_d2, a.big_flag, row_warp_max, g->moved,
                        bad_rank));
         if (n_long_rows > 0) {
-            // Offsets of the long rows' entries, in list order (zeros past it).
+            // Chunk offsets of the long rows, in list order (zeros past it).
             if (small_b) {
                 GHB_TRY(launch(ws, small_scan_kernel<int32_t, 2>, dim3(1), dim3(1024), 0, (const int32_t*)a.big_d,
                                (const int32_t*)a.big_d2, (const int32_t*)nullptr, a.bex, a.bsz, (int32_t*)nullptr,
@@ -982,10 +1023,10 @@ int apply_pass(ghb_workspace* ws, ghb_gpma* g, const uint64_t* keys, const doubl
             }
             GHB_TRY(launch(ws, big_scatter_old_kernel, dim3(wide), dim3(256), 0, (const int32_t*)a.big,
                            (const int32_t*)a.big_tail, (const int32_t*)a.bex, (const int32_t*)a.row_id,
-                           (const int32_t*)a.row_first, (const int32_t*)a.scrX, (const uint64_t*)a.skey,
-                           (const int8_t*)a.typ, (const int32_t*)a.insX, (const int32_t*)a.delX,
-                           (const int64_t*)g->start, (const int32_t*)g->col, (const double*)g->val, scol, sval,
-                           bad_rank));
+                           (const int32_t*)a.row_first, (const int32_t*)a.scrX, (const int32_t*)a.exX,
+                           (const uint64_t*)a.skey, (const int8_t*)a.typ, (const int32_t*)a.insX,
+                           (const int32_t*)a.delX, (const int64_t*)g->start, (const int32_t*)g->col,
+                           (const double*)g->val, scol, sval, bad_rank));
             if (n_ins > 0)
                 GHB_TRY(launch(ws, big_scatter_new_kernel, dim3(gr), dim3(256), 0, (const uint64_t*)a.skey,
                                (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
