@@ -626,10 +626,20 @@ __global__ void row_copy_kernel(int32_t n, const int64_t* __restrict__ sstart, c
     }
 }
 
-// Chunks of the long rows, one warp each (8 entries per lane, loads first):
-// chunk c belongs to the row v with coff[v] <= c < coff[v + 1].
+// chunk_row[c] = v for the chunks coff[v] <= c < coff[v + 1] of each long
+// row, so a chunk finds its row with one load.
+__global__ void chunk_rows_kernel(int32_t n, const int32_t* __restrict__ cc, const int32_t* __restrict__ coff,
+                                  int32_t* __restrict__ chunk_row) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t k = cc[v];
+        for (int32_t i = 0; i < k; ++i) chunk_row[coff[v] + i] = (int32_t)v;
+    }
+}
+
+// Chunks of the long rows, one warp each (8 entries per lane, loads first).
 template <class DstOff>
-__global__ void row_copy_chunk_kernel(int32_t n, const int32_t* __restrict__ coff, const int64_t* __restrict__ sstart,
+__global__ void row_copy_chunk_kernel(int32_t n, const int32_t* __restrict__ coff,
+                                      const int32_t* __restrict__ chunk_row, const int64_t* __restrict__ sstart,
                                       const int32_t* __restrict__ deg, const int32_t* __restrict__ scol,
                                       const double* __restrict__ sval, const DstOff* __restrict__ dst_off,
                                       int32_t* __restrict__ dcol, double* __restrict__ dval) {
@@ -638,7 +648,7 @@ __global__ void row_copy_chunk_kernel(int32_t n, const int32_t* __restrict__ cof
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t c = warp; c < C; c += nwarps) {
-        const int64_t v = seg_of(coff, n, c);
+        const int32_t v = chunk_row[c];
         const int32_t d = deg[v];
         const int32_t j0 = (int32_t)(c - coff[v]) * kCopyChunk;
         const int64_t s = sstart[v] + j0, o = (int64_t)dst_off[v] + j0;
@@ -734,26 +744,32 @@ unsigned grid_of(ghb_workspace* ws, int64_t items, int threads = 256) {
 
 // Copy n rows (sstart/deg into scol/sval) to dst offsets (int32 CSR offsets
 // or int64 arena starts).  `list` holds n + 2 int32.
+// Chunk slots copy_rows needs for a graph of m entries: each long row has at
+// most one partial chunk, and a long row has at least kCopyChunk entries.
+inline int64_t copy_chunk_slots(int64_t m) { return 2 * (m / kCopyChunk) + 1; }
+
 template <class DstOff>
 int copy_rows(ghb_workspace* ws, int32_t n, const int64_t* sstart, const int32_t* deg, const int32_t* scol,
               const double* sval, const DstOff* dst_off, int32_t* dcol, double* dval, int32_t* cc, int32_t* coff,
-              int64_t* block_sums) {
+              int32_t* chunk_row, int64_t* block_sums) {
     const unsigned grid = grid_for(((int64_t)n + 31) / 32 * 32, 256, (int64_t)ws->num_sms * 8);
     const double* sv = dval ? sval : nullptr;
     GHB_TRY(launch(ws, row_copy_kernel<DstOff>, dim3(grid), dim3(256), 0, n, sstart, deg, scol, sv, dst_off, dcol,
                    dval, cc));
     GHB_TRY(scan_exclusive_i32(ws, cc, coff, n, block_sums));
+    GHB_TRY(launch(ws, chunk_rows_kernel, dim3(grid_for(n, 256, (int64_t)ws->num_sms * 8)), dim3(256), 0, n,
+                   (const int32_t*)cc, (const int32_t*)coff, chunk_row));
     GHB_TRY(launch(ws, row_copy_chunk_kernel<DstOff>, dim3(ws->num_sms * 8), dim3(256), 0, n, (const int32_t*)coff,
-                   sstart, deg, scol, sv, dst_off, dcol, dval));
+                   (const int32_t*)chunk_row, sstart, deg, scol, sv, dst_off, dcol, dval));
     return GHB_OK;
 }
 
-// Copy the rows (src_start, g->deg, src_col, src_val) into a fresh arena with
+// Copy the rows (src_start, g->deg, src_col, src_val; `entries` in all) into a fresh arena with
 // want[v] slots for row v and `headroom` spare slots at its end.  On success
 // g->start / cap / col / val / slots / used describe the new arena; the old
 // col / val arrays are freed when they belong to the graph (free_old).
 int repack(ghb_workspace* ws, ghb_gpma* g, const int64_t* src_start, const int32_t* src_col,
-           const double* src_val, int64_t* want, int64_t headroom, bool free_old) {
+           const double* src_val, int64_t* want, int64_t headroom, bool free_old, int64_t entries) {
     const int32_t n = g->n;
     int64_t* nstart = nullptr;
     int32_t* big = nullptr;
@@ -764,8 +780,9 @@ int repack(ghb_workspace* ws, ghb_gpma* g, const int64_t* src_start, const int32
     int st = GHB_OK;
     do {
         if ((st = dev_alloc(&nstart, (int64_t)n + 1))) break;
-        // cc, coff (n + 1 int32 each) and the scan's block sums
-        if ((st = dev_alloc(&big, 2 * ((int64_t)n + 1) + 2 * scan_scratch_words(n)))) break;
+        // cc, coff (n + 1 int32 each), the scan's block sums, the chunk rows
+        if ((st = dev_alloc(&big, 2 * ((int64_t)n + 1) + 2 * scan_scratch_words(n) + copy_chunk_slots(entries))))
+            break;
         // nstart = exclusive scan of want; nstart[n] = total slots.
         cudaError_t e = cudaMemsetAsync(want + n, 0, sizeof(int64_t), ws->stream);
         if (e == cudaSuccess)
@@ -791,7 +808,8 @@ int repack(ghb_workspace* ws, ghb_gpma* g, const int64_t* src_start, const int32
         if ((st = dev_alloc(&ncol, slots))) break;
         if ((st = dev_alloc(&nval, slots))) break;
         if ((st = copy_rows<int64_t>(ws, n, src_start, g->deg, src_col, src_val, nstart, ncol, nval, big,
-                                     big + n + 1, reinterpret_cast<int64_t*>(big + 2 * ((int64_t)n + 1)))))
+                                     big + n + 1, big + 2 * ((int64_t)n + 1) + 2 * scan_scratch_words(n),
+                                     reinterpret_cast<int64_t*>(big + 2 * ((int64_t)n + 1)))))
             break;
         if ((st = launch(ws, set_caps_kernel, dim3(grid_of(ws, n)), dim3(256), 0, (const int64_t*)want, n, g->cap)))
             break;
@@ -972,7 +990,7 @@ int apply_pass(ghb_workspace* ws, ghb_gpma* g, const uint64_t* keys, const doubl
         if (!st) {
             // Headroom for later growth: an eighth of the live entries.
             const int64_t live = g->m + n_ins - n_del;
-            st = repack(ws, g, g->start, g->col, g->val, want, live / 8 + 4096, true);
+            st = repack(ws, g, g->start, g->col, g->val, want, live / 8 + 4096, true, g->m);
         }
         dev_free(want);
         GHB_TRY(st);
@@ -1081,14 +1099,16 @@ int snapshot(ghb_workspace* ws, ghb_gpma* g, bool weights) {
     sizing.take<int64_t>(scan_scratch_words((int64_t)n));
     sizing.take<int32_t>((int64_t)n + 1);
     sizing.take<int32_t>((int64_t)n + 1);
+    sizing.take<int32_t>(copy_chunk_slots(g->m));
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
     int64_t* block_sums = c.take<int64_t>(scan_scratch_words((int64_t)n));
     int32_t* cc = c.take<int32_t>((int64_t)n + 1);
     int32_t* coff = c.take<int32_t>((int64_t)n + 1);
+    int32_t* chunk_row = c.take<int32_t>(copy_chunk_slots(g->m));
     GHB_TRY(scan_exclusive_i32(ws, g->deg, g->s_rowptr, n, block_sums));
     GHB_TRY(copy_rows<int32_t>(ws, n, g->start, g->deg, g->col, g->val, g->s_rowptr, g->s_col,
-                               weights ? g->s_val : nullptr, cc, coff, block_sums));
+                               weights ? g->s_val : nullptr, cc, coff, chunk_row, block_sums));
     g->s_ok = true;
     g->s_val_ok = weights;
     return GHB_OK;
@@ -1287,7 +1307,7 @@ int ghb_gpma_load_csr(ghb_workspace* ws, ghb_gpma* g, const int32_t* rowptr, con
     }
     if (!st) st = launch(ws, widen_rowptr_kernel, dim3(grid_of(ws, n)), dim3(256), 0, rowptr, n, start64);
     if (!st) st = launch(ws, want_cap_kernel, dim3(grid_of(ws, n)), dim3(256), 0, (const int32_t*)g->deg, n, want);
-    if (!st) st = repack(ws, g, start64, col, w ? w : ones, want, m / 8 + 4096, false);
+    if (!st) st = repack(ws, g, start64, col, w ? w : ones, want, m / 8 + 4096, false, m);
     dev_free(start64);
     dev_free(want);
     dev_free(ones);
