@@ -216,7 +216,8 @@ class Workspace:
             pass
 
 
-TUNABLES = ("pr_cache_kb", "pr_threads", "pr_blocks_per_sm", "pr_short", "pr_chunk", "ms_warp_rest", "ms_pull_div")
+TUNABLES = ("pr_cache_kb", "pr_threads", "pr_blocks_per_sm", "pr_short", "pr_chunk", "ms_warp_rest", "ms_pull_div",
+            "pol_band")
 
 
 def tune_set(name: str, value: int, ws=None) -> None:

@@ -128,6 +128,7 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
             dir = has ? (opt->schedule[level] & 1) : dir;
             fmt_req = has ? ((opt->schedule[level] >> 1) & 3) : 0;
         } else {
+            const int prev_dir_rule = dir;
             int heur = dir;
             if (dir == 0 && (double)m_f > (double)m_u / alpha && (double)m_f > (double)m_total / gamma) heur = 1;
             else if (dir == 1 && (double)n_f < (double)n / beta) heur = 0;
@@ -137,7 +138,11 @@ int bfs_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_r
                 bfs_features(feat, n, m_total, n_f, m_f, m_u, level, deg2_f, degmax_f, prev_dir, nf_prev,
                              (double)(n - reached));
                 int d = 0, f = 0;
-                if (policy_pick_level(feat, &d, &f)) {
+                // The network's choices only inside the rule's uncertain band
+                // (rule_margin); the rule's outside it.
+                if (policy_pick_level(feat, &d, &f) &&
+                    rule_margin(prev_dir_rule, n, m_total, n_f, m_f, m_u, alpha, beta, gamma) <
+                        (float)ws->tune.pol_band) {
                     dir = d;
                     fmt_req = f ? 2 : 1;
                     by_net = true;

@@ -144,11 +144,26 @@ __device__ __forceinline__ int32_t p_append(int nd, int fmt, unsigned long long 
 
 }  // namespace
 
+// The learned policy's part of a level decision, kept out of line so that
+// its registers do not weigh on the traversal loops of the kernel below.
+__device__ __noinline__ float level_margin(int dir, int32_t n, int64_t m, int32_t n_f, unsigned long long m_f,
+                                           double m_u, float alpha, float beta, float gamma) {
+    return rule_margin(dir, (double)n, (double)m, (double)n_f, (double)m_f, m_u, alpha, beta, gamma);
+}
+
+// Every thread of the deciding block calls this; the network runs only
+// inside the rule's band and leaves its logits in `logit`.
+__device__ __noinline__ void level_eval(const float* pol, const float* feat, float* h1, float* h2, float* logit,
+                                        float margin, float band) {
+    if (margin < band) policy_eval_block(pol, feat, h1, h2, logit);
+}
+
 __global__ void __launch_bounds__(512) bfs_persistent_kernel(
     int32_t n, int32_t n_active, const int32_t* __restrict__ out_rp, const int32_t* __restrict__ out_col,
     const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col, int32_t src, int32_t max_depth,
     int32_t* depth, uint32_t* visited, uint32_t* f0, uint32_t* f1, uint32_t* f2, int32_t* qa, int32_t* qb,
-    int32_t* big, int policy, float alpha, float beta, float gamma, int64_t m_total, const int8_t* __restrict__ schedule,
+    int32_t* big, int policy, float alpha, float beta, float gamma, float band, int64_t m_total,
+    const int8_t* __restrict__ schedule,
     int32_t schedule_len, const int32_t* __restrict__ perm, int32_t* depth_out, BfsRunState* st,
     const float* __restrict__ pol, float* trace, int32_t trace_cap) {
     const int lane = lane_id();
@@ -168,12 +183,10 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
         f1[w] = 0u;
         f2[w] = 0u;
     }
-    // The network (parameters + normalisation) in shared memory, when the
-    // learned policy is on: every block may be the one that decides.
-    extern __shared__ float s_pol[];
+    // The network (parameters + normalisation, 25 KB) is read from global
+    // memory by whichever block decides a level inside the rule's band; it
+    // stays in L2, and no block pays to stage it in shared memory.
     const bool net = pol != nullptr;
-    if (net)
-        for (int i = threadIdx.x; i < kPolTotal; i += blockDim.x) s_pol[i] = pol[i];
     const bool can_pull = in_rp != nullptr;
     if (gtid == 0) {
         qa[0] = src;
@@ -202,6 +215,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
 
     __shared__ float s_feat[kPolIn], s_h1[kPolH], s_h2[kPolH], s_logit[kPolOut];
     __shared__ int32_t s_dec[2];
+    __shared__ float s_margin;
     __shared__ int32_t s_flag;
 
     __shared__ int32_t s_state[6];
@@ -289,6 +303,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                 } else {
                     if (dir == 0 && (double)mf_next > m_u / alpha && (double)mf_next > (double)m_total / gamma) nd = 1;
                     else if (dir == 1 && (double)nf_next < (double)n / beta) nd = 0;
+                    if (net) s_margin = level_margin(dir, n, m_total, nf_next, mf_next, m_u, alpha, beta, gamma);
                 }
                 bfs_features(s_feat, (double)n, (double)m_total, (double)nf_next, (double)mf_next, m_u, L + 1,
                              (double)vd->d2[nslot], (double)vd->dmax[nslot], dir, (double)n_f,
@@ -300,15 +315,20 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
             }
             if (net) {
                 __syncthreads();
-                policy_eval_block(s_pol, s_feat, s_h1, s_h2, s_logit);
+                // Levels outside the rule's uncertain band keep the rule's
+                // choices: no network evaluation on them (it would sit on
+                // the level's critical path while the grid waits).
+                level_eval(pol, s_feat, s_h1, s_h2, s_logit, s_margin, band);
             }
             if (threadIdx.x == 0) {
                 int nd = s_dec[0], fmt = s_dec[1];
-                if (net) {
+                int by_net = 0;
+                if (net && s_margin < band) {
                     nd = (can_pull && s_logit[kHeadDir + 1] > s_logit[kHeadDir]) ? 1 : 0;
                     fmt = s_logit[kHeadFmt + 1] > s_logit[kHeadFmt] ? 2 : 1;
+                    by_net = 1;
                 }
-                st->by_net = net ? 1 : 0;
+                st->by_net = by_net;
                 st->dir = nd;
                 // The next queue holds the next frontier only if this level
                 // was top-down and appended.
@@ -597,9 +617,8 @@ bool bfs_persistent_available(ghb_workspace* ws, int* blocks) {
     if (!known[dev]) {
         int coop = 0, per_sm = 0;
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-        // Sized with the network in shared memory, so both variants fit.
-        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent_kernel, 512,
-                                                                  sizeof(float) * kPolTotal) == cudaSuccess)
+        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent_kernel, 512, 0) ==
+                        cudaSuccess)
             cached[dev] = std::min(per_sm, 2) * ws->num_sms;
         known[dev] = true;
     }
@@ -668,9 +687,10 @@ int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int
     GHB_CUDA_TRY(cudaStreamSynchronize(st));
     const int64_t m_total = hp[0];
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
-    GHB_TRY(launch_coop(ws, bfs_persistent_kernel, dim3(blocks), dim3(512), pol ? sizeof(float) * kPolTotal : 0, n,
+    GHB_TRY(launch_coop(ws, bfs_persistent_kernel, dim3(blocks), dim3(512), 0, n,
                         n_active, out_rp, out_col, in_rp, in_col, src, max_depth, depth, vis, f0, f1, f2, qa, qb, big,
-                        policy, alpha, beta, gamma, m_total, (const int8_t*)(sched_len ? sched : nullptr), sched_len,
+                        policy, alpha, beta, gamma, (float)ws->tune.pol_band, m_total,
+                        (const int8_t*)(sched_len ? sched : nullptr), sched_len,
                         perm,
                         depth_out, rs, pol, tcap > 0 ? tr : (float*)nullptr, tcap));
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));

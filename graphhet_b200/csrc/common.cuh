@@ -68,6 +68,8 @@ struct Tuning {
     int32_t pr_chunk = 1024;       // longer rows: chunks of this many entries, warp per chunk
     int32_t ms_warp_rest = 512;    // multi-source pull: longer rest of a row -> a block
     int32_t ms_pull_div = 16;      // multi-source: pull when frontier entries > m / ms_pull_div
+    int32_t pol_band = 1;          // learned policy: the network picks a level's direction and format only
+                                   // where the direction rule's test is within 2^pol_band of its threshold
 };
 
 }  // namespace ghb

@@ -20,7 +20,10 @@ constexpr int kHeadDir = 0, kHeadFmt = 2, kHeadDelta = 4, kDeltaBins = 16, kDelt
 
 // The 12 policy features of one BFS level (also the first 12 trace
 // columns), scale-free so that a network trained on scales 16-22 reads a
-// scale-24 graph's levels in the same ranges:
+// scale-24 graph's levels in the same ranges.  (Giving it the graph's size
+// instead, as log2(m), made its decisions at scale 24 extrapolations: it
+// pushed on levels whose frontier held a hundred times the unexplored
+// entries.)
 //  0 log2(1+n_f) - log2(n)          frontier share of the vertices
 //  1 log2(1+m_f) - log2(1+m)        frontier share of the entries
 //  2 log2(1+m_u) - log2(1+m)        unexplored share of the entries
@@ -63,13 +66,22 @@ __host__ __device__ inline void bfs_features(float* f, double n, double m, doubl
     f[11] = log2f((float)(1.0 + (unvisited > 0 ? unvisited : 0.0))) - ln;
 }
 
-// The features of one SSSP call (one width decision per traversal); level is
-// -1 to tell them from BFS levels:
-//  0 log2(1+deg(src))  1 log2(1+mean degree)  2 log2(1+degree variance)
-//  3 -1                4 log2(1+max degree)   5 log2(n)
-//  6 log2(1+m)         7 log2(mean weight / base width)
-//  8 log2(max weight / mean weight)   9 log2(mean weight / min weight)
-// 10 log2(1 + vertices with entries)   11 log2(1+mean degree) - log2(n)
+// The features of one SSSP call (one width decision per traversal): shares
+// and ratios, plus the graph's size (feature 10); feature 3 is -1 to tell
+// them from BFS levels:
+//  0 log2(1+deg(src)) - log2(1+mean degree)
+//  1 log2(1+mean degree)
+//  2 log2(1+std of degree) - log2(1+mean degree)
+//  3 -1
+//  4 log2(1+max degree) - log2(1+mean degree)
+//  5 log2(vertices with entries) - log2(n)
+//  6 log2((max weight - min weight) / mean weight + 1/64)
+//  7 log2(mean weight / base width)
+//  8 log2(max weight / mean weight)
+//  9 log2(mean weight / min weight)
+// 10 log2(1+m)   size of the graph: the best width narrows as the graph's
+//    diameter grows (grids: about 14 at 256 x 256, 11 at 2048 x 2048)
+// 11 log2(1+deg(src)) - log2(1+max degree)
 __host__ __device__ inline void sssp_features(float* f, double n, double m, double n_active, double deg_src,
                                               double deg2_sum, double degmax, double w_mean, double w_min,
                                               double w_max, double base_delta) {
@@ -78,18 +90,40 @@ __host__ __device__ inline void sssp_features(float* f, double n, double m, doub
     double var = deg2_sum / na - mean * mean;
     if (var < 0) var = 0;
     const double tiny = 1e-300;
-    f[0] = log2f((float)(1.0 + deg_src));
-    f[1] = log2f((float)(1.0 + mean));
-    f[2] = log2f((float)(1.0 + var));
+    const float lmean = log2f((float)(1.0 + mean));
+    const float lsrc = log2f((float)(1.0 + deg_src));
+    const float lmax = log2f((float)(1.0 + degmax));
+    f[0] = lsrc - lmean;
+    f[1] = lmean;
+    f[2] = log2f((float)(1.0 + sqrt(var))) - lmean;
     f[3] = -1.0f;
-    f[4] = log2f((float)(1.0 + degmax));
-    f[5] = log2f((float)(n > 0 ? n : 1.0));
-    f[6] = log2f((float)(1.0 + m));
+    f[4] = lmax - lmean;
+    f[5] = log2f((float)na) - log2f((float)(n > 0 ? n : 1.0));
+    f[6] = (float)log2((w_max - w_min) / (w_mean + tiny) + 1.0 / 64.0);
     f[7] = (float)log2((w_mean + tiny) / (base_delta + tiny));
     f[8] = (float)log2((w_max + tiny) / (w_mean + tiny));
     f[9] = (float)log2((w_mean + tiny) / (w_min + tiny));
-    f[10] = log2f((float)(1.0 + n_active));
-    f[11] = f[1] - f[5];
+    f[10] = log2f((float)(1.0 + m));
+    f[11] = lsrc - lmax;
+}
+
+// How far, in log2 units, the direction rule's test is from its threshold
+// at a level: the rule pulls when m_f > m_u / alpha and m_f > m / gamma, and
+// returns to push when n_f < n / beta.  With the learned policy the network
+// chooses a level's direction and output format only where this is below
+// the band (the rule's uncertain zone); farther out the rule's choices
+// stand, so a network reading a graph unlike its training family cannot,
+// say, push a level whose frontier holds many times the unexplored entries.
+__host__ __device__ inline float rule_margin(int dir, double n, double m, double n_f, double m_f, double m_u,
+                                             float alpha, float beta, float gamma) {
+    const float lo = 0.5f;
+    if (dir == 0) {
+        const float lmf = log2f(fmaxf((float)m_f, lo));
+        const float a = lmf - log2f(fmaxf((float)(m_u / alpha), lo));
+        const float b = lmf - log2f(fmaxf((float)(m / gamma), lo));
+        return fabsf(fminf(a, b));
+    }
+    return fabsf(log2f(fmaxf((float)(n / beta), lo)) - log2f(fmaxf((float)n_f, lo)));
 }
 
 // Block-wide evaluation for one feature row.  P: kPolTotal floats (shared or

@@ -127,6 +127,7 @@ const TuneField kTuneFields[] = {
     {"pr_chunk", &ghb::Tuning::pr_chunk, 64, 4096},
     {"ms_warp_rest", &ghb::Tuning::ms_warp_rest, 32, 1 << 20},
     {"ms_pull_div", &ghb::Tuning::ms_pull_div, 1, 1024},
+    {"pol_band", &ghb::Tuning::pol_band, 0, 64},
 };
 const TuneField* tune_field(const char* name) {
     if (!name) return nullptr;

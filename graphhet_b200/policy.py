@@ -224,36 +224,50 @@ def replay_costs(rg, src: int):
 
 
 # ------------------------------------------------------------ SSSP labels
-def sssp_rows(rg, src: int, max_buckets: float = 4096.0, max_ms: float = 2000.0):
-    """One row for the width head: the width rule's features and the fastest
-    of the 16 width bins (each timed once after a warm-up at the rule's width).
-    Bins whose width would give more than max_buckets buckets over the largest
-    finite distance are not run."""
+def sssp_rows(rg, srcs: Sequence[int], max_buckets: float = 4096.0, max_ms: float = 2000.0):
+    """Rows for the width head from several sources of one graph: each
+    source's features, all labelled with the width bin that is fastest over
+    all of them (the sum of their times: one timing per source and bin is
+    noisy, the graph's best width is not), weighted by the rule's width's
+    excess time over that bin.  Bins whose width would give more than
+    max_buckets buckets over a source's largest finite distance are not run
+    and cannot win.  Returns (features[k, 12], label, weight, times[k, 16])
+    or None."""
     import torch
-    import graphhet_b200 as G
-    d0, st0, row = rg.sssp(src, trace=True)
-    base = float(row[14])
-    fin = d0[d0 < 1e300]
-    dmax = float(fin.max().item()) if fin.numel() else 0.0
-    times = np.full(DELTA_BINS, np.inf)
-    for k in range(DELTA_BINS):
-        delta = base * 2.0 ** (k - DELTA_BIN_ZERO)
-        if dmax / delta > max_buckets:
-            continue
-        d, st = rg.sssp(src, delta=delta)
-        times[k] = st["device_ms"]
-        if not torch.equal(d, d0):
-            raise RuntimeError("SSSP distances changed with the bucket width")
-        if st["device_ms"] > max_ms:
-            break
-    if not np.isfinite(times).any():
+    feats, T = [], []
+    for src in srcs:
+        d0, st0, row = rg.sssp(src, trace=True)
+        base = float(row[14])
+        fin = d0[d0 < 1e300]
+        dmax = float(fin.max().item()) if fin.numel() else 0.0
+        times = np.full(DELTA_BINS, np.inf)
+        for k in range(DELTA_BINS):
+            delta = base * 2.0 ** (k - DELTA_BIN_ZERO)
+            if dmax / delta > max_buckets:
+                continue
+            d, st = rg.sssp(src, delta=delta)
+            times[k] = st["device_ms"]
+            if not torch.equal(d, d0):
+                raise RuntimeError("SSSP distances changed with the bucket width")
+            if st["device_ms"] > max_ms:
+                break
+        feats.append(row[:N_FEATURES].astype(np.float32))
+        T.append(times)
+    if not feats:
         return None
-    return row[:N_FEATURES].astype(np.float32), int(np.argmin(times)), times
+    T = np.array(T)
+    tot = T.sum(0)
+    if not np.isfinite(tot).any():
+        return None
+    lab = int(np.argmin(tot))
+    rule = tot[DELTA_BIN_ZERO] if np.isfinite(tot[DELTA_BIN_ZERO]) else np.nanmax(np.where(np.isfinite(tot), tot, np.nan))
+    weight = float(np.clip(rule / tot[lab] - 1.0, 0.05, 10.0))
+    return np.stack(feats), lab, weight, T
 
 
 # ------------------------------------------------------------- collection
 def collect(specs: Sequence[GraphSpec], bfs_sources: int = 6, grid_sources: int = 2, sssp_every: int = 1,
-            sssp_max_scale: int = 20,
+            sssp_max_scale: int = 22, sssp_sources: int = 3,
             log=print) -> Dict[str, np.ndarray]:
     """Training rows from every graph of `specs` (needs a GPU)."""
     import torch
@@ -278,16 +292,13 @@ def collect(specs: Sequence[GraphSpec], bfs_sources: int = 6, grid_sources: int 
             Ws.append(W)
             nrows += len(X)
         if gi % sssp_every == 0 and spec.scale <= sssp_max_scale and srcs:
-            out = sssp_rows(rg, srcs[0])
+            out = sssp_rows(rg, srcs[:sssp_sources])
             if out is not None:
-                f, lab, times = out
-                Xs.append(f[None, :])
-                Ys.append(np.array([[-1, -1, lab]], np.int32))
-                # Weight: the rule's width's excess time over the best width.
-                base = times[DELTA_BIN_ZERO] if np.isfinite(times[DELTA_BIN_ZERO]) else np.nanmax(
-                    np.where(np.isfinite(times), times, np.nan))
-                Ws.append(np.array([float(np.clip(base / times[lab] - 1.0, 0.05, 10.0))], np.float32))
-                nrows += 1
+                f, lab, wt, _ = out
+                Xs.append(f)
+                Ys.append(np.tile(np.array([[-1, -1, lab]], np.int32), (len(f), 1)))
+                Ws.append(np.full(len(f), wt, np.float32))
+                nrows += len(f)
         meta.append(dict(asdict(spec), rows=nrows, n=g.n, m=int(g.m)))
         rg.close()
         del rg, g

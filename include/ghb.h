@@ -66,8 +66,12 @@ ghb_workspace* ghb_default_workspace(void);
  * reference): "pr_cache_kb" PageRank hub cache in shared memory, "pr_threads"
  * and "pr_blocks_per_sm" its persistent blocks, "pr_short" / "pr_chunk" its
  * row split, "ms_warp_rest" / "ms_pull_div" the multi-source BFS's block-row
- * threshold and direction switch.  Results do not depend on them.  Unknown
- * names and values outside the documented ranges are rejected. */
+ * threshold and direction switch, "pol_band" (0-64) the band, in log2
+ * units around the direction rule's threshold, inside which the learned
+ * policy's network chooses a BFS level's direction and output format (0:
+ * never; 64: always).
+ * Results do not depend on them.  Unknown names and values outside the
+ * documented ranges are rejected. */
 int ghb_tune_set(ghb_workspace* ws, const char* name, int32_t value);
 int ghb_tune_get(ghb_workspace* ws, const char* name, int32_t* value);
 
