@@ -57,6 +57,11 @@ struct ghb_gpma {
     int64_t version = 0;
     int64_t stats[GHB_GPMA_STATS] = {};
     unsigned long long* moved = nullptr;  // device: rows moved to fresh slots
+    // The arena a merge rebuild left behind, kept for the next one (the
+    // rebuilds of large batches alternate between the two).
+    int32_t* spare_col = nullptr;
+    double* spare_val = nullptr;
+    int64_t spare_slots = 0;
 };
 
 namespace ghb {
@@ -272,7 +277,9 @@ __device__ __forceinline__ int32_t new_rank(const int32_t* __restrict__ pos, con
 // warp each: rank the surviving entries and the inserts into the row's
 // scratch range, then (after __syncwarp, which orders the warp's scratch
 // writes before its reads) copy the range to the row's slots, in place or
-// to fresh ones at base + relX[k], and finish deg / start / cap.  Longer rows
+// to fresh ones at base + relX[k], and finish deg / start / cap.  In a merge
+// rebuild (dst_start given) the rows go straight to dst_start[r] in the new
+// arena (scol / sval), and the row table is finished by the host.  Longer rows
 // go to `big` (with the chunk counts of their old and new entries in big_d /
 // big_d2, zero past the list) for the grid-wide kernels; big_flag[k] tells
 // them apart.
@@ -289,7 +296,8 @@ __global__ void upd_rows_warp_kernel(const int32_t* __restrict__ row_id, const i
                                      int32_t* __restrict__ big, int32_t* __restrict__ big_tail,
                                      int32_t* __restrict__ big_d, int32_t* __restrict__ big_d2,
                                      int8_t* __restrict__ big_flag, int32_t row_warp_max,
-                                     unsigned long long* __restrict__ moved, unsigned long long* __restrict__ bad_rank) {
+                                     const int64_t* __restrict__ dst_start, unsigned long long* __restrict__ moved,
+                                     unsigned long long* __restrict__ bad_rank) {
     const int lane = lane_id();
     const int64_t K = headX[b];
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -311,7 +319,7 @@ __global__ void upd_rows_warp_kernel(const int32_t* __restrict__ row_id, const i
         if (!changed || is_big) continue;
         const int32_t r = row_id[k];
         const int64_t s = start[r];
-        const int32_t o = scrX[k];
+        const int64_t o = dst_start ? dst_start[r] : (int64_t)scrX[k];
         unsigned long long bad = 0;
         for (int32_t j = lane; j < d; j += 32) {
             const int32_t c = col[s + j];
@@ -335,6 +343,7 @@ __global__ void upd_rows_warp_kernel(const int32_t* __restrict__ row_id, const i
             sval[o + rk] = values[sidx[i]];
         }
         if (bad) atomicAdd(bad_rank, bad);
+        if (dst_start) continue;  // merge rebuild: written to its final place
         __syncwarp();
         const int32_t cp = cap[r];
         const int64_t dst = d2 <= cp ? s : base + relX[k];
@@ -415,6 +424,7 @@ __global__ void big_scatter_old_kernel(const int32_t* __restrict__ big, const in
                                        const int32_t* __restrict__ delX, const int64_t* __restrict__ start,
                                        const int32_t* __restrict__ col, const double* __restrict__ val,
                                        int32_t* __restrict__ scol, double* __restrict__ sval,
+                                       const int64_t* __restrict__ dst_start,
                                        unsigned long long* __restrict__ bad_rank) {
     const int lane = lane_id();
     const int32_t nb = *big_tail;
@@ -428,7 +438,7 @@ __global__ void big_scatter_old_kernel(const int32_t* __restrict__ big, const in
         const int32_t d = exX[k + 1] - exX[k], d2 = scrX[k + 1] - scrX[k];
         const int32_t a = row_first[k], z = row_first[k + 1];
         const int64_t s = start[r];
-        const int32_t o = scrX[k];
+        const int64_t o = dst_start ? dst_start[r] : (int64_t)scrX[k];
         const int32_t j0 = (int32_t)(ch - bex[i]) * kBigChunk;
         unsigned long long bad = 0;
 #pragma unroll 2
@@ -456,7 +466,9 @@ __global__ void big_scatter_new_kernel(const uint64_t* __restrict__ skey, const 
                                        const int32_t* __restrict__ row_first, const int32_t* __restrict__ insX,
                                        const int32_t* __restrict__ delX, const int32_t* __restrict__ scrX,
                                        const int8_t* __restrict__ big_flag, int64_t b, int32_t* __restrict__ scol,
-                                       double* __restrict__ sval, unsigned long long* __restrict__ bad_rank) {
+                                       double* __restrict__ sval, const int32_t* __restrict__ row_id,
+                                       const int64_t* __restrict__ dst_start,
+                                       unsigned long long* __restrict__ bad_rank) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
         if (typ[i] != kIns) continue;
         const int32_t k = headX[i + 1] - 1;
@@ -466,8 +478,9 @@ __global__ void big_scatter_new_kernel(const uint64_t* __restrict__ skey, const 
             atomicAdd(bad_rank, 1ull);
             continue;
         }
-        scol[scrX[k] + rk] = (int32_t)(uint32_t)skey[i];
-        sval[scrX[k] + rk] = values[sidx[i]];
+        const int64_t o = dst_start ? dst_start[row_id[k]] : (int64_t)scrX[k];
+        scol[o + rk] = (int32_t)(uint32_t)skey[i];
+        sval[o + rk] = values[sidx[i]];
     }
 }
 
@@ -530,6 +543,33 @@ __global__ void big_finalize_kernel(const int32_t* __restrict__ big, const int32
             atomicAdd(moved, 1ull);
         }
         deg[r] = d2;
+    }
+}
+
+// Merge rebuild helpers over the batch's rows k < K: changed rows get slots
+// for their new degree, are left out of the copy of the unchanged rows, and
+// take their new degree at the end.
+__global__ void want_changed_kernel(const int32_t* __restrict__ row_id, const int32_t* __restrict__ headX,
+                                    const int32_t* __restrict__ scrX, const int32_t* __restrict__ exX, int64_t b,
+                                    int64_t* __restrict__ want, int32_t* __restrict__ deg_copy) {
+    const int64_t K = headX[b];
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = exX[k + 1] - exX[k], d2 = scrX[k + 1] - scrX[k];
+        if (d == 0 && d2 == 0) continue;
+        const int32_t r = row_id[k];
+        want[r] = slack_cap(d2);
+        deg_copy[r] = 0;
+    }
+}
+
+__global__ void set_changed_deg_kernel(const int32_t* __restrict__ row_id, const int32_t* __restrict__ headX,
+                                       const int32_t* __restrict__ scrX, const int32_t* __restrict__ exX, int64_t b,
+                                       int32_t* __restrict__ deg) {
+    const int64_t K = headX[b];
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = exX[k + 1] - exX[k], d2 = scrX[k + 1] - scrX[k];
+        if (d == 0 && d2 == 0) continue;
+        deg[row_id[k]] = d2;
     }
 }
 
@@ -895,6 +935,148 @@ void carve_pass(Carver& c, int64_t b, size_t tmp_bytes, PassArrays& a) {
     a.tmp = c.take<char>(tmp_bytes);
 }
 
+// The merge rebuild of one pass (see apply_pass): new slots for every row
+// (changed rows sized for their new degree), the unchanged rows copied, the
+// changed ones rebuilt straight into the new arena, then the row table.
+int merge_rebuild(ghb_workspace* ws, ghb_gpma* g, const PassArrays& a, const double* values, int64_t b,
+                  int64_t live_after, int64_t n_modified, int64_t n_ins, int64_t n_long_rows, bool small_b,
+                  int32_t row_warp_max, int64_t K, unsigned long long* bad_rank) {
+    const int32_t n = g->n;
+    const unsigned gr = grid_of(ws, b);
+    const unsigned gn = grid_of(ws, n);
+    const unsigned wide = (unsigned)ws->num_sms * 16;
+    const int64_t ssw = scan_scratch_words(n);
+    // Row-table temporaries in the workspace scratch (this pass needs no
+    // other scratch there): want and nstart (n + 1 int64 each), the copy's
+    // row lengths, its cc / coff / block sums / chunk rows, the scan's temp.
+    size_t tmp_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, (int64_t*)nullptr, (int64_t*)nullptr, (int64_t)n + 1,
+                                  ws->stream);
+    auto carve = [&](Carver& c, int64_t** want, int64_t** nstart, int32_t** degc, int32_t** tmp32, char** tmp) {
+        *want = c.take<int64_t>((int64_t)n + 1);
+        *nstart = c.take<int64_t>((int64_t)n + 1);
+        *degc = c.take<int32_t>(n);
+        *tmp32 = c.take<int32_t>(2 * ((int64_t)n + 1) + 2 * ssw + copy_chunk_slots(g->m));
+        *tmp = c.take<char>(std::max<size_t>(tmp_bytes, 1));
+    };
+    int64_t *want = nullptr, *nstart = nullptr;
+    int32_t *degc = nullptr, *tmp32 = nullptr;
+    char* tmp = nullptr;
+    Carver sizing(nullptr);
+    carve(sizing, &want, &nstart, &degc, &tmp32, &tmp);
+    GHB_TRY(ws_reserve(ws, sizing.off));
+    Carver c(ws->scratch);
+    carve(c, &want, &nstart, &degc, &tmp32, &tmp);
+    int32_t* ncol = nullptr;
+    double* nval = nullptr;
+    int st = GHB_OK;
+    cudaError_t e = cudaSuccess;
+    do {
+        // Weight changes in place first: both copies below read them.
+        if (n_modified > 0 &&
+            (st = launch(ws, upd_modify_kernel, dim3(gr), dim3(256), 0, (const uint64_t*)a.skey,
+                         (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
+                         (const int64_t*)g->start, b, g->val)))
+            break;
+        if ((st = launch(ws, want_cap_kernel, dim3(gn), dim3(256), 0, (const int32_t*)g->deg, n, want))) break;
+        if ((e = cudaMemcpyAsync(degc, g->deg, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToDevice, ws->stream)))
+            break;
+        if ((st = launch(ws, want_changed_kernel, dim3(gr), dim3(256), 0, (const int32_t*)a.row_id,
+                         (const int32_t*)a.headX, (const int32_t*)a.scrX, (const int32_t*)a.exX, b, want, degc)))
+            break;
+        if ((e = cudaMemsetAsync(want + n, 0, sizeof(int64_t), ws->stream))) break;
+        if ((e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, want, nstart, (int64_t)n + 1, ws->stream))) break;
+        ws->launches++;
+        int64_t total = 0;
+        if ((e = cudaMemcpyAsync(&total, nstart + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ws->stream))) break;
+        if ((e = cudaStreamSynchronize(ws->stream))) break;
+        // The new arena: the spare one when it holds the rows with a little
+        // room to grow, else a fresh one with an eighth of the entries to
+        // spare (the next rebuild can then reuse this one's predecessor).
+        int64_t slots = total + live_after / 8 + 4096;
+        if (g->spare_slots >= total + live_after / 32 + 4096) {
+            ncol = g->spare_col;
+            nval = g->spare_val;
+            slots = g->spare_slots;
+            g->spare_col = nullptr;
+            g->spare_val = nullptr;
+            g->spare_slots = 0;
+        } else {
+            dev_free(g->spare_col);
+            dev_free(g->spare_val);
+            g->spare_slots = 0;
+            if ((st = dev_alloc(&ncol, slots))) break;
+            if ((st = dev_alloc(&nval, slots))) break;
+        }
+        if ((st = copy_rows<int64_t>(ws, n, g->start, degc, g->col, g->val, nstart, ncol, nval, tmp32,
+                                     tmp32 + n + 1, tmp32 + 2 * ((int64_t)n + 1) + 2 * ssw,
+                                     reinterpret_cast<int64_t*>(tmp32 + 2 * ((int64_t)n + 1)))))
+            break;
+        if ((e = cudaMemsetAsync(a.big_tail, 0, sizeof(int32_t), ws->stream))) break;
+        if (n_long_rows > 0) {
+            if ((e = cudaMemsetAsync(a.big_d, 0, sizeof(int32_t) * (size_t)b, ws->stream))) break;
+            if ((e = cudaMemsetAsync(a.big_d2, 0, sizeof(int32_t) * (size_t)b, ws->stream))) break;
+        }
+        if ((st = launch(ws, upd_rows_warp_kernel, dim3(grid_for(K * 32, 256, (int64_t)ws->num_sms * 8)), dim3(256),
+                         0, (const int32_t*)a.row_id, (const int32_t*)a.row_first, (const int32_t*)a.headX,
+                         (const int32_t*)a.scrX, (const int32_t*)a.exX, (const int64_t*)a.relX,
+                         (const uint64_t*)a.skey, (const uint32_t*)a.sidx, values, (const int8_t*)a.typ,
+                         (const int32_t*)a.pos, (const int32_t*)a.insX, (const int32_t*)a.delX, (int64_t)0, b,
+                         g->start, g->deg, g->cap, g->col, g->val, ncol, nval, a.big, a.big_tail, a.big_d, a.big_d2,
+                         a.big_flag, row_warp_max, (const int64_t*)nstart, g->moved, bad_rank)))
+            break;
+        if (n_long_rows > 0) {
+            if (small_b)
+                st = launch(ws, small_scan_kernel<int32_t, 2>, dim3(1), dim3(1024), 0, (const int32_t*)a.big_d,
+                            (const int32_t*)a.big_d2, (const int32_t*)nullptr, a.bex, a.bsz, (int32_t*)nullptr, b);
+            else
+                st = scan_exclusive_i32(ws, a.big_d, a.bex, b, a.block_sums);
+            if (st) break;
+            if ((st = launch(ws, big_scatter_old_kernel, dim3(wide), dim3(256), 0, (const int32_t*)a.big,
+                             (const int32_t*)a.big_tail, (const int32_t*)a.bex, (const int32_t*)a.row_id,
+                             (const int32_t*)a.row_first, (const int32_t*)a.scrX, (const int32_t*)a.exX,
+                             (const uint64_t*)a.skey, (const int8_t*)a.typ, (const int32_t*)a.insX,
+                             (const int32_t*)a.delX, (const int64_t*)g->start, (const int32_t*)g->col,
+                             (const double*)g->val, ncol, nval, (const int64_t*)nstart, bad_rank)))
+                break;
+            if (n_ins > 0 &&
+                (st = launch(ws, big_scatter_new_kernel, dim3(gr), dim3(256), 0, (const uint64_t*)a.skey,
+                             (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
+                             (const int32_t*)a.headX, (const int32_t*)a.row_first, (const int32_t*)a.insX,
+                             (const int32_t*)a.delX, (const int32_t*)a.scrX, (const int8_t*)a.big_flag, b, ncol,
+                             nval, (const int32_t*)a.row_id, (const int64_t*)nstart, bad_rank)))
+                break;
+        }
+        // The row table of the new arena.
+        if ((e = cudaMemcpyAsync(g->start, nstart, sizeof(int64_t) * (size_t)n, cudaMemcpyDeviceToDevice,
+                                 ws->stream)))
+            break;
+        if ((st = launch(ws, set_caps_kernel, dim3(gn), dim3(256), 0, (const int64_t*)want, n, g->cap))) break;
+        if ((st = launch(ws, set_changed_deg_kernel, dim3(gr), dim3(256), 0, (const int32_t*)a.row_id,
+                         (const int32_t*)a.headX, (const int32_t*)a.scrX, (const int32_t*)a.exX, b, g->deg)))
+            break;
+        if ((e = cudaStreamSynchronize(ws->stream))) break;
+        // The old arena becomes the spare.
+        g->spare_col = g->col;
+        g->spare_val = g->val;
+        g->spare_slots = g->slots;
+        g->col = ncol;
+        g->val = nval;
+        ncol = nullptr;
+        nval = nullptr;
+        g->slots = slots;
+        g->used = total;
+        g->stats[5]++;
+    } while (false);
+    if (e != cudaSuccess) {
+        set_error(std::string("dynamic-graph merge rebuild: ") + cudaGetErrorString(e));
+        st = GHB_ERR_CUDA;
+    }
+    dev_free(ncol);
+    dev_free(nval);
+    return st;
+}
+
 // One pass of at most kPassUpdates updates.
 int apply_pass(ghb_workspace* ws, ghb_gpma* g, const uint64_t* keys, const double* values, int64_t b,
                int64_t* totals) {
@@ -977,91 +1159,101 @@ int apply_pass(ghb_workspace* ws, ghb_gpma* g, const uint64_t* keys, const doubl
         return GHB_ERR_LIMIT;
     }
 
-    // Slots for rows that outgrow theirs; repack when the arena is full.
-    int64_t base = g->used;
-    bool repacked = false;
-    if (R > 0 && g->used + R > g->slots) {
-        int64_t* want = nullptr;
-        GHB_TRY(dev_alloc(&want, (int64_t)n + 1));
-        int st = launch(ws, want_cap_kernel, dim3(grid_of(ws, n)), dim3(256), 0, (const int32_t*)g->deg, n, want);
-        if (!st)
-            st = launch(ws, want_batch_kernel, dim3(gr), dim3(256), 0, (const int32_t*)a.row_id,
-                        (const int32_t*)a.headX, (const int32_t*)a.scrX, b, want);
-        if (!st) {
-            // Headroom for later growth: an eighth of the live entries.
-            const int64_t live = g->m + n_ins - n_del;
-            st = repack(ws, g, g->start, g->col, g->val, want, live / 8 + 4096, true, g->m);
-        }
-        dev_free(want);
-        GHB_TRY(st);
-        base = g->used;  // every changed row fits now; relX is not used
-        repacked = true;
-    }
-
-    int32_t* scol = nullptr;
-    double* sval = nullptr;
-    // Scratch for the rebuilt rows (S entries) in the workspace scratch.
-    if (S > 0) {
-        Carver sizing2(nullptr);
-        sizing2.take<int32_t>(S);
-        sizing2.take<double>(S);
-        GHB_TRY(ws_reserve(ws, sizing2.off));
-        Carver c2(ws->scratch);
-        scol = c2.take<int32_t>(S);
-        sval = c2.take<double>(S);
-    }
-    if (n_modified > 0)
-        GHB_TRY(launch(ws, upd_modify_kernel, dim3(gr), dim3(256), 0, (const uint64_t*)a.skey,
-                       (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
-                       (const int64_t*)g->start, b, g->val));
-    if (S > 0 || E > 0) {
-        const unsigned wide = (unsigned)ws->num_sms * 16;
-        GHB_CUDA_TRY(cudaMemsetAsync(a.big_tail, 0, sizeof(int32_t), ws->stream));
-        if (n_long_rows > 0) {
-            GHB_CUDA_TRY(cudaMemsetAsync(a.big_d, 0, sizeof(int32_t) * (size_t)b, ws->stream));
-            GHB_CUDA_TRY(cudaMemsetAsync(a.big_d2, 0, sizeof(int32_t) * (size_t)b, ws->stream));
-        }
-        GHB_TRY(launch(ws, upd_rows_warp_kernel, dim3(grid_for(K * 32, 256, (int64_t)ws->num_sms * 8)), dim3(256), 0,
-                       (const int32_t*)a.row_id,
-                       (const int32_t*)a.row_first, (const int32_t*)a.headX, (const int32_t*)a.scrX,
-                       (const int32_t*)a.exX, (const int64_t*)a.relX, (const uint64_t*)a.skey,
-                       (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
-                       (const int32_t*)a.insX, (const int32_t*)a.delX, base, b, g->start, g->deg, g->cap, g->col,
-                       g->val, scol, sval, a.big, a.big_tail, a.big_d, a.big_d2, a.big_flag, row_warp_max, g->moved,
-                       bad_rank));
-        if (n_long_rows > 0) {
-            // Chunk offsets of the long rows, in list order (zeros past it).
-            if (small_b) {
-                GHB_TRY(launch(ws, small_scan_kernel<int32_t, 2>, dim3(1), dim3(1024), 0, (const int32_t*)a.big_d,
-                               (const int32_t*)a.big_d2, (const int32_t*)nullptr, a.bex, a.bsz, (int32_t*)nullptr,
-                               b));
-            } else {
-                GHB_TRY(scan_exclusive_i32(ws, a.big_d, a.bex, b, a.block_sums));
-                GHB_TRY(scan_exclusive_i32(ws, a.big_d2, a.bsz, b, a.block_sums));
+    // A batch whose changed rows hold more than half of the entries is
+    // applied as a merge rebuild: every row is written once into a fresh
+    // arena (unchanged rows copied, changed rows ranked straight into their
+    // new slots), 24 bytes per entry instead of the 48 of a rebuild through
+    // scratch and back in place.
+    if (E > 0 && 2 * E > g->m) {
+        GHB_TRY(merge_rebuild(ws, g, a, values, b, g->m + n_ins - n_del, n_modified, n_ins, n_long_rows, small_b,
+                              row_warp_max, K, bad_rank));
+    } else {
+        // Slots for rows that outgrow theirs; repack when the arena is full.
+        int64_t base = g->used;
+        bool repacked = false;
+        if (R > 0 && g->used + R > g->slots) {
+            int64_t* want = nullptr;
+            GHB_TRY(dev_alloc(&want, (int64_t)n + 1));
+            int st = launch(ws, want_cap_kernel, dim3(grid_of(ws, n)), dim3(256), 0, (const int32_t*)g->deg, n, want);
+            if (!st)
+                st = launch(ws, want_batch_kernel, dim3(gr), dim3(256), 0, (const int32_t*)a.row_id,
+                            (const int32_t*)a.headX, (const int32_t*)a.scrX, b, want);
+            if (!st) {
+                // Headroom for later growth: an eighth of the live entries.
+                const int64_t live = g->m + n_ins - n_del;
+                st = repack(ws, g, g->start, g->col, g->val, want, live / 8 + 4096, true, g->m);
             }
-            GHB_TRY(launch(ws, big_scatter_old_kernel, dim3(wide), dim3(256), 0, (const int32_t*)a.big,
-                           (const int32_t*)a.big_tail, (const int32_t*)a.bex, (const int32_t*)a.row_id,
-                           (const int32_t*)a.row_first, (const int32_t*)a.scrX, (const int32_t*)a.exX,
-                           (const uint64_t*)a.skey, (const int8_t*)a.typ, (const int32_t*)a.insX,
-                           (const int32_t*)a.delX, (const int64_t*)g->start, (const int32_t*)g->col,
-                           (const double*)g->val, scol, sval, bad_rank));
-            if (n_ins > 0)
-                GHB_TRY(launch(ws, big_scatter_new_kernel, dim3(gr), dim3(256), 0, (const uint64_t*)a.skey,
-                               (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
-                               (const int32_t*)a.headX, (const int32_t*)a.row_first, (const int32_t*)a.insX,
-                               (const int32_t*)a.delX, (const int32_t*)a.scrX, (const int8_t*)a.big_flag, b, scol,
-                               sval, bad_rank));
-            GHB_TRY(launch(ws, big_copy_kernel, dim3(wide), dim3(256), 0, (const int32_t*)a.big,
-                           (const int32_t*)a.big_tail, (const int32_t*)a.bsz, (const int32_t*)a.row_id,
-                           (const int32_t*)a.scrX, (const int64_t*)a.relX, (const int64_t*)g->start,
-                           (const int32_t*)g->cap, base, (const int32_t*)scol, (const double*)sval, g->col, g->val));
-            GHB_TRY(launch(ws, big_finalize_kernel, dim3(ws->num_sms), dim3(256), 0, (const int32_t*)a.big,
-                           (const int32_t*)a.big_tail, (const int32_t*)a.row_id, (const int32_t*)a.scrX,
-                           (const int64_t*)a.relX, base, g->start, g->deg, g->cap, g->moved));
+            dev_free(want);
+            GHB_TRY(st);
+            base = g->used;  // every changed row fits now; relX is not used
+            repacked = true;
         }
+
+        int32_t* scol = nullptr;
+        double* sval = nullptr;
+        // Scratch for the rebuilt rows (S entries) in the workspace scratch.
+        if (S > 0) {
+            Carver sizing2(nullptr);
+            sizing2.take<int32_t>(S);
+            sizing2.take<double>(S);
+            GHB_TRY(ws_reserve(ws, sizing2.off));
+            Carver c2(ws->scratch);
+            scol = c2.take<int32_t>(S);
+            sval = c2.take<double>(S);
+        }
+        if (n_modified > 0)
+            GHB_TRY(launch(ws, upd_modify_kernel, dim3(gr), dim3(256), 0, (const uint64_t*)a.skey,
+                           (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
+                           (const int64_t*)g->start, b, g->val));
+        if (S > 0 || E > 0) {
+            const unsigned wide = (unsigned)ws->num_sms * 16;
+            GHB_CUDA_TRY(cudaMemsetAsync(a.big_tail, 0, sizeof(int32_t), ws->stream));
+            if (n_long_rows > 0) {
+                GHB_CUDA_TRY(cudaMemsetAsync(a.big_d, 0, sizeof(int32_t) * (size_t)b, ws->stream));
+                GHB_CUDA_TRY(cudaMemsetAsync(a.big_d2, 0, sizeof(int32_t) * (size_t)b, ws->stream));
+            }
+            GHB_TRY(launch(ws, upd_rows_warp_kernel, dim3(grid_for(K * 32, 256, (int64_t)ws->num_sms * 8)), dim3(256), 0,
+                           (const int32_t*)a.row_id,
+                           (const int32_t*)a.row_first, (const int32_t*)a.headX, (const int32_t*)a.scrX,
+                           (const int32_t*)a.exX, (const int64_t*)a.relX, (const uint64_t*)a.skey,
+                           (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
+                           (const int32_t*)a.insX, (const int32_t*)a.delX, base, b, g->start, g->deg, g->cap, g->col,
+                           g->val, scol, sval, a.big, a.big_tail, a.big_d, a.big_d2, a.big_flag, row_warp_max,
+                           (const int64_t*)nullptr, g->moved, bad_rank));
+            if (n_long_rows > 0) {
+                // Chunk offsets of the long rows, in list order (zeros past it).
+                if (small_b) {
+                    GHB_TRY(launch(ws, small_scan_kernel<int32_t, 2>, dim3(1), dim3(1024), 0, (const int32_t*)a.big_d,
+                                   (const int32_t*)a.big_d2, (const int32_t*)nullptr, a.bex, a.bsz, (int32_t*)nullptr,
+                                   b));
+                } else {
+                    GHB_TRY(scan_exclusive_i32(ws, a.big_d, a.bex, b, a.block_sums));
+                    GHB_TRY(scan_exclusive_i32(ws, a.big_d2, a.bsz, b, a.block_sums));
+                }
+                GHB_TRY(launch(ws, big_scatter_old_kernel, dim3(wide), dim3(256), 0, (const int32_t*)a.big,
+                               (const int32_t*)a.big_tail, (const int32_t*)a.bex, (const int32_t*)a.row_id,
+                               (const int32_t*)a.row_first, (const int32_t*)a.scrX, (const int32_t*)a.exX,
+                               (const uint64_t*)a.skey, (const int8_t*)a.typ, (const int32_t*)a.insX,
+                               (const int32_t*)a.delX, (const int64_t*)g->start, (const int32_t*)g->col,
+                               (const double*)g->val, scol, sval, (const int64_t*)nullptr, bad_rank));
+                if (n_ins > 0)
+                    GHB_TRY(launch(ws, big_scatter_new_kernel, dim3(gr), dim3(256), 0, (const uint64_t*)a.skey,
+                                   (const uint32_t*)a.sidx, values, (const int8_t*)a.typ, (const int32_t*)a.pos,
+                                   (const int32_t*)a.headX, (const int32_t*)a.row_first, (const int32_t*)a.insX,
+                                   (const int32_t*)a.delX, (const int32_t*)a.scrX, (const int8_t*)a.big_flag, b, scol,
+                                   sval, (const int32_t*)a.row_id, (const int64_t*)nullptr, bad_rank));
+                GHB_TRY(launch(ws, big_copy_kernel, dim3(wide), dim3(256), 0, (const int32_t*)a.big,
+                               (const int32_t*)a.big_tail, (const int32_t*)a.bsz, (const int32_t*)a.row_id,
+                               (const int32_t*)a.scrX, (const int64_t*)a.relX, (const int64_t*)g->start,
+                               (const int32_t*)g->cap, base, (const int32_t*)scol, (const double*)sval, g->col, g->val));
+                GHB_TRY(launch(ws, big_finalize_kernel, dim3(ws->num_sms), dim3(256), 0, (const int32_t*)a.big,
+                               (const int32_t*)a.big_tail, (const int32_t*)a.row_id, (const int32_t*)a.scrX,
+                               (const int64_t*)a.relX, base, g->start, g->deg, g->cap, g->moved));
+            }
+        }
+        // Without a repack every row counted in R moved to its new slots.
+        if (!repacked) g->used += R;
     }
-    // Without a repack every row counted in R moved to its new slots.
-    if (!repacked) g->used += R;
     GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned + 8, small + 8, sizeof(int64_t), cudaMemcpyDeviceToHost,
                                  ws->stream));
     GHB_CUDA_TRY(cudaStreamSynchronize(ws->stream));
@@ -1131,6 +1323,9 @@ void release(ghb_gpma* g) {
     dev_free(g->s_col);
     dev_free(g->s_val);
     dev_free(g->moved);
+    dev_free(g->spare_col);
+    dev_free(g->spare_val);
+    g->spare_slots = 0;
 }
 
 // Empty rows, no arena.
@@ -1194,6 +1389,9 @@ int ghb_gpma_clear(ghb_workspace* ws, ghb_gpma* g) {
     GHB_CUDA_TRY(cudaStreamSynchronize(ws->stream));
     dev_free(g->col);
     dev_free(g->val);
+    dev_free(g->spare_col);
+    dev_free(g->spare_val);
+    g->spare_slots = 0;
     GHB_CUDA_TRY(cudaMemsetAsync(g->start, 0, sizeof(int64_t) * (size_t)g->n, ws->stream));
     GHB_CUDA_TRY(cudaMemsetAsync(g->deg, 0, sizeof(int32_t) * (size_t)g->n, ws->stream));
     GHB_CUDA_TRY(cudaMemsetAsync(g->cap, 0, sizeof(int32_t) * (size_t)g->n, ws->stream));
