@@ -161,7 +161,10 @@ struct OrientedVisitor {
 // load-balanced walk over every oriented entry with the binary-search
 // visitor.  (A warp-per-row shared-memory hash variant measured 25 % slower
 // on RMAT scale 24: most oriented rows hold a few entries, so a warp per row
-// leaves most lanes idle, where the walker packs short rows warp-wide.)
+// leaves most lanes idle, where the walker packs short rows warp-wide.
+// Handing the entries whose shorter list exceeds 32 to a warp each, through
+// a list appended to by atomics, measured 4 % faster at scale 22 and 12 %
+// slower at scale 24.)
 int tc_count_oriented(ghb_workspace* ws, int32_t n, const int32_t* orp, const int32_t* ocol, unsigned long long* cnt,
                       const WalkBuffers& wb) {
     return walk(ws, orp, ocol, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
