@@ -21,12 +21,44 @@
 namespace ghb {
 namespace {
 
+__device__ __forceinline__ uint64_t degree_key(uint32_t d, int64_t v) {
+    return ((uint64_t)(0xFFFFFFFFu - d) << 32) | (uint64_t)(uint32_t)v;
+}
+
+// Degree keys (descending degree, then id).  When rowptr (and the in-CSR's)
+// start on 16-byte boundaries a thread takes four vertices with one 16-byte
+// load of rowptr[4q..4q+3] plus rowptr[4q+4].
 __global__ void degree_key_kernel(int32_t n, const int32_t* __restrict__ out_rp, const int32_t* __restrict__ in_rp,
                                   uint64_t* keys) {
-    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const bool vec = ((uintptr_t)out_rp & 15) == 0 && (!in_rp || ((uintptr_t)in_rp & 15) == 0);
+    int64_t v0 = 0;
+    if (vec) {
+        const int64_t quads = n / 4;
+        for (int64_t q = tid; q < quads; q += stride) {
+            const int4 a = reinterpret_cast<const int4*>(out_rp)[q];
+            const int32_t nx = out_rp[4 * q + 4];
+            uint32_t d0 = a.y - a.x, d1 = a.z - a.y, d2 = a.w - a.z, d3 = nx - a.w;
+            if (in_rp) {
+                const int4 b = reinterpret_cast<const int4*>(in_rp)[q];
+                const int32_t ny = in_rp[4 * q + 4];
+                d0 += b.y - b.x;
+                d1 += b.z - b.y;
+                d2 += b.w - b.z;
+                d3 += ny - b.w;
+            }
+            keys[4 * q] = degree_key(d0, 4 * q);
+            keys[4 * q + 1] = degree_key(d1, 4 * q + 1);
+            keys[4 * q + 2] = degree_key(d2, 4 * q + 2);
+            keys[4 * q + 3] = degree_key(d3, 4 * q + 3);
+        }
+        v0 = quads * 4;
+    }
+    for (int64_t v = v0 + tid; v < n; v += stride) {
         uint32_t d = (uint32_t)(out_rp[v + 1] - out_rp[v]);
         if (in_rp) d += (uint32_t)(in_rp[v + 1] - in_rp[v]);
-        keys[v] = ((uint64_t)(0xFFFFFFFFu - d) << 32) | (uint64_t)(uint32_t)v;
+        keys[v] = degree_key(d, v);
     }
 }
 
@@ -43,14 +75,37 @@ __global__ void perm_from_keys_kernel(int32_t n, const uint64_t* __restrict__ ke
     }
 }
 
-// One key per entry: (new row << bits) | new col, value = entry index.
+// One key per entry: (new row << bits) | new col, value = entry index.  A
+// warp per row; rows of 64 or more entries read col with 16-byte loads (four
+// entries a lane) between a scalar head up to the first 4-aligned entry and
+// a scalar tail, when col starts on a 16-byte boundary.
 __global__ void relabel_keys_kernel(int32_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
                                     const int32_t* __restrict__ perm, int bits, uint64_t* keys, uint32_t* vals) {
+    const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const bool vec = ((uintptr_t)col & 15) == 0;
     for (int64_t u = warp; u < n; u += nwarps) {
         const uint64_t nu = (uint64_t)(uint32_t)perm[u] << bits;
-        for (int32_t j = rp[u] + lane_id(); j < rp[u + 1]; j += 32) {
+        const int32_t b = rp[u], e = rp[u + 1];
+        int32_t j0 = b, j1 = b;  // [j0, j1): the 4-aligned body
+        if (vec && e - b >= 64) {
+            j0 = (b + 3) & ~3;
+            j1 = e & ~3;
+        }
+        for (int32_t j = j0 + 4 * lane; j < j1; j += 128) {
+            const int4 c = *reinterpret_cast<const int4*>(col + j);
+            keys[j] = nu | (uint64_t)(uint32_t)perm[c.x];
+            keys[j + 1] = nu | (uint64_t)(uint32_t)perm[c.y];
+            keys[j + 2] = nu | (uint64_t)(uint32_t)perm[c.z];
+            keys[j + 3] = nu | (uint64_t)(uint32_t)perm[c.w];
+            if (vals) *reinterpret_cast<uint4*>(vals + j) = make_uint4(j, j + 1, j + 2, j + 3);
+        }
+        // Head [b, j0) and tail [j1, e) (the whole row when no body).
+        const int32_t head = j0 - b;
+        const int32_t rest = head + (e - j1);
+        for (int32_t t = lane; t < rest; t += 32) {
+            const int32_t j = t < head ? b + t : j1 + (t - head);
             keys[j] = nu | (uint64_t)(uint32_t)perm[col[j]];
             if (vals) vals[j] = (uint32_t)j;
         }
