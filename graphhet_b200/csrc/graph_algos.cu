@@ -58,10 +58,24 @@ __global__ void fill_kernel(int32_t* p, int64_t n, int32_t v) {
 }
 
 // Smallest caller id in each component: cmin[root] = min iperm over members.
+// Most vertices of a power-law graph share one root, the component of new id
+// 0 (the top hub): its members are reduced in registers and each warp issues
+// one atomic, instead of one same-address atomic per member (those serialise
+// at one L2 slice). Other roots take a plain atomic per member.
 __global__ void comp_min_kernel(int32_t n, const int32_t* __restrict__ label_new, const int32_t* __restrict__ iperm,
                                 int32_t* cmin) {
-    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
-        atomicMin(cmin + label_new[v], iperm[v]);
+    const int32_t hot = n > 0 ? label_new[0] : 0;
+    int32_t hot_min = INT_MAX;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t l = label_new[v];
+        const int32_t id = iperm[v];
+        if (l == hot)
+            hot_min = min(hot_min, id);
+        else
+            atomicMin(cmin + l, id);
+    }
+    hot_min = __reduce_min_sync(0xffffffffu, hot_min);
+    if ((threadIdx.x & 31) == 0 && hot_min != INT_MAX) atomicMin(cmin + hot, hot_min);
 }
 
 __global__ void comp_map_kernel(int32_t n, const int32_t* __restrict__ perm, const int32_t* __restrict__ label_new,
