@@ -12,22 +12,35 @@
 //            registers through shuffles, run lengths by ballot
 //   33..256  one warp per row, open-addressing (label -> count) table of 512
 //            slots in shared memory
-//   257..4096 one block per row, 8192-slot shared-memory table
-//   > 4096   one block per row, table in global scratch sized to the row
+//   257..1024 one block per row, 2048-slot shared-memory table (16 KB, so
+//            eight blocks fit an SM)
+//   1025..4096 one block per row, 8192-slot shared-memory table
+//   > 4096   the row is cut into chunks of 4096 entries, each a block: the
+//            chunk counts its labels in a shared-memory table, then adds each
+//            distinct (label, count) to the row's table in global scratch and
+//            lists the slots it claimed; a second kernel scans the listed
+//            slots chunk by chunk, and the last chunk of a row to finish
+//            writes its label.  No row waits on one block, and once labels
+//            converge a chunk sends a few global atomics, not 4096.
 // Every table ends with a max-reduction over (count, -label), which yields
 // the most frequent label with the smallest-label tie-break.
+#include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
-#include "edge_walk.cuh"
 
 namespace ghb {
 namespace {
 
-constexpr int kCdlpClasses = 9;  // 0:empty 1..5: W=2,4,8,16,32  6:warp 7:block 8:global
+// 0:empty 1..5: W=2,4,8,16,32  6:warp 7:block (2048 slots) 8:block (8192 slots) 9:chunked
+constexpr int kCdlpClasses = 10;
+constexpr int kSumLongSlot = 15;  // counts[15]: entries of the chunked-class rows
 constexpr int32_t kEmpty = -1;
 constexpr int32_t kWarpSlots = 512;
+constexpr int32_t kSmallBlockSlots = 2048;
 constexpr int32_t kBlockSlots = 8192;
+constexpr int32_t kChunk = 4096;  // entries per chunk of a chunked-class row
 constexpr int kCdlpThreads = 256;
 
 __device__ __forceinline__ int cdlp_class(int32_t d) {
@@ -38,8 +51,16 @@ __device__ __forceinline__ int cdlp_class(int32_t d) {
     if (d <= 16) return 4;
     if (d <= 32) return 5;
     if (d <= 256) return 6;
-    if (d <= 4096) return 7;
-    return 8;
+    if (d <= 1024) return 7;
+    if (d <= kChunk) return 8;
+    return 9;
+}
+
+// Slots of a chunked-class row's global table: the power of two >= 2 d.
+__host__ __device__ __forceinline__ uint32_t global_cap(int32_t d) {
+    uint32_t c = 1;
+    while (c < 2u * (uint32_t)d) c <<= 1;
+    return c;
 }
 
 __device__ __forceinline__ uint32_t hash_label(int32_t x) {
@@ -76,27 +97,6 @@ __device__ __forceinline__ void table_insert_merged(int32_t* K, int32_t* C, uint
     }
 }
 
-// First iteration over labels that are all distinct, on rows without
-// repeated entries: every count is 1, so the new label is the smallest
-// neighbour label.  Lanes that share a row merge their minimum first.
-struct MinLabelVisitor {
-    const int32_t* lab;
-    int32_t* out;
-    __device__ bool want_row(int32_t) const { return true; }
-    __device__ void operator()(int32_t u, int32_t v, int32_t) const {
-        const int32_t x = lab[v];
-        const unsigned same = __match_any_sync(__activemask(), u);
-        const int32_t m = __reduce_min_sync(same, x);
-        if (lane_id() == __ffs(same) - 1) atomicMin(out + u, m);
-    }
-    __device__ void finish() const {}
-};
-
-__global__ void cdlp_fill_max_kernel(int32_t* p, int32_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        p[i] = 0x7FFFFFFF;
-}
-
 __global__ void cdlp_count_classes_kernel(int32_t n, const int32_t* __restrict__ rp, int32_t* counts) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
          v += (int64_t)gridDim.x * blockDim.x) {
@@ -105,7 +105,7 @@ __global__ void cdlp_count_classes_kernel(int32_t n, const int32_t* __restrict__
         const unsigned same = __match_any_sync(__activemask(), c);
         const int leader = __ffs(same) - 1;
         if (lane_id() == leader) atomicAdd(&counts[c], __popc(same));
-        if (c == 8) atomicAdd(&counts[14], d);
+        if (c == 9) atomicAdd(&counts[kSumLongSlot], d);
     }
 }
 
@@ -139,8 +139,9 @@ __global__ void cdlp_copy_kernel(const int32_t* __restrict__ rows, int32_t count
     }
 }
 
-// W lanes per row, rows of 1..W entries.
-template <int W>
+// W lanes per row, rows of 1..W entries.  kMin: every label of a row is
+// distinct (first iteration), so the row's smallest label is taken directly.
+template <int W, bool kMin>
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_small_kernel(
     const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
     const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
@@ -160,6 +161,12 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_small_kernel(
         }
         int32_t x = 0x7FFFFFFF;
         if (li < d) x = lab[col[b + li]];
+        if (kMin) {
+#pragma unroll
+            for (int o = W / 2; o > 0; o >>= 1) x = min(x, __shfl_xor_sync(0xffffffffu, x, o));
+            if (li == 0 && i < count) out[v] = x;
+            continue;
+        }
         // Bitonic sort, ascending, within each W-lane group.
 #pragma unroll
         for (int k = 2; k <= W; k <<= 1) {
@@ -191,7 +198,9 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_small_kernel(
     }
 }
 
-// One warp per row of 33..256 entries, 512-slot table per warp in shared memory.
+// One warp per row of 33..256 entries, 512-slot table per warp in shared
+// memory (kMin: the row's smallest label, no table).
+template <bool kMin>
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_warp_kernel(
     const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
     const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
@@ -206,6 +215,13 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_warp_kernel(
     for (int64_t i = warp; i < count; i += nwarps) {
         const int32_t v = rows[i];
         const int32_t b = rp[v], e = rp[v + 1];
+        if (kMin) {
+            int32_t m = 0x7FFFFFFF;
+            for (int32_t j = b + lane; j < e; j += 32) m = min(m, lab[col[j]]);
+            m = __reduce_min_sync(0xffffffffu, m);
+            if (lane == 0) out[v] = m;
+            continue;
+        }
         for (int s = lane; s < kWarpSlots; s += 32) {
             K[s] = kEmpty;
             C[s] = 0;
@@ -245,20 +261,32 @@ __device__ __forceinline__ unsigned long long block_max_u64(unsigned long long x
     return r;
 }
 
-// One block per row of 257..4096 entries; 8192-slot table in dynamic smem.
+// One block per row of up to `slots` / 2 entries (classes 7 and 8); the table
+// (the power of two >= 2 x the row, at least 512 slots) lives in 2 x slots
+// ints of dynamic shared memory.  kMin: the row's smallest label, no table.
+template <bool kMin>
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_block_kernel(
     const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
+    const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out, uint32_t slots) {
     extern __shared__ int32_t smem[];
     __shared__ unsigned long long red[32];
     int32_t* K = smem;
-    int32_t* C = smem + kBlockSlots;
+    int32_t* C = smem + slots;
     for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
         const int32_t v = rows[i];
         const int32_t b = rp[v], e = rp[v + 1];
-        // Table of the next power of two >= 2 x the row (at most kBlockSlots).
+        if (kMin) {
+            unsigned long long m = 0;
+            for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+                const unsigned long long key = pack_best(1, lab[col[j]]);
+                m = key > m ? key : m;
+            }
+            m = block_max_u64(m, red);
+            if (threadIdx.x == 0) out[v] = unpack_label(m);
+            continue;
+        }
         uint32_t cap = 512;
-        while (cap < 2u * (uint32_t)(e - b) && cap < (uint32_t)kBlockSlots) cap <<= 1;
+        while (cap < 2u * (uint32_t)(e - b) && cap < slots) cap <<= 1;
         for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
             K[s] = kEmpty;
             C[s] = 0;
@@ -282,59 +310,169 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_block_kernel(
     }
 }
 
-// One block per row of > 4096 entries (many blocks, round robin); each row
-// owns a table in global scratch at tab_off[i] (the next power of two >= 2 x
-// the row), left empty after use, so only the first call clears the pool.
-__global__ void __launch_bounds__(kCdlpThreads) cdlp_global_kernel(
-    const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out,
-    int32_t* pool, const int64_t* __restrict__ tab_off) {
-    __shared__ unsigned long long red[32];
-    for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
-        const int32_t v = rows[i];
-        const int32_t b = rp[v], e = rp[v + 1];
-        const uint32_t cap = (uint32_t)((tab_off[i + 1] - tab_off[i]) / 2);
-        int32_t* K = pool + tab_off[i];
-        int32_t* C = K + cap;
+// Global tables hold slot h as the pair (label, count) at T[2h], T[2h + 1],
+// so a probe, its count and the later read of both touch one sector.
+// Adds cnt to label x in a table of cap slots (cap > 2 x the labels it can
+// hold, so a free slot is always reached).  Returns the slot when this call
+// claimed it for x, else -1.
+__device__ __forceinline__ int32_t global_add(int32_t* T, uint32_t cap, int32_t x, int32_t cnt) {
+    uint32_t h = hash_label(x) & (cap - 1);
+    while (true) {
+        const int32_t k = atomicCAS(&T[2 * h], kEmpty, x);
+        if (k == kEmpty || k == x) {
+            atomicAdd(&T[2 * h + 1], cnt);
+            return k == kEmpty ? (int32_t)h : -1;
+        }
+        h = (h + 1) & (cap - 1);
+    }
+}
+
+// Chunked-class row i owns pool[tab_off[i] ...] (tab_off even): cap slot
+// pairs, then the list of claimed slots (up to d).  chunks[2k], chunks[2k+1]
+// = row index i and the chunk's first entry within the row (a multiple of
+// kChunk).
+struct LongRow {
+    int32_t v, d;
+    uint32_t cap;
+    int32_t *T, *L;
+};
+__device__ __forceinline__ LongRow long_row(const int32_t* rows, const int32_t* rp, int32_t* pool,
+                                            const int64_t* tab_off, int32_t i) {
+    LongRow r;
+    r.v = rows[i];
+    r.d = rp[r.v + 1] - rp[r.v];
+    r.cap = global_cap(r.d);
+    r.T = pool + tab_off[i];
+    r.L = r.T + 2 * (size_t)r.cap;
+    return r;
+}
+
+// Called by thread 0 of a block that has finished its chunk of row i with the
+// chunk's best (count, -label) key: folds it into best[i]; the row's last
+// chunk writes the label and resets the row's counters for the next pass.
+__device__ __forceinline__ void chunk_done(const LongRow& r, int32_t i, unsigned long long b, int32_t* occ,
+                                           int32_t* done, unsigned long long* best, int32_t* out) {
+    if (b) atomicMax(best + i, b);
+    __threadfence();
+    const int32_t nchunks = (r.d + kChunk - 1) / kChunk;
+    if (atomicAdd(done + i, 1) == nchunks - 1) {
+        __threadfence();
+        out[r.v] = unpack_label(atomicExch(best + i, 0ull));
+        occ[i] = 0;
+        done[i] = 0;
+    }
+}
+
+// Pass 1 over the chunks: count the chunk's labels in shared memory, then add
+// each distinct (label, count) to the row's global table; slots claimed here
+// are appended to the row's list (one atomic per warp on occ[i]).
+__global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
+    const int32_t* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+    const int32_t* __restrict__ lab, const int32_t* __restrict__ chunks, int32_t nch, int32_t* pool,
+    const int64_t* __restrict__ tab_off, int32_t* occ) {
+    extern __shared__ int32_t smem[];
+    int32_t* K = smem;
+    int32_t* C = smem + kBlockSlots;
+    for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
+        const int32_t i = chunks[2 * k];
+        const LongRow r = long_row(rows, rp, pool, tab_off, i);
+        const int32_t b = rp[r.v] + chunks[2 * k + 1];
+        const int32_t e = min(b + kChunk, rp[r.v + 1]);
+        uint32_t cap = 512;
+        while (cap < 2u * (uint32_t)(e - b) && cap < (uint32_t)kBlockSlots) cap <<= 1;
+        for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
+            K[s] = kEmpty;
+            C[s] = 0;
+        }
+        __syncthreads();
         for (int32_t j0 = b; j0 < e; j0 += blockDim.x) {
             const int32_t j = j0 + threadIdx.x;
             table_insert_merged(K, C, cap, j < e ? lab[col[j]] : 0, j < e);
         }
         __syncthreads();
-        unsigned long long best = 0;
+        // cap is a multiple of the block size: every warp runs every round.
         for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
-            const int32_t k = __ldcg(&K[s]);
-            if (k != kEmpty) {
-                const unsigned long long key = pack_best((uint32_t)__ldcg(&C[s]), k);
-                best = key > best ? key : best;
-                K[s] = kEmpty;  // leave the table empty for the next iteration
-                C[s] = 0;
+            const int32_t x = K[s];
+            const int32_t claimed = x != kEmpty ? global_add(r.T, r.cap, x, C[s]) : -1;
+            const unsigned m = __ballot_sync(0xffffffffu, claimed >= 0);
+            if (m) {
+                int32_t base = 0;
+                if (lane_id() == 0) base = atomicAdd(occ + i, __popc(m));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (claimed >= 0) r.L[base + __popc(m & ((1u << lane_id()) - 1u))] = claimed;
             }
         }
-        best = block_max_u64(best, red);
-        if (threadIdx.x == 0) out[v] = unpack_label(best);
+        __syncthreads();
     }
 }
 
-// Block per row: keys kEmpty, counts 0.
-__global__ void cdlp_pool_clear_kernel(int32_t* pool, const int64_t* __restrict__ tab_off, int32_t count) {
-    for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
-        const int64_t b = tab_off[i], half = (tab_off[i + 1] - b) / 2;
-        for (int64_t s = threadIdx.x; s < half; s += blockDim.x) {
-            pool[b + s] = kEmpty;
-            pool[b + half + s] = 0;
+// Pass 2 over the same chunks: chunk k of row i takes the claimed slots
+// [j0, j0 + kChunk) of the row's list, folds their (count, label) keys into
+// best[i] and empties those slots for the next iteration.
+__global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_pick_kernel(
+    const int32_t* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ chunks,
+    int32_t nch, int32_t* pool, const int64_t* __restrict__ tab_off, int32_t* occ, int32_t* done,
+    unsigned long long* best, int32_t* __restrict__ out) {
+    __shared__ unsigned long long red[32];
+    for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
+        const int32_t i = chunks[2 * k];
+        const LongRow r = long_row(rows, rp, pool, tab_off, i);
+        const int32_t j0 = chunks[2 * k + 1];
+        const int32_t j1 = min(j0 + kChunk, __ldcg(occ + i));
+        int2* T2 = reinterpret_cast<int2*>(r.T);
+        unsigned long long b = 0;
+        for (int32_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+            const int32_t s = __ldcg(r.L + j);
+            const int2 kc = __ldcg(T2 + s);
+            const unsigned long long key = pack_best((uint32_t)kc.y, kc.x);
+            b = key > b ? key : b;
+            T2[s] = make_int2(kEmpty, 0);
         }
+        b = block_max_u64(b, red);
+        if (threadIdx.x == 0) chunk_done(r, i, b, occ, done, best, out);
     }
 }
 
-// Table sizes of the global-class rows: 2 x (next power of two >= 2 d) ints each.
-__global__ void cdlp_table_sizes_kernel(const int32_t* __restrict__ rows, int32_t count,
-                                        const int32_t* __restrict__ rp, int64_t* sizes) {
+// First iteration (labels distinct, no repeated entries): each chunk's
+// smallest label, folded over the row's chunks as in the pick pass.
+__global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_min_kernel(
+    const int32_t* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+    const int32_t* __restrict__ lab, const int32_t* __restrict__ chunks, int32_t nch, int32_t* pool,
+    const int64_t* __restrict__ tab_off, int32_t* occ, int32_t* done, unsigned long long* best,
+    int32_t* __restrict__ out) {
+    __shared__ unsigned long long red[32];
+    for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
+        const int32_t i = chunks[2 * k];
+        const LongRow r = long_row(rows, rp, pool, tab_off, i);
+        const int32_t b = rp[r.v] + chunks[2 * k + 1];
+        const int32_t e = min(b + kChunk, rp[r.v + 1]);
+        unsigned long long m = 0;
+        for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+            const unsigned long long key = pack_best(1, lab[col[j]]);
+            m = key > m ? key : m;
+        }
+        m = block_max_u64(m, red);
+        if (threadIdx.x == 0) chunk_done(r, i, m, occ, done, best, out);
+    }
+}
+
+// Chunked-class rows: degrees for the host's table layout.
+__global__ void cdlp_long_degrees_kernel(const int32_t* __restrict__ rows, int32_t count,
+                                         const int32_t* __restrict__ rp, int32_t* deg) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t v = rows[i];
-        int64_t cap = 1;
-        while (cap < 2 * (int64_t)(rp[v + 1] - rp[v])) cap <<= 1;
-        sizes[i] = 2 * cap;
+        deg[i] = rp[v + 1] - rp[v];
+    }
+}
+
+// Block per chunked-class row: every slot (kEmpty, 0).
+__global__ void cdlp_pool_clear_kernel(const int32_t* __restrict__ rows, int32_t count,
+                                       const int32_t* __restrict__ rp, int32_t* pool,
+                                       const int64_t* __restrict__ tab_off) {
+    for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
+        const LongRow r = long_row(rows, rp, pool, tab_off, (int32_t)i);
+        int2* T2 = reinterpret_cast<int2*>(r.T);
+        for (uint32_t s = threadIdx.x; s < r.cap; s += blockDim.x) T2[s] = make_int2(kEmpty, 0);
     }
 }
 
@@ -346,7 +484,6 @@ __global__ void cdlp_table_sizes_kernel(const int32_t* __restrict__ rows, int32_
 int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col, int32_t iterations,
              int32_t* labels, const int32_t* init_labels, bool first_min) {
     cudaStream_t st = ws->stream;
-    const unsigned grid_global = ws->num_sms * 8;
     int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
 
     // Pass 1: class sizes.
@@ -365,17 +502,24 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
         cls[k] = hp[k];
         off[k + 1] = off[k] + cls[k];
     }
-    // Global-class tables: 2 x (next power of two >= 2 d) ints per row, so
-    // fewer than 8 ints per entry of those rows.
-    const int64_t pool_bound = cls[8] > 0 ? 8 * (int64_t)hp[14] + 16 : 1;
+    // Chunked-class tables: (label, count) pairs for the power of two >= 2 d
+    // slots, then the claimed-slot list of d ints (rounded up to even), so
+    // fewer than 9 ints per entry plus one per row.
+    const int32_t nlong = cls[9];
+    const int64_t long_entries = hp[kSumLongSlot];
+    const int64_t pool_bound = nlong > 0 ? 9 * long_entries + nlong + 16 : 1;
+    const int64_t chunk_bound = long_entries / kChunk + nlong + 1;
     Carver sizing(nullptr);
     sizing.take<int32_t>(16);
     sizing.take<int32_t>(16);
     sizing.take<int32_t>(n);
     sizing.take<int32_t>(n);
     sizing.take<int32_t>(pool_bound);
-    sizing.take<int64_t>((size_t)cls[8] + 1);
-    WalkBuffers::carve(sizing, n);
+    sizing.take<int64_t>((size_t)nlong + 1);
+    sizing.take<int32_t>(2 * chunk_bound);
+    sizing.take<int32_t>((size_t)nlong + 1);
+    sizing.take<int32_t>((size_t)nlong + 1);
+    sizing.take<unsigned long long>((size_t)nlong + 1);
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
     counts = c.take<int32_t>(16);
@@ -383,64 +527,106 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
     int32_t* rows = c.take<int32_t>(n);
     int32_t* other = c.take<int32_t>(n);
     int32_t* pool = c.take<int32_t>(pool_bound);
-    int64_t* tab_off = c.take<int64_t>((size_t)cls[8] + 1);
-    WalkBuffers wb = WalkBuffers::carve(c, n);
+    int64_t* tab_off = c.take<int64_t>((size_t)nlong + 1);
+    int32_t* chunks = c.take<int32_t>(2 * chunk_bound);
+    int32_t* occ = c.take<int32_t>((size_t)nlong + 1);
+    int32_t* done = c.take<int32_t>((size_t)nlong + 1);
+    unsigned long long* best = c.take<unsigned long long>((size_t)nlong + 1);
 
     for (int k = 0; k < kCdlpClasses; ++k) hp[k] = off[k];
     GHB_CUDA_TRY(cudaMemcpyAsync(cursor, hp, kCdlpClasses * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     GHB_TRY(launch(ws, cdlp_fill_classes_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n, rp,
                    cursor, rows));
-    if (cls[8] > 0) {
-        // Table offsets on the host (a few thousand rows), then an empty pool.
-        GHB_TRY(launch(ws, cdlp_table_sizes_kernel, dim3(grid_for(cls[8], 256, ws->num_sms)), dim3(256), 0,
-                       (const int32_t*)(rows + off[8]), cls[8], rp, tab_off));
-        std::vector<int64_t> sz((size_t)cls[8] + 1);
-        GHB_CUDA_TRY(cudaMemcpyAsync(sz.data(), tab_off, sizeof(int64_t) * cls[8], cudaMemcpyDeviceToHost, st));
+    const int32_t* long_rows = rows + off[9];
+    int32_t nch = 0;
+    if (nlong > 0) {
+        // Table offsets and the chunk list on the host (a few thousand rows),
+        // then empty tables and zero counters.
+        GHB_TRY(launch(ws, cdlp_long_degrees_kernel, dim3(grid_for(nlong, 256, ws->num_sms)), dim3(256), 0,
+                       long_rows, nlong, rp, occ));
+        std::vector<int32_t> deg((size_t)nlong);
+        GHB_CUDA_TRY(cudaMemcpyAsync(deg.data(), occ, sizeof(int32_t) * nlong, cudaMemcpyDeviceToHost, st));
         GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        std::vector<int64_t> toff((size_t)nlong + 1);
+        std::vector<int32_t> ch;
+        ch.reserve(2 * (size_t)chunk_bound);
         int64_t acc = 0;
-        for (int32_t i = 0; i < cls[8]; ++i) {
-            const int64_t x = sz[i];
-            sz[i] = acc;
-            acc += x;
+        for (int32_t i = 0; i < nlong; ++i) {
+            toff[i] = acc;
+            acc += 2 * (int64_t)global_cap(deg[i]) + ((deg[i] + 1) & ~1);  // keeps every tab_off even
+            for (int32_t j = 0; j < deg[i]; j += kChunk) {
+                ch.push_back(i);
+                ch.push_back(j);
+            }
         }
-        sz[cls[8]] = acc;
-        GHB_REQUIRE(acc <= pool_bound, "CDLP table pool bound");
-        GHB_CUDA_TRY(cudaMemcpyAsync(tab_off, sz.data(), sizeof(int64_t) * (cls[8] + 1), cudaMemcpyHostToDevice, st));
-        // Empty = kEmpty keys (0xffffffff) and zero counts; the offsets are
-        // even, so keys and counts are the two halves of each row's table.
-        GHB_TRY(launch(ws, cdlp_pool_clear_kernel, dim3(grid_for(cls[8], 1, grid_global)), dim3(256), 0, pool,
-                       (const int64_t*)tab_off, cls[8]));
-        GHB_CUDA_TRY(cudaStreamSynchronize(st));  // sz is read by the copy above
+        toff[nlong] = acc;
+        nch = (int32_t)(ch.size() / 2);
+        GHB_REQUIRE(acc <= pool_bound && nch <= chunk_bound, "CDLP table pool bound");
+        GHB_CUDA_TRY(cudaMemcpyAsync(tab_off, toff.data(), sizeof(int64_t) * (nlong + 1), cudaMemcpyHostToDevice, st));
+        GHB_CUDA_TRY(cudaMemcpyAsync(chunks, ch.data(), sizeof(int32_t) * ch.size(), cudaMemcpyHostToDevice, st));
+        GHB_CUDA_TRY(cudaMemsetAsync(occ, 0, sizeof(int32_t) * nlong, st));
+        GHB_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(int32_t) * nlong, st));
+        GHB_CUDA_TRY(cudaMemsetAsync(best, 0, sizeof(unsigned long long) * nlong, st));
+        GHB_TRY(launch(ws, cdlp_pool_clear_kernel, dim3(grid_for(nlong, 1, ws->num_sms * 8)), dim3(256), 0, long_rows,
+                       nlong, rp, pool, (const int64_t*)tab_off));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));  // toff and ch are read by the copies above
     }
     if (init_labels)
         GHB_CUDA_TRY(cudaMemcpyAsync(labels, init_labels, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
     else
         GHB_TRY(launch(ws, cdlp_iota_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, labels, n));
 
-    GHB_CUDA_TRY(cudaFuncSetAttribute(cdlp_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(2 * kBlockSlots * sizeof(int32_t))));
+    // Shared-memory classes: as many blocks as fit each SM.
+    const size_t small_smem = 2 * kSmallBlockSlots * sizeof(int32_t), big_smem = 2 * kBlockSlots * sizeof(int32_t);
+    GHB_CUDA_TRY(cudaFuncSetAttribute(cdlp_block_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)big_smem));
+    GHB_CUDA_TRY(cudaFuncSetAttribute(cdlp_chunk_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)big_smem));
+    int per_sm_small = 0, per_sm_big = 0, per_sm_chunk = 0;
+    GHB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_small, cdlp_block_kernel<false>, kCdlpThreads,
+                                                               small_smem));
+    GHB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_big, cdlp_block_kernel<false>, kCdlpThreads,
+                                                               big_smem));
+    GHB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_chunk, cdlp_chunk_count_kernel, kCdlpThreads,
+                                                               big_smem));
+    const unsigned g_small = ws->num_sms * std::max(1, per_sm_small);
+    const unsigned g_big = ws->num_sms * std::max(1, per_sm_big);
+    const unsigned g_chunk = ws->num_sms * std::max(1, per_sm_chunk);
+    const unsigned g = ws->num_sms * 8;
+
+    // One iteration: every class reads cur and writes nxt.  kMin (first
+    // iteration over distinct labels): each row's smallest label.
+    auto iteration = [&](auto min_tag, const int32_t* cur, int32_t* nxt) -> int {
+        constexpr bool M = decltype(min_tag)::value;
+        const int32_t* R = rows;
+        if (cls[0]) GHB_TRY(launch(ws, cdlp_copy_kernel, dim3(grid_for(cls[0], 256, g)), dim3(256), 0, R + off[0], cls[0], cur, nxt));
+        if (cls[1]) GHB_TRY(launch(ws, cdlp_small_kernel<2, M>, dim3(grid_for((int64_t)cls[1] * 2, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[1], cls[1], rp, col, cur, nxt));
+        if (cls[2]) GHB_TRY(launch(ws, cdlp_small_kernel<4, M>, dim3(grid_for((int64_t)cls[2] * 4, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[2], cls[2], rp, col, cur, nxt));
+        if (cls[3]) GHB_TRY(launch(ws, cdlp_small_kernel<8, M>, dim3(grid_for((int64_t)cls[3] * 8, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[3], cls[3], rp, col, cur, nxt));
+        if (cls[4]) GHB_TRY(launch(ws, cdlp_small_kernel<16, M>, dim3(grid_for((int64_t)cls[4] * 16, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[4], cls[4], rp, col, cur, nxt));
+        if (cls[5]) GHB_TRY(launch(ws, cdlp_small_kernel<32, M>, dim3(grid_for((int64_t)cls[5] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[5], cls[5], rp, col, cur, nxt));
+        if (cls[6]) GHB_TRY(launch(ws, cdlp_warp_kernel<M>, dim3(grid_for((int64_t)cls[6] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[6], cls[6], rp, col, cur, nxt));
+        if (M) {
+            if (cls[7] + cls[8]) GHB_TRY(launch(ws, cdlp_block_kernel<true>, dim3(grid_for(cls[7] + cls[8], 1, g)), dim3(kCdlpThreads), 0, R + off[7], cls[7] + cls[8], rp, col, cur, nxt, 0u));
+            if (nlong) GHB_TRY(launch(ws, cdlp_chunk_min_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done, best, nxt));
+            return GHB_OK;
+        }
+        if (cls[7]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[7], 1, g_small)), dim3(kCdlpThreads), small_smem, R + off[7], cls[7], rp, col, cur, nxt, (uint32_t)kSmallBlockSlots));
+        if (cls[8]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[8], 1, g_big)), dim3(kCdlpThreads), big_smem, R + off[8], cls[8], rp, col, cur, nxt, (uint32_t)kBlockSlots));
+        if (nlong) {
+            GHB_TRY(launch(ws, cdlp_chunk_count_kernel, dim3(grid_for(nch, 1, g_chunk)), dim3(kCdlpThreads), big_smem, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ));
+            GHB_TRY(launch(ws, cdlp_chunk_pick_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done, best, nxt));
+        }
+        return GHB_OK;
+    };
+
     int32_t* cur = labels;
     int32_t* nxt = other;
-    const unsigned g = ws->num_sms * 8;
     for (int it = 0; it < iterations; ++it) {
-        const int32_t* R = rows;
-        if (it == 0 && first_min) {
-            GHB_TRY(launch(ws, cdlp_fill_max_kernel, dim3(grid_for(n, 256, g)), dim3(256), 0, nxt, n));
-            GHB_TRY(walk(ws, rp, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
-                         MinLabelVisitor{(const int32_t*)cur, nxt}));
-            if (cls[0]) GHB_TRY(launch(ws, cdlp_copy_kernel, dim3(grid_for(cls[0], 256, g)), dim3(256), 0, R + off[0], cls[0], (const int32_t*)cur, nxt));
-            std::swap(cur, nxt);
-            continue;
-        }
-        if (cls[0]) GHB_TRY(launch(ws, cdlp_copy_kernel, dim3(grid_for(cls[0], 256, g)), dim3(256), 0, R + off[0], cls[0], (const int32_t*)cur, nxt));
-        if (cls[1]) GHB_TRY(launch(ws, cdlp_small_kernel<2>, dim3(grid_for((int64_t)cls[1] * 2, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[1], cls[1], rp, col, (const int32_t*)cur, nxt));
-        if (cls[2]) GHB_TRY(launch(ws, cdlp_small_kernel<4>, dim3(grid_for((int64_t)cls[2] * 4, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[2], cls[2], rp, col, (const int32_t*)cur, nxt));
-        if (cls[3]) GHB_TRY(launch(ws, cdlp_small_kernel<8>, dim3(grid_for((int64_t)cls[3] * 8, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[3], cls[3], rp, col, (const int32_t*)cur, nxt));
-        if (cls[4]) GHB_TRY(launch(ws, cdlp_small_kernel<16>, dim3(grid_for((int64_t)cls[4] * 16, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[4], cls[4], rp, col, (const int32_t*)cur, nxt));
-        if (cls[5]) GHB_TRY(launch(ws, cdlp_small_kernel<32>, dim3(grid_for((int64_t)cls[5] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[5], cls[5], rp, col, (const int32_t*)cur, nxt));
-        if (cls[6]) GHB_TRY(launch(ws, cdlp_warp_kernel, dim3(grid_for((int64_t)cls[6] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[6], cls[6], rp, col, (const int32_t*)cur, nxt));
-        if (cls[7]) GHB_TRY(launch(ws, cdlp_block_kernel, dim3(grid_for(cls[7], 1, ws->num_sms * 2)), dim3(kCdlpThreads), (size_t)(2 * kBlockSlots * sizeof(int32_t)), R + off[7], cls[7], rp, col, (const int32_t*)cur, nxt));
-        if (cls[8]) GHB_TRY(launch(ws, cdlp_global_kernel, dim3(grid_for(cls[8], 1, grid_global)), dim3(kCdlpThreads), 0, R + off[8], cls[8], rp, col, (const int32_t*)cur, nxt, pool, (const int64_t*)tab_off));
+        if (it == 0 && first_min)
+            GHB_TRY(iteration(std::true_type{}, cur, nxt));
+        else
+            GHB_TRY(iteration(std::false_type{}, cur, nxt));
         std::swap(cur, nxt);
     }
     if (cur != labels)

@@ -157,3 +157,28 @@ def test_cdlp_rows_beyond_4096_entries(G):
     rg = G.ResidentGraph(to_gpu(G, og))
     assert np.array_equal(rg.cdlp(10).cpu().numpy(), ref)
     assert np.array_equal(rg.cdlp(3).cpu().numpy(), O.cdlp(og, 3))
+
+
+def test_cdlp_class_edges_and_many_chunks(G):
+    """Rows at each shared-memory class edge (1024 | 1025 and 4096 | 4097
+    entries), rows of one and two chunks (8192 | 8193) and hubs of 20,000 and
+    45,000 entries (5 and 11 chunks of 4096), each hub a vertex of its own
+    joined to distinct RMAT vertices; raw CSR and handle, 1, 2 and 10
+    iterations."""
+    scale = 16
+    base = 1 << scale
+    s, d = O.rmat_edges(scale, 8 << scale, 11)
+    rng = np.random.default_rng(5)
+    degs = (1024, 1025, 4096, 4097, 8192, 8193, 20000, 45000)
+    hs, hd = [s], [d]
+    for k, deg in enumerate(degs):
+        hs.append(np.full(deg, base + k, np.int32))
+        hd.append(rng.choice(base, size=deg, replace=False).astype(np.int32))
+    og = O.make_graph(base + len(degs), np.concatenate(hs), np.concatenate(hd), False, weight_mode=0)
+    assert np.diff(og.rowptr)[base:].tolist() == list(degs)
+    g = to_gpu(G, og)
+    rg = G.ResidentGraph(to_gpu(G, og))
+    for iters in (1, 2, 10):
+        ref = O.cdlp(og, iters)
+        assert np.array_equal(G.cdlp(g, iters).cpu().numpy(), ref), iters
+        assert np.array_equal(rg.cdlp(iters).cpu().numpy(), ref), iters
