@@ -18,12 +18,14 @@
 //   > 4096   the row is cut into chunks of 4096 entries, each a block: the
 //            chunk counts its labels in a shared-memory table, then adds each
 //            distinct (label, count) to the row's table in global scratch and
-//            lists the slots it claimed; a second kernel scans the listed
-//            slots chunk by chunk, and the last chunk of a row to finish
-//            writes its label.  No row waits on one block, and once labels
-//            converge a chunk sends a few global atomics, not 4096.
-// Every table ends with a max-reduction over (count, -label), which yields
-// the most frequent label with the smallest-label tie-break.
+//            lists the slots it claimed; the last chunk of a row to finish
+//            writes its label, and a write-only pass empties the claimed
+//            slots.  No row waits on one block, and once labels converge a
+//            chunk sends a few global atomics, not 4096.
+// Every insert returns the key (count after it, -label); a label's last insert
+// sees its final count, so the max-reduction of those keys yields the most
+// frequent label with the smallest-label tie-break, and no table is scanned
+// for it.
 #include <algorithm>
 #include <type_traits>
 #include <vector>
@@ -80,18 +82,23 @@ __device__ __forceinline__ int32_t unpack_label(unsigned long long k) {
 // (power of two) entries, K = labels, C = counts.  Lanes of the warp holding
 // the same label are merged first (one atomic per distinct label per warp),
 // which matters once labels converge and a hub's row repeats a few labels.
-// Every lane of the warp must call it.
-__device__ __forceinline__ void table_insert_merged(int32_t* K, int32_t* C, uint32_t slots, int32_t x, bool valid) {
+// Every lane of the warp must call it.  Returns, on the lane that inserted for
+// its group, the key (count after this insert, label), else 0.  A label's
+// count only grows and its last insert sees the final count, so the largest
+// key returned over a row names its most frequent label (smallest on ties)
+// without a scan of the table.
+__device__ __forceinline__ unsigned long long table_insert_merged(int32_t* K, int32_t* C, uint32_t slots, int32_t x,
+                                                                  bool valid) {
     const unsigned act = __ballot_sync(0xffffffffu, valid);
-    if (!valid) return;
+    if (!valid) return 0;
     const unsigned same = __match_any_sync(act, x);
-    if (lane_id() != __ffs(same) - 1) return;
+    if (lane_id() != __ffs(same) - 1) return 0;
     uint32_t h = hash_label(x) & (slots - 1);
     while (true) {
         const int32_t k = atomicCAS(&K[h], kEmpty, x);
         if (k == kEmpty || k == x) {
-            atomicAdd(&C[h], __popc(same));
-            return;
+            const int32_t c = atomicAdd(&C[h], __popc(same)) + __popc(same);
+            return pack_best((uint32_t)c, x);
         }
         h = (h + 1) & (slots - 1);
     }
@@ -222,23 +229,20 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_warp_kernel(
             if (lane == 0) out[v] = m;
             continue;
         }
-        for (int s = lane; s < kWarpSlots; s += 32) {
+        // Table of the power of two >= 2 x the row (64..512 slots): clearing
+        // it costs no more than the row's own inserts.
+        uint32_t cap = 64;
+        while (cap < 2u * (uint32_t)(e - b)) cap <<= 1;
+        for (uint32_t s = lane; s < cap; s += 32) {
             K[s] = kEmpty;
             C[s] = 0;
         }
         __syncwarp();
+        unsigned long long best = 0;
         for (int32_t j0 = b; j0 < e; j0 += 32) {
             const int32_t j = j0 + lane;
-            table_insert_merged(K, C, kWarpSlots, j < e ? lab[col[j]] : 0, j < e);
-        }
-        __syncwarp();
-        unsigned long long best = 0;
-        for (int s = lane; s < kWarpSlots; s += 32) {
-            const int32_t k = K[s];
-            if (k != kEmpty) {
-                const unsigned long long key = pack_best((uint32_t)C[s], k);
-                best = key > best ? key : best;
-            }
+            const unsigned long long key = table_insert_merged(K, C, cap, j < e ? lab[col[j]] : 0, j < e);
+            best = key > best ? key : best;
         }
         best = warp_max(best);
         if (lane == 0) out[v] = unpack_label(best);
@@ -292,49 +296,60 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_block_kernel(
             C[s] = 0;
         }
         __syncthreads();
+        unsigned long long best = 0;
         for (int32_t j0 = b; j0 < e; j0 += blockDim.x) {
             const int32_t j = j0 + threadIdx.x;
-            table_insert_merged(K, C, cap, j < e ? lab[col[j]] : 0, j < e);
+            const unsigned long long key = table_insert_merged(K, C, cap, j < e ? lab[col[j]] : 0, j < e);
+            best = key > best ? key : best;
         }
-        __syncthreads();
-        unsigned long long best = 0;
-        for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
-            const int32_t k = K[s];
-            if (k != kEmpty) {
-                const unsigned long long key = pack_best((uint32_t)C[s], k);
-                best = key > best ? key : best;
-            }
-        }
+        // Also orders this row's inserts before the next row's clearing.
         best = block_max_u64(best, red);
         if (threadIdx.x == 0) out[v] = unpack_label(best);
     }
 }
 
-// Global tables hold slot h as the pair (label, count) at T[2h], T[2h + 1],
-// so a probe, its count and the later read of both touch one sector.
+// Global tables hold slot h as one word, label << 32 | count, empty =
+// kSlotEmpty (label kEmpty, count 0): a probe, its count and the later read
+// touch one 8-byte word, and a count is added with one 64-bit atomic that
+// cannot carry into the label (counts stay below 2^31).
+constexpr unsigned long long kSlotEmpty = 0xFFFFFFFF00000000ull;
+
 // Adds cnt to label x in a table of cap slots (cap > 2 x the labels it can
-// hold, so a free slot is always reached).  Returns the slot when this call
-// claimed it for x, else -1.
-__device__ __forceinline__ int32_t global_add(int32_t* T, uint32_t cap, int32_t x, int32_t cnt) {
+// hold, so a free slot is always reached).  The slot is read first, so a
+// label already present costs one atomic add and a new one one CAS.  Sets key
+// to (count after this add, label), as table_insert_merged returns it, and
+// returns the slot when this call claimed it for x, else -1.
+__device__ __forceinline__ int32_t global_add(unsigned long long* T, uint32_t cap, int32_t x, int32_t cnt,
+                                              unsigned long long& key) {
+    const unsigned long long mine = (unsigned long long)(uint32_t)x << 32;
     uint32_t h = hash_label(x) & (cap - 1);
     while (true) {
-        const int32_t k = atomicCAS(&T[2 * h], kEmpty, x);
-        if (k == kEmpty || k == x) {
-            atomicAdd(&T[2 * h + 1], cnt);
-            return k == kEmpty ? (int32_t)h : -1;
+        unsigned long long cur = __ldcg(T + h);
+        if (cur == kSlotEmpty) {
+            cur = atomicCAS(T + h, kSlotEmpty, mine | (uint32_t)cnt);
+            if (cur == kSlotEmpty) {
+                key = pack_best((uint32_t)cnt, x);
+                return (int32_t)h;
+            }
+        }
+        if ((uint32_t)(cur >> 32) == (uint32_t)x) {
+            const unsigned long long old = atomicAdd(T + h, (unsigned long long)cnt);
+            key = pack_best((uint32_t)old + (uint32_t)cnt, x);
+            return -1;
         }
         h = (h + 1) & (cap - 1);
     }
 }
 
 // Chunked-class row i owns pool[tab_off[i] ...] (tab_off even): cap slot
-// pairs, then the list of claimed slots (up to d).  chunks[2k], chunks[2k+1]
+// words, then the list of claimed slots (up to d).  chunks[2k], chunks[2k+1]
 // = row index i and the chunk's first entry within the row (a multiple of
 // kChunk).
 struct LongRow {
     int32_t v, d;
     uint32_t cap;
-    int32_t *T, *L;
+    unsigned long long* T;
+    int32_t* L;
 };
 __device__ __forceinline__ LongRow long_row(const int32_t* rows, const int32_t* rp, int32_t* pool,
                                             const int64_t* tab_off, int32_t i) {
@@ -342,35 +357,39 @@ __device__ __forceinline__ LongRow long_row(const int32_t* rows, const int32_t* 
     r.v = rows[i];
     r.d = rp[r.v + 1] - rp[r.v];
     r.cap = global_cap(r.d);
-    r.T = pool + tab_off[i];
-    r.L = r.T + 2 * (size_t)r.cap;
+    r.T = reinterpret_cast<unsigned long long*>(pool + tab_off[i]);
+    r.L = reinterpret_cast<int32_t*>(r.T + r.cap);
     return r;
 }
 
 // Called by thread 0 of a block that has finished its chunk of row i with the
 // chunk's best (count, -label) key: folds it into best[i]; the row's last
-// chunk writes the label and resets the row's counters for the next pass.
-__device__ __forceinline__ void chunk_done(const LongRow& r, int32_t i, unsigned long long b, int32_t* occ,
-                                           int32_t* done, unsigned long long* best, int32_t* out) {
+// chunk writes the label and resets done[i] and best[i].
+__device__ __forceinline__ void chunk_done(const LongRow& r, int32_t i, unsigned long long b, int32_t* done,
+                                           unsigned long long* best, int32_t* out) {
     if (b) atomicMax(best + i, b);
     __threadfence();
     const int32_t nchunks = (r.d + kChunk - 1) / kChunk;
     if (atomicAdd(done + i, 1) == nchunks - 1) {
         __threadfence();
         out[r.v] = unpack_label(atomicExch(best + i, 0ull));
-        occ[i] = 0;
         done[i] = 0;
     }
 }
 
-// Pass 1 over the chunks: count the chunk's labels in shared memory, then add
-// each distinct (label, count) to the row's global table; slots claimed here
-// are appended to the row's list (one atomic per warp on occ[i]).
+// One iteration of a chunked-class row, per chunk: count the chunk's labels
+// in shared memory, then add each distinct (label, count) to the row's
+// global table, keeping the largest key the adds return (the row's answer once
+// every chunk has added, as in table_insert_merged).  Slots claimed here are
+// appended to the row's list (one atomic per warp on occ[i]) for the reset
+// pass.
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
     const int32_t* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
     const int32_t* __restrict__ lab, const int32_t* __restrict__ chunks, int32_t nch, int32_t* pool,
-    const int64_t* __restrict__ tab_off, int32_t* occ) {
+    const int64_t* __restrict__ tab_off, int32_t* occ, int32_t* done, unsigned long long* best,
+    int32_t* __restrict__ out) {
     extern __shared__ int32_t smem[];
+    __shared__ unsigned long long red[32];
     int32_t* K = smem;
     int32_t* C = smem + kBlockSlots;
     for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
@@ -391,9 +410,12 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
         }
         __syncthreads();
         // cap is a multiple of the block size: every warp runs every round.
+        unsigned long long mx = 0;
         for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
             const int32_t x = K[s];
-            const int32_t claimed = x != kEmpty ? global_add(r.T, r.cap, x, C[s]) : -1;
+            unsigned long long key = 0;
+            const int32_t claimed = x != kEmpty ? global_add(r.T, r.cap, x, C[s], key) : -1;
+            mx = key > mx ? key : mx;
             const unsigned m = __ballot_sync(0xffffffffu, claimed >= 0);
             if (m) {
                 int32_t base = 0;
@@ -402,34 +424,43 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
                 if (claimed >= 0) r.L[base + __popc(m & ((1u << lane_id()) - 1u))] = claimed;
             }
         }
-        __syncthreads();
+        // Also orders this chunk's table reads before the next chunk's clearing.
+        mx = block_max_u64(mx, red);
+        if (threadIdx.x == 0) chunk_done(r, i, mx, done, best, out);
     }
 }
 
-// Pass 2 over the same chunks: chunk k of row i takes the claimed slots
-// [j0, j0 + kChunk) of the row's list, folds their (count, label) keys into
-// best[i] and empties those slots for the next iteration.
-__global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_pick_kernel(
+// After the count pass: empties the slots the pass claimed, by writes only.
+// A sparse table (at most cap / 8 claims, the usual case once labels
+// converge) is reset through its claim list, chunk k taking list entries
+// [j0, j0 + kChunk); a dense one in slot order, chunk k taking the k-th share
+// of the slots.  The row's last chunk resets occ[i] and done[i].
+__global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_reset_kernel(
     const int32_t* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ chunks,
-    int32_t nch, int32_t* pool, const int64_t* __restrict__ tab_off, int32_t* occ, int32_t* done,
-    unsigned long long* best, int32_t* __restrict__ out) {
-    __shared__ unsigned long long red[32];
+    int32_t nch, int32_t* pool, const int64_t* __restrict__ tab_off, int32_t* occ, int32_t* done) {
     for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
         const int32_t i = chunks[2 * k];
         const LongRow r = long_row(rows, rp, pool, tab_off, i);
         const int32_t j0 = chunks[2 * k + 1];
-        const int32_t j1 = min(j0 + kChunk, __ldcg(occ + i));
-        int2* T2 = reinterpret_cast<int2*>(r.T);
-        unsigned long long b = 0;
-        for (int32_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-            const int32_t s = __ldcg(r.L + j);
-            const int2 kc = __ldcg(T2 + s);
-            const unsigned long long key = pack_best((uint32_t)kc.y, kc.x);
-            b = key > b ? key : b;
-            T2[s] = make_int2(kEmpty, 0);
+        const int32_t claims = __ldcg(occ + i);
+        const uint32_t nchunks = (uint32_t)(r.d + kChunk - 1) / kChunk;
+        if ((uint32_t)claims > r.cap / 8) {
+            const uint32_t per = (r.cap + nchunks - 1) / nchunks;
+            const uint32_t s0 = (uint32_t)(j0 / kChunk) * per;
+            const uint32_t s1 = min(s0 + per, r.cap);
+            for (uint32_t s = s0 + threadIdx.x; s < s1; s += blockDim.x) r.T[s] = kSlotEmpty;
+        } else {
+            const int32_t j1 = min(j0 + kChunk, claims);
+            for (int32_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) r.T[__ldcg(r.L + j)] = kSlotEmpty;
         }
-        b = block_max_u64(b, red);
-        if (threadIdx.x == 0) chunk_done(r, i, b, occ, done, best, out);
+        __syncthreads();  // every thread has read occ[i] before it can be reset
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(done + i, 1) == (int32_t)nchunks - 1) {
+                occ[i] = 0;
+                done[i] = 0;
+            }
+        }
     }
 }
 
@@ -438,8 +469,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_pick_kernel(
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_min_kernel(
     const int32_t* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
     const int32_t* __restrict__ lab, const int32_t* __restrict__ chunks, int32_t nch, int32_t* pool,
-    const int64_t* __restrict__ tab_off, int32_t* occ, int32_t* done, unsigned long long* best,
-    int32_t* __restrict__ out) {
+    const int64_t* __restrict__ tab_off, int32_t* done, unsigned long long* best, int32_t* __restrict__ out) {
     __shared__ unsigned long long red[32];
     for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
         const int32_t i = chunks[2 * k];
@@ -452,7 +482,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_min_kernel(
             m = key > m ? key : m;
         }
         m = block_max_u64(m, red);
-        if (threadIdx.x == 0) chunk_done(r, i, m, occ, done, best, out);
+        if (threadIdx.x == 0) chunk_done(r, i, m, done, best, out);
     }
 }
 
@@ -465,14 +495,13 @@ __global__ void cdlp_long_degrees_kernel(const int32_t* __restrict__ rows, int32
     }
 }
 
-// Block per chunked-class row: every slot (kEmpty, 0).
+// Block per chunked-class row: every slot empty.
 __global__ void cdlp_pool_clear_kernel(const int32_t* __restrict__ rows, int32_t count,
                                        const int32_t* __restrict__ rp, int32_t* pool,
                                        const int64_t* __restrict__ tab_off) {
     for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
         const LongRow r = long_row(rows, rp, pool, tab_off, (int32_t)i);
-        int2* T2 = reinterpret_cast<int2*>(r.T);
-        for (uint32_t s = threadIdx.x; s < r.cap; s += blockDim.x) T2[s] = make_int2(kEmpty, 0);
+        for (uint32_t s = threadIdx.x; s < r.cap; s += blockDim.x) r.T[s] = kSlotEmpty;
     }
 }
 
@@ -608,14 +637,14 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
         if (cls[6]) GHB_TRY(launch(ws, cdlp_warp_kernel<M>, dim3(grid_for((int64_t)cls[6] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[6], cls[6], rp, col, cur, nxt));
         if (M) {
             if (cls[7] + cls[8]) GHB_TRY(launch(ws, cdlp_block_kernel<true>, dim3(grid_for(cls[7] + cls[8], 1, g)), dim3(kCdlpThreads), 0, R + off[7], cls[7] + cls[8], rp, col, cur, nxt, 0u));
-            if (nlong) GHB_TRY(launch(ws, cdlp_chunk_min_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done, best, nxt));
+            if (nlong) GHB_TRY(launch(ws, cdlp_chunk_min_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, done, best, nxt));
             return GHB_OK;
         }
         if (cls[7]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[7], 1, g_small)), dim3(kCdlpThreads), small_smem, R + off[7], cls[7], rp, col, cur, nxt, (uint32_t)kSmallBlockSlots));
         if (cls[8]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[8], 1, g_big)), dim3(kCdlpThreads), big_smem, R + off[8], cls[8], rp, col, cur, nxt, (uint32_t)kBlockSlots));
         if (nlong) {
-            GHB_TRY(launch(ws, cdlp_chunk_count_kernel, dim3(grid_for(nch, 1, g_chunk)), dim3(kCdlpThreads), big_smem, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ));
-            GHB_TRY(launch(ws, cdlp_chunk_pick_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done, best, nxt));
+            GHB_TRY(launch(ws, cdlp_chunk_count_kernel, dim3(grid_for(nch, 1, g_chunk)), dim3(kCdlpThreads), big_smem, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done, best, nxt));
+            GHB_TRY(launch(ws, cdlp_chunk_reset_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done));
         }
         return GHB_OK;
     };
