@@ -104,6 +104,39 @@ __device__ __forceinline__ unsigned long long table_insert_merged(int32_t* K, in
     }
 }
 
+// Inserts the row entries [j0, e) taken R rounds at a time, entry
+// j0 + r * stride + t on thread t of round r: the R column loads issue
+// before the R label gathers and those before the inserts, so a thread has R
+// loads in flight instead of a chain of R round trips.  Every lane of the
+// warp must call it (rounds past e are skipped warp-uniformly).  Returns the
+// largest key the inserts returned.
+template <int R>
+__device__ __forceinline__ unsigned long long insert_rows(int32_t* K, int32_t* C, uint32_t slots,
+                                                          const int32_t* __restrict__ col,
+                                                          const int32_t* __restrict__ lab, int32_t b, int32_t e,
+                                                          int stride, int t) {
+    unsigned long long best = 0;
+    for (int64_t j0 = b; j0 < e; j0 += (int64_t)R * stride) {
+        int32_t x[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int64_t j = j0 + (int64_t)r * stride + t;
+            x[r] = j < e ? col[j] : -1;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) x[r] = x[r] >= 0 ? lab[x[r]] : 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int64_t jr = j0 + (int64_t)r * stride;
+            if (jr < e) {
+                const unsigned long long key = table_insert_merged(K, C, slots, x[r], jr + t < e);
+                best = key > best ? key : best;
+            }
+        }
+    }
+    return best;
+}
+
 __global__ void cdlp_count_classes_kernel(int32_t n, const int32_t* __restrict__ rp, int32_t* counts) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
          v += (int64_t)gridDim.x * blockDim.x) {
@@ -238,12 +271,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_warp_kernel(
             C[s] = 0;
         }
         __syncwarp();
-        unsigned long long best = 0;
-        for (int32_t j0 = b; j0 < e; j0 += 32) {
-            const int32_t j = j0 + lane;
-            const unsigned long long key = table_insert_merged(K, C, cap, j < e ? lab[col[j]] : 0, j < e);
-            best = key > best ? key : best;
-        }
+        unsigned long long best = insert_rows<8>(K, C, cap, col, lab, b, e, 32, lane);
         best = warp_max(best);
         if (lane == 0) out[v] = unpack_label(best);
         __syncwarp();
@@ -296,12 +324,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_block_kernel(
             C[s] = 0;
         }
         __syncthreads();
-        unsigned long long best = 0;
-        for (int32_t j0 = b; j0 < e; j0 += blockDim.x) {
-            const int32_t j = j0 + threadIdx.x;
-            const unsigned long long key = table_insert_merged(K, C, cap, j < e ? lab[col[j]] : 0, j < e);
-            best = key > best ? key : best;
-        }
+        unsigned long long best = insert_rows<4>(K, C, cap, col, lab, b, e, blockDim.x, threadIdx.x);
         // Also orders this row's inserts before the next row's clearing.
         best = block_max_u64(best, red);
         if (threadIdx.x == 0) out[v] = unpack_label(best);
@@ -404,10 +427,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
             C[s] = 0;
         }
         __syncthreads();
-        for (int32_t j0 = b; j0 < e; j0 += blockDim.x) {
-            const int32_t j = j0 + threadIdx.x;
-            table_insert_merged(K, C, cap, j < e ? lab[col[j]] : 0, j < e);
-        }
+        insert_rows<4>(K, C, cap, col, lab, b, e, blockDim.x, threadIdx.x);
         __syncthreads();
         // cap is a multiple of the block size: every warp runs every round.
         unsigned long long mx = 0;
