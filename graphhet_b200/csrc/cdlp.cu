@@ -149,18 +149,21 @@ __global__ void cdlp_count_classes_kernel(int32_t n, const int32_t* __restrict__
     }
 }
 
+// Class lists hold each row as {v, begin, end, 0}: a row kernel reads its
+// row's bounds with the row itself, one load instead of two dependent ones.
 __global__ void cdlp_fill_classes_kernel(int32_t n, const int32_t* __restrict__ rp, int32_t* cursor,
-                                         int32_t* rows) {
+                                         int4* rows) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
          v += (int64_t)gridDim.x * blockDim.x) {
-        const int c = cdlp_class(rp[v + 1] - rp[v]);
+        const int32_t b = rp[v], e = rp[v + 1];
+        const int c = cdlp_class(e - b);
         const unsigned active = __activemask();
         const unsigned same = __match_any_sync(active, c);
         const int leader = __ffs(same) - 1;
         int32_t base = 0;
         if (lane_id() == leader) base = atomicAdd(&cursor[c], __popc(same));
         base = __shfl_sync(same, base, leader);
-        rows[base + __popc(same & ((1u << lane_id()) - 1u))] = (int32_t)v;
+        rows[base + __popc(same & ((1u << lane_id()) - 1u))] = make_int4((int32_t)v, b, e, 0);
     }
 }
 
@@ -170,11 +173,11 @@ __global__ void cdlp_iota_kernel(int32_t* p, int32_t n) {
         p[i] = (int32_t)i;
 }
 
-__global__ void cdlp_copy_kernel(const int32_t* __restrict__ rows, int32_t count,
+__global__ void cdlp_copy_kernel(const int4* __restrict__ rows, int32_t count,
                                  const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t v = rows[i];
+        const int32_t v = rows[i].x;
         out[v] = lab[v];
     }
 }
@@ -183,7 +186,7 @@ __global__ void cdlp_copy_kernel(const int32_t* __restrict__ rows, int32_t count
 // distinct (first iteration), so the row's smallest label is taken directly.
 template <int W, bool kMin>
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_small_kernel(
-    const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
+    const int4* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
     const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
     const int lane = lane_id();
     const int li = lane & (W - 1);
@@ -195,46 +198,47 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_small_kernel(
         const int64_t i = group + r * ngroups;
         int32_t v = -1, b = 0, d = 0;
         if (i < count) {
-            v = rows[i];
-            b = rp[v];
-            d = rp[v + 1] - b;
+            const int4 ri = rows[i];
+            v = ri.x;
+            b = ri.y;
+            d = ri.z - ri.y;
         }
         int32_t x = 0x7FFFFFFF;
         if (li < d) x = lab[col[b + li]];
-        if (kMin) {
+        if constexpr (kMin) {
 #pragma unroll
             for (int o = W / 2; o > 0; o >>= 1) x = min(x, __shfl_xor_sync(0xffffffffu, x, o));
             if (li == 0 && i < count) out[v] = x;
-            continue;
-        }
-        // Bitonic sort, ascending, within each W-lane group.
+        } else {
+            // Bitonic sort, ascending, within each W-lane group.
 #pragma unroll
-        for (int k = 2; k <= W; k <<= 1) {
+            for (int k = 2; k <= W; k <<= 1) {
 #pragma unroll
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                const int32_t y = __shfl_xor_sync(0xffffffffu, x, j);
-                const bool up = (li & k) == 0;
-                const bool lower = (li & j) == 0;
-                x = (lower == up) ? min(x, y) : max(x, y);
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const int32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+                    const bool up = (li & k) == 0;
+                    const bool lower = (li & j) == 0;
+                    x = (lower == up) ? min(x, y) : max(x, y);
+                }
             }
-        }
-        // Run starts inside the group, then run length = next start - start.
-        const int32_t prev = __shfl_up_sync(0xffffffffu, x, 1);
-        const bool valid = li < d;
-        const bool start = valid && (li == 0 || prev != x);
-        const unsigned starts = __ballot_sync(0xffffffffu, start) & gmask;
-        unsigned long long best = 0;
-        if (start) {
-            const unsigned above = starts & ~((2u << lane) - 1u);
-            const int next_li = above ? ((__ffs(above) - 1) & (W - 1)) : d;
-            best = pack_best((uint32_t)(next_li - li), x);
-        }
+            // Run starts inside the group, then run length = next start - start.
+            const int32_t prev = __shfl_up_sync(0xffffffffu, x, 1);
+            const bool valid = li < d;
+            const bool start = valid && (li == 0 || prev != x);
+            const unsigned starts = __ballot_sync(0xffffffffu, start) & gmask;
+            unsigned long long best = 0;
+            if (start) {
+                const unsigned above = starts & ~((2u << lane) - 1u);
+                const int next_li = above ? ((__ffs(above) - 1) & (W - 1)) : d;
+                best = pack_best((uint32_t)(next_li - li), x);
+            }
 #pragma unroll
-        for (int o = W / 2; o > 0; o >>= 1) {
-            const unsigned long long y = __shfl_xor_sync(0xffffffffu, best, o);
-            best = y > best ? y : best;
+            for (int o = W / 2; o > 0; o >>= 1) {
+                const unsigned long long y = __shfl_xor_sync(0xffffffffu, best, o);
+                best = y > best ? y : best;
+            }
+            if (li == 0 && i < count) out[v] = unpack_label(best);
         }
-        if (li == 0 && i < count) out[v] = unpack_label(best);
     }
 }
 
@@ -242,7 +246,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_small_kernel(
 // memory (kMin: the row's smallest label, no table).
 template <bool kMin>
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_warp_kernel(
-    const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
+    const int4* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
     const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
     __shared__ int32_t keys[kCdlpThreads / 32][kWarpSlots];
     __shared__ int32_t cnts[kCdlpThreads / 32][kWarpSlots];
@@ -253,8 +257,8 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_warp_kernel(
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t i = warp; i < count; i += nwarps) {
-        const int32_t v = rows[i];
-        const int32_t b = rp[v], e = rp[v + 1];
+        const int4 ri = rows[i];
+        const int32_t v = ri.x, b = ri.y, e = ri.z;
         if (kMin) {
             int32_t m = 0x7FFFFFFF;
             for (int32_t j = b + lane; j < e; j += 32) m = min(m, lab[col[j]]);
@@ -298,15 +302,15 @@ __device__ __forceinline__ unsigned long long block_max_u64(unsigned long long x
 // ints of dynamic shared memory.  kMin: the row's smallest label, no table.
 template <bool kMin>
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_block_kernel(
-    const int32_t* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
+    const int4* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
     const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out, uint32_t slots) {
     extern __shared__ int32_t smem[];
     __shared__ unsigned long long red[32];
     int32_t* K = smem;
     int32_t* C = smem + slots;
     for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
-        const int32_t v = rows[i];
-        const int32_t b = rp[v], e = rp[v + 1];
+        const int4 ri = rows[i];
+        const int32_t v = ri.x, b = ri.y, e = ri.z;
         if (kMin) {
             unsigned long long m = 0;
             for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
@@ -338,22 +342,17 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_block_kernel(
 constexpr unsigned long long kSlotEmpty = 0xFFFFFFFF00000000ull;
 
 // Adds cnt to label x in a table of cap slots (cap > 2 x the labels it can
-// hold, so a free slot is always reached).  The slot is read first, so a
-// label already present costs one atomic add and a new one one CAS.  Sets key
-// to (count after this add, label), as table_insert_merged returns it, and
+// hold, so a free slot is always reached), probing from slot h.  Sets key to
+// (count after this add, label), as table_insert_merged returns it, and
 // returns the slot when this call claimed it for x, else -1.
-__device__ __forceinline__ int32_t global_add(unsigned long long* T, uint32_t cap, int32_t x, int32_t cnt,
-                                              unsigned long long& key) {
-    const unsigned long long mine = (unsigned long long)(uint32_t)x << 32;
-    uint32_t h = hash_label(x) & (cap - 1);
+__device__ __forceinline__ int32_t global_add_from(unsigned long long* T, uint32_t cap, uint32_t h, int32_t x,
+                                                   int32_t cnt, unsigned long long& key) {
+    const unsigned long long mine = ((unsigned long long)(uint32_t)x << 32) | (uint32_t)cnt;
     while (true) {
-        unsigned long long cur = __ldcg(T + h);
+        const unsigned long long cur = atomicCAS(T + h, kSlotEmpty, mine);
         if (cur == kSlotEmpty) {
-            cur = atomicCAS(T + h, kSlotEmpty, mine | (uint32_t)cnt);
-            if (cur == kSlotEmpty) {
-                key = pack_best((uint32_t)cnt, x);
-                return (int32_t)h;
-            }
+            key = pack_best((uint32_t)cnt, x);
+            return (int32_t)h;
         }
         if ((uint32_t)(cur >> 32) == (uint32_t)x) {
             const unsigned long long old = atomicAdd(T + h, (unsigned long long)cnt);
@@ -369,16 +368,18 @@ __device__ __forceinline__ int32_t global_add(unsigned long long* T, uint32_t ca
 // = row index i and the chunk's first entry within the row (a multiple of
 // kChunk).
 struct LongRow {
-    int32_t v, d;
+    int32_t v, b, d;
     uint32_t cap;
     unsigned long long* T;
     int32_t* L;
 };
-__device__ __forceinline__ LongRow long_row(const int32_t* rows, const int32_t* rp, int32_t* pool,
+__device__ __forceinline__ LongRow long_row(const int4* rows, const int32_t* rp, int32_t* pool,
                                             const int64_t* tab_off, int32_t i) {
     LongRow r;
-    r.v = rows[i];
-    r.d = rp[r.v + 1] - rp[r.v];
+    const int4 ri = rows[i];
+    r.v = ri.x;
+    r.b = ri.y;
+    r.d = ri.z - ri.y;
     r.cap = global_cap(r.d);
     r.T = reinterpret_cast<unsigned long long*>(pool + tab_off[i]);
     r.L = reinterpret_cast<int32_t*>(r.T + r.cap);
@@ -407,7 +408,7 @@ __device__ __forceinline__ void chunk_done(const LongRow& r, int32_t i, unsigned
 // appended to the row's list (one atomic per warp on occ[i]) for the reset
 // pass.
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
-    const int32_t* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+    const int4* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
     const int32_t* __restrict__ lab, const int32_t* __restrict__ chunks, int32_t nch, int32_t* pool,
     const int64_t* __restrict__ tab_off, int32_t* occ, int32_t* done, unsigned long long* best,
     int32_t* __restrict__ out) {
@@ -418,8 +419,8 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
     for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
         const int32_t i = chunks[2 * k];
         const LongRow r = long_row(rows, rp, pool, tab_off, i);
-        const int32_t b = rp[r.v] + chunks[2 * k + 1];
-        const int32_t e = min(b + kChunk, rp[r.v + 1]);
+        const int32_t b = r.b + chunks[2 * k + 1];
+        const int32_t e = min(b + kChunk, r.b + r.d);
         uint32_t cap = 512;
         while (cap < 2u * (uint32_t)(e - b) && cap < (uint32_t)kBlockSlots) cap <<= 1;
         for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
@@ -429,19 +430,56 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
         __syncthreads();
         insert_rows<4>(K, C, cap, col, lab, b, e, blockDim.x, threadIdx.x);
         __syncthreads();
-        // cap is a multiple of the block size: every warp runs every round.
+        // The chunk's distinct labels go to the global table kF per thread at
+        // a time: the kF home-slot CASes issue together, then the adds for
+        // labels found there, and only a slot held by another label is probed
+        // one step at a time.  cap is a multiple of the block size: every
+        // warp runs every round.
+        constexpr int kF = 4;
         unsigned long long mx = 0;
-        for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
-            const int32_t x = K[s];
-            unsigned long long key = 0;
-            const int32_t claimed = x != kEmpty ? global_add(r.T, r.cap, x, C[s], key) : -1;
-            mx = key > mx ? key : mx;
-            const unsigned m = __ballot_sync(0xffffffffu, claimed >= 0);
-            if (m) {
-                int32_t base = 0;
-                if (lane_id() == 0) base = atomicAdd(occ + i, __popc(m));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (claimed >= 0) r.L[base + __popc(m & ((1u << lane_id()) - 1u))] = claimed;
+        for (uint32_t s0 = 0; s0 < cap; s0 += kF * blockDim.x) {
+            int32_t x[kF], c[kF];
+            uint32_t h[kF];
+            unsigned long long cur[kF], old[kF];
+#pragma unroll
+            for (int q = 0; q < kF; ++q) {
+                const uint32_t s = s0 + q * blockDim.x + threadIdx.x;
+                x[q] = s < cap ? K[s] : kEmpty;
+                c[q] = s < cap ? C[s] : 0;
+                h[q] = hash_label(x[q]) & (r.cap - 1);
+                cur[q] = x[q] != kEmpty ? atomicCAS(r.T + h[q], kSlotEmpty,
+                                                    ((unsigned long long)(uint32_t)x[q] << 32) | (uint32_t)c[q])
+                                        : kSlotEmpty;
+            }
+#pragma unroll
+            for (int q = 0; q < kF; ++q) {
+                old[q] = 0;
+                if (x[q] != kEmpty && cur[q] != kSlotEmpty && (uint32_t)(cur[q] >> 32) == (uint32_t)x[q])
+                    old[q] = atomicAdd(r.T + h[q], (unsigned long long)c[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < kF; ++q) {
+                if (s0 + q * blockDim.x >= cap) break;
+                int32_t claimed = -1;
+                unsigned long long key = 0;
+                if (x[q] != kEmpty) {
+                    if (cur[q] == kSlotEmpty) {
+                        claimed = (int32_t)h[q];
+                        key = pack_best((uint32_t)c[q], x[q]);
+                    } else if ((uint32_t)(cur[q] >> 32) == (uint32_t)x[q]) {
+                        key = pack_best((uint32_t)old[q] + (uint32_t)c[q], x[q]);
+                    } else {
+                        claimed = global_add_from(r.T, r.cap, (h[q] + 1) & (r.cap - 1), x[q], c[q], key);
+                    }
+                }
+                mx = key > mx ? key : mx;
+                const unsigned m = __ballot_sync(0xffffffffu, claimed >= 0);
+                if (m) {
+                    int32_t base = 0;
+                    if (lane_id() == 0) base = atomicAdd(occ + i, __popc(m));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (claimed >= 0) r.L[base + __popc(m & ((1u << lane_id()) - 1u))] = claimed;
+                }
             }
         }
         // Also orders this chunk's table reads before the next chunk's clearing.
@@ -456,7 +494,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
 // [j0, j0 + kChunk); a dense one in slot order, chunk k taking the k-th share
 // of the slots.  The row's last chunk resets occ[i] and done[i].
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_reset_kernel(
-    const int32_t* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ chunks,
+    const int4* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ chunks,
     int32_t nch, int32_t* pool, const int64_t* __restrict__ tab_off, int32_t* occ, int32_t* done) {
     for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
         const int32_t i = chunks[2 * k];
@@ -487,15 +525,15 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_reset_kernel(
 // First iteration (labels distinct, no repeated entries): each chunk's
 // smallest label, folded over the row's chunks as in the pick pass.
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_min_kernel(
-    const int32_t* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+    const int4* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
     const int32_t* __restrict__ lab, const int32_t* __restrict__ chunks, int32_t nch, int32_t* pool,
     const int64_t* __restrict__ tab_off, int32_t* done, unsigned long long* best, int32_t* __restrict__ out) {
     __shared__ unsigned long long red[32];
     for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
         const int32_t i = chunks[2 * k];
         const LongRow r = long_row(rows, rp, pool, tab_off, i);
-        const int32_t b = rp[r.v] + chunks[2 * k + 1];
-        const int32_t e = min(b + kChunk, rp[r.v + 1]);
+        const int32_t b = r.b + chunks[2 * k + 1];
+        const int32_t e = min(b + kChunk, r.b + r.d);
         unsigned long long m = 0;
         for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
             const unsigned long long key = pack_best(1, lab[col[j]]);
@@ -507,16 +545,15 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_min_kernel(
 }
 
 // Chunked-class rows: degrees for the host's table layout.
-__global__ void cdlp_long_degrees_kernel(const int32_t* __restrict__ rows, int32_t count,
+__global__ void cdlp_long_degrees_kernel(const int4* __restrict__ rows, int32_t count,
                                          const int32_t* __restrict__ rp, int32_t* deg) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t v = rows[i];
-        deg[i] = rp[v + 1] - rp[v];
+        deg[i] = rows[i].z - rows[i].y;
     }
 }
 
 // Block per chunked-class row: every slot empty.
-__global__ void cdlp_pool_clear_kernel(const int32_t* __restrict__ rows, int32_t count,
+__global__ void cdlp_pool_clear_kernel(const int4* __restrict__ rows, int32_t count,
                                        const int32_t* __restrict__ rp, int32_t* pool,
                                        const int64_t* __restrict__ tab_off) {
     for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
@@ -561,7 +598,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
     Carver sizing(nullptr);
     sizing.take<int32_t>(16);
     sizing.take<int32_t>(16);
-    sizing.take<int32_t>(n);
+    sizing.take<int4>(n);
     sizing.take<int32_t>(n);
     sizing.take<int32_t>(pool_bound);
     sizing.take<int64_t>((size_t)nlong + 1);
@@ -573,7 +610,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
     Carver c(ws->scratch);
     counts = c.take<int32_t>(16);
     int32_t* cursor = c.take<int32_t>(16);
-    int32_t* rows = c.take<int32_t>(n);
+    int4* rows = c.take<int4>(n);
     int32_t* other = c.take<int32_t>(n);
     int32_t* pool = c.take<int32_t>(pool_bound);
     int64_t* tab_off = c.take<int64_t>((size_t)nlong + 1);
@@ -586,7 +623,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
     GHB_CUDA_TRY(cudaMemcpyAsync(cursor, hp, kCdlpClasses * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     GHB_TRY(launch(ws, cdlp_fill_classes_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n, rp,
                    cursor, rows));
-    const int32_t* long_rows = rows + off[9];
+    const int4* long_rows = rows + off[9];
     int32_t nch = 0;
     if (nlong > 0) {
         // Table offsets and the chunk list on the host (a few thousand rows),
@@ -647,7 +684,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
     // iteration over distinct labels): each row's smallest label.
     auto iteration = [&](auto min_tag, const int32_t* cur, int32_t* nxt) -> int {
         constexpr bool M = decltype(min_tag)::value;
-        const int32_t* R = rows;
+        const int4* R = rows;
         if (cls[0]) GHB_TRY(launch(ws, cdlp_copy_kernel, dim3(grid_for(cls[0], 256, g)), dim3(256), 0, R + off[0], cls[0], cur, nxt));
         if (cls[1]) GHB_TRY(launch(ws, cdlp_small_kernel<2, M>, dim3(grid_for((int64_t)cls[1] * 2, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[1], cls[1], rp, col, cur, nxt));
         if (cls[2]) GHB_TRY(launch(ws, cdlp_small_kernel<4, M>, dim3(grid_for((int64_t)cls[2] * 4, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[2], cls[2], rp, col, cur, nxt));
