@@ -109,7 +109,7 @@ __device__ __forceinline__ void mssp_relax_range(int32_t v, int32_t eb, int32_t 
             const unsigned long long old = atomicMin(p, nb);
             if (nb < old && nd < hi) {
                 atomicOr(act_next + (int64_t)u * words + (s >> 6), 1ull << (s & 63));
-                if (atomicExch(inq_next + u, 1) == 0) queue_next[atomicAdd(&cnt->queued, 1)] = u;
+                if (atomicExch(inq_next + u, 1) == 0) queue_next[warp_append_active(&cnt->queued)] = u;
             }
         }
     };
