@@ -15,13 +15,13 @@
 //   257..1024 one block per row, 2048-slot shared-memory table (16 KB, so
 //            eight blocks fit an SM)
 //   1025..4096 one block per row, 8192-slot shared-memory table
-//   > 4096   the row is cut into chunks of 4096 entries, each a block: the
+//   > 4096   the row is cut into chunks of 2048 entries, each a block: the
 //            chunk counts its labels in a shared-memory table, then adds each
 //            distinct (label, count) to the row's table in global scratch and
 //            lists the slots it claimed; the last chunk of a row to finish
 //            writes its label, and a write-only pass empties the claimed
 //            slots.  No row waits on one block, and once labels converge a
-//            chunk sends a few global atomics, not 4096.
+//            chunk sends a few global atomics, not 2048.
 // Every insert returns the key (count after it, -label); a label's last insert
 // sees its final count, so the max-reduction of those keys yields the most
 // frequent label with the smallest-label tie-break, and no table is scanned
@@ -42,7 +42,9 @@ constexpr int32_t kEmpty = -1;
 constexpr int32_t kWarpSlots = 512;
 constexpr int32_t kSmallBlockSlots = 2048;
 constexpr int32_t kBlockSlots = 8192;
-constexpr int32_t kChunk = 4096;  // entries per chunk of a chunked-class row
+constexpr int32_t kLongRow = kBlockSlots / 2;  // longer rows are chunked
+constexpr int32_t kChunk = 2048;               // entries per chunk of a chunked-class row
+constexpr int32_t kChunkSlots = 2 * kChunk;    // its shared-memory table (32 KB)
 constexpr int kCdlpThreads = 256;
 
 __device__ __forceinline__ int cdlp_class(int32_t d) {
@@ -54,7 +56,7 @@ __device__ __forceinline__ int cdlp_class(int32_t d) {
     if (d <= 32) return 5;
     if (d <= 256) return 6;
     if (d <= 1024) return 7;
-    if (d <= kChunk) return 8;
+    if (d <= kLongRow) return 8;
     return 9;
 }
 
@@ -415,14 +417,14 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
     extern __shared__ int32_t smem[];
     __shared__ unsigned long long red[32];
     int32_t* K = smem;
-    int32_t* C = smem + kBlockSlots;
+    int32_t* C = smem + kChunkSlots;
     for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
         const int32_t i = chunks[2 * k];
         const LongRow r = long_row(rows, rp, pool, tab_off, i);
         const int32_t b = r.b + chunks[2 * k + 1];
         const int32_t e = min(b + kChunk, r.b + r.d);
         uint32_t cap = 512;
-        while (cap < 2u * (uint32_t)(e - b) && cap < (uint32_t)kBlockSlots) cap <<= 1;
+        while (cap < 2u * (uint32_t)(e - b) && cap < (uint32_t)kChunkSlots) cap <<= 1;
         for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
             K[s] = kEmpty;
             C[s] = 0;
@@ -664,17 +666,18 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
 
     // Shared-memory classes: as many blocks as fit each SM.
     const size_t small_smem = 2 * kSmallBlockSlots * sizeof(int32_t), big_smem = 2 * kBlockSlots * sizeof(int32_t);
+    const size_t chunk_smem = 2 * kChunkSlots * sizeof(int32_t);
     GHB_CUDA_TRY(cudaFuncSetAttribute(cdlp_block_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)big_smem));
     GHB_CUDA_TRY(cudaFuncSetAttribute(cdlp_chunk_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)big_smem));
+                                      (int)chunk_smem));
     int per_sm_small = 0, per_sm_big = 0, per_sm_chunk = 0;
     GHB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_small, cdlp_block_kernel<false>, kCdlpThreads,
                                                                small_smem));
     GHB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_big, cdlp_block_kernel<false>, kCdlpThreads,
                                                                big_smem));
     GHB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_chunk, cdlp_chunk_count_kernel, kCdlpThreads,
-                                                               big_smem));
+                                                               chunk_smem));
     const unsigned g_small = ws->num_sms * std::max(1, per_sm_small);
     const unsigned g_big = ws->num_sms * std::max(1, per_sm_big);
     const unsigned g_chunk = ws->num_sms * std::max(1, per_sm_chunk);
@@ -700,7 +703,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
         if (cls[7]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[7], 1, g_small)), dim3(kCdlpThreads), small_smem, R + off[7], cls[7], rp, col, cur, nxt, (uint32_t)kSmallBlockSlots));
         if (cls[8]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[8], 1, g_big)), dim3(kCdlpThreads), big_smem, R + off[8], cls[8], rp, col, cur, nxt, (uint32_t)kBlockSlots));
         if (nlong) {
-            GHB_TRY(launch(ws, cdlp_chunk_count_kernel, dim3(grid_for(nch, 1, g_chunk)), dim3(kCdlpThreads), big_smem, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done, best, nxt));
+            GHB_TRY(launch(ws, cdlp_chunk_count_kernel, dim3(grid_for(nch, 1, g_chunk)), dim3(kCdlpThreads), chunk_smem, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done, best, nxt));
             GHB_TRY(launch(ws, cdlp_chunk_reset_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done));
         }
         return GHB_OK;
