@@ -14,7 +14,8 @@
 //            slots in shared memory
 //   257..1024 one block per row, 2048-slot shared-memory table (16 KB, so
 //            eight blocks fit an SM)
-//   1025..4096 one block per row, 8192-slot shared-memory table
+//   1025..2048 one block per row, 4096-slot shared-memory table (32 KB)
+//   2049..4096 one block per row, 8192-slot shared-memory table
 //   > 4096   the row is cut into chunks of 2048 entries, each a block: the
 //            chunk counts its labels in a shared-memory table, then adds each
 //            distinct (label, count) to the row's table in global scratch and
@@ -35,12 +36,14 @@
 namespace ghb {
 namespace {
 
-// 0:empty 1..5: W=2,4,8,16,32  6:warp 7:block (2048 slots) 8:block (8192 slots) 9:chunked
-constexpr int kCdlpClasses = 10;
+// 0:empty 1..5: W=2,4,8,16,32  6:warp 7:block (2048 slots) 8:block (4096 slots)
+// 9:block (8192 slots) 10:chunked
+constexpr int kCdlpClasses = 11;
 constexpr int kSumLongSlot = 15;  // counts[15]: entries of the chunked-class rows
 constexpr int32_t kEmpty = -1;
 constexpr int32_t kWarpSlots = 512;
 constexpr int32_t kSmallBlockSlots = 2048;
+constexpr int32_t kMidBlockSlots = 4096;
 constexpr int32_t kBlockSlots = 8192;
 constexpr int32_t kLongRow = kBlockSlots / 2;  // longer rows are chunked
 constexpr int32_t kChunk = 2048;               // entries per chunk of a chunked-class row
@@ -56,8 +59,9 @@ __device__ __forceinline__ int cdlp_class(int32_t d) {
     if (d <= 32) return 5;
     if (d <= 256) return 6;
     if (d <= 1024) return 7;
-    if (d <= kLongRow) return 8;
-    return 9;
+    if (d <= 2048) return 8;
+    if (d <= kLongRow) return 9;
+    return 10;
 }
 
 // Slots of a chunked-class row's global table: the power of two >= 2 d.
@@ -147,7 +151,7 @@ __global__ void cdlp_count_classes_kernel(int32_t n, const int32_t* __restrict__
         const unsigned same = __match_any_sync(__activemask(), c);
         const int leader = __ffs(same) - 1;
         if (lane_id() == leader) atomicAdd(&counts[c], __popc(same));
-        if (c == 9) atomicAdd(&counts[kSumLongSlot], d);
+        if (c == 10) atomicAdd(&counts[kSumLongSlot], d);
     }
 }
 
@@ -593,7 +597,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
     // Chunked-class tables: (label, count) pairs for the power of two >= 2 d
     // slots, then the claimed-slot list of d ints (rounded up to even), so
     // fewer than 9 ints per entry plus one per row.
-    const int32_t nlong = cls[9];
+    const int32_t nlong = cls[10];
     const int64_t long_entries = hp[kSumLongSlot];
     const int64_t pool_bound = nlong > 0 ? 9 * long_entries + nlong + 16 : 1;
     const int64_t chunk_bound = long_entries / kChunk + nlong + 1;
@@ -625,7 +629,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
     GHB_CUDA_TRY(cudaMemcpyAsync(cursor, hp, kCdlpClasses * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     GHB_TRY(launch(ws, cdlp_fill_classes_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n, rp,
                    cursor, rows));
-    const int4* long_rows = rows + off[9];
+    const int4* long_rows = rows + off[10];
     int32_t nch = 0;
     if (nlong > 0) {
         // Table offsets and the chunk list on the host (a few thousand rows),
@@ -666,19 +670,22 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
 
     // Shared-memory classes: as many blocks as fit each SM.
     const size_t small_smem = 2 * kSmallBlockSlots * sizeof(int32_t), big_smem = 2 * kBlockSlots * sizeof(int32_t);
-    const size_t chunk_smem = 2 * kChunkSlots * sizeof(int32_t);
+    const size_t chunk_smem = 2 * kChunkSlots * sizeof(int32_t), mid_smem = 2 * kMidBlockSlots * sizeof(int32_t);
     GHB_CUDA_TRY(cudaFuncSetAttribute(cdlp_block_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)big_smem));
     GHB_CUDA_TRY(cudaFuncSetAttribute(cdlp_chunk_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)chunk_smem));
-    int per_sm_small = 0, per_sm_big = 0, per_sm_chunk = 0;
+    int per_sm_small = 0, per_sm_mid = 0, per_sm_big = 0, per_sm_chunk = 0;
     GHB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_small, cdlp_block_kernel<false>, kCdlpThreads,
                                                                small_smem));
+    GHB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_mid, cdlp_block_kernel<false>, kCdlpThreads,
+                                                               mid_smem));
     GHB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_big, cdlp_block_kernel<false>, kCdlpThreads,
                                                                big_smem));
     GHB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_chunk, cdlp_chunk_count_kernel, kCdlpThreads,
                                                                chunk_smem));
     const unsigned g_small = ws->num_sms * std::max(1, per_sm_small);
+    const unsigned g_mid = ws->num_sms * std::max(1, per_sm_mid);
     const unsigned g_big = ws->num_sms * std::max(1, per_sm_big);
     const unsigned g_chunk = ws->num_sms * std::max(1, per_sm_chunk);
     const unsigned g = ws->num_sms * 8;
@@ -696,12 +703,14 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
         if (cls[5]) GHB_TRY(launch(ws, cdlp_small_kernel<32, M>, dim3(grid_for((int64_t)cls[5] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[5], cls[5], rp, col, cur, nxt));
         if (cls[6]) GHB_TRY(launch(ws, cdlp_warp_kernel<M>, dim3(grid_for((int64_t)cls[6] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[6], cls[6], rp, col, cur, nxt));
         if (M) {
-            if (cls[7] + cls[8]) GHB_TRY(launch(ws, cdlp_block_kernel<true>, dim3(grid_for(cls[7] + cls[8], 1, g)), dim3(kCdlpThreads), 0, R + off[7], cls[7] + cls[8], rp, col, cur, nxt, 0u));
+            const int32_t nblock = cls[7] + cls[8] + cls[9];
+            if (nblock) GHB_TRY(launch(ws, cdlp_block_kernel<true>, dim3(grid_for(nblock, 1, g)), dim3(kCdlpThreads), 0, R + off[7], nblock, rp, col, cur, nxt, 0u));
             if (nlong) GHB_TRY(launch(ws, cdlp_chunk_min_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, done, best, nxt));
             return GHB_OK;
         }
         if (cls[7]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[7], 1, g_small)), dim3(kCdlpThreads), small_smem, R + off[7], cls[7], rp, col, cur, nxt, (uint32_t)kSmallBlockSlots));
-        if (cls[8]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[8], 1, g_big)), dim3(kCdlpThreads), big_smem, R + off[8], cls[8], rp, col, cur, nxt, (uint32_t)kBlockSlots));
+        if (cls[8]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[8], 1, g_mid)), dim3(kCdlpThreads), mid_smem, R + off[8], cls[8], rp, col, cur, nxt, (uint32_t)kMidBlockSlots));
+        if (cls[9]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[9], 1, g_big)), dim3(kCdlpThreads), big_smem, R + off[9], cls[9], rp, col, cur, nxt, (uint32_t)kBlockSlots));
         if (nlong) {
             GHB_TRY(launch(ws, cdlp_chunk_count_kernel, dim3(grid_for(nch, 1, g_chunk)), dim3(kCdlpThreads), chunk_smem, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done, best, nxt));
             GHB_TRY(launch(ws, cdlp_chunk_reset_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done));

@@ -160,16 +160,16 @@ def test_cdlp_rows_beyond_4096_entries(G):
 
 
 def test_cdlp_class_edges_and_many_chunks(G):
-    """Rows at each class edge (1024 | 1025 and 4096 | 4097 entries, the
-    last the first chunked row), rows of four and five chunks of 2048
-    (8192 | 8193) and hubs of 20,000 and 45,000 entries (10 and 22 chunks),
-    each hub a vertex of its own joined to distinct RMAT vertices; raw CSR
-    and handle, 1, 2 and 10 iterations."""
+    """Rows at each class edge (1024 | 1025, 2048 | 2049 and 4096 | 4097
+    entries, the last the first chunked row), rows of four and five chunks
+    of 2048 (8192 | 8193) and hubs of 20,000 and 45,000 entries (10 and 22
+    chunks), each hub a vertex of its own joined to distinct RMAT vertices;
+    raw CSR and handle, 1, 2 and 10 iterations."""
     scale = 16
     base = 1 << scale
     s, d = O.rmat_edges(scale, 8 << scale, 11)
     rng = np.random.default_rng(5)
-    degs = (1024, 1025, 4096, 4097, 8192, 8193, 20000, 45000)
+    degs = (1024, 1025, 2048, 2049, 4096, 4097, 8192, 8193, 20000, 45000)
     hs, hd = [s], [d]
     for k, deg in enumerate(degs):
         hs.append(np.full(deg, base + k, np.int32))
