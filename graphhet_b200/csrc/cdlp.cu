@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
         const int32_t i = chunks[2 * k];
         const LongRow r = long_row(rows, rp, pool, tab_off, i);
         const int32_t b = r.b + chunks[2 * k + 1];
-        const int32_t e = min(b + kChunk, r.b + r.d);
+        const int32_t e = (int32_t)min((int64_t)b + kChunk, (int64_t)r.b + r.d);
         uint32_t cap = 512;
         while (cap < 2u * (uint32_t)(e - b) && cap < (uint32_t)kChunkSlots) cap <<= 1;
         for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_reset_kernel(
             const uint32_t s1 = min(s0 + per, r.cap);
             for (uint32_t s = s0 + threadIdx.x; s < s1; s += blockDim.x) r.T[s] = kSlotEmpty;
         } else {
-            const int32_t j1 = min(j0 + kChunk, claims);
+            const int32_t j1 = (int32_t)min((int64_t)j0 + kChunk, (int64_t)claims);
             for (int32_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) r.T[__ldcg(r.L + j)] = kSlotEmpty;
         }
         __syncthreads();  // every thread has read occ[i] before it can be reset
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_min_kernel(
         const int32_t i = chunks[2 * k];
         const LongRow r = long_row(rows, rp, pool, tab_off, i);
         const int32_t b = r.b + chunks[2 * k + 1];
-        const int32_t e = min(b + kChunk, r.b + r.d);
+        const int32_t e = (int32_t)min((int64_t)b + kChunk, (int64_t)r.b + r.d);
         unsigned long long m = 0;
         for (int32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
             const unsigned long long key = pack_best(1, lab[col[j]]);
@@ -644,11 +644,13 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
         ch.reserve(2 * (size_t)chunk_bound);
         int64_t acc = 0;
         for (int32_t i = 0; i < nlong; ++i) {
+            // global_cap needs 2 d <= 2^31.
+            GHB_REQUIRE(deg[i] <= (1 << 30), "CDLP: a row holds more than 2^30 entries");
             toff[i] = acc;
             acc += 2 * (int64_t)global_cap(deg[i]) + ((deg[i] + 1) & ~1);  // keeps every tab_off even
-            for (int32_t j = 0; j < deg[i]; j += kChunk) {
+            for (int64_t j = 0; j < deg[i]; j += kChunk) {
                 ch.push_back(i);
-                ch.push_back(j);
+                ch.push_back((int32_t)j);
             }
         }
         toff[nlong] = acc;
