@@ -6,8 +6,9 @@
 // device first) take the oriented path: keep u->v only when
 // (deg v, v) > (deg u, u), so every triangle is found once, at its
 // lowest-ranked vertex, and oriented rows hold at most O(sqrt m) entries.
-// Each oriented entry (u, v) intersects N+(v) with N+(u) by binary search
-// (N+(u) is reused by all of u's entries and stays in L1).  A triangle adds 1
+// Each oriented entry (u, v) intersects N+(u) and N+(v): it walks the shorter
+// list and binary-searches the longer, each search starting where the last
+// ended (N+(u) is reused by all of u's entries and stays in L1).  A triangle adds 1
 // to each of its three vertices; the reference's count is 6x that (each
 // triangle is met from its 6 ordered edges), and its int32 wraps.
 //
@@ -21,6 +22,16 @@ namespace ghb {
 namespace {
 
 constexpr int32_t kTcFlagLoop = 1, kTcFlagUnsorted = 2, kTcFlagAsym = 4;
+
+// First position in [b, e) of a sorted row whose entry is >= x (e if none).
+__device__ __forceinline__ int32_t lower_bound_from(const int32_t* __restrict__ col, int32_t b, int32_t e, int32_t x) {
+    while (b < e) {
+        const int32_t mid = b + ((e - b) >> 1);
+        if (col[mid] < x) b = mid + 1;
+        else e = mid;
+    }
+    return b;
+}
 
 __device__ __forceinline__ bool row_contains(const int32_t* __restrict__ col, int32_t b, int32_t e, int32_t x) {
     while (b < e) {
@@ -139,14 +150,25 @@ struct OrientedVisitor {
     unsigned long long* cnt;
     __device__ bool want_row(int32_t) const { return true; }
     __device__ void operator()(int32_t u, int32_t v, int32_t) const {
-        const int32_t ub = orp[u], ue = orp[u + 1];
-        const int32_t vb = orp[v], ve = orp[v + 1];
+        // Walk the shorter of N+(u), N+(v) and search the longer; both are
+        // strictly increasing, so each search starts where the last ended.
+        int32_t sb = orp[v], se = orp[v + 1];
+        int32_t lb = orp[u], le = orp[u + 1];
+        if (se - sb > le - lb) {
+            const int32_t tb = sb, te = se;
+            sb = lb;
+            se = le;
+            lb = tb;
+            le = te;
+        }
         unsigned long long found = 0;
-        for (int32_t k = vb; k < ve; ++k) {
+        for (int32_t k = sb; k < se && lb < le; ++k) {
             const int32_t w = ocol[k];
-            if (row_contains(ocol, ub, ue, w)) {
+            lb = lower_bound_from(ocol, lb, le, w);
+            if (lb < le && ocol[lb] == w) {
                 atomicAdd(cnt + w, 1ull);
                 ++found;
+                ++lb;
             }
         }
         if (found) {
