@@ -6,9 +6,9 @@
 // device first) take the oriented path: keep u->v only when
 // (deg v, v) > (deg u, u), so every triangle is found once, at its
 // lowest-ranked vertex, and oriented rows hold at most O(sqrt m) entries.
-// Each oriented entry (u, v) intersects N+(u) and N+(v): it walks the shorter
-// list and gallops through the longer, each search starting where the last
-// ended (N+(u) is reused by all of u's entries and stays in L1).  A triangle adds 1
+// Each oriented entry (u, v) intersects N+(u) and N+(v): it walks one list
+// and gallops through the other, each search starting where the last ended
+// (N+(u) is reused by all of u's entries and stays in L1).  A triangle adds 1
 // to each of its three vertices; the reference's count is 6x that (each
 // triangle is met from its 6 ordered edges), and its int32 wraps.
 //
@@ -160,13 +160,16 @@ struct OrientedVisitor {
     unsigned long long* cnt;
     __device__ bool want_row(int32_t) const { return true; }
     __device__ void operator()(int32_t u, int32_t v, int32_t) const {
-        // Walk the shorter of N+(u), N+(v) and search the longer; both are
-        // strictly increasing, so each search starts where the last ended.
-        // (Plain binary searches from the last hit measured 1.46x slower at
-        // RMAT scale 24.)
+        // Walk N+(v) and search N+(u), which the lanes walking u's row share
+        // (it stays in L1); both are strictly increasing, so each search
+        // starts where the last ended, and the walk stops once N+(u) is
+        // passed.  A long N+(v) over a much shorter N+(u) is walked the other
+        // way round.  (Swapping whenever N+(v) is longer measured 4 % slower
+        // on 2,000 small ER graphs and 10 % slower on RMAT scale 24; plain
+        // binary searches from the last hit 1.46x slower on RMAT scale 24.)
         int32_t sb = orp[v], se = orp[v + 1];
         int32_t lb = orp[u], le = orp[u + 1];
-        if (se - sb > le - lb) {
+        if (se - sb > 64 && se - sb > 4 * (le - lb)) {
             const int32_t tb = sb, te = se;
             sb = lb;
             se = le;
