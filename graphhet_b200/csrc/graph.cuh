@@ -33,6 +33,10 @@ struct ghb_graph {
     // first SSSP call; same rowptr), for delta-stepping's light/heavy split.
     int32_t* sw_col = nullptr;
     double* sw_w = nullptr;
+    // Triangle counting's input check on this (immutable) graph: -1 until the
+    // first TC call, then its flags (0 = symmetric, loop-free, strictly
+    // increasing rows: the oriented path).
+    mutable int32_t tc_flags = -1;
     int64_t device_bytes = 0;
     float build_ms = 0.f;
 };

@@ -44,6 +44,8 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
              int32_t* labels, const int32_t* init_labels, bool first_min);
 int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
            int32_t* counts32, int64_t* total);
+int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
+                  int32_t* counts32, int64_t* total, int32_t* flags_cache);
 int pagerank_run(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int32_t* in_col, const int32_t* out_rp,
                  const ghb_pr_options* o, double* rank, int32_t* iters_run);
 int msbfs_batch(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_rp, const int32_t* out_col,
@@ -284,7 +286,7 @@ int ghb_graph_tc(ghb_workspace* ws, const ghb_graph* g, int64_t* counts64, int32
     GRAPH_PRELUDE();
     GHB_TRY(ws_reserve_stage(ws, sizeof(int64_t) * (size_t)g->n));
     int64_t* cnew = static_cast<int64_t*>(ws->stage);
-    GHB_TRY(tc_run(ws, g->n, g->rowptr, g->col, cnew, nullptr, total));
+    GHB_TRY(tc_run_cached(ws, g->n, g->rowptr, g->col, cnew, nullptr, total, &g->tc_flags));
     return launch(ws, tc_map_kernel, dim3(grid_for(g->n, 256, ws->num_sms * 8)), dim3(256), 0, g->n,
                   (const int32_t*)g->perm, (const int64_t*)cnew, counts64, counts32);
 }

@@ -301,8 +301,10 @@ int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* row
     return GHB_OK;
 }
 
-int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
-           int32_t* counts32, int64_t* total) {
+// flags_cache (may be NULL): the input check's flags for this CSR, -1 when
+// not yet known; a known value skips the check.
+int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
+                  int32_t* counts32, int64_t* total, int32_t* flags_cache) {
     cudaStream_t st = ws->stream;
     int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
     GHB_CUDA_TRY(cudaMemcpyAsync(hp, rowptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
@@ -329,14 +331,19 @@ int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* c
     int64_t* bsums = c.take<int64_t>(scan_scratch_words(n));
     int32_t* ocol = c.take<int32_t>(m > 0 ? m : 1);
 
-    GHB_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int32_t), st));
     GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * n, st));
     GHB_CUDA_TRY(cudaMemsetAsync(tot, 0, sizeof(unsigned long long), st));
-    GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
-                 CheckVisitor{rowptr, col, flags}));
-    GHB_CUDA_TRY(cudaMemcpyAsync(hp, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    GHB_CUDA_TRY(cudaStreamSynchronize(st));
-    const bool oriented = hp[0] == 0;
+    int32_t check = flags_cache ? *flags_cache : -1;
+    if (check < 0) {
+        GHB_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int32_t), st));
+        GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
+                     CheckVisitor{rowptr, col, flags}));
+        GHB_CUDA_TRY(cudaMemcpyAsync(hp, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        check = hp[0];
+        if (flags_cache) *flags_cache = check;
+    }
+    const bool oriented = check == 0;
     if (oriented) {
         GHB_CUDA_TRY(cudaMemsetAsync(keep, 0, sizeof(int32_t) * n, st));
         GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n,
@@ -361,6 +368,11 @@ int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* c
         *total = (int64_t)(oriented ? s / 3 : s / 18);
     }
     return GHB_OK;
+}
+
+int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
+           int32_t* counts32, int64_t* total) {
+    return tc_run_cached(ws, n, rowptr, col, counts64, counts32, total, nullptr);
 }
 
 }  // namespace ghb
