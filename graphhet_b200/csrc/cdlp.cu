@@ -192,8 +192,8 @@ __global__ void cdlp_copy_kernel(const int4* __restrict__ rows, int32_t count,
 // distinct (first iteration), so the row's smallest label is taken directly.
 template <int W, bool kMin>
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_small_kernel(
-    const int4* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
+    const int4* __restrict__ rows, int32_t count, const int32_t* __restrict__ col,
+    const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
     const int lane = lane_id();
     const int li = lane & (W - 1);
     const int64_t group = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / W;
@@ -252,8 +252,8 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_small_kernel(
 // memory (kMin: the row's smallest label, no table).
 template <bool kMin>
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_warp_kernel(
-    const int4* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
+    const int4* __restrict__ rows, int32_t count, const int32_t* __restrict__ col,
+    const int32_t* __restrict__ lab, int32_t* __restrict__ out) {
     __shared__ int32_t keys[kCdlpThreads / 32][kWarpSlots];
     __shared__ int32_t cnts[kCdlpThreads / 32][kWarpSlots];
     const int lane = lane_id();
@@ -308,8 +308,8 @@ __device__ __forceinline__ unsigned long long block_max_u64(unsigned long long x
 // ints of dynamic shared memory.  kMin: the row's smallest label, no table.
 template <bool kMin>
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_block_kernel(
-    const int4* __restrict__ rows, int32_t count, const int32_t* __restrict__ rp,
-    const int32_t* __restrict__ col, const int32_t* __restrict__ lab, int32_t* __restrict__ out, uint32_t slots) {
+    const int4* __restrict__ rows, int32_t count, const int32_t* __restrict__ col,
+    const int32_t* __restrict__ lab, int32_t* __restrict__ out, uint32_t slots) {
     extern __shared__ int32_t smem[];
     __shared__ unsigned long long red[32];
     int32_t* K = smem;
@@ -379,7 +379,7 @@ struct LongRow {
     unsigned long long* T;
     int32_t* L;
 };
-__device__ __forceinline__ LongRow long_row(const int4* rows, const int32_t* rp, int32_t* pool,
+__device__ __forceinline__ LongRow long_row(const int4* rows, int32_t* pool,
                                             const int64_t* tab_off, int32_t i) {
     LongRow r;
     const int4 ri = rows[i];
@@ -414,7 +414,7 @@ __device__ __forceinline__ void chunk_done(const LongRow& r, int32_t i, unsigned
 // appended to the row's list (one atomic per warp on occ[i]) for the reset
 // pass.
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
-    const int4* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+    const int4* __restrict__ rows, const int32_t* __restrict__ col,
     const int32_t* __restrict__ lab, const int32_t* __restrict__ chunks, int32_t nch, int32_t* pool,
     const int64_t* __restrict__ tab_off, int32_t* occ, int32_t* done, unsigned long long* best,
     int32_t* __restrict__ out) {
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
     int32_t* C = smem + kChunkSlots;
     for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
         const int32_t i = chunks[2 * k];
-        const LongRow r = long_row(rows, rp, pool, tab_off, i);
+        const LongRow r = long_row(rows, pool, tab_off, i);
         const int32_t b = r.b + chunks[2 * k + 1];
         const int32_t e = (int32_t)min((int64_t)b + kChunk, (int64_t)r.b + r.d);
         uint32_t cap = 512;
@@ -500,11 +500,11 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_count_kernel(
 // [j0, j0 + kChunk); a dense one in slot order, chunk k taking the k-th share
 // of the slots.  The row's last chunk resets occ[i] and done[i].
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_reset_kernel(
-    const int4* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ chunks,
+    const int4* __restrict__ rows, const int32_t* __restrict__ chunks,
     int32_t nch, int32_t* pool, const int64_t* __restrict__ tab_off, int32_t* occ, int32_t* done) {
     for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
         const int32_t i = chunks[2 * k];
-        const LongRow r = long_row(rows, rp, pool, tab_off, i);
+        const LongRow r = long_row(rows, pool, tab_off, i);
         const int32_t j0 = chunks[2 * k + 1];
         const int32_t claims = __ldcg(occ + i);
         const uint32_t nchunks = (uint32_t)(r.d + kChunk - 1) / kChunk;
@@ -531,13 +531,13 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_reset_kernel(
 // First iteration (labels distinct, no repeated entries): each chunk's
 // smallest label, folded over the row's chunks as in the pick pass.
 __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_min_kernel(
-    const int4* __restrict__ rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+    const int4* __restrict__ rows, const int32_t* __restrict__ col,
     const int32_t* __restrict__ lab, const int32_t* __restrict__ chunks, int32_t nch, int32_t* pool,
     const int64_t* __restrict__ tab_off, int32_t* done, unsigned long long* best, int32_t* __restrict__ out) {
     __shared__ unsigned long long red[32];
     for (int64_t k = blockIdx.x; k < nch; k += gridDim.x) {
         const int32_t i = chunks[2 * k];
-        const LongRow r = long_row(rows, rp, pool, tab_off, i);
+        const LongRow r = long_row(rows, pool, tab_off, i);
         const int32_t b = r.b + chunks[2 * k + 1];
         const int32_t e = (int32_t)min((int64_t)b + kChunk, (int64_t)r.b + r.d);
         unsigned long long m = 0;
@@ -551,19 +551,17 @@ __global__ void __launch_bounds__(kCdlpThreads) cdlp_chunk_min_kernel(
 }
 
 // Chunked-class rows: degrees for the host's table layout.
-__global__ void cdlp_long_degrees_kernel(const int4* __restrict__ rows, int32_t count,
-                                         const int32_t* __restrict__ rp, int32_t* deg) {
+__global__ void cdlp_long_degrees_kernel(const int4* __restrict__ rows, int32_t count, int32_t* deg) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
         deg[i] = rows[i].z - rows[i].y;
     }
 }
 
 // Block per chunked-class row: every slot empty.
-__global__ void cdlp_pool_clear_kernel(const int4* __restrict__ rows, int32_t count,
-                                       const int32_t* __restrict__ rp, int32_t* pool,
+__global__ void cdlp_pool_clear_kernel(const int4* __restrict__ rows, int32_t count, int32_t* pool,
                                        const int64_t* __restrict__ tab_off) {
     for (int64_t i = blockIdx.x; i < count; i += gridDim.x) {
-        const LongRow r = long_row(rows, rp, pool, tab_off, (int32_t)i);
+        const LongRow r = long_row(rows, pool, tab_off, (int32_t)i);
         for (uint32_t s = threadIdx.x; s < r.cap; s += blockDim.x) r.T[s] = kSlotEmpty;
     }
 }
@@ -635,7 +633,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
         // Table offsets and the chunk list on the host (a few thousand rows),
         // then empty tables and zero counters.
         GHB_TRY(launch(ws, cdlp_long_degrees_kernel, dim3(grid_for(nlong, 256, ws->num_sms)), dim3(256), 0,
-                       long_rows, nlong, rp, occ));
+                       long_rows, nlong, occ));
         std::vector<int32_t> deg((size_t)nlong);
         GHB_CUDA_TRY(cudaMemcpyAsync(deg.data(), occ, sizeof(int32_t) * nlong, cudaMemcpyDeviceToHost, st));
         GHB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -662,7 +660,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
         GHB_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(int32_t) * nlong, st));
         GHB_CUDA_TRY(cudaMemsetAsync(best, 0, sizeof(unsigned long long) * nlong, st));
         GHB_TRY(launch(ws, cdlp_pool_clear_kernel, dim3(grid_for(nlong, 1, ws->num_sms * 8)), dim3(256), 0, long_rows,
-                       nlong, rp, pool, (const int64_t*)tab_off));
+                       nlong, pool, (const int64_t*)tab_off));
         GHB_CUDA_TRY(cudaStreamSynchronize(st));  // toff and ch are read by the copies above
     }
     if (init_labels)
@@ -698,24 +696,24 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
         constexpr bool M = decltype(min_tag)::value;
         const int4* R = rows;
         if (cls[0]) GHB_TRY(launch(ws, cdlp_copy_kernel, dim3(grid_for(cls[0], 256, g)), dim3(256), 0, R + off[0], cls[0], cur, nxt));
-        if (cls[1]) GHB_TRY(launch(ws, cdlp_small_kernel<2, M>, dim3(grid_for((int64_t)cls[1] * 2, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[1], cls[1], rp, col, cur, nxt));
-        if (cls[2]) GHB_TRY(launch(ws, cdlp_small_kernel<4, M>, dim3(grid_for((int64_t)cls[2] * 4, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[2], cls[2], rp, col, cur, nxt));
-        if (cls[3]) GHB_TRY(launch(ws, cdlp_small_kernel<8, M>, dim3(grid_for((int64_t)cls[3] * 8, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[3], cls[3], rp, col, cur, nxt));
-        if (cls[4]) GHB_TRY(launch(ws, cdlp_small_kernel<16, M>, dim3(grid_for((int64_t)cls[4] * 16, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[4], cls[4], rp, col, cur, nxt));
-        if (cls[5]) GHB_TRY(launch(ws, cdlp_small_kernel<32, M>, dim3(grid_for((int64_t)cls[5] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[5], cls[5], rp, col, cur, nxt));
-        if (cls[6]) GHB_TRY(launch(ws, cdlp_warp_kernel<M>, dim3(grid_for((int64_t)cls[6] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[6], cls[6], rp, col, cur, nxt));
+        if (cls[1]) GHB_TRY(launch(ws, cdlp_small_kernel<2, M>, dim3(grid_for((int64_t)cls[1] * 2, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[1], cls[1], col, cur, nxt));
+        if (cls[2]) GHB_TRY(launch(ws, cdlp_small_kernel<4, M>, dim3(grid_for((int64_t)cls[2] * 4, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[2], cls[2], col, cur, nxt));
+        if (cls[3]) GHB_TRY(launch(ws, cdlp_small_kernel<8, M>, dim3(grid_for((int64_t)cls[3] * 8, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[3], cls[3], col, cur, nxt));
+        if (cls[4]) GHB_TRY(launch(ws, cdlp_small_kernel<16, M>, dim3(grid_for((int64_t)cls[4] * 16, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[4], cls[4], col, cur, nxt));
+        if (cls[5]) GHB_TRY(launch(ws, cdlp_small_kernel<32, M>, dim3(grid_for((int64_t)cls[5] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[5], cls[5], col, cur, nxt));
+        if (cls[6]) GHB_TRY(launch(ws, cdlp_warp_kernel<M>, dim3(grid_for((int64_t)cls[6] * 32, kCdlpThreads, g)), dim3(kCdlpThreads), 0, R + off[6], cls[6], col, cur, nxt));
         if (M) {
             const int32_t nblock = cls[7] + cls[8] + cls[9];
-            if (nblock) GHB_TRY(launch(ws, cdlp_block_kernel<true>, dim3(grid_for(nblock, 1, g)), dim3(kCdlpThreads), 0, R + off[7], nblock, rp, col, cur, nxt, 0u));
-            if (nlong) GHB_TRY(launch(ws, cdlp_chunk_min_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, done, best, nxt));
+            if (nblock) GHB_TRY(launch(ws, cdlp_block_kernel<true>, dim3(grid_for(nblock, 1, g)), dim3(kCdlpThreads), 0, R + off[7], nblock, col, cur, nxt, 0u));
+            if (nlong) GHB_TRY(launch(ws, cdlp_chunk_min_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, done, best, nxt));
             return GHB_OK;
         }
-        if (cls[7]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[7], 1, g_small)), dim3(kCdlpThreads), small_smem, R + off[7], cls[7], rp, col, cur, nxt, (uint32_t)kSmallBlockSlots));
-        if (cls[8]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[8], 1, g_mid)), dim3(kCdlpThreads), mid_smem, R + off[8], cls[8], rp, col, cur, nxt, (uint32_t)kMidBlockSlots));
-        if (cls[9]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[9], 1, g_big)), dim3(kCdlpThreads), big_smem, R + off[9], cls[9], rp, col, cur, nxt, (uint32_t)kBlockSlots));
+        if (cls[7]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[7], 1, g_small)), dim3(kCdlpThreads), small_smem, R + off[7], cls[7], col, cur, nxt, (uint32_t)kSmallBlockSlots));
+        if (cls[8]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[8], 1, g_mid)), dim3(kCdlpThreads), mid_smem, R + off[8], cls[8], col, cur, nxt, (uint32_t)kMidBlockSlots));
+        if (cls[9]) GHB_TRY(launch(ws, cdlp_block_kernel<false>, dim3(grid_for(cls[9], 1, g_big)), dim3(kCdlpThreads), big_smem, R + off[9], cls[9], col, cur, nxt, (uint32_t)kBlockSlots));
         if (nlong) {
-            GHB_TRY(launch(ws, cdlp_chunk_count_kernel, dim3(grid_for(nch, 1, g_chunk)), dim3(kCdlpThreads), chunk_smem, long_rows, rp, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done, best, nxt));
-            GHB_TRY(launch(ws, cdlp_chunk_reset_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, rp, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done));
+            GHB_TRY(launch(ws, cdlp_chunk_count_kernel, dim3(grid_for(nch, 1, g_chunk)), dim3(kCdlpThreads), chunk_smem, long_rows, col, cur, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done, best, nxt));
+            GHB_TRY(launch(ws, cdlp_chunk_reset_kernel, dim3(grid_for(nch, 1, g)), dim3(kCdlpThreads), 0, long_rows, (const int32_t*)chunks, nch, pool, (const int64_t*)tab_off, occ, done));
         }
         return GHB_OK;
     };
