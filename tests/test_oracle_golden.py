@@ -91,3 +91,26 @@ def test_oracle_planted_mistake_is_caught():
     d = O.bfs(g, int(z["src"]))
     d[np.argmax(d < 2**31 - 1)] += 1
     assert not np.array_equal(d, z["bfs"])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="compiled reference (oracle/_ref) not built")
+def test_oracle_matches_compiled_reference_on_hub_rows():
+    """CDLP and TC on rows at the GPU kernels' class edges (1024 | 1025,
+    2048 | 2049, 4096 | 4097 entries) and on hubs of 9,000 and 20,000 entries,
+    each hub a vertex of its own joined to distinct RMAT vertices: the oracle
+    the GPU parity tests use agrees with the reference's CPU code there."""
+    scale = 15
+    base = 1 << scale
+    s, d = O.rmat_edges(scale, 4 << scale, 13)
+    rng = np.random.default_rng(17)
+    degs = (1024, 1025, 2048, 2049, 4096, 4097, 9000, 20000)
+    hs, hd = [s], [d]
+    for k, deg in enumerate(degs):
+        hs.append(np.full(deg, base + k, np.int32))
+        hd.append(rng.choice(base, size=deg, replace=False).astype(np.int32))
+    g = O.make_graph(base + len(degs), np.concatenate(hs), np.concatenate(hd), False, weight_mode=0)
+    assert np.diff(g.rowptr)[base:].tolist() == list(degs)
+    r = O.Ref().load(g)
+    for iters in (1, 2, 10):
+        assert np.array_equal(O.cdlp(g, iters), r.cdlp(iters)), iters
+    assert np.array_equal(O.tc(g), r.tc())
