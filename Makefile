@@ -7,7 +7,9 @@ CXX       := g++
 CC        := gcc
 ARCH      := -gencode arch=compute_100a,code=sm_100a
 NVFLAGS   := $(ARCH) -O3 -lineinfo -std=c++17 -Xcompiler -fPIC -Iinclude --expt-relaxed-constexpr
-REF_ROOT  ?= /root/reference
+# REF_ROOT: path to the GraphHET source tree (MDNDDD/GraphHET).  Required for
+# oracle/_ref and the drop-in build; both are skipped when it is not given.
+REF_ROOT  ?=
 BUILD     := build/obj
 
 CU_SRC    := $(wildcard graphhet_b200/csrc/*.cu)
@@ -32,7 +34,7 @@ oracle:
 # and linked to libghb.so: the drop-in check.
 DROPIN    := build/dropin
 dropin: graphhet_b200/libghb.so
-	@if [ -f "$(REF_ROOT)/src/LDBC/LDBC_GPU_csr.cu" ]; then \
+	@if [ -n "$(REF_ROOT)" ] && [ -f "$(REF_ROOT)/src/LDBC/LDBC_GPU_csr.cu" ]; then \
 	  mkdir -p $(DROPIN) && \
 	  $(NVCC) $(ARCH) -O2 -std=c++17 -Iinclude -I$(REF_ROOT)/include $(REF_ROOT)/src/GPU_csr/GPU_csr_example.cu \
 	    -o $(DROPIN)/GPU_csr_example -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' && \
@@ -42,7 +44,7 @@ dropin: graphhet_b200/libghb.so
 	    -o $(DROPIN)/GPU_gpma_example -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' && \
 	  $(NVCC) $(ARCH) -O2 -std=c++17 -Iinclude -I$(REF_ROOT)/include $(REF_ROOT)/src/LDBC/LDBC_GPU_gpma.cu \
 	    -o $(DROPIN)/LDBC_GPU_gpma -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' ; \
-	else echo "reference drivers not found under $(REF_ROOT): skipping the drop-in build"; fi
+	else echo "REF_ROOT (the GraphHET source tree) not given or without src/: skipping the drop-in build"; fi
 
 clean:
 	rm -rf build graphhet_b200/libghb.so

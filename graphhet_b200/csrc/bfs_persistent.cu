@@ -60,6 +60,9 @@ struct BfsRunState {
     int32_t pad2;
     unsigned long long t_prev;       // global timer at the previous decision
     unsigned long long t_comp;       // global timer after this level's compaction
+    unsigned long long bar_limit_ns; // grid-barrier wait limit (set by the host before the launch)
+    unsigned bar_extra;              // arrivals beyond the grid every barrier waits for (0; tests: 1)
+    unsigned pad3;
 };
 
 namespace {
@@ -124,16 +127,19 @@ __device__ __forceinline__ void p_visit(int32_t v, uint32_t* visited, uint32_t* 
 }
 
 __device__ __forceinline__ bool p_barrier(BfsRunState* st) {
-    return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, NoLeader());
+    return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, NoLeader(), st->bar_limit_ns,
+                            st->bar_extra);
 }
 template <class F>
 __device__ __forceinline__ bool p_barrier(BfsRunState* st, const F& leader) {
-    return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, leader);
+    return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, leader, st->bar_limit_ns,
+                            st->bar_extra);
 }
 // Barrier whose decision runs on every thread of the last block to arrive.
 template <class F>
 __device__ __forceinline__ bool p_barrier_block(BfsRunState* st, const F& leader) {
-    return grid_sync_block_leader(&st->bar_count, &st->bar_release, &st->status, leader);
+    return grid_sync_block_leader(&st->bar_count, &st->bar_release, &st->status, leader, st->bar_limit_ns,
+                                  st->bar_extra);
 }
 
 // Output format of a top-down level: fmt 1 queue, 2 bitmap only, 0 by the
@@ -684,6 +690,12 @@ int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int
     int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
     GHB_CUDA_TRY(cudaMemcpyAsync(hp, out_rp + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     GHB_CUDA_TRY(cudaMemsetAsync(rs, 0, sizeof(BfsRunState), st));
+    {
+        // Barrier limit and test knob (pageable source: staged by the call).
+        const unsigned long long bar[2] = {(unsigned long long)ws->tune.barrier_limit_us * 1000ull,
+                                           (unsigned long long)ws->tune.barrier_extra};
+        GHB_CUDA_TRY(cudaMemcpyAsync(&rs->bar_limit_ns, bar, sizeof(bar), cudaMemcpyHostToDevice, st));
+    }
     GHB_CUDA_TRY(cudaStreamSynchronize(st));
     const int64_t m_total = hp[0];
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));

@@ -70,6 +70,9 @@ struct Tuning {
     int32_t ms_pull_div = 16;      // multi-source: pull when frontier entries > m / ms_pull_div
     int32_t pol_band = 1;          // learned policy: the network picks a level's direction and format only
                                    // where the direction rule's test is within 2^pol_band of its threshold
+    int32_t barrier_limit_us = 2000000;  // persistent kernels: a grid-barrier wait gives up after this long
+    int32_t barrier_extra = 0;     // test knob: barriers wait for this many arrivals beyond the grid, so
+                                   // every wait runs out and the timeout path is exercised (0 or 1)
 };
 
 }  // namespace ghb
@@ -257,14 +260,17 @@ struct NoLeader {
     __device__ void operator()() const {}
 };
 
+// `extra` (normally 0) adds arrivals that never come: the tests use it to
+// make every wait run out.
 template <class Leader>
 __device__ __forceinline__ bool grid_sync_leader(unsigned* count, unsigned* release, int32_t* status,
-                                                 const Leader& leader, uint64_t limit_ns = 2000000000ull) {
+                                                 const Leader& leader, uint64_t limit_ns = 2000000000ull,
+                                                 unsigned extra = 0) {
     __shared__ int s_ok2;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+        const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z + extra;
         __threadfence();
         const unsigned old = atomicAdd(count, 1u);
         const unsigned epoch = old / nblocks + 1u;
@@ -301,12 +307,13 @@ __device__ __forceinline__ bool grid_sync_leader(unsigned* count, unsigned* rele
 // decision can use the whole block (the policy network's layers).
 template <class Leader>
 __device__ __forceinline__ bool grid_sync_block_leader(unsigned* count, unsigned* release, int32_t* status,
-                                                       const Leader& leader, uint64_t limit_ns = 2000000000ull) {
+                                                       const Leader& leader, uint64_t limit_ns = 2000000000ull,
+                                                       unsigned extra = 0) {
     __shared__ int s_ok3, s_last3;
     __shared__ unsigned s_epoch3;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+        const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z + extra;
         __threadfence();
         const unsigned old = atomicAdd(count, 1u);
         s_epoch3 = old / nblocks + 1u;

@@ -2,6 +2,7 @@
 // permutations to map results back to the caller's vertex ids.
 #pragma once
 
+#include <atomic>
 #include <vector>
 
 #include "common.cuh"
@@ -35,8 +36,9 @@ struct ghb_graph {
     double* sw_w = nullptr;
     // Triangle counting's input check on this (immutable) graph: -1 until the
     // first TC call, then its flags (0 = symmetric, loop-free, strictly
-    // increasing rows: the oriented path).
-    mutable int32_t tc_flags = -1;
+    // increasing rows: the oriented path).  Atomic (relaxed): two host
+    // threads may run TC on one handle; both compute the same flags.
+    mutable std::atomic<int32_t> tc_flags{-1};
     int64_t device_bytes = 0;
     float build_ms = 0.f;
 };

@@ -45,7 +45,7 @@ int cdlp_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* col
 int tc_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
            int32_t* counts32, int64_t* total);
 int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
-                  int32_t* counts32, int64_t* total, int32_t* flags_cache);
+                  int32_t* counts32, int64_t* total, std::atomic<int32_t>* flags_cache);
 int pagerank_run(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int32_t* in_col, const int32_t* out_rp,
                  const ghb_pr_options* o, double* rank, int32_t* iters_run);
 int msbfs_batch(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_rp, const int32_t* out_col,

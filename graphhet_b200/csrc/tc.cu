@@ -14,6 +14,8 @@
 //
 // Any other input takes the generic path: the reference's merge over every
 // entry, kept for exact parity on directed or unusual inputs.
+#include <atomic>
+
 #include "common.cuh"
 #include "edge_walk.cuh"
 #include "scan.cuh"
@@ -304,7 +306,7 @@ int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* row
 // flags_cache (may be NULL): the input check's flags for this CSR, -1 when
 // not yet known; a known value skips the check.
 int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, int64_t* counts64,
-                  int32_t* counts32, int64_t* total, int32_t* flags_cache) {
+                  int32_t* counts32, int64_t* total, std::atomic<int32_t>* flags_cache) {
     cudaStream_t st = ws->stream;
     int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
     GHB_CUDA_TRY(cudaMemcpyAsync(hp, rowptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
@@ -333,7 +335,7 @@ int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
 
     GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * n, st));
     GHB_CUDA_TRY(cudaMemsetAsync(tot, 0, sizeof(unsigned long long), st));
-    int32_t check = flags_cache ? *flags_cache : -1;
+    int32_t check = flags_cache ? flags_cache->load(std::memory_order_relaxed) : -1;
     if (check < 0) {
         GHB_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int32_t), st));
         GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
@@ -341,7 +343,7 @@ int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
         GHB_CUDA_TRY(cudaMemcpyAsync(hp, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         GHB_CUDA_TRY(cudaStreamSynchronize(st));
         check = hp[0];
-        if (flags_cache) *flags_cache = check;
+        if (flags_cache) flags_cache->store(check, std::memory_order_relaxed);
     }
     const bool oriented = check == 0;
     if (oriented) {

@@ -229,7 +229,9 @@ static __device__ __align__(256) unsigned char g_wcc_noalloc_scratch[ghb::kNoAll
 namespace ghb {
 
 // Device address of the scratch array on the current device, looked up once
-// per device (with that device current) and cached.
+// per device (with that device current) and cached for the process's life.
+// A cudaDeviceReset would leave the cached address stale; the header says
+// that a reset device must not be used with this entry point again.
 static int noalloc_scratch_address(void** out) {
     int dev = 0;
     GHB_CUDA_TRY(cudaGetDevice(&dev));

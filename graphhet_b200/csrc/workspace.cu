@@ -128,6 +128,8 @@ const TuneField kTuneFields[] = {
     {"ms_warp_rest", &ghb::Tuning::ms_warp_rest, 32, 1 << 20},
     {"ms_pull_div", &ghb::Tuning::ms_pull_div, 1, 1024},
     {"pol_band", &ghb::Tuning::pol_band, 0, 64},
+    {"barrier_limit_us", &ghb::Tuning::barrier_limit_us, 100, 60000000},
+    {"barrier_extra", &ghb::Tuning::barrier_extra, 0, 1},
 };
 const TuneField* tune_field(const char* name) {
     if (!name) return nullptr;

@@ -69,9 +69,14 @@ ghb_workspace* ghb_default_workspace(void);
  * threshold and direction switch, "pol_band" (0-64) the band, in log2
  * units around the direction rule's threshold, inside which the learned
  * policy's network chooses a BFS level's direction and output format (0:
- * never; 64: always).
- * Results do not depend on them.  Unknown names and values outside the
- * documented ranges are rejected. */
+ * never; 64: always), "barrier_limit_us" (100 - 60,000,000; default
+ * 2,000,000) how long a persistent kernel's grid-barrier wait lasts before
+ * it gives up and the call returns GHB_ERR_TIMEOUT.
+ * Results do not depend on them.  "barrier_extra" (0 or 1) is a test knob:
+ * 1 makes every grid barrier of the persistent kernels wait for one arrival
+ * more than there are blocks, so every wait runs out after barrier_limit_us
+ * and the call returns GHB_ERR_TIMEOUT (the workspace stays usable).
+ * Unknown names and values outside the documented ranges are rejected. */
 int ghb_tune_set(ghb_workspace* ws, const char* name, int32_t value);
 int ghb_tune_get(ghb_workspace* ws, const char* name, int32_t* value);
 
@@ -266,10 +271,13 @@ int ghb_wcc(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* 
  * array inside libghb.so, held by every GPU that loads the library until the
  * process exits.  Limit: at most 268,435,456 (2^28) CSR entries; larger
  * graphs are rejected with GHB_ERR_INVALID_ARGUMENT.  The first call on a
- * device looks up the array's address (cudaGetSymbolAddress): make that first
- * call before any stream capture.  Every call shares the array, so calls that
- * overlap on the GPU race: serialise them.  Reads rowptr[n] back once and
- * synchronises `stream`. */
+ * device does a one-time set-up: it looks up the array's device address
+ * (cudaGetSymbolAddress) and keeps it for the life of the process; make that
+ * first call before any stream capture begins.  A device reset
+ * (cudaDeviceReset) is not supported: the kept address would be stale, so do
+ * not call this function on a device after resetting it.  Every call shares
+ * the array, so calls that overlap on the GPU race: serialise them.  Each
+ * call reads rowptr[n] back and synchronises `stream`. */
 int ghb_wcc_noalloc(int32_t n, const int32_t* rowptr, const int32_t* col, int32_t* label,
                     void* stream);
 

@@ -1,0 +1,66 @@
+"""The bounded grid barrier's timeout path.
+
+Every wait of a persistent kernel on its grid barrier gives up after the
+workspace's "barrier_limit_us"; the kernel then leaves and the call returns
+GHB_ERR_TIMEOUT, with the device still usable.  The test knob
+"barrier_extra" makes every barrier wait for one arrival more than there are
+blocks, a wait that nothing ends, so the limit is what ends it.  Nothing
+faults or hangs: each block's wait ends on its own clock after about a
+millisecond.  The same workspace then runs a normal traversal, checked
+against the oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GHB_ERR_TIMEOUT = 4
+
+
+@pytest.fixture(scope="module")
+def G():
+    import graphhet_b200 as G
+    G.lib()
+    return G
+
+
+def test_bfs_barrier_timeout_then_recovers(G):
+    og = O.rmat_graph(12, 16, 42, directed=False)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    g = G.CSRGraph(n=og.n, rowptr=t(og.rowptr), col=t(og.col), w=None, directed=False)
+    ws = G.Workspace()
+    rg = G.ResidentGraph(g, ws=ws)
+    src = int(np.argmax(np.diff(og.rowptr)))
+    L = G.lib()
+    depth = torch.empty(og.n, dtype=torch.int32, device="cuda")
+    st = G.TraversalStats()
+    opt = G.BfsOptions(policy=G.POLICY_HEURISTIC)
+
+    G.tune_set("barrier_limit_us", 1000, ws=ws)
+    G.tune_set("barrier_extra", 1, ws=ws)
+    rc = L.ghb_graph_bfs(ws.handle, rg._h, src, G.INT32_MAX, G._ptr(depth), ctypes.byref(opt), ctypes.byref(st))
+    assert rc == GHB_ERR_TIMEOUT
+    assert "timed out" in L.ghb_last_error().decode()
+    assert L.ghb_status_string(rc).decode() == "device wait timed out"
+    torch.cuda.synchronize()  # the context is intact: no sticky error
+
+    G.tune_set("barrier_extra", 0, ws=ws)
+    G.tune_set("barrier_limit_us", 2000000, ws=ws)
+    rc = L.ghb_graph_bfs(ws.handle, rg._h, src, G.INT32_MAX, G._ptr(depth), ctypes.byref(opt), ctypes.byref(st))
+    assert rc == 0, L.ghb_last_error().decode()
+    assert np.array_equal(depth.cpu().numpy(), O.bfs(og, src))
+    rg.close()
+
+
+def test_barrier_knobs_are_range_checked(G):
+    ws = G.Workspace()
+    with pytest.raises(G.GhbError):
+        G.tune_set("barrier_extra", 2, ws=ws)
+    with pytest.raises(G.GhbError):
+        G.tune_set("barrier_limit_us", 10, ws=ws)
+    assert G.tune_get("barrier_limit_us", ws=ws) == 2000000
+    assert G.tune_get("barrier_extra", ws=ws) == 0
