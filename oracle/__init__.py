@@ -57,6 +57,7 @@ def port() -> ctypes.CDLL:
             "orc_pagerank": (None, [_i32, _p, _p, _p, _f64, _i32, _p]),
             "orc_cdlp": (None, [_i32, _p, _p, _p, _p, _i32, _p]),
             "orc_tc": (None, [_i32, _p, _p, _p]),
+            "orc_tc_oriented": (_i64, [_i32, _p, _p, _p]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)
@@ -194,6 +195,16 @@ def tc(g: Graph):
     c = np.empty(g.n, np.int32)
     port().orc_tc(g.n, _np_ptr(g.rowptr), _np_ptr(g.col), _np_ptr(c))
     return c
+
+
+def tc_oriented(g: Graph):
+    """Per-vertex 6x triangle counts (int64, exact) and the triangle total by
+    degree orientation, on all host threads: the checker for graphs where
+    the reference's quadratic merge (tc above) does not finish.  Needs a
+    symmetric, loop-free CSR without repeated entries."""
+    c = np.empty(g.n, np.int64)
+    t = port().orc_tc_oriented(g.n, _np_ptr(g.rowptr), _np_ptr(g.col), _np_ptr(c))
+    return c, int(t)
 
 
 # ------------------------------------------------------- dynamic graph
