@@ -43,7 +43,9 @@ dropin: graphhet_b200/libghb.so
 	  $(NVCC) $(ARCH) -O2 -std=c++17 -Iinclude -I$(REF_ROOT)/include $(REF_ROOT)/src/GPU_gpma/GPU_gpma_example.cu \
 	    -o $(DROPIN)/GPU_gpma_example -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' && \
 	  $(NVCC) $(ARCH) -O2 -std=c++17 -Iinclude -I$(REF_ROOT)/include $(REF_ROOT)/src/LDBC/LDBC_GPU_gpma.cu \
-	    -o $(DROPIN)/LDBC_GPU_gpma -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' ; \
+	    -o $(DROPIN)/LDBC_GPU_gpma -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' && \
+	  $(NVCC) $(ARCH) -O3 -std=c++17 -Iinclude -I$(REF_ROOT)/include graphhet_b200/dropin_bfs_bench.cu \
+	    -o $(DROPIN)/dropin_bfs_bench -Lgraphhet_b200 -lghb -Xlinker -rpath -Xlinker '$$ORIGIN/../../graphhet_b200' ; \
 	else echo "REF_ROOT (the GraphHET source tree) not given or without src/: skipping the drop-in build"; fi
 
 clean:

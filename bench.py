@@ -365,6 +365,7 @@ def run_ours(args, world, rank, local):
     parity = {}
     if rank == 0 and args.extras:
         out["extra"] = extras(args, G, g, rg, srcs, ws, parity if args.parity else None)
+        out["dropin_e2e"] = dropin_leg(args, srcs[:8])
     if rank == 0 and args.parity:
         # Outputs at the benchmark size against the CPU checkers, and the
         # reference's CPU code timed on the same graph (outside every timed
@@ -744,6 +745,31 @@ def pr_precision(G, hbm, scale=25, seed=11, fraction=0.1, parity=None):
                       "fp64_last_l1": h64[-1] if h64 else None}
     rp.close()
     return out
+
+
+def dropin_leg(args, srcs):
+    """The reference-facing Cuda_BFS (include/GPU_csr/algorithm/GPU_BFS_csr.cuh)
+    end to end on this workload, timed by the C++ driver build/dropin/
+    dropin_bfs_bench as the reference's LDBC driver times it
+    (LDBC_GPU_csr.cu:82-95): names in, host vector of (name, depth) out."""
+    exe = os.path.join(ROOT, "build", "dropin", "dropin_bfs_bench")
+    if not os.path.exists(exe):
+        return {"unavailable": "build/dropin/dropin_bfs_bench not built (make dropin with REF_ROOT)"}
+    cmd = [exe, str(args.scale), str(args.edge_factor), str(args.seed), ",".join(str(s) for s in srcs)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "dropin_bfs_bench exceeded 600 s"}
+    line = (r.stdout.strip().splitlines() or [""])[-1]
+    try:
+        d = json.loads(line)
+    except ValueError:
+        return {"unavailable": f"dropin_bfs_bench rc={r.returncode}: {r.stderr.strip()[-300:]}"}
+    d["rc"] = r.returncode
+    d["note"] = ("Cuda_BFS(graph, csr, name) per source: BFS on the CSR_graph's resident copy, depth vector to a "
+                 "pageable host vector, ids -> names (vector<pair<string,int>>); bfs_plus_copy = the same call's "
+                 "device work and copy without the naming")
+    return d
 
 
 def rel_l1(a, b):

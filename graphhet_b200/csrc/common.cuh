@@ -73,6 +73,9 @@ struct Tuning {
     int32_t barrier_limit_us = 2000000;  // persistent kernels: a grid-barrier wait gives up after this long
     int32_t barrier_extra = 0;     // test knob: barriers wait for this many arrivals beyond the grid, so
                                    // every wait runs out and the timeout path is exercised (0 or 1)
+    int32_t sssp_persistent = 1;   // SSSP: 1 = one cooperative launch per traversal, 0 = host-driven rounds
+    int32_t tc_hash = 1;           // TC: 1 = shared-memory hash probes per oriented row, 0 = galloping merges
+    int32_t tc_block_row = 8192;   // TC hash path: longest oriented row a block hashes; longer rows gallop
 };
 
 }  // namespace ghb

@@ -248,6 +248,7 @@ int ghb_graph_destroy(ghb_graph* g) {
     cudaFree(g->outdeg);
     cudaFree(g->sw_col);
     cudaFree(g->sw_w);
+    cudaFree(g->sw_le);
     if (g->directed) {
         cudaFree(g->in_rowptr);
         cudaFree(g->in_col);

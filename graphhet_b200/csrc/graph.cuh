@@ -34,6 +34,10 @@ struct ghb_graph {
     // first SSSP call; same rowptr), for delta-stepping's light/heavy split.
     int32_t* sw_col = nullptr;
     double* sw_w = nullptr;
+    // First entry of each weight-sorted row whose weight is >= sw_le_delta
+    // (the light/heavy boundary of the last SSSP width used; built on demand).
+    int32_t* sw_le = nullptr;
+    double sw_le_delta = -1.0;
     // Triangle counting's input check on this (immutable) graph: -1 until the
     // first TC call, then its flags (0 = symmetric, loop-free, strictly
     // increasing rows: the oriented path).  Atomic (relaxed): two host

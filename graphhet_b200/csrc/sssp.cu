@@ -29,6 +29,13 @@
 #include "policy.cuh"
 
 namespace ghb {
+
+bool sssp_persistent_available(ghb_workspace* ws, int* blocks);
+int sssp_persistent_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const int32_t* le, const int32_t* col,
+                        const double* wt, int32_t src, double inf, double delta, double* dist, const int32_t* perm,
+                        double* out, ghb_traversal_stats* stats);
+int graph_light_ends(ghb_workspace* ws, ghb_graph* g, double delta, const int32_t** le);
+
 namespace {
 
 struct SsspCounters {
@@ -429,6 +436,10 @@ int sssp_run(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t*
     cudaStream_t st = ws->stream;
     double delta = 0.0;
     GHB_TRY(sssp_choose_delta(ws, n, rowptr, w, src, opt, &delta));
+    int blocks = 0;
+    if (ws->tune.sssp_persistent && sssp_persistent_available(ws, &blocks))
+        return sssp_persistent_run(ws, n, rowptr, nullptr, col, w, src, inf, delta, dist_out, nullptr, nullptr,
+                                   stats);
 
     Carver sizing(nullptr);
     auto carve = [&](Carver& c, WalkBuffers* wb, int32_t** qa, int32_t** qb, int32_t** fa, int32_t** fb,
@@ -593,6 +604,15 @@ int sssp_delta_run(ghb_workspace* ws, ghb_graph* g, int32_t src, double inf, dou
         b &= ~((1ull << 25) - 1);
         std::memcpy(&delta, &b, sizeof(b));
         if (!(delta > 0)) delta = 1.0;
+    }
+    {
+        int blocks = 0;
+        if (ws->tune.sssp_persistent && sssp_persistent_available(ws, &blocks)) {
+            const int32_t* le = nullptr;
+            GHB_TRY(graph_light_ends(ws, g, delta, &le));
+            return sssp_persistent_run(ws, n, g->rowptr, le, g->sw_col, g->sw_w, src, inf, delta, dist_out, nullptr,
+                                       nullptr, stats);
+        }
     }
     auto carve = [&](Carver& c, WalkBuffers* wb, int32_t** qa, int32_t** qb, int32_t** fa, int32_t** fb, int32_t** ns,
                      int32_t** fs, int32_t** rs, int32_t** R, int32_t** le, SsspCounters** cnt, double** minfar,

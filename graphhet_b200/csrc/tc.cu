@@ -6,10 +6,12 @@
 // device first) take the oriented path: keep u->v only when
 // (deg v, v) > (deg u, u), so every triangle is found once, at its
 // lowest-ranked vertex, and oriented rows hold at most O(sqrt m) entries.
-// Each oriented entry (u, v) intersects N+(u) and N+(v): it walks one list
-// and gallops through the other, each search starting where the last ended
-// (N+(u) is reused by all of u's entries and stays in L1).  A triangle adds 1
-// to each of its three vertices; the reference's count is 6x that (each
+// Each oriented row N+(a) is put in a shared-memory hash and every w of
+// every N+(b), b in N+(a), is probed with all lanes busy (the hash path
+// below); rows too long for a block's hash, or every row when the
+// workspace's tc_hash knob is 0, intersect N+(u) and N+(v) per entry by
+// walking one list and galloping through the other.  A triangle adds 1 to
+// each of its three vertices; the reference's count is 6x that (each
 // triangle is met from its 6 ordered edges), and its int32 wraps.
 //
 // Any other input takes the generic path: the reference's merge over every
@@ -196,9 +198,199 @@ struct OrientedVisitor {
     __device__ void finish() const {}
 };
 
+// ---- hash-probe counting: one row a of the oriented CSR at a time.
+//
+// N+(a) goes into a shared-memory hash (open addressing, at most half
+// full); the lists N+(b), b in N+(a), are then walked with every lane busy
+// (lists of 32 entries or more by the whole warp, shorter ones packed
+// warp-wide over a scan of their lengths) and each w probed: a hit is the
+// triangle (a, b, w).  a's count is summed in registers, b's in a shared
+// counter per entry of N+(a) (one global add per oriented edge that closes
+// any), w's by a global add per triangle.  Rows of up to kTcWarpRow entries
+// take a warp each (256-slot hash), rows up to kTcBlockRow a block each
+// (hash of up to 16,384 slots); longer ones go to the galloping visitor.
+constexpr int32_t kTcWarpRow = 128;
+constexpr int32_t kTcWarpSlots = 256;
+constexpr int32_t kTcBlockRow = 8192;
+constexpr int kTcWarpBlock = 256;   // threads of the warp-per-row kernel
+constexpr int kTcBlockThreads = 512;
+
+__device__ __forceinline__ uint32_t tc_hash(int32_t w, int shift) {
+    return ((uint32_t)w * 2654435761u) >> shift;
+}
+
+__device__ __forceinline__ void tc_insert(int32_t* keys, uint32_t mask, int shift, int32_t w) {
+    uint32_t h = tc_hash(w, shift);
+    while (atomicCAS(keys + h, -1, w) != -1) h = (h + 1) & mask;
+}
+
+__device__ __forceinline__ bool tc_probe(const int32_t* keys, uint32_t mask, int shift, int32_t w) {
+    uint32_t h = tc_hash(w, shift);
+    while (true) {
+        const int32_t k = keys[h];
+        if (k == w) return true;
+        if (k < 0) return false;
+        h = (h + 1) & mask;
+    }
+}
+
+// The warp's share of row a: entries [g0, g1) of N+(a) (every 32-entry
+// group from g0 with the given stride), probing the hash `keys`.  Adds w's
+// hits to cnt, b's to bc[index in N+(a)]; returns a's hits (lane 0 holds
+// those of whole-warp lists, every lane those it probed itself).
+__device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __restrict__ orp,
+                                                           const int32_t* __restrict__ ocol, int32_t ab, int32_t k,
+                                                           int32_t g0, int32_t stride, const int32_t* keys,
+                                                           uint32_t mask, int shift, int32_t* bc,
+                                                           unsigned long long* cnt) {
+    const int lane = lane_id();
+    unsigned long long a_hits = 0;
+    for (int32_t g = g0; g < k; g += stride) {
+        const int32_t i = g + lane;
+        int32_t lb = 0, le = 0;
+        if (i < k) {
+            const int32_t b = ocol[ab + i];
+            lb = orp[b];
+            le = orp[b + 1];
+        }
+        unsigned med = __ballot_sync(0xffffffffu, le - lb >= 32);
+        while (med) {
+            const int leader = __ffs(med) - 1;
+            med &= med - 1;
+            const int32_t mb = __shfl_sync(0xffffffffu, lb, leader);
+            const int32_t me = __shfl_sync(0xffffffffu, le, leader);
+            unsigned hits = 0;
+            for (int32_t j = mb + lane; j < me; j += 32) {
+                const int32_t w = ocol[j];
+                if (tc_probe(keys, mask, shift, w)) {
+                    ++hits;
+                    atomicAdd(cnt + w, 1ull);
+                }
+            }
+            hits = warp_sum(hits);
+            if (lane == 0 && hits) {
+                atomicAdd(bc + g + leader, (int32_t)hits);
+                a_hits += hits;
+            }
+        }
+        if (le - lb >= 32) le = lb;
+        const int32_t d = le - lb;
+        int32_t incl = d;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += x;
+        }
+        const int32_t excl = incl - d;
+        const int32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        for (int32_t k0 = 0; k0 < total; k0 += 32) {
+            const int32_t kk = k0 + lane;
+            int owner = 0;
+#pragma unroll
+            for (int s = 16; s >= 1; s >>= 1) {
+                const int cand = owner + s;
+                const int32_t ev = __shfl_sync(0xffffffffu, excl, cand);
+                if (ev <= kk) owner = cand;
+            }
+            const int32_t ob = __shfl_sync(0xffffffffu, lb, owner);
+            const int32_t oe = __shfl_sync(0xffffffffu, excl, owner);
+            if (kk < total) {
+                const int32_t w = ocol[ob + (kk - oe)];
+                if (tc_probe(keys, mask, shift, w)) {
+                    atomicAdd(bc + g + owner, 1);
+                    atomicAdd(cnt + w, 1ull);
+                    ++a_hits;
+                }
+            }
+        }
+    }
+    return a_hits;
+}
+
+// Rows of 1..kTcWarpRow oriented entries, a warp each; longer rows are
+// listed for the block kernel (up to block_row <= kTcBlockRow entries) or
+// the galloping walk.
+__global__ void __launch_bounds__(kTcWarpBlock) tc_hash_warp_kernel(int32_t n, const int32_t* __restrict__ orp,
+                                                                    const int32_t* __restrict__ ocol,
+                                                                    unsigned long long* cnt, int32_t* lists,
+                                                                    int32_t* tails, int32_t block_row) {
+    __shared__ int32_t s_keys[kTcWarpBlock / 32][kTcWarpSlots];
+    __shared__ int32_t s_bc[kTcWarpBlock / 32][kTcWarpRow];
+    const int lane = lane_id();
+    int32_t* keys = s_keys[threadIdx.x >> 5];
+    int32_t* bc = s_bc[threadIdx.x >> 5];
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t a = warp; a < n; a += nwarps) {
+        const int32_t ab = orp[a], k = orp[a + 1] - ab;
+        if (k == 0) continue;
+        if (k > kTcWarpRow) {
+            if (lane == 0) {
+                if (k <= block_row) lists[atomicAdd(tails, 1)] = (int32_t)a;
+                else lists[n + atomicAdd(tails + 1, 1)] = (int32_t)a;
+            }
+            continue;
+        }
+        for (int s = lane; s < kTcWarpSlots; s += 32) keys[s] = -1;
+        for (int s = lane; s < k; s += 32) bc[s] = 0;
+        __syncwarp();
+        const int shift = 32 - 8;  // 256 slots
+        for (int32_t i = lane; i < k; i += 32) tc_insert(keys, kTcWarpSlots - 1, shift, ocol[ab + i]);
+        __syncwarp();
+        unsigned long long a_hits =
+            tc_row_share(orp, ocol, ab, k, 0, 32, keys, kTcWarpSlots - 1, shift, bc, cnt);
+        __syncwarp();
+        a_hits = warp_sum(a_hits);
+        if (lane == 0 && a_hits) atomicAdd(cnt + a, a_hits);
+        for (int32_t i = lane; i < k; i += 32)
+            if (bc[i]) atomicAdd(cnt + ocol[ab + i], (unsigned long long)bc[i]);
+        __syncwarp();
+    }
+}
+
+// Rows of kTcWarpRow+1 .. kTcBlockRow oriented entries (listed by the warp
+// kernel), a block each; dynamic shared memory: the hash (a power of two
+// >= 2k slots) and the per-entry counters.
+__global__ void __launch_bounds__(kTcBlockThreads) tc_hash_block_kernel(const int32_t* __restrict__ orp,
+                                                                        const int32_t* __restrict__ ocol,
+                                                                        unsigned long long* cnt,
+                                                                        const int32_t* __restrict__ rows,
+                                                                        const int32_t* count) {
+    extern __shared__ int32_t s_dyn[];
+    __shared__ unsigned long long s_hits;
+    const int32_t nrows = *count;
+    const int warp_in_block = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    for (int32_t r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int32_t a = rows[r];
+        const int32_t ab = orp[a], k = orp[a + 1] - ab;
+        int log2cap = 1;
+        while ((1 << log2cap) < 2 * k) ++log2cap;
+        const uint32_t cap = 1u << log2cap;
+        int32_t* keys = s_dyn;
+        int32_t* bc = s_dyn + cap;
+        for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) keys[s] = -1;
+        for (int32_t s = threadIdx.x; s < k; s += blockDim.x) bc[s] = 0;
+        if (threadIdx.x == 0) s_hits = 0;
+        __syncthreads();
+        const int shift = 32 - log2cap;
+        for (int32_t i = threadIdx.x; i < k; i += blockDim.x) tc_insert(keys, cap - 1, shift, ocol[ab + i]);
+        __syncthreads();
+        unsigned long long a_hits =
+            tc_row_share(orp, ocol, ab, k, warp_in_block * 32, warps * 32, keys, cap - 1, shift, bc, cnt);
+        a_hits = warp_sum(a_hits);
+        if (lane_id() == 0 && a_hits) atomicAdd(&s_hits, a_hits);
+        __syncthreads();
+        if (threadIdx.x == 0 && s_hits) atomicAdd(cnt + a, s_hits);
+        for (int32_t i = threadIdx.x; i < k; i += blockDim.x)
+            if (bc[i]) atomicAdd(cnt + ocol[ab + i], (unsigned long long)bc[i]);
+        __syncthreads();
+    }
+}
+
 // Triangles of the oriented CSR into cnt (zeroed by the caller): the
-// load-balanced walk over every oriented entry with the binary-search
-// visitor.  (A warp-per-row shared-memory hash variant measured 25 % slower
+// hash-probe kernels above, then the load-balanced walk with the galloping
+// visitor below for rows longer than kTcBlockRow.  `lists` holds 2n + 8
+// ints of scratch.  (A warp-per-row shared-memory hash variant measured 25 % slower
 // on RMAT scale 24: most oriented rows hold a few entries, so a warp per row
 // leaves most lanes idle, where the walker packs short rows warp-wide.
 // Handing the entries whose shorter list exceeds 32 to a warp each, through
@@ -209,9 +401,27 @@ struct OrientedVisitor {
 // 32-bit counters, twice as slow with 64-bit ones: the L2's same-address
 // reductions keep up better than a block's shared-memory atomics.)
 int tc_count_oriented(ghb_workspace* ws, int32_t n, const int32_t* orp, const int32_t* ocol, unsigned long long* cnt,
-                      const WalkBuffers& wb) {
-    return walk(ws, orp, ocol, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
-                OrientedVisitor{orp, ocol, cnt});
+                      const WalkBuffers& wb, int32_t* lists) {
+    if (!ws->tune.tc_hash)
+        return walk(ws, orp, ocol, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
+                    OrientedVisitor{orp, ocol, cnt});
+    int32_t* tails = lists + 2 * (size_t)n;
+    GHB_CUDA_TRY(cudaMemsetAsync(tails, 0, 2 * sizeof(int32_t), ws->stream));
+    GHB_TRY(launch(ws, tc_hash_warp_kernel, dim3(grid_for((int64_t)n * 32, kTcWarpBlock, ws->num_sms * 8)),
+                   dim3(kTcWarpBlock), 0, n, orp, ocol, cnt, lists, tails,
+                   std::min<int32_t>(std::max<int32_t>(ws->tune.tc_block_row, kTcWarpRow), kTcBlockRow)));
+    const size_t smem = sizeof(int32_t) * (size_t)(2 * kTcBlockRow + kTcBlockRow);
+    static bool attr_set[64] = {false};
+    if (ws->device >= 0 && ws->device < 64 && !attr_set[ws->device]) {
+        GHB_CUDA_TRY(cudaFuncSetAttribute(tc_hash_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+        attr_set[ws->device] = true;
+    }
+    GHB_TRY(launch(ws, tc_hash_block_kernel, dim3(ws->num_sms * 2), dim3(kTcBlockThreads), smem, orp, ocol, cnt,
+                   (const int32_t*)lists, (const int32_t*)tails));
+    // Rows over kTcBlockRow oriented entries: the galloping walk.
+    return walk(ws, orp, ocol, (const int32_t*)(lists + n), (const int32_t*)(tails + 1), (int64_t)0,
+                (int64_t)ws->num_sms * 64, wb, OrientedVisitor{orp, ocol, cnt});
 }
 
 // The reference's merge over every entry (any CSR).
@@ -274,6 +484,7 @@ size_t tc_oriented_bytes(int32_t n, int64_t m) {
     c.take<int32_t>((size_t)n + 1);
     c.take<int64_t>(scan_scratch_words(n));
     c.take<int32_t>(m > 0 ? m : 1);
+    c.take<int32_t>(2 * (size_t)n + 8);
     return c.off;
 }
 
@@ -286,6 +497,7 @@ int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* row
     int32_t* orp = c.take<int32_t>((size_t)n + 1);
     int64_t* bsums = c.take<int64_t>(scan_scratch_words(n));
     int32_t* ocol = c.take<int32_t>(m > 0 ? m : 1);
+    int32_t* lists = c.take<int32_t>(2 * (size_t)n + 8);
     GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * ((size_t)n + 1), st));
     GHB_CUDA_TRY(cudaMemsetAsync(keep, 0, sizeof(int32_t) * n, st));
     GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
@@ -295,7 +507,7 @@ int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* row
                    rowptr, col, (const int32_t*)orp, ocol));
     GHB_TRY(launch(ws, orient_fill_long_kernel, dim3(ws->num_sms), dim3(1024), 0, n, rowptr, col, (const int32_t*)orp,
                    ocol));
-    GHB_TRY(tc_count_oriented(ws, n, orp, ocol, cnt, wb));
+    GHB_TRY(tc_count_oriented(ws, n, orp, ocol, cnt, wb, lists));
     if (counts64)
         GHB_TRY(launch(ws, tc_finish_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n,
                        (const unsigned long long*)cnt, 6, counts64, (int32_t*)nullptr,
@@ -322,6 +534,7 @@ int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
     sizing.take<int32_t>((size_t)n + 1);
     sizing.take<int64_t>(scan_scratch_words(n));
     sizing.take<int32_t>(m > 0 ? m : 1);
+    sizing.take<int32_t>(2 * (size_t)n + 8);
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
     WalkBuffers wb = WalkBuffers::carve(c, n);
@@ -332,6 +545,7 @@ int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
     int32_t* orp = c.take<int32_t>((size_t)n + 1);
     int64_t* bsums = c.take<int64_t>(scan_scratch_words(n));
     int32_t* ocol = c.take<int32_t>(m > 0 ? m : 1);
+    int32_t* lists = c.take<int32_t>(2 * (size_t)n + 8);
 
     GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * n, st));
     GHB_CUDA_TRY(cudaMemsetAsync(tot, 0, sizeof(unsigned long long), st));
@@ -355,7 +569,7 @@ int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
                        n, rowptr, col, (const int32_t*)orp, ocol));
         GHB_TRY(launch(ws, orient_fill_long_kernel, dim3(ws->num_sms), dim3(1024), 0, n, rowptr, col,
                        (const int32_t*)orp, ocol));
-        GHB_TRY(tc_count_oriented(ws, n, orp, ocol, cnt, wb));
+        GHB_TRY(tc_count_oriented(ws, n, orp, ocol, cnt, wb, lists));
     } else {
         GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
                      MergeVisitor{rowptr, col, cnt}));

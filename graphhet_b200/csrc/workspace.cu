@@ -130,6 +130,9 @@ const TuneField kTuneFields[] = {
     {"pol_band", &ghb::Tuning::pol_band, 0, 64},
     {"barrier_limit_us", &ghb::Tuning::barrier_limit_us, 100, 60000000},
     {"barrier_extra", &ghb::Tuning::barrier_extra, 0, 1},
+    {"sssp_persistent", &ghb::Tuning::sssp_persistent, 0, 1},
+    {"tc_hash", &ghb::Tuning::tc_hash, 0, 1},
+    {"tc_block_row", &ghb::Tuning::tc_block_row, 128, 8192},
 };
 const TuneField* tune_field(const char* name) {
     if (!name) return nullptr;

@@ -22,6 +22,8 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <cstddef>
+#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -87,6 +89,99 @@ inline void parallel_rows(int n, F f) {
         }
     }
     for (auto& th : pool) th.join();
+}
+
+// Run f(part, begin, end) over `parts` equal slices of [0, n), one thread each.
+template <class F>
+inline void parallel_rows_parts(int n, unsigned parts, F f) {
+    if (parts <= 1) {
+        f(0u, 0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < parts; ++t) {
+        const int b = (int)((long long)n * t / parts), e = (int)((long long)n * (t + 1) / parts);
+        pool.emplace_back([=]() { f(t, b, e); });
+    }
+    for (auto& th : pool) th.join();
+}
+
+// Resident (degree-relabelled) copies of the CSR_graphs that the drop-in
+// algorithms run on (ghb_graph_create), built on a CSR_graph's first
+// algorithm call and kept until that CSR_graph releases its arrays, so the
+// reference's drivers reach the relabelled kernels without changing a line.
+// The reference has no counterpart: its entry points read the CSR arrays
+// directly on every call (e.g. GPU_BFS_csr.cuh:258-283).  Keyed on every
+// device array and the sizes; the arrays must not be rewritten in place
+// while the CSR_graph lives (the reference never does).
+struct ResidentEntry {
+    const void* key[6];
+    int vertices;
+    std::size_t entries;
+    ghb_graph* graph;
+};
+
+inline std::mutex& resident_mutex() {
+    static std::mutex m;
+    return m;
+}
+
+inline std::vector<ResidentEntry>& resident_entries() {
+    static std::vector<ResidentEntry> v;
+    return v;
+}
+
+// Drops (and frees) the resident copies built from the CSR whose out-row
+// array is out_pointer.
+inline void resident_forget(const void* out_pointer) {
+    if (!out_pointer) return;
+    std::lock_guard<std::mutex> lock(resident_mutex());
+    auto& es = resident_entries();
+    for (std::size_t i = 0; i < es.size();) {
+        if (es[i].key[0] == out_pointer) {
+            ghb_graph_destroy(es[i].graph);
+            es.erase(es.begin() + (std::ptrdiff_t)i);
+        } else {
+            ++i;
+        }
+    }
+}
+
+// The resident copy of a CSR (built on first use; NULL after a failure,
+// which is printed).  in_* equal to out_* (or NULL) means undirected.
+inline ghb_graph* resident_graph(ghb_workspace* ws, int vertices, std::size_t entries, const int* out_p,
+                                 const int* out_e, const double* out_w, const int* in_p, const int* in_e,
+                                 const double* in_w) {
+    const void* key[6] = {out_p, out_e, out_w, in_p, in_e, in_w};
+    std::lock_guard<std::mutex> lock(resident_mutex());
+    auto& es = resident_entries();
+    for (auto& e : es) {
+        bool same = e.vertices == vertices && e.entries == entries;
+        for (int k = 0; k < 6 && same; ++k) same = e.key[k] == key[k];
+        if (same) return e.graph;
+    }
+    // A new CSR at an address of an old one: the old copy is stale.
+    for (std::size_t i = 0; i < es.size();) {
+        if (es[i].key[0] == out_p) {
+            ghb_graph_destroy(es[i].graph);
+            es.erase(es.begin() + (std::ptrdiff_t)i);
+        } else {
+            ++i;
+        }
+    }
+    ghb_graph* g = nullptr;
+    const bool undirected = in_p == nullptr || in_p == out_p;
+    const int status = ghb_graph_create(ws, vertices, out_p, entries ? out_e : nullptr, entries ? out_w : nullptr,
+                                        undirected ? nullptr : in_p, undirected ? nullptr : in_e,
+                                        undirected ? nullptr : in_w, &g);
+    if (!ghb_ok(status, "ghb_graph_create")) return nullptr;
+    ResidentEntry e;
+    for (int k = 0; k < 6; ++k) e.key[k] = key[k];
+    e.vertices = vertices;
+    e.entries = entries;
+    e.graph = g;
+    es.push_back(e);
+    return g;
 }
 
 }  // namespace ghb_dropin
@@ -158,6 +253,7 @@ private:
 
     void release() {
         using namespace ghb_dropin;
+        resident_forget(out_pointer);
         if (is_directed) {
             device_free(in_pointer);
             device_free(in_edge);

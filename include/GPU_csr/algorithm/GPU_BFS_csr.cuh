@@ -1,6 +1,8 @@
 // GPU_BFS_csr.cuh - drop-in Cuda_BFS / csr_bfs (reference:
 // include/GPU_csr/algorithm/GPU_BFS_csr.cuh:13, 258-334) over libghb's
-// direction-optimising BFS (ghb_bfs).  Depth of unreached vertices: INT_MAX.
+// direction-optimising BFS: Cuda_BFS on the CSR_graph's resident relabelled
+// copy (ghb_graph_bfs), csr_bfs on the raw arrays it is given (ghb_bfs).
+// Depth of unreached vertices: INT_MAX.
 #pragma once
 
 #include <climits>
@@ -37,11 +39,11 @@ inline std::vector<std::pair<std::string, int>> Cuda_BFS(graph_structure<double>
     const int V = graph.V;
     const int src = graph.vertex_str_to_id[src_v];
     std::vector<int> depth;
-    DeviceBuffer<int> d((std::size_t)V);
-    // The in-CSR (aliasing the out-CSR when undirected) enables bottom-up levels.
-    if (ghb_ok(ghb_bfs(workspace(), V, csr_graph.out_pointer, csr_graph.out_edge, csr_graph.in_pointer,
-                       csr_graph.in_edge, src, max_depth, d.p, nullptr, nullptr),
-               "ghb_bfs"))
-        d.to_host(depth);
-    return graph.res_trans_id_val(depth);
+    // The CSR_graph's resident relabelled copy (built on its first call; the
+    // in-CSR, aliasing the out-CSR when undirected, enables bottom-up levels).
+    ghb_graph* g = resident(csr_graph, V);
+    int* d = result_buffer<int>((std::size_t)V);
+    if (g && d && ghb_ok(ghb_graph_bfs(workspace(), g, src, max_depth, d, nullptr, nullptr), "ghb_graph_bfs"))
+        result_to_host(d, (std::size_t)V, depth);
+    return trans_id_val(graph, depth);
 }

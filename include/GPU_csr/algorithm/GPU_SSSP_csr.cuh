@@ -1,7 +1,9 @@
 // GPU_SSSP_csr.cuh - drop-in Cuda_SSSP / csr_sssp (reference:
 // include/GPU_csr/algorithm/GPU_SSSP_csr.cuh:253-327) over libghb's FP64
-// delta-stepping (ghb_sssp).  Unreached vertices get INF (LDBC passes
-// DBL_MAX).  The distances equal the CPU Dijkstra's bit for bit.
+// delta-stepping: Cuda_SSSP on the CSR_graph's resident relabelled copy
+// (ghb_graph_sssp), csr_sssp on the raw arrays it is given (ghb_sssp).
+// Unreached vertices get INF (LDBC passes DBL_MAX).  The distances equal the
+// CPU Dijkstra's bit for bit.
 #pragma once
 
 #include <string>
@@ -29,10 +31,14 @@ inline std::vector<double> csr_sssp(int* keys, double* values, int* row_offsets,
 inline std::vector<std::pair<std::string, double>> Cuda_SSSP(graph_structure<double>& graph,
                                                              CSR_graph<double>& csr_graph, std::string src_v,
                                                              double max_dis) {
+    using namespace ghb_dropin;
     const int V = (int)csr_graph.OUTs_Neighbor_start_pointers.size() - 1;
-    const int E = (int)csr_graph.OUTs_Edges.size();
     const int src = graph.vertex_str_to_id[src_v];
-    std::vector<double> d = csr_sssp(csr_graph.out_edge, csr_graph.out_edge_weight, csr_graph.out_pointer,
-                                     (SIZE_TYPE)V, (SIZE_TYPE)E, (SIZE_TYPE)src, max_dis);
-    return graph.res_trans_id_val(d);
+    std::vector<double> d;
+    ghb_graph* g = resident(csr_graph, V);
+    double* dist = result_buffer<double>((std::size_t)V);
+    if (g && dist &&
+        ghb_ok(ghb_graph_sssp(workspace(), g, src, max_dis, dist, nullptr, nullptr), "ghb_graph_sssp"))
+        result_to_host(dist, (std::size_t)V, d);
+    return trans_id_val(graph, d);
 }

@@ -1,5 +1,7 @@
 // GPU_TC_csr.cuh - drop-in Cuda_TC / Cuda_TC_PerNode (reference:
-// include/GPU_csr/algorithm/GPU_TC_csr.cuh:46-68) over ghb_tc: the
+// include/GPU_csr/algorithm/GPU_TC_csr.cuh:46-68): Cuda_TC over ghb_graph_tc on
+// the CSR_graph's resident relabelled copy, Cuda_TC_PerNode over ghb_tc on
+// the raw arrays it is given: the
 // reference's per-vertex counts (6 x triangles on a symmetric graph), in its
 // wrapping int32.
 #pragma once
@@ -23,6 +25,11 @@ inline std::vector<int> Cuda_TC_PerNode(int* d_row_offsets, int* d_col_indices, 
 
 inline std::vector<std::pair<std::string, int>> Cuda_TC(graph_structure<double>& graph,
                                                         CSR_graph<double>& csr_graph) {
-    std::vector<int> c = Cuda_TC_PerNode(csr_graph.out_pointer, csr_graph.out_edge, graph.V);
-    return graph.res_trans_id_val(c);
+    using namespace ghb_dropin;
+    std::vector<int> c;
+    ghb_graph* g = resident(csr_graph, graph.V);
+    int* counts = result_buffer<int>((std::size_t)graph.V);
+    if (g && counts && ghb_ok(ghb_graph_tc(workspace(), g, nullptr, counts, nullptr), "ghb_graph_tc"))
+        result_to_host(counts, (std::size_t)graph.V, c);
+    return trans_id_val(graph, c);
 }

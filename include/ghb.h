@@ -71,7 +71,12 @@ ghb_workspace* ghb_default_workspace(void);
  * policy's network chooses a BFS level's direction and output format (0:
  * never; 64: always), "barrier_limit_us" (100 - 60,000,000; default
  * 2,000,000) how long a persistent kernel's grid-barrier wait lasts before
- * it gives up and the call returns GHB_ERR_TIMEOUT.
+ * it gives up and the call returns GHB_ERR_TIMEOUT, "sssp_persistent" (0 or
+ * 1; default 1) whether SSSP runs as one cooperative launch per traversal
+ * or as host-driven rounds, "tc_hash" (0 or 1; default 1) whether triangle
+ * counting probes a shared-memory hash of each oriented row or gallops
+ * through sorted rows, "tc_block_row" (128 - 8192; default 8192) the longest
+ * oriented row the hash path takes (longer rows gallop).
  * Results do not depend on them.  "barrier_extra" (0 or 1) is a test knob:
  * 1 makes every grid barrier of the persistent kernels wait for one arrival
  * more than there are blocks, so every wait runs out after barrier_limit_us

@@ -446,9 +446,10 @@ def test_mssssp_matches_single_source(G, count):
 
 
 def test_tc_complete_graph_long_oriented_rows(G):
-    """K_1060: the oriented rows of the first vertices exceed the warp hash
-    kernel's 1,024 entries (binary-search path), the rest take the hash
-    path; every vertex is in C(1059, 2) triangles (the reference counts 6x)."""
+    """K_1060: oriented rows of 0..1059 entries, so every hash path runs
+    (warp hash up to 128 entries, block hash above), and with the block
+    path capped at 200 entries the longest rows take the galloping walk;
+    every vertex is in C(1059, 2) triangles (the reference counts 6x)."""
     n = 1060
     iu = torch.triu_indices(n, n, 1)
     src, dst = iu[0].int().cuda(), iu[1].int().cuda()
@@ -461,3 +462,25 @@ def test_tc_complete_graph_long_oriented_rows(G):
     rg = G.ResidentGraph(g)
     c64, c32, total = rg.tc()
     assert total == triangles and bool((c32 == per_vertex).all())
+    ws = G.Workspace()
+    for knob, value in (("tc_block_row", 200), ("tc_hash", 0)):
+        G.tune_set(knob, value, ws=ws)
+        c64, c32, total = G.tc(g, ws=ws)
+        assert total == triangles and bool((c32 == per_vertex).all()), knob
+
+
+def test_tc_hash_paths_match_oracle(G):
+    """Oriented hash-probe TC against the oracle on RMAT (hub rows over the
+    warp hash's 128 entries) and a sparse ER graph, with and without the
+    block path, and against the galloping path."""
+    for og in (O.rmat_graph(14, 16, 3, directed=False, weight_mode=0),
+               O.make_graph(20000, *O.er_edges(20000, 60000, 8), False, weight_mode=0)):
+        g = to_gpu(G, og)
+        ref = O.tc(og)
+        ws = G.Workspace()
+        for knob, value in ((None, None), ("tc_block_row", 128), ("tc_hash", 0)):
+            if knob:
+                G.tune_set(knob, value, ws=ws)
+            c64, c32, total = G.tc(g, ws=ws)
+            assert np.array_equal(c32.cpu().numpy(), ref), knob
+            assert int(c64.sum()) == 18 * total

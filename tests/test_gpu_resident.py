@@ -115,6 +115,39 @@ def test_resident_sssp_light_heavy_deltas(G):
         assert np.array_equal(rg.sssp(77, delta=delta)[0].cpu().numpy(), O.sssp(og, 77))
 
 
+def test_sssp_one_launch_matches_host_rounds_and_oracle(G):
+    """The whole-traversal SSSP launch against the host-driven rounds and the
+    oracle: hubs whose light and heavy ranges span many 1024-entry chunks,
+    widths from below every weight (a split per settled distance) to above
+    all of them, raw CSR and resident graph, and its pass counters."""
+    scale = 14
+    base = 1 << scale
+    s, d = O.rmat_edges(scale, 8 << scale, 23)
+    rng = np.random.default_rng(5)
+    hs, hd = [s], [d]
+    for k, deg in enumerate((1023, 1025, 3000, 9000)):
+        hs.append(np.full(deg, base + k, np.int32))
+        hd.append(rng.choice(base, size=deg, replace=False).astype(np.int32))
+    og = O.make_graph(base + 4, np.concatenate(hs), np.concatenate(hd), False, weight_mode=1, weight_seed=8)
+    g = to_gpu(G, og)
+    ws = G.Workspace()
+    rg = G.ResidentGraph(g, ws=ws)
+    for src in (base + 3, base + 1, int(np.argmax(np.diff(og.rowptr)))):
+        ref = O.sssp(og, src)
+        for delta in (1e-6, 0.02, 0.4, 3.0):
+            d1, st1 = rg.sssp(src, delta=delta, ws=ws)
+            assert np.array_equal(d1.cpu().numpy(), ref), (src, delta)
+            d2, _ = G.sssp(g, src, delta=delta, ws=ws)
+            assert np.array_equal(d2.cpu().numpy(), ref), (src, delta)
+            assert st1["levels"] >= 1 and st1["edges_examined"] >= st1["edges_reached"]
+        G.tune_set("sssp_persistent", 0, ws=ws)
+        d3, _ = rg.sssp(src, ws=ws)
+        d4, _ = G.sssp(g, src, ws=ws)
+        G.tune_set("sssp_persistent", 1, ws=ws)
+        assert np.array_equal(d3.cpu().numpy(), ref) and np.array_equal(d4.cpu().numpy(), ref)
+    rg.close()
+
+
 def test_resident_cdlp_and_wcc_with_repeated_entries(G):
     """A symmetric CSR whose rows repeat some entries (so label counts of 2
     occur in the first CDLP iteration) and a directed graph: CDLP and WCC on

@@ -64,3 +64,24 @@ def test_barrier_knobs_are_range_checked(G):
         G.tune_set("barrier_limit_us", 10, ws=ws)
     assert G.tune_get("barrier_limit_us", ws=ws) == 2000000
     assert G.tune_get("barrier_extra", ws=ws) == 0
+
+
+def test_sssp_barrier_timeout_then_recovers(G):
+    og = O.rmat_graph(12, 16, 42, directed=False)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    g = G.CSRGraph(n=og.n, rowptr=t(og.rowptr), col=t(og.col), w=t(og.w), directed=False)
+    ws = G.Workspace()
+    rg = G.ResidentGraph(g, ws=ws)
+    src = int(np.argmax(np.diff(og.rowptr)))
+    G.tune_set("barrier_limit_us", 1000, ws=ws)
+    G.tune_set("barrier_extra", 1, ws=ws)
+    for call in (lambda: rg.sssp(src, ws=ws), lambda: G.sssp(g, src, ws=ws)):
+        with pytest.raises(G.GhbError, match="timed out"):
+            call()
+    torch.cuda.synchronize()
+    G.tune_set("barrier_extra", 0, ws=ws)
+    G.tune_set("barrier_limit_us", 2000000, ws=ws)
+    ref = O.sssp(og, src)
+    assert np.array_equal(rg.sssp(src, ws=ws)[0].cpu().numpy(), ref)
+    assert np.array_equal(G.sssp(g, src, ws=ws)[0].cpu().numpy(), ref)
+    rg.close()
