@@ -116,6 +116,8 @@ _SIGS = {
     "ghb_graph_bfs": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p]),
     "ghb_graph_bfs_pred": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p, _p]),
     "ghb_graph_msbfs": (ctypes.c_int, [_p, _p, _p, _i32, _p, _p]),
+    "ghb_graph_msbfs_reserve": (ctypes.c_int, [_p, _p, _i32]),
+    "ghb_graph_msbfs_launch": (ctypes.c_int, [_p, _p, _p, _i32, _p]),
     "ghb_graph_sssp": (ctypes.c_int, [_p, _p, _i32, _f64, _p, _p, _p]),
     "ghb_graph_mssssp": (ctypes.c_int, [_p, _p, _p, _i32, _f64, _p, _p]),
     "ghb_graph_sssp_pred": (ctypes.c_int, [_p, _p, _i32, _f64, _p, _p, _p, _p]),
@@ -663,6 +665,17 @@ class ResidentGraph:
         _check(lib().ghb_graph_msbfs(_ws(ws), self._h, _ptr(sd), len(sd), _ptr(depth), ctypes.byref(st)),
                "ghb_graph_msbfs")
         return depth[: len(sd) * self.n].view(len(sd), self.n), st.as_dict()
+
+    def msbfs_reserve(self, n_src, ws=None):
+        """Size the workspace for msbfs_launch with up to n_src sources."""
+        _check(lib().ghb_graph_msbfs_reserve(_ws(ws), self._h, int(n_src)), "ghb_graph_msbfs_reserve")
+
+    def msbfs_launch(self, srcs_dev, out, ws=None):
+        """Launch-only multi-source BFS (one cooperative launch per 256
+        sources; recordable in a CUDA graph): srcs_dev is an int32 device
+        tensor, out an int32 device tensor of len(srcs_dev) * n entries."""
+        _check(lib().ghb_graph_msbfs_launch(_ws(ws), self._h, _ptr(srcs_dev), srcs_dev.numel(), _ptr(out)),
+               "ghb_graph_msbfs_launch")
 
     def mssssp(self, srcs, inf=DBL_MAX, out=None, ws=None):
         """Distances from every source (n_src x n), passes of up to 256."""

@@ -76,6 +76,7 @@ struct Tuning {
     int32_t sssp_persistent = 1;   // SSSP: 1 = one cooperative launch per traversal, 0 = host-driven rounds
     int32_t tc_hash = 1;           // TC: 1 = shared-memory hash probes per oriented row, 0 = galloping merges
     int32_t tc_block_row = 8192;   // TC hash path: longest oriented row a block hashes; longer rows gallop
+    int32_t ms_persistent = 1;     // multi-source BFS: 1 = one cooperative launch per pass, 0 = host-driven levels
 };
 
 }  // namespace ghb

@@ -51,6 +51,12 @@ int pagerank_run(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int32
 int msbfs_batch(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* out_rp, const int32_t* out_col,
                 const int32_t* in_rp, const int32_t* in_col, const int32_t* srcs_dev, int32_t k,
                 const int32_t* perm, int32_t* depth, int64_t* levels_out, int64_t* examined_out);
+size_t msbfs_persistent_bytes(int32_t n, int64_t m, int32_t n_src);
+bool msbfs_persistent_available(ghb_workspace* ws, int32_t n_src);
+int msbfs_persistent(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, const int32_t* out_rp,
+                     const int32_t* out_col, const int32_t* in_rp, const int32_t* in_col, const int32_t* srcs,
+                     int32_t n_src, const int32_t* perm, int32_t* depth, bool finish, int64_t* levels_out,
+                     int64_t* examined_out);
 
 namespace {
 
@@ -163,6 +169,28 @@ int ghb_graph_msbfs(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, 
         GHB_REQUIRE(hs[i] >= 0 && hs[i] < g->n, "source outside [0, n)");
         hs[i] = g->perm_host[hs[i]];
     }
+    if (n_src > 0 && msbfs_persistent_available(ws, n_src)) {
+        // One cooperative launch per pass; the kernel maps the caller's
+        // sources and writes depths in the caller's ids through perm.
+        int64_t levels = 0, examined = 0;
+        GHB_TRY(ws_reserve(ws, msbfs_persistent_bytes(g->n, g->m, n_src)));
+        if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
+        GHB_TRY(msbfs_persistent(ws, g->n, g->n_active, g->m, g->rowptr, g->col, g->in_rowptr, g->in_col, srcs, n_src,
+                                 (const int32_t*)g->perm, depth, true, &levels, &examined));
+        if (stats) {
+            GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
+            GHB_CUDA_TRY(cudaEventSynchronize(ws->ev_stop));
+            float ms = 0.f;
+            GHB_CUDA_TRY(cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop));
+            stats->levels = (int32_t)levels;
+            stats->pull_levels = 0;
+            stats->reached = -1;
+            stats->edges_reached = -1;
+            stats->edges_examined = examined;
+            stats->device_ms = ms;
+        }
+        return GHB_OK;
+    }
     // Sources in the graph's ids; depths go straight to the caller's rows.
     GHB_TRY(ws_reserve_stage(ws, sizeof(int32_t) * kMsPass));
     int32_t* snew = static_cast<int32_t*>(ws->stage);
@@ -188,6 +216,28 @@ int ghb_graph_msbfs(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, 
         stats->device_ms = ms;
     }
     return GHB_OK;
+}
+
+int ghb_graph_msbfs_reserve(ghb_workspace* ws, const ghb_graph* g, int32_t n_src) {
+    GRAPH_PRELUDE();
+    GHB_REQUIRE(n_src >= 1, "n_src must be >= 1");
+    if (!msbfs_persistent_available(ws, n_src)) {
+        set_error("whole-pass multi-source BFS unavailable (no cooperative launch, or ms_persistent = 0)");
+        return GHB_ERR_UNSUPPORTED;
+    }
+    return ws_reserve(ws, msbfs_persistent_bytes(g->n, g->m, n_src));
+}
+
+int ghb_graph_msbfs_launch(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
+                           int32_t* depth) {
+    GRAPH_PRELUDE();
+    GHB_REQUIRE(srcs && depth && n_src >= 1, "bad arguments");
+    if (!msbfs_persistent_available(ws, n_src)) {
+        set_error("whole-pass multi-source BFS unavailable (no cooperative launch, or ms_persistent = 0)");
+        return GHB_ERR_UNSUPPORTED;
+    }
+    return msbfs_persistent(ws, g->n, g->n_active, g->m, g->rowptr, g->col, g->in_rowptr, g->in_col, srcs, n_src,
+                            (const int32_t*)g->perm, depth, false, nullptr, nullptr);
 }
 
 int ghb_graph_mssssp(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src, double inf,

@@ -133,6 +133,7 @@ const TuneField kTuneFields[] = {
     {"sssp_persistent", &ghb::Tuning::sssp_persistent, 0, 1},
     {"tc_hash", &ghb::Tuning::tc_hash, 0, 1},
     {"tc_block_row", &ghb::Tuning::tc_block_row, 128, 8192},
+    {"ms_persistent", &ghb::Tuning::ms_persistent, 0, 1},
 };
 const TuneField* tune_field(const char* name) {
     if (!name) return nullptr;

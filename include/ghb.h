@@ -76,7 +76,9 @@ ghb_workspace* ghb_default_workspace(void);
  * or as host-driven rounds, "tc_hash" (0 or 1; default 1) whether triangle
  * counting probes a shared-memory hash of each oriented row or gallops
  * through sorted rows, "tc_block_row" (128 - 8192; default 8192) the longest
- * oriented row the hash path takes (longer rows gallop).
+ * oriented row the hash path takes (longer rows gallop), "ms_persistent" (0
+ * or 1; default 1) whether a multi-source BFS pass is one cooperative launch
+ * or host-driven levels.
  * Results do not depend on them.  "barrier_extra" (0 or 1) is a test knob:
  * 1 makes every grid barrier of the persistent kernels wait for one arrival
  * more than there are blocks, so every wait runs out after barrier_limit_us
@@ -356,6 +358,20 @@ int ghb_graph_bfs_pred(ghb_workspace* ws, const ghb_graph* g, int32_t src, int32
                        ghb_traversal_stats* stats);
 int ghb_graph_msbfs(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
                     int32_t* depth, ghb_traversal_stats* stats);
+/* The same multi-source BFS as launches only, for CUDA-graph capture (no
+ * counterpart in the reference, which runs one source per call): each pass
+ * of up to 256 sources is one cooperative launch that runs every level, its
+ * direction choices and the depth output on the device, with no host
+ * round trip and no allocation.  Call ghb_graph_msbfs_reserve once (outside
+ * any capture) with the largest n_src to size the workspace; a launch whose
+ * workspace is too small fails with GHB_ERR_INVALID_ARGUMENT.  Sources are
+ * caller ids on the device and are not checked on the host: a source
+ * outside [0, n) is skipped and its depth row is all INT32_MAX.  A grid
+ * barrier that times out leaves the pass's output incomplete without a
+ * status (ghb_graph_msbfs reports it). */
+int ghb_graph_msbfs_reserve(ghb_workspace* ws, const ghb_graph* g, int32_t n_src);
+int ghb_graph_msbfs_launch(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
+                           int32_t* depth);
 int ghb_graph_mssssp(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
                      double inf, double* dist, ghb_traversal_stats* stats);
 int ghb_graph_sssp(ghb_workspace* ws, const ghb_graph* g, int32_t src, double inf, double* dist,

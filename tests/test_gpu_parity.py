@@ -347,6 +347,54 @@ def test_msbfs_long_diameter(G, count):
     rg.close()
 
 
+def test_msbfs_one_launch_pass_and_graph_replay(G):
+    """A 256-source pass as one cooperative launch: equal to the host-driven
+    levels and to single-source runs, with a hub of 5,000 leaves (push rows
+    cut into chunks) and isolated / duplicate sources; then the launch-only
+    entry recorded in a CUDA graph and replayed twice, bit-exact."""
+    scale = 13
+    s, d = O.rmat_edges(scale, 8 << scale, 77)
+    hub = np.full(5000, 9, np.int32)
+    leaves = np.arange(100, 5100, dtype=np.int32)
+    og = O.make_graph(1 << scale, np.concatenate([s, hub]), np.concatenate([d, leaves]), False)
+    g = to_gpu(G, og)
+    rng = np.random.default_rng(11)
+    srcs = rng.integers(0, og.n, 256).astype(np.int32)
+    srcs[1] = srcs[0]
+    srcs[2] = 9
+    iso = np.nonzero(np.diff(og.rowptr) == 0)[0]
+    if iso.size:
+        srcs[3] = iso[0]
+    ws = G.Workspace()
+    rg = G.ResidentGraph(g, ws=ws)
+    one, st1 = rg.msbfs(srcs, ws=ws)
+    one = one.cpu().numpy()
+    G.tune_set("ms_persistent", 0, ws=ws)
+    host = rg.msbfs(srcs, ws=ws)[0].cpu().numpy()
+    G.tune_set("ms_persistent", 1, ws=ws)
+    assert np.array_equal(one, host)
+    assert st1["levels"] >= 1
+    for i in (0, 1, 2, 3, 64, 128, 200, 255):
+        assert np.array_equal(one[i], O.bfs(og, int(srcs[i]))), i
+    # Launch-only entry, captured in a CUDA graph on a side stream.
+    sd = torch.from_numpy(srcs).cuda()
+    out = torch.full((256 * og.n,), -5, dtype=torch.int32, device="cuda")
+    rg.msbfs_reserve(256, ws=ws)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(graph, stream=side):
+            rg.msbfs_launch(sd, out, ws=ws)
+    for _ in range(2):
+        out.fill_(-5)
+        graph.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().reshape(256, og.n), one)
+    del graph
+    rg.close()
+
+
 def test_union_batch_wcc_tc_and_graph_capture(G):
     """Many ER graphs as one disjoint-union CSR: WCC labels and triangle
     counts equal the oracle's per graph; the launch-only call recorded in a
