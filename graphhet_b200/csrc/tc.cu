@@ -47,6 +47,16 @@ __device__ __forceinline__ int32_t lower_bound_from(const int32_t* __restrict__ 
     return b;
 }
 
+// First position in [b, e) of a sorted row whose entry is > x (e if none).
+__device__ __forceinline__ int32_t upper_bound_pos(const int32_t* __restrict__ col, int32_t b, int32_t e, int32_t x) {
+    while (b < e) {
+        const int32_t mid = b + ((e - b) >> 1);
+        if (col[mid] <= x) b = mid + 1;
+        else e = mid;
+    }
+    return b;
+}
+
 __device__ __forceinline__ bool row_contains(const int32_t* __restrict__ col, int32_t b, int32_t e, int32_t x) {
     while (b < e) {
         const int32_t mid = (b + e) >> 1;
@@ -245,6 +255,7 @@ __device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __rest
                                                            unsigned long long* cnt) {
     const int lane = lane_id();
     unsigned long long a_hits = 0;
+    const int32_t amin = ocol[ab], amax = ocol[ab + k - 1];
     for (int32_t g = g0; g < k; g += stride) {
         const int32_t i = g + lane;
         int32_t lb = 0, le = 0;
@@ -252,6 +263,10 @@ __device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __rest
             const int32_t b = ocol[ab + i];
             lb = orp[b];
             le = orp[b + 1];
+            // Only N+(b)'s entries inside [min N+(a), max N+(a)] can be in
+            // N+(a) (both rows ascending): cut the rest off first.
+            lb = lower_bound_from(ocol, lb, le, amin);
+            le = upper_bound_pos(ocol, lb, le, amax);
         }
         unsigned med = __ballot_sync(0xffffffffu, le - lb >= 32);
         while (med) {
