@@ -418,6 +418,96 @@ def regret(rg, sources: Sequence[int], repeats: int = 3) -> Dict[str, float]:
                 regret_beamer14=tot["beamer14"] / o - 1.0)
 
 
+def collect_sssp(specs: Sequence[GraphSpec], sssp_max_scale: int = 22, sssp_sources: int = 3,
+                 log=print) -> Dict[str, np.ndarray]:
+    """Width-head rows only (sssp_rows on every graph of `specs` up to
+    sssp_max_scale), timed with the current SSSP kernels; G[i] is the index
+    of the graph that row i came from."""
+    import torch
+    import graphhet_b200 as G
+    Xs, Ls, Ws, Gs = [], [], [], []
+    t0 = time.time()
+    for gi, spec in enumerate(specs):
+        if spec.scale > sssp_max_scale:
+            continue
+        g = build_graph(spec)
+        rg = G.ResidentGraph(g)
+        srcs = pick_sources(g, sssp_sources, spec.seed)
+        out = sssp_rows(rg, srcs) if srcs else None
+        if out is not None:
+            f, lab, wt, _ = out
+            Xs.append(f)
+            Ls.append(np.full(len(f), lab, np.int32))
+            Ws.append(np.full(len(f), wt, np.float32))
+            Gs.append(np.full(len(f), gi, np.int32))
+        rg.close()
+        del rg, g
+        torch.cuda.empty_cache()
+        if log and (gi % 20 == 0 or gi == len(specs) - 1):
+            log("graph %d/%d %s scale %d (%.0f s)" % (gi + 1, len(specs), spec.kind, spec.scale, time.time() - t0))
+    return dict(X=np.concatenate(Xs).astype(np.float32), L=np.concatenate(Ls), W=np.concatenate(Ws),
+                G=np.concatenate(Gs))
+
+
+def hidden(params: np.ndarray, norm: np.ndarray, X: np.ndarray) -> np.ndarray:
+    """The network's second hidden layer (ReLU) for rows X, on the host."""
+    p = params.astype(np.float64)
+    o = 0
+    W1 = p[o:o + 12 * 64].reshape(12, 64); o += 12 * 64
+    b1 = p[o:o + 64]; o += 64
+    W2 = p[o:o + 64 * 64].reshape(64, 64); o += 64 * 64
+    b2 = p[o:o + 64]
+    x = (X.astype(np.float64) - norm[:12]) * norm[12:]
+    h1 = np.maximum(x @ W1 + b1, 0.0)
+    return np.maximum(h1 @ W2 + b2, 0.0)
+
+
+def refit_width_head(params: np.ndarray, norm: np.ndarray, X: np.ndarray, L: np.ndarray, W: np.ndarray,
+                     epochs: int = 4000, lr: float = 1e-2, l2: float = 1e-4) -> np.ndarray:
+    """New weights for the width head only: weighted softmax regression of
+    the labels L (bins 0..15) on the fixed hidden layer, by Adam on the host.
+    The BFS heads and the shared layers keep their values, so every BFS
+    decision of the network is unchanged."""
+    H = hidden(params, norm, X)
+    n, k = H.shape[0], DELTA_BINS
+    o3 = 12 * 64 + 64 + 64 * 64 + 64
+    W3 = params[o3:o3 + 64 * 20].astype(np.float64).reshape(64, 20)
+    b3 = params[o3 + 64 * 20:o3 + 64 * 20 + 20].astype(np.float64)
+    A, c = W3[:, 4:20].copy(), b3[4:20].copy()
+    Y = np.zeros((n, k))
+    Y[np.arange(n), L] = 1.0
+    w = (W / W.mean()).reshape(-1, 1)
+    mA, vA, mc, vc = np.zeros_like(A), np.zeros_like(A), np.zeros_like(c), np.zeros_like(c)
+    for t in range(1, epochs + 1):
+        z = H @ A + c
+        z -= z.max(1, keepdims=True)
+        pz = np.exp(z)
+        pz /= pz.sum(1, keepdims=True)
+        g = (pz - Y) * w / n
+        gA = H.T @ g + l2 * A
+        gc = g.sum(0)
+        for prm, grd, m1, m2 in ((A, gA, mA, vA), (c, gc, mc, vc)):
+            m1 *= 0.9
+            m1 += 0.1 * grd
+            m2 *= 0.999
+            m2 += 0.001 * grd * grd
+            prm -= lr * (m1 / (1 - 0.9 ** t)) / (np.sqrt(m2 / (1 - 0.999 ** t)) + 1e-8)
+    out = params.astype(np.float32).copy()
+    W3[:, 4:20] = A
+    b3[4:20] = c
+    out[o3:o3 + 64 * 20] = W3.reshape(-1).astype(np.float32)
+    out[o3 + 64 * 20:o3 + 64 * 20 + 20] = b3.astype(np.float32)
+    return out
+
+
+def width_accuracy(params, norm, X, L) -> float:
+    H = hidden(params, norm, X)
+    o3 = 12 * 64 + 64 + 64 * 64 + 64
+    W3 = params[o3:o3 + 64 * 20].astype(np.float64).reshape(64, 20)
+    b3 = params[o3 + 64 * 20:o3 + 64 * 20 + 20].astype(np.float64)
+    return float(((H @ W3[:, 4:20] + b3[4:20]).argmax(1) == L).mean())
+
+
 def main(argv=None) -> int:
     import argparse
     import torch
@@ -427,7 +517,32 @@ def main(argv=None) -> int:
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--out", default=WEIGHTS_PATH)
     ap.add_argument("--data", default=None, help="save / reuse the collected rows (.npz)")
+    ap.add_argument("--refit-width", action="store_true",
+                    help="re-time the SSSP widths on the training graphs with the current kernels and refit the "
+                         "width head of the installed network (the BFS heads are kept)")
     a = ap.parse_args(argv)
+    if a.refit_width:
+        params, norm, info = load(WEIGHTS_PATH)
+        if a.data and os.path.exists(a.data):
+            z = np.load(a.data)
+            d = dict(X=z["X"], L=z["L"], W=z["W"], G=z["G"])
+        else:
+            d = collect_sssp(training_specs(a.graphs))
+            if a.data:
+                np.savez(a.data, **d)
+        val = d["G"] % 10 == 0  # every tenth graph held out
+        p_tr = refit_width_head(params, norm, d["X"][~val], d["L"][~val], d["W"][~val])
+        acc = dict(before_train=width_accuracy(params, norm, d["X"][~val], d["L"][~val]),
+                   before_val=width_accuracy(params, norm, d["X"][val], d["L"][val]),
+                   after_train=width_accuracy(p_tr, norm, d["X"][~val], d["L"][~val]),
+                   after_val=width_accuracy(p_tr, norm, d["X"][val], d["L"][val]))
+        p_all = refit_width_head(params, norm, d["X"], d["L"], d["W"])
+        info = dict(info, width_refit=dict(rows=int(len(d["X"])), graphs=int(len(np.unique(d["G"]))),
+                                           accuracy=acc, label_hist=np.bincount(d["L"], minlength=DELTA_BINS).tolist(),
+                                           kernel="one-launch SSSP"))
+        save(a.out, p_all, norm, info)
+        print(json.dumps(info["width_refit"]))
+        return 0
     if a.data and os.path.exists(a.data):
         z = np.load(a.data)
         data = dict(X=z["X"], Y=z["Y"], W=z["W"] if "W" in z else None, meta=z["meta"])

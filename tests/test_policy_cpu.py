@@ -95,3 +95,22 @@ def test_level_weights_follow_the_cost_gap():
     assert w[1] > w[2]  # a wrong direction at level 1 costs 4 ms, at level 2 0.05 ms
     X, Y, W = P.level_rows(np.zeros((3, 24), np.float32), sched, cost, weights=w)
     assert len(W) == 2 and W[0] == np.float32(w[1])
+
+
+def test_width_head_refit_keeps_bfs_decisions_and_learns_labels():
+    """Refitting the SSSP width head touches only its 16 logits' weights:
+    the shared layers and the BFS heads keep their values bit for bit, and
+    the refit head follows labels that depend on the hidden features."""
+    rng = np.random.default_rng(3)
+    params = P.init_params(1)
+    X = rng.normal(size=(300, 12)).astype(np.float32)
+    norm = P.norm_of(X)
+    H = P.hidden(params, norm, X)
+    L = (H[:, :16].argmax(1)).astype(np.int32)  # a labelling the hidden layer can express
+    out = P.refit_width_head(params, norm, X, L, np.ones(len(L), np.float32), epochs=1500)
+    o3 = 12 * 64 + 64 + 64 * 64 + 64
+    assert np.array_equal(out[:o3], params[:o3])
+    W3o, W3p = out[o3:o3 + 1280].reshape(64, 20), params[o3:o3 + 1280].reshape(64, 20)
+    assert np.array_equal(W3o[:, :4], W3p[:, :4])
+    assert np.array_equal(out[o3 + 1280:o3 + 1284], params[o3 + 1280:o3 + 1284])
+    assert P.width_accuracy(out, norm, X, L) > P.width_accuracy(params, norm, X, L) + 0.3
