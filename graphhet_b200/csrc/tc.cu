@@ -223,6 +223,9 @@ constexpr int32_t kTcWarpRow = 128;
 constexpr int32_t kTcWarpSlots = 256;
 constexpr int32_t kTcBlockRow = 8192;
 constexpr int kTcWarpBlock = 256;   // threads of the warp-per-row kernel
+// A list N+(b) over kTcSearchRatio x |N+(a)| entries is searched for N+(a)'s
+// entries (k binary searches) rather than probed entry by entry.
+constexpr int32_t kTcSearchRatio = 16;
 constexpr int kTcBlockThreads = 512;
 
 __device__ __forceinline__ uint32_t tc_hash(int32_t w, int shift) {
@@ -275,11 +278,27 @@ __device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __rest
             const int32_t mb = __shfl_sync(0xffffffffu, lb, leader);
             const int32_t me = __shfl_sync(0xffffffffu, le, leader);
             unsigned hits = 0;
-            for (int32_t j = mb + lane; j < me; j += 32) {
-                const int32_t w = ocol[j];
-                if (tc_probe(keys, mask, shift, w)) {
-                    ++hits;
-                    atomicAdd(cnt + w, 1ull);
+            if (me - mb > kTcSearchRatio * k) {
+                // N+(b) much longer than N+(a): look N+(a)'s own entries up
+                // in N+(b) by binary search instead (the same intersection).
+                for (int32_t i0 = 0; i0 < k; i0 += 32) {
+                    const int32_t i = i0 + lane;
+                    if (i < k) {
+                        const int32_t x = ocol[ab + i];
+                        const int32_t p = lower_bound_from(ocol, mb, me, x);
+                        if (p < me && ocol[p] == x) {
+                            ++hits;
+                            atomicAdd(cnt + x, 1ull);
+                        }
+                    }
+                }
+            } else {
+                for (int32_t j = mb + lane; j < me; j += 32) {
+                    const int32_t w = ocol[j];
+                    if (tc_probe(keys, mask, shift, w)) {
+                        ++hits;
+                        atomicAdd(cnt + w, 1ull);
+                    }
                 }
             }
             hits = warp_sum(hits);
