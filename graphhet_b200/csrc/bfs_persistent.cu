@@ -311,9 +311,12 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                     else if (dir == 1 && (double)nf_next < (double)n / beta) nd = 0;
                     if (net) s_margin = level_margin(dir, n, m_total, nf_next, mf_next, m_u, alpha, beta, gamma);
                 }
-                bfs_features(s_feat, (double)n, (double)m_total, (double)nf_next, (double)mf_next, m_u, L + 1,
-                             (double)vd->d2[nslot], (double)vd->dmax[nslot], dir, (double)n_f,
-                             (double)n - 1.0 - (double)(reached_prev + nf_next));
+                // Features only for the network or a trace: they sit on the
+                // level's critical path while the grid waits.
+                if (net || trace)
+                    bfs_features(s_feat, (double)n, (double)m_total, (double)nf_next, (double)mf_next, m_u, L + 1,
+                                 (double)vd->d2[nslot], (double)vd->dmax[nslot], dir, (double)n_f,
+                                 (double)n - 1.0 - (double)(reached_prev + nf_next));
                 if (trace && L + 1 < trace_cap)
                     for (int k = 0; k < kPolIn; ++k) trace[(size_t)(L + 1) * GHB_TRACE_COLS + k] = s_feat[k];
                 s_dec[0] = nd;
@@ -625,11 +628,12 @@ bool bfs_persistent_available(ghb_workspace* ws, int* blocks) {
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
         if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_persistent_kernel, 512, 0) ==
                         cudaSuccess)
-            cached[dev] = std::min(per_sm, 2) * ws->num_sms;
+            cached[dev] = std::min(per_sm, 2);
         known[dev] = true;
     }
-    *blocks = cached[dev];
-    return cached[dev] > 0;
+    // Blocks per SM: the workspace's bfs_blocks_per_sm, at most what fits.
+    *blocks = std::min(cached[dev], (int)ws->tune.bfs_blocks_per_sm) * ws->num_sms;
+    return *blocks > 0;
 }
 
 // One cooperative launch for the whole traversal.  depth: per-vertex output

@@ -134,6 +134,7 @@ const TuneField kTuneFields[] = {
     {"tc_hash", &ghb::Tuning::tc_hash, 0, 1},
     {"tc_block_row", &ghb::Tuning::tc_block_row, 128, 8192},
     {"ms_persistent", &ghb::Tuning::ms_persistent, 0, 1},
+    {"bfs_blocks_per_sm", &ghb::Tuning::bfs_blocks_per_sm, 1, 2},
 };
 const TuneField* tune_field(const char* name) {
     if (!name) return nullptr;

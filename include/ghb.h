@@ -78,7 +78,8 @@ ghb_workspace* ghb_default_workspace(void);
  * through sorted rows, "tc_block_row" (128 - 8192; default 8192) the longest
  * oriented row the hash path takes (longer rows gallop), "ms_persistent" (0
  * or 1; default 1) whether a multi-source BFS pass is one cooperative launch
- * or host-driven levels.
+ * or host-driven levels, "bfs_blocks_per_sm" (1 or 2; default 2) the blocks
+ * per SM of the whole-traversal BFS launch.
  * Results do not depend on them.  "barrier_extra" (0 or 1) is a test knob:
  * 1 makes every grid barrier of the persistent kernels wait for one arrival
  * more than there are blocks, so every wait runs out after barrier_limit_us
