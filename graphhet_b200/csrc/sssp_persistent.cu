@@ -99,13 +99,16 @@ struct SpCtx {
     int32_t round, phase, epoch;
 };
 
-// Relax entry j of a row whose source distance is du.
-__device__ __forceinline__ void sp_relax(const SpCtx& c, double du, int32_t j, unsigned long long& exam,
-                                         unsigned long long* s_fmin) {
-    ++exam;
-    const int32_t v = c.col[j];
-    const double nd = du + c.wt[j];
-    if (nd < sp_dist(c.dist, v)) {
+// Entries a lane relaxes per step: their column, weight and distance loads
+// are all issued before any compare, so a lane keeps kSpBatch gathers in
+// flight instead of one dependent chain.
+constexpr int kSpBatch = 4;
+
+// The compare-and-update part of relaxing an entry u -> v, nd = d[u] + w,
+// cur = the distance of v read before.
+__device__ __forceinline__ void sp_update(const SpCtx& c, int32_t v, double nd, double cur,
+                                          unsigned long long* s_fmin) {
+    if (nd < cur) {
         const unsigned long long nb = (unsigned long long)__double_as_longlong(nd);
         const unsigned long long old = atomicMin(c.dist + v, nb);
         if (nb < old) {
@@ -117,6 +120,45 @@ __device__ __forceinline__ void sp_relax(const SpCtx& c, double du, int32_t j, u
                 atomicMin(s_fmin, nb);
             }
         }
+    }
+}
+
+// Relax entries j[q] (those with ok[q]) of rows whose source distances are
+// du[q].
+__device__ __forceinline__ void sp_relax_batch(const SpCtx& c, const double* du, const int32_t* j, const bool* ok,
+                                               unsigned long long& exam, unsigned long long* s_fmin) {
+    int32_t v[kSpBatch];
+    double w[kSpBatch], cur[kSpBatch];
+#pragma unroll
+    for (int q = 0; q < kSpBatch; ++q) {
+        v[q] = ok[q] ? c.col[j[q]] : 0;
+        w[q] = ok[q] ? c.wt[j[q]] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < kSpBatch; ++q) cur[q] = ok[q] ? sp_dist(c.dist, v[q]) : 0.0;
+#pragma unroll
+    for (int q = 0; q < kSpBatch; ++q)
+        if (ok[q]) {
+            ++exam;
+            sp_update(c, v[q], du[q] + w[q], cur[q], s_fmin);
+        }
+}
+
+// Relax [jb, je) of one row (distance du) with the whole warp.
+__device__ __forceinline__ void sp_warp_range(const SpCtx& c, double du, int32_t jb, int32_t je,
+                                              unsigned long long& exam, unsigned long long* s_fmin) {
+    const int lane = lane_id();
+    for (int32_t j0 = jb + lane; j0 < je; j0 += 32 * kSpBatch) {
+        int32_t jj[kSpBatch];
+        bool ok[kSpBatch];
+        double dd[kSpBatch];
+#pragma unroll
+        for (int q = 0; q < kSpBatch; ++q) {
+            jj[q] = j0 + 32 * q;
+            ok[q] = jj[q] < je;
+            dd[q] = du;
+        }
+        sp_relax_batch(c, dd, jj, ok, exam, s_fmin);
     }
 }
 
@@ -143,7 +185,7 @@ __device__ __forceinline__ void sp_rows(const SpCtx& c, int32_t u, int32_t b, in
         const int32_t lb = __shfl_sync(0xffffffffu, b, leader);
         const int32_t lend = __shfl_sync(0xffffffffu, e, leader);
         const double ld = __shfl_sync(0xffffffffu, du, leader);
-        for (int32_t j = lb + lane; j < lend; j += 32) sp_relax(c, ld, j, exam, s_fmin);
+        sp_warp_range(c, ld, lb, lend, exam, s_fmin);
     }
     if (e - b >= 32) e = b;
     // Shorter rows: gathered warp-wide over a scan of their lengths.
@@ -156,19 +198,27 @@ __device__ __forceinline__ void sp_rows(const SpCtx& c, int32_t u, int32_t b, in
     }
     const int32_t excl = incl - d;
     const int32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    for (int32_t k0 = 0; k0 < total; k0 += 32) {
-        const int32_t k = k0 + lane;
-        int owner = 0;
+    for (int32_t k0 = 0; k0 < total; k0 += 32 * kSpBatch) {
+        int32_t jj[kSpBatch];
+        bool ok[kSpBatch];
+        double dd[kSpBatch];
 #pragma unroll
-        for (int s = 16; s >= 1; s >>= 1) {
-            const int cand = owner + s;
-            const int32_t ev = __shfl_sync(0xffffffffu, excl, cand);
-            if (ev <= k) owner = cand;
+        for (int q = 0; q < kSpBatch; ++q) {
+            const int32_t k = k0 + 32 * q + lane;
+            int owner = 0;
+#pragma unroll
+            for (int s = 16; s >= 1; s >>= 1) {
+                const int cand = owner + s;
+                const int32_t ev = __shfl_sync(0xffffffffu, excl, cand);
+                if (ev <= k) owner = cand;
+            }
+            const int32_t ob = __shfl_sync(0xffffffffu, b, owner);
+            const int32_t oe = __shfl_sync(0xffffffffu, excl, owner);
+            dd[q] = __shfl_sync(0xffffffffu, du, owner);
+            ok[q] = k < total;
+            jj[q] = ob + (k - oe);
         }
-        const int32_t ob = __shfl_sync(0xffffffffu, b, owner);
-        const int32_t oe = __shfl_sync(0xffffffffu, excl, owner);
-        const double od = __shfl_sync(0xffffffffu, du, owner);
-        if (k < total) sp_relax(c, od, ob + (k - oe), exam, s_fmin);
+        sp_relax_batch(c, dd, jj, ok, exam, s_fmin);
     }
 }
 
@@ -276,7 +326,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent_kernel(
             for (int64_t i = warp; i < nc; i += nwarps) {
                 const int4 ch = chunks[i];
                 const double du = sp_dist(dist, ch.x);
-                for (int32_t j = ch.y + lane; j < ch.z; j += 32) sp_relax(c, du, j, exam, &s_fmin);
+                sp_warp_range(c, du, ch.y, ch.z, exam, &s_fmin);
             }
             // Queue rows, 32 per warp.
             for (int64_t base = warp * 32; base < nq; base += nwarps * 32) {
