@@ -226,7 +226,11 @@ constexpr int kTcWarpBlock = 256;   // threads of the warp-per-row kernel
 // A list N+(b) over kTcSearchRatio x |N+(a)| entries is searched for N+(a)'s
 // entries (k binary searches) rather than probed entry by entry.
 constexpr int32_t kTcSearchRatio = 16;
-constexpr int kTcBlockThreads = 512;
+constexpr int kTcBlockThreads = 128;
+constexpr int32_t kTcSlice = 512;     // entries of N+(a) per slice-kernel item
+constexpr int32_t kTcMidRow = 1024;   // rows up to this many entries: a 2,048-slot hash
+constexpr int kTcMidLog2 = 11;
+constexpr int kTcBigLog2 = 14;        // 16,384 slots for rows up to kTcBlockRow
 
 __device__ __forceinline__ uint32_t tc_hash(int32_t w, int shift) {
     return ((uint32_t)w * 2654435761u) >> shift;
@@ -247,22 +251,23 @@ __device__ __forceinline__ bool tc_probe(const int32_t* keys, uint32_t mask, int
     }
 }
 
-// The warp's share of row a: entries [g0, g1) of N+(a) (every 32-entry
-// group from g0 with the given stride), probing the hash `keys`.  Adds w's
-// hits to cnt, b's to bc[index in N+(a)]; returns a's hits (lane 0 holds
-// those of whole-warp lists, every lane those it probed itself).
+// The warp's share of row a (k entries): entries [g0, g_end) of N+(a), the
+// 32-entry groups from g0 with the given stride, probing the hash `keys`.
+// Adds w's hits to cnt, b's to bc[(index in N+(a)) - bc_off]; returns a's
+// hits (lane 0 holds those of whole-warp lists, every lane those it probed
+// itself).
 __device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __restrict__ orp,
                                                            const int32_t* __restrict__ ocol, int32_t ab, int32_t k,
-                                                           int32_t g0, int32_t stride, const int32_t* keys,
-                                                           uint32_t mask, int shift, int32_t* bc,
-                                                           unsigned long long* cnt) {
+                                                           int32_t g0, int32_t g_end, int32_t stride,
+                                                           const int32_t* keys, uint32_t mask, int shift, int32_t* bc,
+                                                           int32_t bc_off, unsigned long long* cnt) {
     const int lane = lane_id();
     unsigned long long a_hits = 0;
     const int32_t amin = ocol[ab], amax = ocol[ab + k - 1];
-    for (int32_t g = g0; g < k; g += stride) {
+    for (int32_t g = g0; g < g_end; g += stride) {
         const int32_t i = g + lane;
         int32_t lb = 0, le = 0;
-        if (i < k) {
+        if (i < g_end) {
             const int32_t b = ocol[ab + i];
             lb = orp[b];
             le = orp[b + 1];
@@ -303,7 +308,7 @@ __device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __rest
             }
             hits = warp_sum(hits);
             if (lane == 0 && hits) {
-                atomicAdd(bc + g + leader, (int32_t)hits);
+                atomicAdd(bc + g + leader - bc_off, (int32_t)hits);
                 a_hits += hits;
             }
         }
@@ -331,7 +336,7 @@ __device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __rest
             if (kk < total) {
                 const int32_t w = ocol[ob + (kk - oe)];
                 if (tc_probe(keys, mask, shift, w)) {
-                    atomicAdd(bc + g + owner, 1);
+                    atomicAdd(bc + g + owner - bc_off, 1);
                     atomicAdd(cnt + w, 1ull);
                     ++a_hits;
                 }
@@ -341,13 +346,17 @@ __device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __rest
     return a_hits;
 }
 
-// Rows of 1..kTcWarpRow oriented entries, a warp each; longer rows are
-// listed for the block kernel (up to block_row <= kTcBlockRow entries) or
-// the galloping walk.
+// Rows of 1..kTcWarpRow oriented entries, a warp each.  Longer rows, up to
+// block_row <= kTcBlockRow entries, are listed for the slice kernels as
+// (row, first entry) items of kTcSlice entries each, in two classes by the
+// hash the row needs (items[0..]: up to kTcMidRow entries, items[item_cap..]:
+// longer); rows over block_row go to huge[] for the galloping walk.
+// tails: [0], [1] the two item counts, [2] the huge rows.
 __global__ void __launch_bounds__(kTcWarpBlock) tc_hash_warp_kernel(int32_t n, const int32_t* __restrict__ orp,
                                                                     const int32_t* __restrict__ ocol,
-                                                                    unsigned long long* cnt, int32_t* lists,
-                                                                    int32_t* tails, int32_t block_row) {
+                                                                    unsigned long long* cnt, int2* items,
+                                                                    int64_t item_cap, int32_t* huge, int32_t* tails,
+                                                                    int32_t block_row) {
     __shared__ int32_t s_keys[kTcWarpBlock / 32][kTcWarpSlots];
     __shared__ int32_t s_bc[kTcWarpBlock / 32][kTcWarpRow];
     const int lane = lane_id();
@@ -359,9 +368,16 @@ __global__ void __launch_bounds__(kTcWarpBlock) tc_hash_warp_kernel(int32_t n, c
         const int32_t ab = orp[a], k = orp[a + 1] - ab;
         if (k == 0) continue;
         if (k > kTcWarpRow) {
-            if (lane == 0) {
-                if (k <= block_row) lists[atomicAdd(tails, 1)] = (int32_t)a;
-                else lists[n + atomicAdd(tails + 1, 1)] = (int32_t)a;
+            if (k <= block_row) {
+                const int cls = k <= kTcMidRow ? 0 : 1;
+                const int32_t ns = (k + kTcSlice - 1) / kTcSlice;
+                int32_t pos = 0;
+                if (lane == 0) pos = atomicAdd(tails + cls, ns);
+                pos = __shfl_sync(0xffffffffu, pos, 0);
+                for (int32_t s = lane; s < ns; s += 32)
+                    items[cls * item_cap + pos + s] = make_int2((int32_t)a, s * kTcSlice);
+            } else if (lane == 0) {
+                huge[atomicAdd(tails + 2, 1)] = (int32_t)a;
             }
             continue;
         }
@@ -372,7 +388,7 @@ __global__ void __launch_bounds__(kTcWarpBlock) tc_hash_warp_kernel(int32_t n, c
         for (int32_t i = lane; i < k; i += 32) tc_insert(keys, kTcWarpSlots - 1, shift, ocol[ab + i]);
         __syncwarp();
         unsigned long long a_hits =
-            tc_row_share(orp, ocol, ab, k, 0, 32, keys, kTcWarpSlots - 1, shift, bc, cnt);
+            tc_row_share(orp, ocol, ab, k, 0, k, 32, keys, kTcWarpSlots - 1, shift, bc, 0, cnt);
         __syncwarp();
         a_hits = warp_sum(a_hits);
         if (lane == 0 && a_hits) atomicAdd(cnt + a, a_hits);
@@ -382,41 +398,47 @@ __global__ void __launch_bounds__(kTcWarpBlock) tc_hash_warp_kernel(int32_t n, c
     }
 }
 
-// Rows of kTcWarpRow+1 .. kTcBlockRow oriented entries (listed by the warp
-// kernel), a block each; dynamic shared memory: the hash (a power of two
-// >= 2k slots) and the per-entry counters.
-__global__ void __launch_bounds__(kTcBlockThreads) tc_hash_block_kernel(const int32_t* __restrict__ orp,
+// Slices of rows over kTcWarpRow entries (items listed by the warp kernel),
+// a 128-thread block per item: the block hashes the whole row N+(a) (a
+// power of two >= 2k slots, at most 2^CAP_LOG2) and probes for the
+// kTcSlice entries b of its slice, four warps side by side.  Small blocks
+// keep many rows in flight per SM; slices spread the longest rows over
+// many blocks.  DYN: the hash lives in dynamic shared memory.
+template <int CAP_LOG2, bool DYN>
+__global__ void __launch_bounds__(kTcBlockThreads) tc_hash_slice_kernel(const int32_t* __restrict__ orp,
                                                                         const int32_t* __restrict__ ocol,
-                                                                        unsigned long long* cnt,
-                                                                        const int32_t* __restrict__ rows,
+                                                                        unsigned long long* cnt, const int2* items,
                                                                         const int32_t* count) {
     extern __shared__ int32_t s_dyn[];
+    __shared__ int32_t s_static[DYN ? 1 : (1 << CAP_LOG2)];
+    __shared__ int32_t s_bc[kTcSlice];
     __shared__ unsigned long long s_hits;
-    const int32_t nrows = *count;
+    int32_t* keys = DYN ? s_dyn : s_static;
+    const int32_t nitems = *count;
     const int warp_in_block = threadIdx.x >> 5, warps = blockDim.x >> 5;
-    for (int32_t r = blockIdx.x; r < nrows; r += gridDim.x) {
-        const int32_t a = rows[r];
+    for (int32_t r = blockIdx.x; r < nitems; r += gridDim.x) {
+        const int2 it = items[r];
+        const int32_t a = it.x, gs = it.y;
         const int32_t ab = orp[a], k = orp[a + 1] - ab;
+        const int32_t ge = min(k, gs + kTcSlice);
         int log2cap = 1;
         while ((1 << log2cap) < 2 * k) ++log2cap;
         const uint32_t cap = 1u << log2cap;
-        int32_t* keys = s_dyn;
-        int32_t* bc = s_dyn + cap;
         for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) keys[s] = -1;
-        for (int32_t s = threadIdx.x; s < k; s += blockDim.x) bc[s] = 0;
+        for (int32_t s = threadIdx.x; s < ge - gs; s += blockDim.x) s_bc[s] = 0;
         if (threadIdx.x == 0) s_hits = 0;
         __syncthreads();
         const int shift = 32 - log2cap;
         for (int32_t i = threadIdx.x; i < k; i += blockDim.x) tc_insert(keys, cap - 1, shift, ocol[ab + i]);
         __syncthreads();
-        unsigned long long a_hits =
-            tc_row_share(orp, ocol, ab, k, warp_in_block * 32, warps * 32, keys, cap - 1, shift, bc, cnt);
+        unsigned long long a_hits = tc_row_share(orp, ocol, ab, k, gs + warp_in_block * 32, ge, warps * 32, keys,
+                                                 cap - 1, shift, s_bc, gs, cnt);
         a_hits = warp_sum(a_hits);
         if (lane_id() == 0 && a_hits) atomicAdd(&s_hits, a_hits);
         __syncthreads();
         if (threadIdx.x == 0 && s_hits) atomicAdd(cnt + a, s_hits);
-        for (int32_t i = threadIdx.x; i < k; i += blockDim.x)
-            if (bc[i]) atomicAdd(cnt + ocol[ab + i], (unsigned long long)bc[i]);
+        for (int32_t i = threadIdx.x; i < ge - gs; i += blockDim.x)
+            if (s_bc[i]) atomicAdd(cnt + ocol[ab + gs + i], (unsigned long long)s_bc[i]);
         __syncthreads();
     }
 }
@@ -434,27 +456,42 @@ __global__ void __launch_bounds__(kTcBlockThreads) tc_hash_block_kernel(const in
 // counters measured 10 % slower at scale 22 and 17 % slower at scale 24 with
 // 32-bit counters, twice as slow with 64-bit ones: the L2's same-address
 // reductions keep up better than a block's shared-memory atomics.)
-int tc_count_oriented(ghb_workspace* ws, int32_t n, const int32_t* orp, const int32_t* ocol, unsigned long long* cnt,
-                      const WalkBuffers& wb, int32_t* lists) {
+// Items per class of the slice kernels for a CSR of n rows and m entries.
+int64_t tc_item_cap(int32_t n, int64_t m) { return (int64_t)n + m / kTcSlice + 64; }
+
+}  // namespace
+
+// Scratch ints that tc_count_oriented's `lists` must hold.
+size_t tc_lists_ints(int32_t n, int64_t m) { return (size_t)(4 * tc_item_cap(n, m) + n + 8); }
+
+namespace {
+
+int tc_count_oriented(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* orp, const int32_t* ocol,
+                      unsigned long long* cnt, const WalkBuffers& wb, int32_t* lists) {
     if (!ws->tune.tc_hash)
         return walk(ws, orp, ocol, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
                     OrientedVisitor{orp, ocol, cnt});
-    int32_t* tails = lists + 2 * (size_t)n;
-    GHB_CUDA_TRY(cudaMemsetAsync(tails, 0, 2 * sizeof(int32_t), ws->stream));
+    const int64_t item_cap = tc_item_cap(n, m);
+    int2* items = reinterpret_cast<int2*>(lists);
+    int32_t* huge = lists + 4 * item_cap;
+    int32_t* tails = huge + n;
+    GHB_CUDA_TRY(cudaMemsetAsync(tails, 0, 4 * sizeof(int32_t), ws->stream));
     GHB_TRY(launch(ws, tc_hash_warp_kernel, dim3(grid_for((int64_t)n * 32, kTcWarpBlock, ws->num_sms * 8)),
-                   dim3(kTcWarpBlock), 0, n, orp, ocol, cnt, lists, tails,
+                   dim3(kTcWarpBlock), 0, n, orp, ocol, cnt, items, item_cap, huge, tails,
                    std::min<int32_t>(std::max<int32_t>(ws->tune.tc_block_row, kTcWarpRow), kTcBlockRow)));
-    const size_t smem = sizeof(int32_t) * (size_t)(2 * kTcBlockRow + kTcBlockRow);
+    GHB_TRY(launch(ws, tc_hash_slice_kernel<kTcMidLog2, false>, dim3(ws->num_sms * 12), dim3(kTcBlockThreads), 0,
+                   orp, ocol, cnt, (const int2*)items, (const int32_t*)tails));
+    const size_t smem = sizeof(int32_t) << kTcBigLog2;
     static bool attr_set[64] = {false};
     if (ws->device >= 0 && ws->device < 64 && !attr_set[ws->device]) {
-        GHB_CUDA_TRY(cudaFuncSetAttribute(tc_hash_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
+        GHB_CUDA_TRY(cudaFuncSetAttribute(tc_hash_slice_kernel<kTcBigLog2, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set[ws->device] = true;
     }
-    GHB_TRY(launch(ws, tc_hash_block_kernel, dim3(ws->num_sms * 2), dim3(kTcBlockThreads), smem, orp, ocol, cnt,
-                   (const int32_t*)lists, (const int32_t*)tails));
-    // Rows over kTcBlockRow oriented entries: the galloping walk.
-    return walk(ws, orp, ocol, (const int32_t*)(lists + n), (const int32_t*)(tails + 1), (int64_t)0,
+    GHB_TRY(launch(ws, tc_hash_slice_kernel<kTcBigLog2, true>, dim3(ws->num_sms * 3), dim3(kTcBlockThreads), smem,
+                   orp, ocol, cnt, (const int2*)(items + item_cap), (const int32_t*)(tails + 1)));
+    // Rows over the block path's length: the galloping walk.
+    return walk(ws, orp, ocol, (const int32_t*)huge, (const int32_t*)(tails + 2), (int64_t)0,
                 (int64_t)ws->num_sms * 64, wb, OrientedVisitor{orp, ocol, cnt});
 }
 
@@ -518,7 +555,7 @@ size_t tc_oriented_bytes(int32_t n, int64_t m) {
     c.take<int32_t>((size_t)n + 1);
     c.take<int64_t>(scan_scratch_words(n));
     c.take<int32_t>(m > 0 ? m : 1);
-    c.take<int32_t>(2 * (size_t)n + 8);
+    c.take<int32_t>(tc_lists_ints(n, m));
     return c.off;
 }
 
@@ -531,7 +568,7 @@ int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* row
     int32_t* orp = c.take<int32_t>((size_t)n + 1);
     int64_t* bsums = c.take<int64_t>(scan_scratch_words(n));
     int32_t* ocol = c.take<int32_t>(m > 0 ? m : 1);
-    int32_t* lists = c.take<int32_t>(2 * (size_t)n + 8);
+    int32_t* lists = c.take<int32_t>(tc_lists_ints(n, m));
     GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * ((size_t)n + 1), st));
     GHB_CUDA_TRY(cudaMemsetAsync(keep, 0, sizeof(int32_t) * n, st));
     GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
@@ -541,7 +578,7 @@ int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* row
                    rowptr, col, (const int32_t*)orp, ocol));
     GHB_TRY(launch(ws, orient_fill_long_kernel, dim3(ws->num_sms), dim3(1024), 0, n, rowptr, col, (const int32_t*)orp,
                    ocol));
-    GHB_TRY(tc_count_oriented(ws, n, orp, ocol, cnt, wb, lists));
+    GHB_TRY(tc_count_oriented(ws, n, m, orp, ocol, cnt, wb, lists));
     if (counts64)
         GHB_TRY(launch(ws, tc_finish_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n,
                        (const unsigned long long*)cnt, 6, counts64, (int32_t*)nullptr,
@@ -568,7 +605,7 @@ int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
     sizing.take<int32_t>((size_t)n + 1);
     sizing.take<int64_t>(scan_scratch_words(n));
     sizing.take<int32_t>(m > 0 ? m : 1);
-    sizing.take<int32_t>(2 * (size_t)n + 8);
+    sizing.take<int32_t>(tc_lists_ints(n, m));
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
     WalkBuffers wb = WalkBuffers::carve(c, n);
@@ -579,7 +616,7 @@ int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
     int32_t* orp = c.take<int32_t>((size_t)n + 1);
     int64_t* bsums = c.take<int64_t>(scan_scratch_words(n));
     int32_t* ocol = c.take<int32_t>(m > 0 ? m : 1);
-    int32_t* lists = c.take<int32_t>(2 * (size_t)n + 8);
+    int32_t* lists = c.take<int32_t>(tc_lists_ints(n, m));
 
     GHB_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * n, st));
     GHB_CUDA_TRY(cudaMemsetAsync(tot, 0, sizeof(unsigned long long), st));
@@ -603,7 +640,7 @@ int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
                        n, rowptr, col, (const int32_t*)orp, ocol));
         GHB_TRY(launch(ws, orient_fill_long_kernel, dim3(ws->num_sms), dim3(1024), 0, n, rowptr, col,
                        (const int32_t*)orp, ocol));
-        GHB_TRY(tc_count_oriented(ws, n, orp, ocol, cnt, wb, lists));
+        GHB_TRY(tc_count_oriented(ws, n, m, orp, ocol, cnt, wb, lists));
     } else {
         GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
                      MergeVisitor{rowptr, col, cnt}));
