@@ -9,17 +9,17 @@
 //
 //   LIGHT  relax the light range (entries with w < delta of the weight-sorted
 //          rows; the whole row when there is no split) of every near-queue
-//          vertex, plus the row chunks the previous pass deferred.  An
-//          improvement below the bucket's end queues the vertex for the next
-//          LIGHT pass, one at or above it goes to the far list.  Each queued
-//          vertex also joins R, the bucket's settled set.
+//          vertex.  An improvement below the bucket's end queues the vertex
+//          for the next LIGHT pass, one at or above it goes to the far list.
+//          Each queued vertex also joins R, the bucket's settled set.
 //   HEAVY  relax the heavy range (w >= delta) of every vertex of R once.
+//   CHUNK  after a LIGHT or HEAVY pass that met rows of more than kSpDirect
+//          entries: those rows, cut into kSpChunk-entry chunks, a chunk per
+//          warp, in the same round (same stamps, same next queue).
 //   SPLIT  move the far list's entries below the next bucket's end into the
 //          near queue; drop entries already settled; keep the rest.
 //
-// Rows longer than kSsspChunk entries are cut into chunks: a pass relaxes
-// the first chunk and hands the rest to the next pass, whose warps share
-// them.  The next bucket's end follows the smallest pending far distance
+// The next bucket's end follows the smallest pending far distance
 // (kept in shared memory per block, one global atomic per block and pass),
 // so empty buckets cost nothing.
 //
@@ -35,11 +35,16 @@
 
 namespace ghb {
 
-constexpr int32_t kSsspChunk = 1024;
+// Rows of up to kSpDirect entries are relaxed where the queue hands them to a
+// warp; longer ones are cut into kSpChunk-entry chunks that a CHUNK pass, in
+// the same round, spreads over every warp (a warp walking a few 1,024-entry
+// rows while the rest of the grid waits at the barrier was the bottleneck).
+constexpr int32_t kSpDirect = 64;
+constexpr int32_t kSpChunk = 256;
 constexpr int kSsspThreads = 512;
 constexpr unsigned long long kSsspTimeBudgetNs = 120ull * 1000000000ull;  // two minutes
 
-enum SsspMode : int32_t { kLight = 0, kHeavy = 1, kSplit = 2, kDone = 3 };
+enum SsspMode : int32_t { kLight = 0, kHeavy = 1, kSplit = 2, kDone = 3, kChunk = 4 };
 
 struct SsspRunState {
     unsigned bar_count;  // barrier arrivals (own cache line)
@@ -52,12 +57,12 @@ struct SsspRunState {
     int32_t phase;        // stamp of the far list being filled
     int32_t epoch;        // stamp of R (bumped after every HEAVY pass)
     int32_t nq;           // items of the current queue (near queue, or R in HEAVY)
-    int32_t nc;           // chunk items of the current pass
+    int32_t nc;           // chunk items of the current (CHUNK) pass
     int32_t qsel;         // near queue buffer read by the current pass
-    int32_t csel;         // chunk buffer read by the current pass
+    int32_t chunk_of;     // the pass (LIGHT or HEAVY) whose rows a CHUNK pass finishes
     int32_t fsel;         // far buffer filled by relaxations
     int32_t q_tail;       // appends to the next near queue
-    int32_t c_tail;       // appends to the next chunk list
+    int32_t c_tail;       // chunks appended by the current pass
     int32_t r_tail;       // appends to R
     int32_t far_tail;     // entries of the far list being filled
     int32_t kept_tail;    // entries kept by a SPLIT pass
@@ -67,7 +72,7 @@ struct SsspRunState {
     double delta;
     unsigned long long fmin;  // smallest pending far distance (bits; an upper bound on stale entries)
     unsigned long long examined;
-    long long passes, light_passes, heavy_passes, splits;
+    long long passes, light_passes, heavy_passes, splits, chunk_passes;
     long long pass_budget;            // passes allowed (set by the host)
     unsigned long long t_start;       // global timer at the start
     unsigned long long bar_limit_ns;
@@ -93,7 +98,7 @@ struct SpCtx {
     int32_t* R;
     int32_t* q_next;
     int32_t* far_cur;
-    int4* c_next;
+    int4* chunks;
     SsspRunState* st;
     double thr;
     int32_t round, phase, epoch;
@@ -163,19 +168,19 @@ __device__ __forceinline__ void sp_warp_range(const SpCtx& c, double du, int32_t
 }
 
 // Relax [b, e) of the rows held by the warp's lanes (u < 0: none).  Rows
-// longer than kSsspChunk keep their first chunk; the rest is appended to
-// the next pass's chunk list.
+// longer than kSpDirect are appended, whole, to the chunk list of the CHUNK
+// pass that follows.
 __device__ __forceinline__ void sp_rows(const SpCtx& c, int32_t u, int32_t b, int32_t e, double du,
                                         unsigned long long& exam, unsigned long long* s_fmin) {
     const int lane = lane_id();
-    if (e - b > kSsspChunk) {
-        const int32_t extra = (e - b - 1) / kSsspChunk;  // chunks after the first
-        const int32_t pos = atomicAdd(&c.st->c_tail, extra);
-        for (int32_t k = 1; k <= extra; ++k) {
-            const int32_t cb = b + k * kSsspChunk;
-            c.c_next[pos + k - 1] = make_int4(u, cb, min(e, cb + kSsspChunk), 0);
+    if (e - b > kSpDirect) {
+        const int32_t nch = (e - b + kSpChunk - 1) / kSpChunk;
+        const int32_t pos = atomicAdd(&c.st->c_tail, nch);
+        for (int32_t k = 0; k < nch; ++k) {
+            const int32_t cb = b + k * kSpChunk;
+            c.chunks[pos + k] = make_int4(u, cb, min(e, cb + kSpChunk), 0);
         }
-        e = b + kSsspChunk;
+        e = b;
     }
     // Rows of 32 entries or more: the whole warp, one row at a time.
     unsigned med = __ballot_sync(0xffffffffu, e - b >= 32);
@@ -245,8 +250,8 @@ __device__ __forceinline__ double sp_next_thr(double thr, double delta, double m
 
 __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent_kernel(
     int32_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ le, const int32_t* __restrict__ col,
-    const double* __restrict__ wt, int32_t src, double inf, double* dist_d, int32_t* qa, int32_t* qb, int4* ca,
-    int4* cb, int32_t* fa, int32_t* fb, int32_t* near_stamp, int32_t* far_stamp, int32_t* r_stamp, int32_t* R,
+    const double* __restrict__ wt, int32_t src, double inf, double* dist_d, int32_t* qa, int32_t* qb, int4* chunks,
+    int32_t* fa, int32_t* fb, int32_t* near_stamp, int32_t* far_stamp, int32_t* r_stamp, int32_t* R,
     SsspRunState* st, const int32_t* __restrict__ perm, double* out) {
     unsigned long long* dist = reinterpret_cast<unsigned long long*>(dist_d);
     const int64_t gtid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -284,7 +289,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent_kernel(
             s_state[1] = vs->nq;
             s_state[2] = vs->nc;
             s_state[3] = vs->qsel;
-            s_state[4] = vs->csel;
+            s_state[4] = vs->chunk_of;
             s_state[5] = vs->fsel;
             s_state[6] = vs->round;
             s_state[7] = vs->phase;
@@ -298,7 +303,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent_kernel(
         const int32_t mode = s_state[0];
         if (mode == kDone) break;
         const int32_t nq = s_state[1], nc = s_state[2];
-        const int32_t qsel = s_state[3], csel = s_state[4], fsel = s_state[5];
+        const int32_t qsel = s_state[3], fsel = s_state[5];
         SpCtx c;
         c.rp = rp;
         c.le = le;
@@ -311,7 +316,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent_kernel(
         c.R = R;
         c.q_next = qsel ? qa : qb;
         c.far_cur = fsel ? fb : fa;
-        c.c_next = csel ? ca : cb;
+        c.chunks = chunks;
         c.st = st;
         c.thr = s_thr;
         c.round = s_state[6];
@@ -319,15 +324,15 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent_kernel(
         c.epoch = s_state[8];
         unsigned long long exam = 0;
 
-        if (mode == kLight || mode == kHeavy) {
-            const int32_t* q = mode == kHeavy ? R : (qsel ? qb : qa);
-            const int4* chunks = csel ? cb : ca;
-            // Chunks deferred by the previous pass, one per warp.
+        if (mode == kChunk) {
+            // The long rows of the pass just finished, a chunk per warp.
             for (int64_t i = warp; i < nc; i += nwarps) {
-                const int4 ch = chunks[i];
+                const int4 ch = __ldcg(chunks + i);
                 const double du = sp_dist(dist, ch.x);
                 sp_warp_range(c, du, ch.y, ch.z, exam, &s_fmin);
             }
+        } else if (mode == kLight || mode == kHeavy) {
+            const int32_t* q = mode == kHeavy ? R : (qsel ? qb : qa);
             // Queue rows, 32 per warp.
             for (int64_t base = warp * 32; base < nq; base += nwarps * 32) {
                 const int64_t i = base + lane;
@@ -377,15 +382,25 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent_kernel(
         const bool ok = sp_barrier(st, [&]() {
             SsspRunState* s = st;
             volatile SsspRunState* v = st;
-            const int32_t md = v->mode;
-            const int32_t nq_next = v->q_tail, nc_next = v->c_tail;
+            const int32_t md0 = v->mode;
             s->passes = v->passes + 1;
+            if ((md0 == kLight || md0 == kHeavy) && v->c_tail > 0) {
+                // Long rows were cut into chunks: a CHUNK pass finishes them
+                // in the same round (same stamps, same next queue).
+                s->nc = v->c_tail;
+                s->c_tail = 0;
+                s->chunk_of = md0;
+                s->mode = kChunk;
+                return;
+            }
+            if (md0 == kChunk) s->chunk_passes = v->chunk_passes + 1;
+            const int32_t md = md0 == kChunk ? v->chunk_of : md0;
+            const int32_t nq_next = v->q_tail;
             s->q_tail = 0;
             s->c_tail = 0;
             s->qsel = v->qsel ^ 1;
-            s->csel = v->csel ^ 1;
             s->nq = nq_next;
-            s->nc = nc_next;
+            s->nc = 0;
             if (md == kSplit) {
                 s->far_tail = v->kept_tail;
                 s->kept_tail = 0;
@@ -400,7 +415,7 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent_kernel(
                 s->light_passes = v->light_passes + 1;
             }
             int32_t next = kDone;
-            if (nq_next > 0 || nc_next > 0) {
+            if (nq_next > 0) {
                 next = kLight;
             } else if (md == kLight && v->r_tail > 0) {
                 next = kHeavy;
@@ -524,13 +539,14 @@ int sssp_persistent_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const i
     GHB_CUDA_TRY(cudaMemcpyAsync(hp, rp + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     GHB_CUDA_TRY(cudaStreamSynchronize(st));
     const int64_t m = hp[0];
-    const int64_t chunk_cap = m / kSsspChunk + 64;
-    auto carve = [&](Carver& c, int32_t** qa, int32_t** qb, int4** ca, int4** cb, int32_t** fa, int32_t** fb,
+    // Chunks of one pass: rows over kSpDirect entries, ceil(len / kSpChunk)
+    // each, so fewer than m / kSpChunk + m / kSpDirect.
+    const int64_t chunk_cap = m / 32 + 64;
+    auto carve = [&](Carver& c, int32_t** qa, int32_t** qb, int4** ch, int32_t** fa, int32_t** fb,
                      int32_t** ns, int32_t** fs, int32_t** rs, int32_t** R, SsspRunState** rs_state) {
         *qa = c.take<int32_t>(n);
         *qb = c.take<int32_t>(n);
-        *ca = c.take<int4>(chunk_cap);
-        *cb = c.take<int4>(chunk_cap);
+        *ch = c.take<int4>(chunk_cap);
         *fa = c.take<int32_t>(n);
         *fb = c.take<int32_t>(n);
         *ns = c.take<int32_t>(n);
@@ -540,13 +556,13 @@ int sssp_persistent_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const i
         *rs_state = c.take<SsspRunState>(1);
     };
     int32_t *qa, *qb, *fa, *fb, *ns, *fs, *rs, *R;
-    int4 *ca, *cb;
+    int4* ch;
     SsspRunState* rstate;
     Carver sizing(nullptr);
-    carve(sizing, &qa, &qb, &ca, &cb, &fa, &fb, &ns, &fs, &rs, &R, &rstate);
+    carve(sizing, &qa, &qb, &ch, &fa, &fb, &ns, &fs, &rs, &R, &rstate);
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
-    carve(c, &qa, &qb, &ca, &cb, &fa, &fb, &ns, &fs, &rs, &R, &rstate);
+    carve(c, &qa, &qb, &ch, &fa, &fb, &ns, &fs, &rs, &R, &rstate);
 
     GHB_CUDA_TRY(cudaMemsetAsync(rstate, 0, sizeof(SsspRunState), st));
     {
@@ -565,7 +581,7 @@ int sssp_persistent_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const i
     }
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
     GHB_TRY(launch_coop(ws, sssp_persistent_kernel, dim3(blocks), dim3(kSsspThreads), 0, n, rp, le, col, wt, src, inf,
-                        dist, qa, qb, ca, cb, fa, fb, ns, fs, rs, R, rstate, perm, out));
+                        dist, qa, qb, ch, fa, fb, ns, fs, rs, R, rstate, perm, out));
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
     GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, rstate, sizeof(SsspRunState), cudaMemcpyDeviceToHost, st));
     GHB_CUDA_TRY(cudaStreamSynchronize(st));
@@ -590,7 +606,7 @@ int sssp_persistent_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const i
         float ms = 0.f;
         GHB_CUDA_TRY(cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop));
         const unsigned long long* ha = reinterpret_cast<const unsigned long long*>(ws->host_pinned);
-        stats->levels = (int32_t)(h.light_passes + h.heavy_passes);
+        stats->levels = (int32_t)(h.light_passes + h.heavy_passes + h.chunk_passes);
         stats->pull_levels = (int32_t)h.splits;
         stats->edges_reached = (int64_t)ha[0];
         stats->reached = (int64_t)ha[1];
