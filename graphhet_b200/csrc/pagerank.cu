@@ -229,9 +229,10 @@ __global__ void pr_chunk_rows_kernel(int32_t nlong, const int32_t* __restrict__ 
         for (int32_t c = chunk_prefix[i] + lane_id(); c < chunk_prefix[i + 1]; c += 32) chunk_row[c] = (int32_t)i;
 }
 
-// One warp per chunk of `chunk` entries: a partial sum, four independent
-// 32-wide loads in flight per lane, hub contributions from shared memory.
-template <class T>
+// One warp per chunk of `chunk` entries: a partial sum, G independent
+// 32-wide loads in flight per lane (4 or 8: the workspace's pr_gathers),
+// hub contributions from shared memory.
+template <class T, int G>
 __global__ void __launch_bounds__(kPrPersistThreads) pr_chunk_kernel(
     int32_t n, const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col,
     const int32_t* __restrict__ long_rows, const int32_t* __restrict__ chunk_prefix,
@@ -252,18 +253,18 @@ __global__ void __launch_bounds__(kPrPersistThreads) pr_chunk_kernel(
         const int32_t b = rb + (int32_t)(ch - chunk_prefix[i]) * chunk;
         const int32_t e = min(re, b + chunk);
         KSum<T> acc;
-        for (int32_t j0 = b; j0 < e; j0 += 128) {
-            int32_t x[4];
+        for (int32_t j0 = b; j0 < e; j0 += 32 * G) {
+            int32_t x[G];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < G; ++k) {
                 const int32_t j = j0 + lane + 32 * k;
                 x[k] = j < e ? ld_stream(in_col + j, pol_stream) : -1;
             }
-            T y[4];
+            T y[G];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) y[k] = x[k] >= 0 ? gather<T>(cache, K, contrib_old, x[k], pol_keep) : (T)0;
+            for (int k = 0; k < G; ++k) y[k] = x[k] >= 0 ? gather<T>(cache, K, contrib_old, x[k], pol_keep) : (T)0;
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
+            for (int k = 0; k < G; ++k)
                 if (x[k] >= 0) acc.add(y[k]);
         }
 #pragma unroll
@@ -385,7 +386,9 @@ int pagerank_impl(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int3
     const unsigned g = ws->num_sms * 8;
     GHB_CUDA_TRY(cudaFuncSetAttribute(pr_rows_short_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)cache_bytes));
-    GHB_CUDA_TRY(cudaFuncSetAttribute(pr_chunk_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    GHB_CUDA_TRY(cudaFuncSetAttribute(pr_chunk_kernel<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)cache_bytes));
+    GHB_CUDA_TRY(cudaFuncSetAttribute(pr_chunk_kernel<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)cache_bytes));
     GHB_CUDA_TRY(cudaMemsetAsync(ps, 0, sizeof(double) * nparts, st));
     GHB_CUDA_TRY(cudaMemsetAsync(pl, 0, sizeof(double) * nparts, st));
@@ -418,7 +421,8 @@ int pagerank_impl(ghb_workspace* ws, int32_t n, const int32_t* in_rp, const int3
                        (const int32_t*)outdeg, (const T*)c_cur, (const T*)r_cur, r_nxt, c_nxt, (const PrScalars*)sc, d,
                        track ? 1 : 0, ps, pl, short_max, cache_elems));
         if (nlong > 0) {
-            GHB_TRY(launch(ws, pr_chunk_kernel<T>, dim3(grid_rows), dim3(pthreads), cache_bytes, n, in_rp, in_col,
+            GHB_TRY(launch(ws, ws->tune.pr_gathers == 8 ? pr_chunk_kernel<T, 8> : pr_chunk_kernel<T, 4>,
+                           dim3(grid_rows), dim3(pthreads), cache_bytes, n, in_rp, in_col,
                            (const int32_t*)long_rows, (const int32_t*)cpre, (const int32_t*)crow, nchunks,
                            (const T*)c_cur, csum, chunk, cache_elems));
         }

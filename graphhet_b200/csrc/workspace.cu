@@ -135,6 +135,7 @@ const TuneField kTuneFields[] = {
     {"tc_block_row", &ghb::Tuning::tc_block_row, 128, 8192},
     {"ms_persistent", &ghb::Tuning::ms_persistent, 0, 1},
     {"bfs_blocks_per_sm", &ghb::Tuning::bfs_blocks_per_sm, 1, 2},
+    {"pr_gathers", &ghb::Tuning::pr_gathers, 4, 8},
 };
 const TuneField* tune_field(const char* name) {
     if (!name) return nullptr;
@@ -152,6 +153,7 @@ int ghb_tune_set(ghb_workspace* ws, const char* name, int32_t value) {
     GHB_REQUIRE(value >= f->lo && value <= f->hi,
                 std::string(f->name) + " outside [" + std::to_string(f->lo) + ", " + std::to_string(f->hi) + "]");
     if (f->field == &ghb::Tuning::pr_threads) GHB_REQUIRE(value % 32 == 0, "pr_threads must be a multiple of 32");
+    if (f->field == &ghb::Tuning::pr_gathers) GHB_REQUIRE(value == 4 || value == 8, "pr_gathers must be 4 or 8");
     ws->tune.*(f->field) = value;
     return GHB_OK;
 }
