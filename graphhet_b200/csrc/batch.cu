@@ -252,7 +252,7 @@ int ghb_mssssp(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_
     ws = ws_resolve(ws);
     GHB_REQUIRE(ws, "no workspace");
     GHB_REQUIRE(n >= 1 && n_src >= 0, "bad sizes");
-    GHB_REQUIRE(rowptr && dist && srcs, "NULL argument");
+    GHB_REQUIRE(rowptr && col && w && dist && srcs, "NULL argument");
     GHB_REQUIRE(inf >= 0, "inf must be >= 0");
     cudaStream_t st = ws->stream;
     std::vector<int32_t> hs(n_src > 0 ? n_src : 1);

@@ -48,9 +48,15 @@ struct MsspCounters {
     unsigned long long examined; // entries relaxed
 };
 
-__global__ void mssp_fill_kernel(unsigned long long* d, int64_t count, unsigned long long v) {
+// Each phase is a __device__ body (grid-stride) with a thin kernel around
+// it: the host-driven pass launches the kernels, the whole-pass cooperative
+// kernel (mssp_pass_kernel) calls the bodies between its grid barriers.
+__device__ __forceinline__ void mssp_fill_body(unsigned long long* d, int64_t count, unsigned long long v) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
         d[i] = v;
+}
+__global__ void mssp_fill_kernel(unsigned long long* d, int64_t count, unsigned long long v) {
+    mssp_fill_body(d, count, v);
 }
 
 __global__ void mssp_seed_kernel(const int32_t* __restrict__ srcs, int32_t k, int32_t ks, unsigned long long* d) {
@@ -59,10 +65,9 @@ __global__ void mssp_seed_kernel(const int32_t* __restrict__ srcs, int32_t k, in
 }
 
 // Bucket start: act bits of the distances in [lo, hi), queue, pending min.
-__global__ void __launch_bounds__(256) mssp_scan_kernel(int32_t n_scan, int32_t ks, int32_t words, double lo,
-                                                        double hi, const unsigned long long* __restrict__ d,
-                                                        unsigned long long* act, int32_t* queue,
-                                                        MsspCounters* cnt) {
+__device__ __forceinline__ void mssp_scan_body(int32_t n_scan, int32_t ks, int32_t words, double lo, double hi,
+                                               const unsigned long long* d, unsigned long long* act, int32_t* queue,
+                                               MsspCounters* cnt) {
     const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -90,18 +95,24 @@ __global__ void __launch_bounds__(256) mssp_scan_kernel(int32_t n_scan, int32_t 
     if (lane == 0 && pmin < INFINITY)
         atomicMin(&cnt->pmin, (unsigned long long)__double_as_longlong(pmin));
 }
+__global__ void __launch_bounds__(256) mssp_scan_kernel(int32_t n_scan, int32_t ks, int32_t words, double lo,
+                                                        double hi, const unsigned long long* d,
+                                                        unsigned long long* act, int32_t* queue,
+                                                        MsspCounters* cnt) {
+    mssp_scan_body(n_scan, ks, words, lo, hi, d, act, queue, cnt);
+}
 
 // Relax entries [eb, ee) of v's row for v's active sources.
 __device__ __forceinline__ void mssp_relax_range(int32_t v, int32_t eb, int32_t ee, int32_t ks, int32_t words,
                                                  double hi, const int32_t* __restrict__ col,
                                                  const double* __restrict__ wt, unsigned long long* d,
-                                                 const unsigned long long* __restrict__ act_cur,
+                                                 const unsigned long long* act_cur,
                                                  unsigned long long* act_next, int32_t* inq_next,
                                                  int32_t* queue_next, MsspCounters* cnt,
                                                  unsigned long long& examined) {
     const int lane = lane_id();
     int nact = 0;
-    for (int w = 0; w < words; ++w) nact += __popcll(act_cur[(int64_t)v * words + w]);
+    for (int w = 0; w < words; ++w) nact += __popcll(__ldcg(act_cur + (int64_t)v * words + w));
     auto relax_one = [&](int32_t u, int s, double nd) {
         unsigned long long* p = d + (int64_t)u * ks + s;
         const unsigned long long nb = (unsigned long long)__double_as_longlong(nd);
@@ -122,7 +133,7 @@ __device__ __forceinline__ void mssp_relax_range(int32_t v, int32_t eb, int32_t 
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
             const int s = lane + 32 * t;
-            a[t] = t < groups && ((act_cur[(int64_t)v * words + (s >> 6)] >> (s & 63)) & 1ull);
+            a[t] = t < groups && ((__ldcg(act_cur + (int64_t)v * words + (s >> 6)) >> (s & 63)) & 1ull);
             dv[t] = a[t] ? __longlong_as_double((long long)__ldcg(d + (int64_t)v * ks + s)) : 0.0;
         }
         for (int32_t j = eb; j < ee; ++j) {
@@ -136,7 +147,7 @@ __device__ __forceinline__ void mssp_relax_range(int32_t v, int32_t eb, int32_t 
     } else {
         // Lanes over entries, the few active sources one after another.
         for (int w = 0; w < words; ++w) {
-            unsigned long long bits = act_cur[(int64_t)v * words + w];
+            unsigned long long bits = __ldcg(act_cur + (int64_t)v * words + w);
             while (bits) {
                 const int s = w * 64 + __ffsll((long long)bits) - 1;
                 bits &= bits - 1;
@@ -227,6 +238,196 @@ __global__ void mssp_clear_kernel(int32_t q, const int32_t* __restrict__ queue, 
     }
 }
 
+// ---------------------------------------------------------------------------
+// The whole pass in one cooperative launch: set-up, every bucket scan and
+// relaxation round (long rows as 256-entry chunks in a CHUNK phase of the
+// same round, then the clear of the processed vertices' act words), the
+// output, separated by the bounded grid barrier; the last block to arrive
+// decides the next phase (the host-driven pass's rules: rounds until the
+// queue is empty, then the next bucket, empty buckets skipped through the
+// smallest pending distance).  No host round trip inside a pass.
+
+constexpr int kMsspThreads = 256;
+enum MsspPhase : int32_t { kMpScan = 0, kMpRelax = 1, kMpChunks = 2, kMpClear = 3, kMpDone = 4 };
+
+struct MsspRunState {
+    unsigned bar_count;  // barrier arrivals (own cache line)
+    unsigned pad_a[31];
+    unsigned bar_release;  // barrier epochs (own cache line)
+    unsigned pad_b[31];
+    int32_t status;
+    int32_t phase;     // MsspPhase of the next phase
+    int32_t sel;       // which (act, inq, queue) set is current (0: a)
+    int32_t q;         // vertices queued for the current round
+    int32_t nchunks;   // long-row chunks of the current round
+    int32_t c_tail;    // chunks appended by the relax phase
+    int32_t pad0, pad1;
+    double lo;         // current bucket [lo, lo + delta)
+    double delta;
+    long long rounds, budget;
+    unsigned long long examined;
+};
+
+__device__ __forceinline__ double mp_pmin(const MsspCounters* c) {
+    const unsigned long long b = *(volatile const unsigned long long*)&c->pmin;
+    return b == kInfBits ? INFINITY : __longlong_as_double((long long)b);
+}
+
+__global__ void __launch_bounds__(kMsspThreads) mssp_pass_kernel(
+    int32_t n, int32_t n_active, int32_t k, int32_t ks, int32_t words, const int32_t* __restrict__ rp,
+    const int32_t* __restrict__ col, const double* __restrict__ wt, const int32_t* srcs, const int32_t* __restrict__ perm,
+    double inf, double* dist_out, unsigned long long* d, unsigned long long* act_a, unsigned long long* act_b,
+    int32_t* inq_a, int32_t* inq_b, int32_t* q_a, int32_t* q_b, int4* chunks, MsspCounters* cnt, MsspRunState* st,
+    unsigned long long bar_limit_ns, unsigned bar_extra) {
+    const int64_t gtid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t gsize = (int64_t)gridDim.x * blockDim.x;
+    const int64_t warp = gtid >> 5;
+    const int64_t nwarps = gsize >> 5;
+    const int lane = lane_id();
+    auto barrier = [&]() {
+        return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, NoLeader(), bar_limit_ns, bar_extra);
+    };
+    // ---- set-up: distances +inf, act / inq words zero, the sources at 0
+    mssp_fill_body(d, (int64_t)n * ks, kInfBits);
+    for (int64_t i = gtid; i < (int64_t)n * words; i += gsize) {
+        act_a[i] = 0ull;
+        act_b[i] = 0ull;
+    }
+    for (int64_t i = gtid; i < n; i += gsize) {
+        inq_a[i] = 0;
+        inq_b[i] = 0;
+    }
+    if (gtid == 0) {
+        cnt->queued = 0;
+        cnt->big = 0;
+        cnt->pmin = kInfBits;
+        cnt->examined = 0;
+    }
+    if (!barrier()) return;
+    if (blockIdx.x == 0 && (int)threadIdx.x < k) d[(int64_t)srcs[threadIdx.x] * ks + threadIdx.x] = 0ull;
+    if (!barrier()) return;
+
+    __shared__ int32_t s_st[4];
+    __shared__ double s_lo;
+    while (true) {
+        if (threadIdx.x == 0) {
+            volatile MsspRunState* v = st;
+            s_st[0] = v->phase;
+            s_st[1] = v->sel;
+            s_st[2] = v->q;
+            s_st[3] = v->nchunks;
+            s_lo = v->lo;
+        }
+        __syncthreads();
+        const int32_t phase = s_st[0];
+        if (phase == kMpDone) break;
+        const int32_t sel = s_st[1], q = s_st[2], nch = s_st[3];
+        unsigned long long* act_cur = sel ? act_b : act_a;
+        unsigned long long* act_next = sel ? act_a : act_b;
+        int32_t* inq_cur = sel ? inq_b : inq_a;
+        int32_t* inq_next = sel ? inq_a : inq_b;
+        int32_t* q_cur = sel ? q_b : q_a;
+        int32_t* q_next = sel ? q_a : q_b;
+        MsspCounters* cn = cnt;  // the round being filled
+        const double lo = s_lo, hi = lo + st->delta;
+        unsigned long long examined = 0;
+        if (phase == kMpScan) {
+            mssp_scan_body(n_active, ks, words, lo, hi, d, act_cur, q_cur, cn);
+        } else if (phase == kMpRelax) {
+            for (int64_t i = warp; i < q; i += nwarps) {
+                const int32_t v = __ldcg(q_cur + i);
+                const int32_t eb = rp[v], ee = rp[v + 1];
+                if (ee - eb > kMsspWarpRow) {
+                    const int32_t nc = (ee - eb + kMsspChunk - 1) / kMsspChunk;
+                    int32_t pos = 0;
+                    if (lane == 0) pos = atomicAdd(&st->c_tail, nc);
+                    pos = __shfl_sync(0xffffffffu, pos, 0);
+                    for (int32_t c = lane; c < nc; c += 32)
+                        chunks[pos + c] = make_int4(v, eb + c * kMsspChunk, min(ee, eb + (c + 1) * kMsspChunk), 0);
+                    continue;
+                }
+                mssp_relax_range(v, eb, ee, ks, words, hi, col, wt, d, act_cur, act_next, inq_next, q_next, cn,
+                                 examined);
+            }
+        } else if (phase == kMpChunks) {
+            for (int64_t i = warp; i < nch; i += nwarps) {
+                const int4 ch = __ldcg(chunks + i);
+                mssp_relax_range(ch.x, ch.y, ch.z, ks, words, hi, col, wt, d, act_cur, act_next, inq_next, q_next,
+                                 cn, examined);
+            }
+        } else {  // kMpClear: the processed vertices' act words and queue flags
+            for (int64_t i = gtid; i < q; i += gsize) {
+                const int32_t v = __ldcg(q_cur + i);
+                for (int w = 0; w < words; ++w) act_cur[(int64_t)v * words + w] = 0ull;
+                inq_cur[v] = 0;
+            }
+        }
+        if (lane == 0 && examined) atomicAdd(&cn->examined, examined);
+        const bool ok = grid_sync_leader(
+            &st->bar_count, &st->bar_release, &st->status,
+            [&]() {
+                MsspRunState* s = st;
+                volatile MsspRunState* v = st;
+                volatile MsspCounters* c = cnt;
+                int32_t next = kMpDone;
+                if (phase == kMpRelax && v->c_tail > 0) {
+                    s->nchunks = v->c_tail;
+                    s->c_tail = 0;
+                    next = kMpChunks;
+                } else if (phase == kMpRelax || phase == kMpChunks) {
+                    next = kMpClear;
+                } else {
+                    // After a scan or a clear: the queue just filled decides.
+                    int32_t queued;
+                    if (phase == kMpClear) {
+                        s->examined = v->examined + c->examined;
+                        queued = c->queued;  // the next round's queue (q_next)
+                        s->sel = v->sel ^ 1;
+                    } else {
+                        queued = c->queued;  // the bucket's start set (q_cur)
+                    }
+                    const double pmin = mp_pmin(cnt);
+                    c->queued = 0;
+                    c->examined = 0;
+                    c->pmin = kInfBits;
+                    if (queued > 0) {
+                        s->q = queued;
+                        s->rounds = v->rounds + 1;
+                        next = kMpRelax;
+                        if (v->rounds + 1 > v->budget) {
+                            s->status = kDevOverflow;
+                            next = kMpDone;
+                        }
+                    } else if (phase == kMpClear) {
+                        s->lo = v->lo + v->delta;  // next bucket
+                        next = kMpScan;
+                    } else {
+                        // An empty bucket: jump to the one holding the
+                        // smallest pending distance, or stop.
+                        if (pmin < INFINITY) {
+                            const double dl = v->delta;
+                            double nlo = floor(pmin / dl) * dl;
+                            if (nlo > pmin || nlo + dl <= pmin) nlo = pmin;  // rounding: the bucket must hold pmin
+                            s->lo = nlo;
+                            next = kMpScan;
+                        }
+                    }
+                }
+                s->phase = next;
+            },
+            bar_limit_ns, bar_extra);
+        if (!ok) return;
+    }
+    // ---- output in the caller's ids
+    for (int64_t v = gtid; v < n; v += gsize) {
+        const int64_t p = perm ? perm[v] : v;
+        for (int s = 0; s < k; ++s) {
+            const unsigned long long b = __ldcg(d + p * ks + s);
+            dist_out[(int64_t)s * n + v] = b == kInfBits ? inf : __longlong_as_double((long long)b);
+        }
+    }
+}
+
 // dist_out[s * n + v] = dist[perm[v] * ks + s] (inf where unreached).
 __global__ void __launch_bounds__(256) mssp_out_kernel(int32_t n, int32_t k, int32_t ks,
                                                        const int32_t* __restrict__ perm,
@@ -247,6 +448,93 @@ __global__ void __launch_bounds__(256) mssp_out_kernel(int32_t n, int32_t k, int
 // (the single-source rule) times 4 (a pass has 256 sources' work per bucket,
 // so fewer, fuller buckets pay).
 int sssp_pick_delta(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const double* w, double* delta);
+
+static int mssp_pass_blocks(ghb_workspace* ws) {
+    static int cached[64] = {0};
+    const int dev = ws->device;
+    if (dev < 0 || dev >= 64) return 0;
+    if (!cached[dev]) {
+        int coop = 0, per_sm = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mssp_pass_kernel, kMsspThreads, 0) ==
+                        cudaSuccess)
+            cached[dev] = std::max(0, std::min(per_sm, 4)) * ws->num_sms;
+        if (!cached[dev]) cached[dev] = -1;
+    }
+    return cached[dev] > 0 ? cached[dev] : 0;
+}
+
+// One pass of k <= 256 sources as one cooperative launch (graph ids on the
+// device in srcs_dev); the same results and the same bucket / round rules
+// as mssssp_pass below.
+int mssssp_pass_one_launch(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, const int32_t* rp,
+                           const int32_t* col, const double* wt, const int32_t* srcs_dev, int32_t k, double delta,
+                           double inf, const int32_t* perm, double* dist_out, int64_t* rounds_out,
+                           int64_t* examined_out) {
+    GHB_REQUIRE(k >= 1 && k <= 256, "multi-source SSSP pass of 1..256 sources");
+    GHB_REQUIRE(delta > 0 && std::isfinite(delta), "bucket width must be positive");
+    const int blocks = mssp_pass_blocks(ws);
+    if (blocks <= 0) {
+        set_error("cooperative launch unavailable");
+        return GHB_ERR_UNSUPPORTED;
+    }
+    cudaStream_t st = ws->stream;
+    const int32_t ks = (k + 31) & ~31;
+    const int32_t words = (ks + 63) / 64;
+    // Chunks of one round: rows over kMsspWarpRow entries, ceil(len / 256) each.
+    const int64_t chunk_cap = m / kMsspChunk + m / kMsspWarpRow + 64;
+    auto carve = [&](Carver& c, unsigned long long** d, unsigned long long** aa, unsigned long long** ab,
+                     int32_t** ia, int32_t** ib, int32_t** qa, int32_t** qb, int4** ch, MsspCounters** cnt,
+                     MsspRunState** rs) {
+        *d = c.take<unsigned long long>((size_t)n * ks);
+        *aa = c.take<unsigned long long>((size_t)n * words);
+        *ab = c.take<unsigned long long>((size_t)n * words);
+        *ia = c.take<int32_t>(n);
+        *ib = c.take<int32_t>(n);
+        *qa = c.take<int32_t>(n);
+        *qb = c.take<int32_t>(n);
+        *ch = c.take<int4>(chunk_cap);
+        *cnt = c.take<MsspCounters>(1);
+        *rs = c.take<MsspRunState>(1);
+    };
+    unsigned long long *d, *act_a, *act_b;
+    int32_t *inq_a, *inq_b, *q_a, *q_b;
+    int4* ch;
+    MsspCounters* cnt;
+    MsspRunState* rs;
+    Carver sizing(nullptr);
+    carve(sizing, &d, &act_a, &act_b, &inq_a, &inq_b, &q_a, &q_b, &ch, &cnt, &rs);
+    GHB_TRY(ws_reserve(ws, sizing.off));
+    Carver c(ws->scratch);
+    carve(c, &d, &act_a, &act_b, &inq_a, &inq_b, &q_a, &q_b, &ch, &cnt, &rs);
+    GHB_CUDA_TRY(cudaMemsetAsync(rs, 0, sizeof(MsspRunState), st));
+    {
+        // Bucket width and round budget (pageable sources: staged by the copies).
+        const double dl = delta;
+        const long long budget = 64ll * n + 4096;
+        GHB_CUDA_TRY(cudaMemcpyAsync(&rs->delta, &dl, sizeof(dl), cudaMemcpyHostToDevice, st));
+        GHB_CUDA_TRY(cudaMemcpyAsync(&rs->budget, &budget, sizeof(budget), cudaMemcpyHostToDevice, st));
+    }
+    GHB_TRY(launch_coop(ws, mssp_pass_kernel, dim3(blocks), dim3(kMsspThreads), (size_t)0, n, n_active, k, ks, words,
+                        rp, col, wt, srcs_dev, perm, inf, dist_out, d, act_a, act_b, inq_a, inq_b, q_a, q_b, ch, cnt,
+                        rs, (unsigned long long)ws->tune.barrier_limit_us * 1000ull,
+                        (unsigned)ws->tune.barrier_extra));
+    GHB_CUDA_TRY(cudaMemcpyAsync(ws->host_pinned, rs, sizeof(MsspRunState), cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    MsspRunState h;
+    std::memcpy(&h, ws->host_pinned, sizeof(h));
+    if (h.status == kDevOverflow) {
+        set_error("multi-source SSSP round budget exceeded");
+        return GHB_ERR_LIMIT;
+    }
+    if (h.status != kDevOk) {
+        set_error("multi-source SSSP: grid barrier timed out");
+        return GHB_ERR_TIMEOUT;
+    }
+    if (rounds_out) *rounds_out += h.rounds;
+    if (examined_out) *examined_out += (int64_t)h.examined;
+    return GHB_OK;
+}
 
 // One pass of k <= 256 sources.  n_active: vertices [n_active, n) have no
 // entries.  perm (may be NULL) maps output ids to graph ids.
@@ -381,11 +669,23 @@ int mssssp_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* rp
     int32_t* sdev = static_cast<int32_t*>(ws->stage);
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
     int64_t rounds = 0, examined = 0;
+    int64_t m = 0;
+    const bool one_launch = ws->tune.mssp_persistent && mssp_pass_blocks(ws) > 0;
+    if (one_launch) {
+        int32_t* hp = reinterpret_cast<int32_t*>(ws->host_pinned);
+        GHB_CUDA_TRY(cudaMemcpyAsync(hp, rp + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        GHB_CUDA_TRY(cudaStreamSynchronize(st));
+        m = hp[0];
+    }
     for (int32_t s0 = 0; s0 < n_src; s0 += 256) {
         const int32_t k = std::min<int32_t>(256, n_src - s0);
         GHB_CUDA_TRY(cudaMemcpyAsync(sdev, srcs_host + s0, sizeof(int32_t) * k, cudaMemcpyHostToDevice, st));
-        GHB_TRY(mssssp_pass(ws, n, n_active, rp, col, wt, sdev, k, delta, inf, perm, dist + (int64_t)s0 * n, &rounds,
-                            &examined));
+        if (one_launch)
+            GHB_TRY(mssssp_pass_one_launch(ws, n, n_active, m, rp, col, wt, sdev, k, delta, inf, perm,
+                                           dist + (int64_t)s0 * n, &rounds, &examined));
+        else
+            GHB_TRY(mssssp_pass(ws, n, n_active, rp, col, wt, sdev, k, delta, inf, perm, dist + (int64_t)s0 * n,
+                                &rounds, &examined));
     }
     GHB_CUDA_TRY(cudaStreamSynchronize(st));
     if (stats) {

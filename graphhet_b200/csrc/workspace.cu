@@ -136,6 +136,7 @@ const TuneField kTuneFields[] = {
     {"ms_persistent", &ghb::Tuning::ms_persistent, 0, 1},
     {"bfs_blocks_per_sm", &ghb::Tuning::bfs_blocks_per_sm, 1, 2},
     {"pr_gathers", &ghb::Tuning::pr_gathers, 4, 8},
+    {"mssp_persistent", &ghb::Tuning::mssp_persistent, 0, 1},
 };
 const TuneField* tune_field(const char* name) {
     if (!name) return nullptr;

@@ -80,7 +80,9 @@ ghb_workspace* ghb_default_workspace(void);
  * or 1; default 1) whether a multi-source BFS pass is one cooperative launch
  * or host-driven levels, "bfs_blocks_per_sm" (1 or 2; default 2) the blocks
  * per SM of the whole-traversal BFS launch, "pr_gathers" (4 or 8) the
- * contribution gathers PageRank keeps in flight per lane on long rows.
+ * contribution gathers PageRank keeps in flight per lane on long rows,
+ * "mssp_persistent" (0 or 1; default 1) whether a multi-source SSSP pass is
+ * one cooperative launch or host-driven rounds.
  * Results do not depend on them.  "barrier_extra" (0 or 1) is a test knob:
  * 1 makes every grid barrier of the persistent kernels wait for one arrival
  * more than there are blocks, so every wait runs out after barrier_limit_us

@@ -464,10 +464,14 @@ def test_dangling_selection_matches_oracle_and_pagerank(G):
 def test_mssssp_matches_single_source(G, count):
     """Multi-source SSSP (one bucketed traversal per 256 sources): every row
     equals the oracle's Dijkstra bit for bit, on the raw CSR and the
-    relabelled handle, RMAT with U(0,1] weights and a grid with integer
-    weights; duplicate and isolated sources included."""
+    relabelled handle, RMAT with U(0,1] weights (one with a 1,585-entry
+    row, relaxed as 256-entry chunks) and a grid with integer weights;
+    duplicate and isolated sources included."""
     import ctypes
-    for og in (O.rmat_graph(11, 8, 3 + count), O.grid_graph(20, 30, count)):
+    graphs = [O.rmat_graph(11, 8, 3 + count), O.grid_graph(20, 30, count)]
+    if count in (64, 300):
+        graphs.append(O.rmat_graph(12, 24, 5))
+    for og in graphs:
         g = to_gpu(G, og)
         rng = np.random.default_rng(count)
         srcs = rng.integers(0, og.n, count).astype(np.int32)
@@ -476,21 +480,31 @@ def test_mssssp_matches_single_source(G, count):
         iso = np.nonzero(np.diff(og.rowptr) == 0)[0]
         if iso.size and count > 3:
             srcs[2] = iso[0]
-        d = torch.empty(count * og.n, dtype=torch.float64, device="cuda")
-        st = G.TraversalStats()
-        G._check(G.lib().ghb_mssssp(G._ws(None), og.n, G._ptr(g.rowptr), G._ptr(g.col), G._ptr(g.w),
-                                    G._ptr(torch.from_numpy(srcs).cuda()), count, G.DBL_MAX, G._ptr(d),
-                                    ctypes.byref(st)), "ghb_mssssp")
-        d = d.cpu().numpy().reshape(count, og.n)
-        rg = G.ResidentGraph(g)
-        dr = rg.mssssp(srcs)[0].cpu().numpy()
+        outs = {}
+        for one_launch in (1, 0):
+            G.tune_set("mssp_persistent", one_launch)
+            try:
+                d = torch.empty(count * og.n, dtype=torch.float64, device="cuda")
+                st = G.TraversalStats()
+                G._check(G.lib().ghb_mssssp(G._ws(None), og.n, G._ptr(g.rowptr), G._ptr(g.col), G._ptr(g.w),
+                                            G._ptr(torch.from_numpy(srcs).cuda()), count, G.DBL_MAX, G._ptr(d),
+                                            ctypes.byref(st)), "ghb_mssssp")
+                assert st.levels > 0 and st.edges_examined > 0
+                rg = G.ResidentGraph(g)
+                outs[one_launch] = (d.cpu().numpy().reshape(count, og.n), rg.mssssp(srcs)[0].cpu().numpy())
+                rg.close()
+            finally:
+                G.tune_set("mssp_persistent", 1)
+        # Both drivers (one cooperative launch per pass, host-driven rounds)
+        # give the same bits on every row.
+        assert np.array_equal(outs[1][0], outs[0][0]) and np.array_equal(outs[1][1], outs[0][1])
+        d, dr = outs[1]
         check = sorted({0, 1, 2, count // 2, count - 1} | set(range(0, count, 37)))
         for i in check:
             if i < count:
                 ref = O.sssp(og, int(srcs[i]))
                 assert np.array_equal(d[i], ref), i
                 assert np.array_equal(dr[i], ref), i
-        rg.close()
 
 
 def test_tc_complete_graph_long_oriented_rows(G):

@@ -85,3 +85,29 @@ def test_sssp_barrier_timeout_then_recovers(G):
     assert np.array_equal(rg.sssp(src, ws=ws)[0].cpu().numpy(), ref)
     assert np.array_equal(G.sssp(g, src, ws=ws)[0].cpu().numpy(), ref)
     rg.close()
+
+
+def test_multi_source_barrier_timeout_then_recovers(G):
+    """The one-launch multi-source BFS and SSSP passes give up on the same
+    bounded barrier, return GHB_ERR_TIMEOUT, and the workspace runs the
+    next pass normally."""
+    og = O.rmat_graph(12, 16, 42, directed=False)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    g = G.CSRGraph(n=og.n, rowptr=t(og.rowptr), col=t(og.col), w=t(og.w), directed=False)
+    ws = G.Workspace()
+    rg = G.ResidentGraph(g, ws=ws)
+    srcs = np.array([0, 5, 17, 300, 4095], dtype=np.int32)
+    G.tune_set("barrier_limit_us", 1000, ws=ws)
+    G.tune_set("barrier_extra", 1, ws=ws)
+    for call in (lambda: rg.msbfs(srcs, ws=ws), lambda: rg.mssssp(srcs, ws=ws)):
+        with pytest.raises(G.GhbError, match="timed out"):
+            call()
+    torch.cuda.synchronize()
+    G.tune_set("barrier_extra", 0, ws=ws)
+    G.tune_set("barrier_limit_us", 2000000, ws=ws)
+    depth = rg.msbfs(srcs, ws=ws)[0].cpu().numpy().reshape(len(srcs), og.n)
+    dist = rg.mssssp(srcs, ws=ws)[0].cpu().numpy().reshape(len(srcs), og.n)
+    for i, s in enumerate(srcs):
+        assert np.array_equal(depth[i], O.bfs(og, int(s)))
+        assert np.array_equal(dist[i], O.sssp(og, int(s)))
+    rg.close()
