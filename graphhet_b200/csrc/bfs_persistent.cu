@@ -108,19 +108,24 @@ __device__ __forceinline__ void p_flush(PAcc a, BfsRunState* st, int slot, bool 
     __syncthreads();
 }
 
-// Claim v for level `next_depth`.
+// Claim v for level `next_depth`.  filter: read the visited word before
+// the atomic (saves atomics on large frontiers, where most targets are
+// already visited); small frontiers skip it, since the read is one more
+// dependent round trip per level.  v's row bounds are read before the
+// claim so that they arrive while the atomic is in flight.
 __device__ __forceinline__ void p_visit(int32_t v, uint32_t* visited, uint32_t* f_next, int32_t* depth,
                                         int32_t next_depth, int32_t* q_next, int32_t* tail, bool append,
-                                        const int32_t* __restrict__ rowptr, PAcc& acc) {
+                                        const int32_t* __restrict__ rowptr, PAcc& acc, bool filter = true) {
     const uint32_t bit = 1u << (v & 31);
     uint32_t* wp = visited + (v >> 5);
-    if (*wp & bit) return;
+    if (filter && (*wp & bit)) return;
+    const int32_t rb = rowptr[v], re = rowptr[v + 1];
     if (atomicOr(wp, bit) & bit) return;
     depth[v] = next_depth;
     atomicOr(f_next + (v >> 5), bit);
     if (append) q_next[warp_append_active(tail)] = v;
     else acc.nf += 1;
-    const unsigned dv = (unsigned)(rowptr[v + 1] - rowptr[v]);
+    const unsigned dv = (unsigned)(re - rb);
     acc.mf += dv;
     acc.d2 += (unsigned long long)dv * dv;
     acc.dm = dv > acc.dm ? dv : acc.dm;
@@ -382,10 +387,21 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                 if (!p_barrier(st, [&]() { st->t_comp = global_timer_ns(); })) return;
             }
             // Short and medium rows; rows of >= kBigList entries deferred.
-            for (int64_t base = warp * 32; base < n_f; base += nwarps * 32) {
+            // A warp takes vpw frontier vertices (one per lane): 32 on large
+            // frontiers; on small ones fewer, so that the frontier's entries
+            // spread over every warp of the grid instead of queueing behind
+            // each other in a few warps (each pass of a warp over its
+            // entries is a chain of dependent loads and atomics).
+            int32_t vpw = 32;
+            if ((int64_t)n_f < nwarps * 16) {
+                vpw = 1;
+                while (vpw < 32 && (int64_t)vpw * nwarps < n_f) vpw <<= 1;
+            }
+            const bool filter = vpw == 32;
+            for (int64_t base = warp * vpw; base < n_f; base += nwarps * vpw) {
                 const int64_t i = base + lane;
                 int32_t b = 0, e = 0;
-                if (i < n_f) {
+                if (lane < vpw && i < n_f) {
                     const int32_t u = q_cur[i];
                     b = out_rp[u];
                     e = out_rp[u + 1];
@@ -403,7 +419,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                     const int32_t le = __shfl_sync(0xffffffffu, e, leader);
                     for (int32_t j = lb + lane; j < le; j += 32)
                         p_visit(out_col[j], visited, f_next, depth, next_depth, q_next, &st->nf[nslot], append,
-                                out_rp, acc);
+                                out_rp, acc, filter);
                 }
                 if (e - b >= 32) e = b;
                 const int32_t d = e - b;
@@ -428,7 +444,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                     const int32_t oe = __shfl_sync(0xffffffffu, excl, owner);
                     if (k < total)
                         p_visit(out_col[ob + (k - oe)], visited, f_next, depth, next_depth, q_next, &st->nf[nslot],
-                                append, out_rp, acc);
+                                append, out_rp, acc, filter);
                 }
             }
             for (int64_t w = gtid; w < words; w += gsize) f_clear[w] = 0u;

@@ -663,7 +663,7 @@ int mssssp_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* rp
     cudaStream_t st = ws->stream;
     if (!(delta > 0)) {
         GHB_TRY(sssp_pick_delta(ws, n, rp, wt, &delta));
-        delta *= 4.0;
+        delta = std::ldexp(delta, ws->tune.mssp_width_log2);
     }
     GHB_TRY(ws_reserve_stage(ws, sizeof(int32_t) * 256));
     int32_t* sdev = static_cast<int32_t*>(ws->stage);

@@ -137,6 +137,7 @@ const TuneField kTuneFields[] = {
     {"bfs_blocks_per_sm", &ghb::Tuning::bfs_blocks_per_sm, 1, 2},
     {"pr_gathers", &ghb::Tuning::pr_gathers, 4, 8},
     {"mssp_persistent", &ghb::Tuning::mssp_persistent, 0, 1},
+    {"mssp_width_log2", &ghb::Tuning::mssp_width_log2, -10, 10},
 };
 const TuneField* tune_field(const char* name) {
     if (!name) return nullptr;
