@@ -80,6 +80,7 @@ struct Tuning {
     int32_t bfs_blocks_per_sm = 2; // whole-traversal BFS: 512-thread blocks per SM (1 or 2)
     int32_t pr_gathers = 4;        // PageRank long rows: contribution gathers in flight per lane (4 or 8)
     int32_t mssp_persistent = 1;   // multi-source SSSP: 1 = one cooperative launch per pass, 0 = host-driven
+    int32_t tc_trim_min = 0;       // triangle counting: lists N+(b) over this many entries are range-trimmed
     int32_t mssp_width_log2 = 2;   // multi-source SSSP bucket width: the single-source rule's times 2^k
 };
 

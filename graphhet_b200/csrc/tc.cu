@@ -108,16 +108,22 @@ struct KeepCountVisitor {
     __device__ void finish() const {}
 };
 
-// Ordered fill of the oriented rows: warp per row (block per row when long).
+// Ordered fill of the oriented rows: a warp per row; rows over kWalkBig
+// entries are listed in long_rows (count in [0], rows from [1]) for
+// orient_fill_long_kernel.
 __global__ void __launch_bounds__(256) orient_fill_kernel(int32_t n, const int32_t* __restrict__ rowptr,
                                                           const int32_t* __restrict__ col,
-                                                          const int32_t* __restrict__ orp, int32_t* ocol) {
+                                                          const int32_t* __restrict__ orp, int32_t* ocol,
+                                                          int32_t* long_rows) {
     const int lane = lane_id();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t u = warp; u < n; u += nwarps) {
         const int32_t b = rowptr[u], e = rowptr[u + 1];
-        if (e - b > kWalkBig) continue;  // long rows: orient_fill_long_kernel
+        if (e - b > kWalkBig) {
+            if (lane == 0) long_rows[1 + atomicAdd(long_rows, 1)] = (int32_t)u;
+            continue;
+        }
         int32_t out = orp[u];
         for (int32_t j0 = b; j0 < e; j0 += 32) {
             const int32_t j = j0 + lane;
@@ -134,35 +140,54 @@ __global__ void __launch_bounds__(256) orient_fill_kernel(int32_t n, const int32
     }
 }
 
-__global__ void __launch_bounds__(1024) orient_fill_long_kernel(int32_t n, const int32_t* __restrict__ rowptr,
+// The listed long rows, a block per row: each thread takes kOrientItems
+// consecutive entries per step (their loads issued together), a block scan
+// of the kept counts places them in row order.
+constexpr int kOrientItems = 8;
+__global__ void __launch_bounds__(1024) orient_fill_long_kernel(const int32_t* __restrict__ rowptr,
                                                                 const int32_t* __restrict__ col,
-                                                                const int32_t* __restrict__ orp, int32_t* ocol) {
+                                                                const int32_t* __restrict__ orp, int32_t* ocol,
+                                                                const int32_t* __restrict__ long_rows) {
     __shared__ int32_t wsum[32];
-    __shared__ int32_t carry;
-    for (int64_t u = blockIdx.x; u < n; u += gridDim.x) {
+    const int lane = lane_id(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int32_t nl = long_rows[0];
+    for (int32_t r = blockIdx.x; r < nl; r += gridDim.x) {
+        const int32_t u = long_rows[1 + r];
         const int32_t b = rowptr[u], e = rowptr[u + 1];
-        if (e - b <= kWalkBig) continue;
-        if (threadIdx.x == 0) carry = orp[u];
-        __syncthreads();
-        for (int32_t j0 = b; j0 < e; j0 += blockDim.x) {
-            const int32_t j = j0 + threadIdx.x;
-            int32_t v = 0;
-            bool k = false;
-            if (j < e) {
-                v = col[j];
-                k = ranks_above(rowptr, (int32_t)u, v);
+        const int32_t du = e - b;
+        int32_t out = orp[u];
+        for (int32_t j0 = b; j0 < e; j0 += (int32_t)blockDim.x * kOrientItems) {
+            const int32_t jt = j0 + (int32_t)threadIdx.x * kOrientItems;
+            int32_t v[kOrientItems];
+#pragma unroll
+            for (int q = 0; q < kOrientItems; ++q) v[q] = jt + q < e ? col[jt + q] : -1;
+            int32_t dv[kOrientItems];
+#pragma unroll
+            for (int q = 0; q < kOrientItems; ++q) dv[q] = v[q] >= 0 ? rowptr[v[q] + 1] - rowptr[v[q]] : -1;
+            unsigned keep = 0;
+#pragma unroll
+            for (int q = 0; q < kOrientItems; ++q)
+                if (v[q] >= 0 && (dv[q] > du || (dv[q] == du && v[q] > u))) keep |= 1u << q;
+            const int32_t c = __popc(keep);
+            int32_t incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += x;
             }
-            const unsigned km = __ballot_sync(0xffffffffu, k);
-            if (lane_id() == 0) wsum[threadIdx.x >> 5] = __popc(km);
+            if (lane == 31) wsum[wid] = incl;
             __syncthreads();
             int32_t before = 0, all = 0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-                if (w < (int)(threadIdx.x >> 5)) before += wsum[w];
-                all += wsum[w];
+            for (int w = 0; w < nw; ++w) {
+                const int32_t x = wsum[w];
+                if (w < wid) before += x;
+                all += x;
             }
-            if (k) ocol[carry + before + __popc(km & ((1u << lane_id()) - 1u))] = v;
-            __syncthreads();
-            if (threadIdx.x == 0) carry += all;
+            int32_t pos = out + before + incl - c;
+#pragma unroll
+            for (int q = 0; q < kOrientItems; ++q)
+                if ((keep >> q) & 1u) ocol[pos++] = v[q];
+            out += all;
             __syncthreads();
         }
     }
@@ -260,7 +285,7 @@ __device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __rest
                                                            const int32_t* __restrict__ ocol, int32_t ab, int32_t k,
                                                            int32_t g0, int32_t g_end, int32_t stride,
                                                            const int32_t* keys, uint32_t mask, int shift, int32_t* bc,
-                                                           int32_t bc_off, unsigned long long* cnt) {
+                                                           int32_t bc_off, unsigned long long* cnt, int32_t trim_min) {
     const int lane = lane_id();
     unsigned long long a_hits = 0;
     const int32_t amin = ocol[ab], amax = ocol[ab + k - 1];
@@ -272,9 +297,13 @@ __device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __rest
             lb = orp[b];
             le = orp[b + 1];
             // Only N+(b)'s entries inside [min N+(a), max N+(a)] can be in
-            // N+(a) (both rows ascending): cut the rest off first.
-            lb = lower_bound_from(ocol, lb, le, amin);
-            le = upper_bound_pos(ocol, lb, le, amax);
+            // N+(a) (both rows ascending): lists over trim_min entries are
+            // cut to that range first (two binary searches, a chain of
+            // dependent loads that short lists do not repay).
+            if (le - lb > trim_min) {
+                lb = lower_bound_from(ocol, lb, le, amin);
+                le = upper_bound_pos(ocol, lb, le, amax);
+            }
         }
         unsigned med = __ballot_sync(0xffffffffu, le - lb >= 32);
         while (med) {
@@ -356,7 +385,7 @@ __global__ void __launch_bounds__(kTcWarpBlock) tc_hash_warp_kernel(int32_t n, c
                                                                     const int32_t* __restrict__ ocol,
                                                                     unsigned long long* cnt, int2* items,
                                                                     int64_t item_cap, int32_t* huge, int32_t* tails,
-                                                                    int32_t block_row) {
+                                                                    int32_t block_row, int32_t trim_min) {
     __shared__ int32_t s_keys[kTcWarpBlock / 32][kTcWarpSlots];
     __shared__ int32_t s_bc[kTcWarpBlock / 32][kTcWarpRow];
     const int lane = lane_id();
@@ -388,7 +417,7 @@ __global__ void __launch_bounds__(kTcWarpBlock) tc_hash_warp_kernel(int32_t n, c
         for (int32_t i = lane; i < k; i += 32) tc_insert(keys, kTcWarpSlots - 1, shift, ocol[ab + i]);
         __syncwarp();
         unsigned long long a_hits =
-            tc_row_share(orp, ocol, ab, k, 0, k, 32, keys, kTcWarpSlots - 1, shift, bc, 0, cnt);
+            tc_row_share(orp, ocol, ab, k, 0, k, 32, keys, kTcWarpSlots - 1, shift, bc, 0, cnt, trim_min);
         __syncwarp();
         a_hits = warp_sum(a_hits);
         if (lane == 0 && a_hits) atomicAdd(cnt + a, a_hits);
@@ -408,7 +437,7 @@ template <int CAP_LOG2, bool DYN>
 __global__ void __launch_bounds__(kTcBlockThreads) tc_hash_slice_kernel(const int32_t* __restrict__ orp,
                                                                         const int32_t* __restrict__ ocol,
                                                                         unsigned long long* cnt, const int2* items,
-                                                                        const int32_t* count) {
+                                                                        const int32_t* count, int32_t trim_min) {
     extern __shared__ int32_t s_dyn[];
     __shared__ int32_t s_static[DYN ? 1 : (1 << CAP_LOG2)];
     __shared__ int32_t s_bc[kTcSlice];
@@ -432,7 +461,7 @@ __global__ void __launch_bounds__(kTcBlockThreads) tc_hash_slice_kernel(const in
         for (int32_t i = threadIdx.x; i < k; i += blockDim.x) tc_insert(keys, cap - 1, shift, ocol[ab + i]);
         __syncthreads();
         unsigned long long a_hits = tc_row_share(orp, ocol, ab, k, gs + warp_in_block * 32, ge, warps * 32, keys,
-                                                 cap - 1, shift, s_bc, gs, cnt);
+                                                 cap - 1, shift, s_bc, gs, cnt, trim_min);
         a_hits = warp_sum(a_hits);
         if (lane_id() == 0 && a_hits) atomicAdd(&s_hits, a_hits);
         __syncthreads();
@@ -478,9 +507,10 @@ int tc_count_oriented(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* or
     GHB_CUDA_TRY(cudaMemsetAsync(tails, 0, 4 * sizeof(int32_t), ws->stream));
     GHB_TRY(launch(ws, tc_hash_warp_kernel, dim3(grid_for((int64_t)n * 32, kTcWarpBlock, ws->num_sms * 8)),
                    dim3(kTcWarpBlock), 0, n, orp, ocol, cnt, items, item_cap, huge, tails,
-                   std::min<int32_t>(std::max<int32_t>(ws->tune.tc_block_row, kTcWarpRow), kTcBlockRow)));
+                   std::min<int32_t>(std::max<int32_t>(ws->tune.tc_block_row, kTcWarpRow), kTcBlockRow),
+                   ws->tune.tc_trim_min));
     GHB_TRY(launch(ws, tc_hash_slice_kernel<kTcMidLog2, false>, dim3(ws->num_sms * 12), dim3(kTcBlockThreads), 0,
-                   orp, ocol, cnt, (const int2*)items, (const int32_t*)tails));
+                   orp, ocol, cnt, (const int2*)items, (const int32_t*)tails, ws->tune.tc_trim_min));
     const size_t smem = sizeof(int32_t) << kTcBigLog2;
     static bool attr_set[64] = {false};
     if (ws->device >= 0 && ws->device < 64 && !attr_set[ws->device]) {
@@ -489,7 +519,8 @@ int tc_count_oriented(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* or
         attr_set[ws->device] = true;
     }
     GHB_TRY(launch(ws, tc_hash_slice_kernel<kTcBigLog2, true>, dim3(ws->num_sms * 3), dim3(kTcBlockThreads), smem,
-                   orp, ocol, cnt, (const int2*)(items + item_cap), (const int32_t*)(tails + 1)));
+                   orp, ocol, cnt, (const int2*)(items + item_cap), (const int32_t*)(tails + 1),
+                   ws->tune.tc_trim_min));
     // Rows over the block path's length: the galloping walk.
     return walk(ws, orp, ocol, (const int32_t*)huge, (const int32_t*)(tails + 2), (int64_t)0,
                 (int64_t)ws->num_sms * 64, wb, OrientedVisitor{orp, ocol, cnt});
@@ -542,6 +573,18 @@ __global__ void tc_finish_kernel(int32_t n, const unsigned long long* __restrict
 
 }  // namespace
 
+// The oriented CSR's columns (orp already scanned); `lists` (at least n + 1
+// ints, the counting scratch, free until the count) holds the long-row list.
+static int orient_fill(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int32_t* col, const int32_t* orp,
+                       int32_t* ocol, int32_t* lists) {
+    GHB_CUDA_TRY(cudaMemsetAsync(lists, 0, sizeof(int32_t), ws->stream));
+    GHB_TRY(launch(ws, orient_fill_kernel, dim3(grid_for((int64_t)n * 32, 256, ws->num_sms * 8)), dim3(256), 0, n,
+                   rowptr, col, orp, ocol, lists));
+    GHB_TRY(launch(ws, orient_fill_long_kernel, dim3(ws->num_sms * 2), dim3(1024), 0, rowptr, col, orp, ocol,
+                   (const int32_t*)lists));
+    return GHB_OK;
+}
+
 // Oriented triangle counting with no host round trip and no allocation: the
 // caller guarantees a symmetric, loop-free CSR with strictly increasing rows
 // and m = rowptr[n] entries, and passes tc_oriented_bytes(n, m) bytes of
@@ -574,10 +617,7 @@ int tc_oriented_core(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* row
     GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,
                  KeepCountVisitor{rowptr, keep}));
     GHB_TRY(scan_exclusive_i32(ws, keep, orp, n, bsums));
-    GHB_TRY(launch(ws, orient_fill_kernel, dim3(grid_for((int64_t)n * 32, 256, ws->num_sms * 8)), dim3(256), 0, n,
-                   rowptr, col, (const int32_t*)orp, ocol));
-    GHB_TRY(launch(ws, orient_fill_long_kernel, dim3(ws->num_sms), dim3(1024), 0, n, rowptr, col, (const int32_t*)orp,
-                   ocol));
+    GHB_TRY(orient_fill(ws, n, rowptr, col, orp, ocol, lists));
     GHB_TRY(tc_count_oriented(ws, n, m, orp, ocol, cnt, wb, lists));
     if (counts64)
         GHB_TRY(launch(ws, tc_finish_kernel, dim3(grid_for(n, 256, ws->num_sms * 8)), dim3(256), 0, n,
@@ -636,10 +676,7 @@ int tc_run_cached(ghb_workspace* ws, int32_t n, const int32_t* rowptr, const int
         GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n,
                      wb, KeepCountVisitor{rowptr, keep}));
         GHB_TRY(scan_exclusive_i32(ws, keep, orp, n, bsums));
-        GHB_TRY(launch(ws, orient_fill_kernel, dim3(grid_for((int64_t)n * 32, 256, ws->num_sms * 8)), dim3(256), 0,
-                       n, rowptr, col, (const int32_t*)orp, ocol));
-        GHB_TRY(launch(ws, orient_fill_long_kernel, dim3(ws->num_sms), dim3(1024), 0, n, rowptr, col,
-                       (const int32_t*)orp, ocol));
+        GHB_TRY(orient_fill(ws, n, rowptr, col, orp, ocol, lists));
         GHB_TRY(tc_count_oriented(ws, n, m, orp, ocol, cnt, wb, lists));
     } else {
         GHB_TRY(walk(ws, rowptr, col, (const int32_t*)nullptr, (const int32_t*)nullptr, (int64_t)n, (int64_t)n, wb,

@@ -138,6 +138,7 @@ const TuneField kTuneFields[] = {
     {"pr_gathers", &ghb::Tuning::pr_gathers, 4, 8},
     {"mssp_persistent", &ghb::Tuning::mssp_persistent, 0, 1},
     {"mssp_width_log2", &ghb::Tuning::mssp_width_log2, -10, 10},
+    {"tc_trim_min", &ghb::Tuning::tc_trim_min, 0, 1 << 20},
 };
 const TuneField* tune_field(const char* name) {
     if (!name) return nullptr;

@@ -533,14 +533,17 @@ def test_tc_complete_graph_long_oriented_rows(G):
 
 def test_tc_hash_paths_match_oracle(G):
     """Oriented hash-probe TC against the oracle on RMAT (hub rows over the
-    warp hash's 128 entries) and a sparse ER graph, with and without the
-    block path, and against the galloping path."""
+    warp hash's 128 entries, rows over 4,096 entries oriented by the
+    long-row kernel) and a sparse ER graph, with the range trim on every
+    list, on lists over 32 entries and on none, with and without the block
+    path, and against the galloping path."""
     for og in (O.rmat_graph(14, 16, 3, directed=False, weight_mode=0),
                O.make_graph(20000, *O.er_edges(20000, 60000, 8), False, weight_mode=0)):
         g = to_gpu(G, og)
         ref = O.tc(og)
         ws = G.Workspace()
-        for knob, value in ((None, None), ("tc_block_row", 128), ("tc_hash", 0)):
+        for knob, value in ((None, None), ("tc_trim_min", 32), ("tc_trim_min", 1 << 20), ("tc_block_row", 128),
+                            ("tc_hash", 0)):
             if knob:
                 G.tune_set(knob, value, ws=ws)
             c64, c32, total = G.tc(g, ws=ws)
