@@ -82,7 +82,10 @@ ghb_workspace* ghb_default_workspace(void);
  * per SM of the whole-traversal BFS launch, "pr_gathers" (4 or 8) the
  * contribution gathers PageRank keeps in flight per lane on long rows,
  * "mssp_persistent" (0 or 1; default 1) whether a multi-source SSSP pass is
- * one cooperative launch or host-driven rounds.
+ * one cooperative launch or host-driven rounds, "mssp_width_log2" (-10 -
+ * 10; default 2) the multi-source bucket width as the single-source weight
+ * rule's times 2^k, "tc_trim_min" (0 - 2^20; default 0) the shortest list
+ * N+(b) that triangle counting cuts to N+(a)'s id range before probing.
  * Results do not depend on them.  "barrier_extra" (0 or 1) is a test knob:
  * 1 makes every grid barrier of the persistent kernels wait for one arrival
  * more than there are blocks, so every wait runs out after barrier_limit_us
