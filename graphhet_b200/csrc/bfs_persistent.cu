@@ -36,8 +36,8 @@ constexpr int32_t kBigChunk = 256;
 struct BfsRunState {
     unsigned bar_count;            // barrier arrivals (own cache line)
     unsigned pad_a[31];
-    unsigned bar_release;          // barrier epochs (own cache line)
-    unsigned pad_b[31];
+    unsigned long long bar_release; // barrier epoch (low 16 bits) and the next level's state (own cache line)
+    unsigned pad_b[30];
     int32_t status;
     int32_t level;       // current level
     int32_t dir;         // 0 top-down, 1 bottom-up
@@ -131,20 +131,81 @@ __device__ __forceinline__ void p_visit(int32_t v, uint32_t* visited, uint32_t* 
     acc.dm = dv > acc.dm ? dv : acc.dm;
 }
 
-__device__ __forceinline__ bool p_barrier(BfsRunState* st) {
-    return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, NoLeader(), st->bar_limit_ns,
-                            st->bar_extra);
+// The release word of the traversal's grid barriers carries, above the
+// 16-bit epoch, the next level's state (payload bits below), so that a
+// waiting block learns it from the load that ends its wait instead of
+// reading the run state after it: one dependent round trip less per level.
+constexpr unsigned long long kPlNf = 0x7fffffffull;  // next frontier size
+constexpr unsigned long long kPlDone = 1ull << 32;
+constexpr unsigned long long kPlDir = 1ull << 33;      // bottom-up
+constexpr unsigned long long kPlAppend = 1ull << 34;   // top-down level appends to the queue
+constexpr unsigned long long kPlQueueOk = 1ull << 35;  // the queue holds the frontier
+constexpr unsigned long long kPlBig = 1ull << 36;      // long rows deferred: no decision yet
+
+__device__ __forceinline__ unsigned long long p_payload(int32_t nf, bool done, int dir, bool append, bool queue_ok) {
+    return ((unsigned long long)nf & kPlNf) | (done ? kPlDone : 0ull) | (dir ? kPlDir : 0ull) |
+           (append ? kPlAppend : 0ull) | (queue_ok ? kPlQueueOk : 0ull);
 }
-template <class F>
-__device__ __forceinline__ bool p_barrier(BfsRunState* st, const F& leader) {
-    return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, leader, st->bar_limit_ns,
-                            st->bar_extra);
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
 }
-// Barrier whose decision runs on every thread of the last block to arrive.
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Grid barrier of the traversal (the ordering of grid_sync_block_leader):
+// every thread of the last block to arrive runs leader() (which may contain
+// __syncthreads) and leaves the payload in *s_pl; the other blocks get it
+// there from the release word.  Bounded: a wait over bar_limit_ns raises
+// the status and returns false.
 template <class F>
-__device__ __forceinline__ bool p_barrier_block(BfsRunState* st, const F& leader) {
-    return grid_sync_block_leader(&st->bar_count, &st->bar_release, &st->status, leader, st->bar_limit_ns,
-                                  st->bar_extra);
+__device__ __forceinline__ bool p_sync(BfsRunState* st, const F& leader, unsigned long long* s_pl) {
+    __shared__ int s_ok4, s_last4;
+    __shared__ unsigned s_ep4;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned nblocks = gridDim.x + st->bar_extra;
+        const unsigned old = atom_add_acq_rel_u32(&st->bar_count, 1u);
+        s_ep4 = (old / nblocks + 1u) & 0xffffu;
+        s_last4 = (old % nblocks == nblocks - 1u) ? 1 : 0;
+        s_ok4 = 1;
+    }
+    __syncthreads();
+    if (s_last4) {
+        leader();
+        __syncthreads();
+        if (threadIdx.x == 0) st_release_u64(&st->bar_release, (*s_pl << 16) | s_ep4);
+    } else if (threadIdx.x == 0) {
+        const unsigned ep = s_ep4;
+        const uint64_t limit = st->bar_limit_ns;
+        unsigned spins = 0;
+        uint64_t t0 = 0;
+        while (true) {
+            const unsigned long long v = ld_acquire_u64(&st->bar_release);
+            if ((int16_t)(uint16_t)((unsigned)v - ep) >= 0) {
+                *s_pl = v >> 16;
+                break;
+            }
+            if ((++spins & 127u) == 0) {
+                if (*(volatile int32_t*)&st->status != 0) {
+                    s_ok4 = 0;
+                    break;
+                }
+                const uint64_t t = global_timer_ns();
+                if (t0 == 0) t0 = t;
+                else if (t - t0 > limit) {
+                    atomicExch(&st->status, (int32_t)kDevBarrierTimeout);
+                    s_ok4 = 0;
+                    break;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    return s_ok4 != 0;
 }
 
 // Output format of a top-down level: fmt 1 queue, 2 bitmap only, 0 by the
@@ -169,7 +230,7 @@ __device__ __noinline__ void level_eval(const float* pol, const float* feat, flo
     if (margin < band) policy_eval_block(pol, feat, h1, h2, logit);
 }
 
-__global__ void __launch_bounds__(512) bfs_persistent_kernel(
+__global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(
     int32_t n, int32_t n_active, const int32_t* __restrict__ out_rp, const int32_t* __restrict__ out_col,
     const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col, int32_t src, int32_t max_depth,
     int32_t* depth, uint32_t* visited, uint32_t* f0, uint32_t* f1, uint32_t* f2, int32_t* qa, int32_t* qb,
@@ -199,59 +260,54 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
     // stays in L2, and no block pays to stage it in shared memory.
     const bool net = pol != nullptr;
     const bool can_pull = in_rp != nullptr;
-    if (gtid == 0) {
-        qa[0] = src;
+    // The first level's state, worked out by every block (s_pl: the state
+    // payload each barrier hands on; see p_sync).
+    __shared__ unsigned long long s_pl;
+    if (threadIdx.x == 0) {
         const unsigned ds = (unsigned)(out_rp[src + 1] - out_rp[src]);
-        st->nf[0] = 1;
-        st->mf[0] = ds;
-        st->d2[0] = (unsigned long long)ds * ds;
-        st->dmax[0] = ds;
-        st->m_r = ds;
         int d0 = 0, f0req = 0;
         if (policy == GHB_POLICY_SCHEDULE && schedule && schedule_len > 0) {
             d0 = can_pull ? (schedule[0] & 1) : 0;
             f0req = (schedule[0] >> 1) & 3;
         }
-        st->append = p_append(d0, f0req, ds);
-        st->queue_ok = 1;
-        st->level = 0;
-        st->dir = d0;
-        st->done = max_depth <= 0 ? 1 : 0;
-        st->t_prev = global_timer_ns();
-        if (trace && trace_cap > 0)
-            bfs_features(trace, (double)n, (double)m_total, 1.0, (double)ds, (double)(m_total - (int64_t)ds), 0,
-                         (double)ds * ds, (double)ds, 0, 1.0, (double)n - 1.0);
+        const int32_t app0 = p_append(d0, f0req, ds);
+        s_pl = p_payload(1, max_depth <= 0, d0, app0 != 0, true);
+        if (blockIdx.x == 0) {
+            qa[0] = src;
+            st->nf[0] = 1;
+            st->mf[0] = ds;
+            st->d2[0] = (unsigned long long)ds * ds;
+            st->dmax[0] = ds;
+            st->m_r = ds;
+            st->append = app0;
+            st->queue_ok = 1;
+            st->level = 0;
+            st->dir = d0;
+            st->done = max_depth <= 0 ? 1 : 0;
+            st->t_prev = global_timer_ns();
+            if (trace && trace_cap > 0)
+                bfs_features(trace, (double)n, (double)m_total, 1.0, (double)ds, (double)(m_total - (int64_t)ds), 0,
+                             (double)ds * ds, (double)ds, 0, 1.0, (double)n - 1.0);
+        }
     }
-    if (!p_barrier(st)) return;
+    if (!p_sync(st, [] {}, &s_pl)) return;
 
     __shared__ float s_feat[kPolIn], s_h1[kPolH], s_h2[kPolH], s_logit[kPolOut];
     __shared__ int32_t s_dec[2];
     __shared__ float s_margin;
     __shared__ int32_t s_flag;
 
-    __shared__ int32_t s_state[6];
     volatile BfsRunState* vs = st;
-    while (true) {
-        // Settled by the previous barrier: every block reads the same values.
-        // Thread 0 reads them and shares them (all threads reading the same
-        // L2 line would serialise thousands of requests per level).
-        if (threadIdx.x == 0) {
-            const int32_t lv = vs->level;
-            s_state[0] = vs->done;
-            s_state[1] = lv;
-            s_state[2] = vs->dir;
-            s_state[3] = vs->append;
-            s_state[4] = vs->nf[lv % 3];
-            s_state[5] = vs->queue_ok;
-        }
-        __syncthreads();
-        if (s_state[0]) break;
-        const int32_t L = s_state[1];
-        const int dir = s_state[2];
+    // One iteration per level in every block; the level's state arrived
+    // with the previous barrier's release (s_pl).
+    for (int32_t L = 0;; ++L) {
+        const unsigned long long pl = s_pl;
+        if (pl & kPlDone) break;
+        const int dir = (pl & kPlDir) ? 1 : 0;
         const int slot = L % 3, nslot = (L + 1) % 3, cslot = (L + 2) % 3;
-        const bool append = s_state[3] != 0;
-        const int32_t n_f = s_state[4];
-        const bool queue_ok = s_state[5] != 0;
+        const bool append = (pl & kPlAppend) != 0;
+        const int32_t n_f = (int32_t)(pl & kPlNf);
+        const bool queue_ok = (pl & kPlQueueOk) != 0;
         // (selects, not an indexed array: an array would live in local memory)
         uint32_t* f_cur = slot == 0 ? f0 : (slot == 1 ? f1 : f2);
         uint32_t* f_next = nslot == 0 ? f0 : (nslot == 1 ? f1 : f2);
@@ -350,7 +406,9 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                 st->queue_ok = (dir == 0 && append) ? 1 : 0;
                 st->qcount = 0;
                 st->level = L + 1;
-                st->done = (nf_next == 0 || L + 1 >= max_depth) ? 1 : 0;
+                const bool done = nf_next == 0 || L + 1 >= max_depth;
+                st->done = done ? 1 : 0;
+                s_pl = p_payload(nf_next, done, nd, p_append(nd, fmt, mf_next) != 0, dir == 0 && append);
                 st->nf[cslot] = 0;
                 st->mf[cslot] = 0;
                 st->d2[cslot] = 0;
@@ -384,7 +442,10 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                         q_cur[pos++] = (int32_t)(w * 32 + b);
                     }
                 }
-                if (!p_barrier(st, [&]() { st->t_comp = global_timer_ns(); })) return;
+                if (!p_sync(st, [&]() {
+                        if (threadIdx.x == 0) st->t_comp = global_timer_ns();
+                    }, &s_pl))
+                    return;
             }
             // Short and medium rows; rows of >= kBigList entries deferred.
             // A warp takes vpw frontier vertices (one per lane): 32 on large
@@ -451,16 +512,18 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
             p_flush(acc, st, nslot, !append);
             acc = PAcc();
             // Decide now unless long rows were deferred (then after them).
-            if (!p_barrier_block(st, [&]() {
+            if (!p_sync(st, [&]() {
                     if (threadIdx.x == 0) s_flag = ((volatile BfsRunState*)st)->big[slot] == 0 ? 1 : 0;
                     __syncthreads();
                     if (s_flag) decide();
-                }))
+                    else if (threadIdx.x == 0) s_pl |= kPlBig;
+                }, &s_pl))
                 return;
             __shared__ int32_t s_nbig;
-            if (threadIdx.x == 0) s_nbig = vs->big[slot];
+            const bool big_pending = (s_pl & kPlBig) != 0;
+            if (big_pending && threadIdx.x == 0) s_nbig = vs->big[slot];
             __syncthreads();
-            const int32_t nbig = s_nbig;
+            const int32_t nbig = big_pending ? s_nbig : 0;
             if (nbig > 0) {
                 if (nbig <= kBigChunkRows) {
                     // Deferred rows cut into kBigChunk-entry chunks shared by
@@ -541,7 +604,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
                     }
                 }
                 p_flush(acc, st, nslot, !append);
-                if (!p_barrier_block(st, decide)) return;
+                if (!p_sync(st, decide, &s_pl)) return;
             }
         } else {
             // Bottom-up over the active vertices: a warp owns a bitmap word.
@@ -619,7 +682,7 @@ __global__ void __launch_bounds__(512) bfs_persistent_kernel(
             }
             for (int64_t w = gtid; w < words; w += gsize) f_clear[w] = 0u;
             p_flush(acc, st, nslot, true);
-            if (!p_barrier_block(st, decide)) return;
+            if (!p_sync(st, decide, &s_pl)) return;
         }
 
     }
