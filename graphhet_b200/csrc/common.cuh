@@ -74,12 +74,14 @@ struct Tuning {
     int32_t barrier_extra = 0;     // test knob: barriers wait for this many arrivals beyond the grid, so
                                    // every wait runs out and the timeout path is exercised (0 or 1)
     int32_t sssp_persistent = 1;   // SSSP: 1 = one cooperative launch per traversal, 0 = host-driven rounds
+    int32_t sssp_adapt = 0;        // one-launch SSSP: 1 = bucket widths adapt from bucket to bucket
     int32_t tc_hash = 1;           // TC: 1 = shared-memory hash probes per oriented row, 0 = galloping merges
     int32_t tc_block_row = 8192;   // TC hash path: longest oriented row a block hashes; longer rows gallop
     int32_t ms_persistent = 1;     // multi-source BFS: 1 = one cooperative launch per pass, 0 = host-driven levels
     int32_t bfs_blocks_per_sm = 2; // whole-traversal BFS: 512-thread blocks per SM (1 or 2)
     int32_t pr_gathers = 4;        // PageRank long rows: contribution gathers in flight per lane (4 or 8)
     int32_t mssp_persistent = 1;   // multi-source SSSP: 1 = one cooperative launch per pass, 0 = host-driven
+    int32_t tc_slice_blocks = 16;  // triangle counting: blocks per SM of the 2,048-slot slice kernel
     int32_t tc_trim_min = 0;       // triangle counting: lists N+(b) over this many entries are range-trimmed
     int32_t mssp_width_log2 = 2;   // multi-source SSSP bucket width: the single-source rule's times 2^k
 };

@@ -78,6 +78,13 @@ struct SsspRunState {
     unsigned long long bar_limit_ns;
     unsigned bar_extra;
     unsigned pad1;
+    // Bucket width: the light/heavy split stays at delta; the width of the
+    // buckets may move within [width_min, width_max] from one bucket to the
+    // next (equal to delta when the width does not adapt).
+    double width, width_min, width_max;
+    long long lp_mark;              // LIGHT passes before the current bucket
+    unsigned long long ex_mark;     // entries examined before the current bucket
+    unsigned long long adapt_work;  // a bucket examining fewer entries is small
 };
 
 namespace {
@@ -236,6 +243,10 @@ __device__ __forceinline__ bool sp_barrier(SsspRunState* st, const F& leader) {
     return grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, leader, st->bar_limit_ns,
                             st->bar_extra);
 }
+
+// Bucket-width adaptation: more LIGHT passes than this in a bucket halve
+// the next bucket's width.
+constexpr long long kSpAdaptLight = 4;
 
 // End of the bucket that holds distance mn, on the grid thr + k * delta.
 __device__ __forceinline__ double sp_next_thr(double thr, double delta, double mn) {
@@ -426,9 +437,25 @@ __global__ void __launch_bounds__(kSsspThreads, 2) sssp_persistent_kernel(
                 // settled later; a SPLIT that queues nothing then repeats
                 // with the exact minimum of the entries it kept).
                 const unsigned long long fb_ = v->fmin;
-                const double thr = v->thr, delta = v->delta;
+                const double thr = v->thr;
+                // The next bucket's width: halved after a bucket that took
+                // more than kSpAdaptLight LIGHT passes (its vertices were
+                // relaxed again and again), doubled after one that took at
+                // most two and examined little (passes with too little work
+                // for the grid).  Exact distances do not depend on it: the
+                // passes form a label-correcting loop in which a HEAVY pass
+                // that lowers a distance inside the bucket sends it back to
+                // a LIGHT pass, and R is refilled after every HEAVY pass.
+                double width = v->width;
+                const long long lp = v->light_passes - v->lp_mark;
+                const unsigned long long ex = v->examined - v->ex_mark;
+                if (lp > kSpAdaptLight) width = fmax(width * 0.5, v->width_min);
+                else if (lp <= 2 && ex < v->adapt_work) width = fmin(width * 2.0, v->width_max);
+                s->width = width;
+                s->lp_mark = v->light_passes;
+                s->ex_mark = v->examined;
                 const double mn = fb_ == ~0ull ? thr : __longlong_as_double((long long)fb_);
-                s->new_thr = sp_next_thr(thr, delta, mn);
+                s->new_thr = sp_next_thr(thr, width, mn);
                 s->fmin = ~0ull;
                 s->nq = v->far_tail;
                 s->phase = v->phase + 1;
@@ -578,6 +605,13 @@ int sssp_persistent_run(ghb_workspace* ws, int32_t n, const int32_t* rp, const i
         // bound any correct run, as in the host-driven loop.
         const long long budget = 64ll * n + 1024;
         GHB_CUDA_TRY(cudaMemcpyAsync(&rstate->pass_budget, &budget, sizeof(budget), cudaMemcpyHostToDevice, st));
+        // Bucket widths: delta, or from delta / 64 to delta * 64 when they
+        // adapt; a bucket is small below eight entries per thread.
+        const bool adapt = ws->tune.sssp_adapt != 0;
+        const double wd[3] = {delta, adapt ? delta / 64.0 : delta, adapt ? delta * 64.0 : delta};
+        GHB_CUDA_TRY(cudaMemcpyAsync(&rstate->width, wd, sizeof(wd), cudaMemcpyHostToDevice, st));
+        const unsigned long long work = 8ull * (unsigned long long)blocks * kSsspThreads;
+        GHB_CUDA_TRY(cudaMemcpyAsync(&rstate->adapt_work, &work, sizeof(work), cudaMemcpyHostToDevice, st));
     }
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
     GHB_TRY(launch_coop(ws, sssp_persistent_kernel, dim3(blocks), dim3(kSsspThreads), 0, n, rp, le, col, wt, src, inf,

@@ -509,7 +509,8 @@ int tc_count_oriented(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* or
                    dim3(kTcWarpBlock), 0, n, orp, ocol, cnt, items, item_cap, huge, tails,
                    std::min<int32_t>(std::max<int32_t>(ws->tune.tc_block_row, kTcWarpRow), kTcBlockRow),
                    ws->tune.tc_trim_min));
-    GHB_TRY(launch(ws, tc_hash_slice_kernel<kTcMidLog2, false>, dim3(ws->num_sms * 12), dim3(kTcBlockThreads), 0,
+    GHB_TRY(launch(ws, tc_hash_slice_kernel<kTcMidLog2, false>, dim3(ws->num_sms * ws->tune.tc_slice_blocks),
+                   dim3(kTcBlockThreads), 0,
                    orp, ocol, cnt, (const int2*)items, (const int32_t*)tails, ws->tune.tc_trim_min));
     const size_t smem = sizeof(int32_t) << kTcBigLog2;
     static bool attr_set[64] = {false};

@@ -131,6 +131,7 @@ const TuneField kTuneFields[] = {
     {"barrier_limit_us", &ghb::Tuning::barrier_limit_us, 100, 60000000},
     {"barrier_extra", &ghb::Tuning::barrier_extra, 0, 1},
     {"sssp_persistent", &ghb::Tuning::sssp_persistent, 0, 1},
+    {"sssp_adapt", &ghb::Tuning::sssp_adapt, 0, 1},
     {"tc_hash", &ghb::Tuning::tc_hash, 0, 1},
     {"tc_block_row", &ghb::Tuning::tc_block_row, 128, 8192},
     {"ms_persistent", &ghb::Tuning::ms_persistent, 0, 1},
@@ -139,6 +140,7 @@ const TuneField kTuneFields[] = {
     {"mssp_persistent", &ghb::Tuning::mssp_persistent, 0, 1},
     {"mssp_width_log2", &ghb::Tuning::mssp_width_log2, -10, 10},
     {"tc_trim_min", &ghb::Tuning::tc_trim_min, 0, 1 << 20},
+    {"tc_slice_blocks", &ghb::Tuning::tc_slice_blocks, 1, 16},
 };
 const TuneField* tune_field(const char* name) {
     if (!name) return nullptr;

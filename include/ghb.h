@@ -85,7 +85,12 @@ ghb_workspace* ghb_default_workspace(void);
  * one cooperative launch or host-driven rounds, "mssp_width_log2" (-10 -
  * 10; default 2) the multi-source bucket width as the single-source weight
  * rule's times 2^k, "tc_trim_min" (0 - 2^20; default 0) the shortest list
- * N+(b) that triangle counting cuts to N+(a)'s id range before probing.
+ * N+(b) that triangle counting cuts to N+(a)'s id range before probing,
+ * "tc_slice_blocks" (1 - 16; default 16) the blocks per SM of the slice
+ * kernel for oriented rows of 129 - 1,024 entries, "sssp_adapt" (0 or 1;
+ * default 0) whether the one-launch SSSP halves or doubles the bucket width
+ * from one bucket to the next (the light/heavy split stays at the width
+ * chosen for the call).
  * Results do not depend on them.  "barrier_extra" (0 or 1) is a test knob:
  * 1 makes every grid barrier of the persistent kernels wait for one arrival
  * more than there are blocks, so every wait runs out after barrier_limit_us

@@ -542,8 +542,8 @@ def test_tc_hash_paths_match_oracle(G):
         g = to_gpu(G, og)
         ref = O.tc(og)
         ws = G.Workspace()
-        for knob, value in ((None, None), ("tc_trim_min", 32), ("tc_trim_min", 1 << 20), ("tc_block_row", 128),
-                            ("tc_hash", 0)):
+        for knob, value in ((None, None), ("tc_slice_blocks", 1), ("tc_trim_min", 32), ("tc_trim_min", 1 << 20),
+                            ("tc_block_row", 128), ("tc_hash", 0)):
             if knob:
                 G.tune_set(knob, value, ws=ws)
             c64, c32, total = G.tc(g, ws=ws)

@@ -148,6 +148,30 @@ def test_sssp_one_launch_matches_host_rounds_and_oracle(G):
     rg.close()
 
 
+def test_sssp_adaptive_widths_match_oracle(G):
+    """Bucket widths that move from bucket to bucket (sssp_adapt = 1) on the
+    one-launch SSSP, widths far below and far above the light/heavy split:
+    distances equal the oracle's on the resident graph (split rows) and the
+    raw CSR (no split), RMAT with U(0,1] weights and a grid with integer
+    weights."""
+    for og in (O.rmat_graph(14, 16, 31, directed=False), O.grid_graph(60, 70, 9)):
+        g = to_gpu(G, og)
+        ws = G.Workspace()
+        rg = G.ResidentGraph(g, ws=ws)
+        G.tune_set("sssp_adapt", 1, ws=ws)
+        deg = np.diff(og.rowptr)
+        for src in (int(np.argmax(deg)), int(np.nonzero(deg)[0][-1])):
+            ref = O.sssp(og, src)
+            for delta in (0.0, 1e-4, 0.05, 2.0, 500.0):
+                d1, _ = rg.sssp(src, delta=delta, ws=ws)
+                assert np.array_equal(d1.cpu().numpy(), ref), (src, delta)
+                d2, _ = G.sssp(g, src, delta=delta, ws=ws)
+                assert np.array_equal(d2.cpu().numpy(), ref), (src, delta)
+        G.tune_set("sssp_adapt", 0, ws=ws)
+        assert G.tune_get("sssp_adapt", ws=ws) == 0
+        rg.close()
+
+
 def test_resident_cdlp_and_wcc_with_repeated_entries(G):
     """A symmetric CSR whose rows repeat some entries (so label counts of 2
     occur in the first CDLP iteration) and a directed graph: CDLP and WCC on
