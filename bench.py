@@ -334,9 +334,37 @@ def run_ours(args, world, rank, local):
     e1.record(stream)
     barrier_sync(world)
     e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
+    e2e_int32 = {"value": round(total_edges / (e2e_ms / 1e3) / 1e9, 3), "unit": "GTEPS",
+                 "d2h_bytes_per_step": 4 * n * len(srcs),
+                 "note": "ghb_graph_bfs into a device buffer, then a torch copy of the int32 depths to pinned host "
+                         "memory on a second stream, overlapped with the next BFS"}
+    del dbuf, hbuf
+
+    # ---- e2e through the C ABI's host-buffer entry: every step is one
+    # ghb_graph_bfs_many_host call that leaves all 64 depth vectors, int32,
+    # in a host array (traversal, byte copy over PCIe and host widening
+    # pipelined inside the call).  The array is written once before timing
+    # so that no page is first touched inside the timed region.
+    host_out = np.zeros((len(srcs), n), dtype=np.int32)
+    rg.bfs_many_host(srcs, out=host_out)
+    barrier_sync(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        _, hst = rg.bfs_many_host(srcs, out=host_out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier_sync(world)
+    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
+    byte_rows = hst["levels"] < 255
     e2e = {"value": round(total_edges / (e2e_ms / 1e3) / 1e9, 3), "unit": "GTEPS",
-           "h2d_bytes_per_step": 4 * len(srcs), "d2h_bytes_per_step": 4 * n * len(srcs),
-           "note": "depth of every BFS copied to pinned host memory, overlapped with the next BFS on a copy stream"}
+           "h2d_bytes_per_step": 4 * len(srcs), "d2h_bytes_per_step": (1 if byte_rows else 4) * n * len(srcs),
+           "note": "ghb_graph_bfs_many_host: all 64 depth vectors as int32 in a host array each step; the GPU "
+                   "traverses one source while the copy engine brings the previous one's depths as one byte "
+                   "each and host threads widen the one before",
+           "int32_copy_variant": e2e_int32}
+    del host_out
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "GTEPS", "n_gpus": world, "steps": args.steps,

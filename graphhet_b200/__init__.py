@@ -115,6 +115,7 @@ _SIGS = {
     "ghb_graph_perm": (ctypes.c_int, [_p, ctypes.POINTER(_p), ctypes.POINTER(_p)]),
     "ghb_graph_bfs": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p]),
     "ghb_graph_bfs_pred": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p, _p]),
+    "ghb_graph_bfs_many_host": (ctypes.c_int, [_p, _p, _p, _i32, _i32, _p, _i32, _p, _p]),
     "ghb_graph_msbfs": (ctypes.c_int, [_p, _p, _p, _i32, _p, _p]),
     "ghb_graph_msbfs_reserve": (ctypes.c_int, [_p, _p, _i32]),
     "ghb_graph_msbfs_launch": (ctypes.c_int, [_p, _p, _p, _i32, _p]),
@@ -650,6 +651,25 @@ class ResidentGraph:
             rows = min(trace_cap, st.levels)
             return depth, st.as_dict(), np.frombuffer(trace, dtype=np.float32).reshape(trace_cap, TRACE_COLS)[:rows].copy()
         return depth, st.as_dict()
+
+    def bfs_many_host(self, srcs, out=None, max_depth=INT32_MAX, policy=POLICY_HEURISTIC, host_threads=0,
+                      ws=None):
+        """Depths from every source into a host array (numpy int32, n_src x
+        n), the sources pipelined through the GPU, the copy engine and host
+        threads.  Returns (array, stats); stats["device_ms"] is the call's
+        wall time."""
+        import numpy as np
+        sh = np.ascontiguousarray(np.asarray(srcs, dtype=np.int32))
+        if out is None:
+            out = np.empty((len(sh), self.n), dtype=np.int32)
+        if out.dtype != np.int32 or not out.flags.c_contiguous or out.size < len(sh) * self.n:
+            raise ValueError("out must be a C-contiguous int32 array of n_src x n entries")
+        opt = BfsOptions(policy=policy)
+        st = TraversalStats()
+        _check(lib().ghb_graph_bfs_many_host(_ws(ws), self._h, sh.ctypes.data_as(_p), len(sh), max_depth,
+                                             out.ctypes.data_as(_p), host_threads, ctypes.byref(opt),
+                                             ctypes.byref(st)), "ghb_graph_bfs_many_host")
+        return out, st.as_dict()
 
     def bfs_pred(self, src, max_depth=INT32_MAX, ws=None):
         depth, pred = self._i32(), self._i32()

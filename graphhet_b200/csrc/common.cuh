@@ -103,6 +103,14 @@ struct ghb_workspace {
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
     int64_t launches = 0;
     ghb::Tuning tune;
+    // Many-source BFS into host memory (bfs_host.cu): device depth and byte
+    // buffers, pinned byte buffers, a copy stream and its events.
+    void* pipe_dev = nullptr;
+    size_t pipe_dev_cap = 0;
+    void* pipe_host = nullptr;
+    size_t pipe_host_cap = 0;
+    cudaStream_t pipe_stream = nullptr;
+    cudaEvent_t pipe_ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace ghb {

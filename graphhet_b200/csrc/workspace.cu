@@ -109,6 +109,12 @@ int ghb_workspace_destroy(ghb_workspace* ws) {
     if (ws->ev_stop) cudaEventDestroy(ws->ev_stop);
     if (ws->ev_a) cudaEventDestroy(ws->ev_a);
     if (ws->ev_b) cudaEventDestroy(ws->ev_b);
+    if (ws->pipe_stream) cudaStreamSynchronize(ws->pipe_stream);
+    if (ws->pipe_dev) cudaFree(ws->pipe_dev);
+    if (ws->pipe_host) cudaFreeHost(ws->pipe_host);
+    if (ws->pipe_stream) cudaStreamDestroy(ws->pipe_stream);
+    for (cudaEvent_t e : ws->pipe_ev)
+        if (e) cudaEventDestroy(e);
     delete ws;
     return GHB_OK;
 }
@@ -196,6 +202,13 @@ int ghb_workspace_trim(ghb_workspace* ws) {
     if (ws->stage) GHB_CUDA_TRY(cudaFree(ws->stage));
     ws->stage = nullptr;
     ws->stage_cap = 0;
+    if (ws->pipe_stream) GHB_CUDA_TRY(cudaStreamSynchronize(ws->pipe_stream));
+    if (ws->pipe_dev) GHB_CUDA_TRY(cudaFree(ws->pipe_dev));
+    ws->pipe_dev = nullptr;
+    ws->pipe_dev_cap = 0;
+    if (ws->pipe_host) GHB_CUDA_TRY(cudaFreeHost(ws->pipe_host));
+    ws->pipe_host = nullptr;
+    ws->pipe_host_cap = 0;
     return GHB_OK;
 }
 

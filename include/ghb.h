@@ -365,6 +365,20 @@ int ghb_graph_perm(const ghb_graph* g, const int32_t** perm, const int32_t** ipe
 
 int ghb_graph_bfs(ghb_workspace* ws, const ghb_graph* g, int32_t src, int32_t max_depth,
                   int32_t* depth, const ghb_bfs_options* options, ghb_traversal_stats* stats);
+/* BFS from each of n_src sources into the caller's HOST array depth_host
+ * (n_src x n int32, row i for srcs[i], caller's ids; srcs is a host array):
+ * the same values as n_src calls of ghb_graph_bfs followed by copies to the
+ * host.  No counterpart in the reference, whose Cuda_BFS returns one host
+ * vector per call (GPU_BFS_csr.cuh:320-327).  The sources are pipelined:
+ * the GPU traverses one while the copy engine brings the previous one's
+ * depths over as one byte each (traversals under 255 levels; deeper ones
+ * as int32) and host_threads host threads (0: up to 16) widen the one
+ * before into depth_host.  stats: levels is the maximum, the other counts
+ * are sums, device_ms is the call's wall time.  The workspace keeps two
+ * device depth buffers, their byte copies and two pinned byte buffers. */
+int ghb_graph_bfs_many_host(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
+                            int32_t max_depth, int32_t* depth_host, int32_t host_threads,
+                            const ghb_bfs_options* options, ghb_traversal_stats* stats);
 int ghb_graph_bfs_pred(ghb_workspace* ws, const ghb_graph* g, int32_t src, int32_t max_depth,
                        int32_t* depth, int32_t* pred, const ghb_bfs_options* options,
                        ghb_traversal_stats* stats);

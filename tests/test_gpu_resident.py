@@ -172,6 +172,38 @@ def test_sssp_adaptive_widths_match_oracle(G):
         rg.close()
 
 
+def test_bfs_many_host_matches_oracle(G):
+    """Many BFS into a host array (GPU traversal, byte copies, host
+    widening, pipelined): every row equals the oracle's depths.  A 600-vertex
+    path beside an RMAT component makes some traversals run over 255 levels
+    (their int32 depths are copied instead), in both pipeline slots; also a
+    depth limit, one host thread, a repeated and an isolated source, and the
+    error for a source outside [0, n)."""
+    s, d = O.rmat_edges(12, 8 << 12, 41)
+    base, plen = 1 << 12, 600
+    ps = np.arange(base, base + plen - 1, dtype=np.int32)
+    og = O.make_graph(base + plen, np.concatenate([s, ps]), np.concatenate([d, ps + 1]), False, weight_mode=0)
+    rg = G.ResidentGraph(to_gpu(G, og))
+    deg = np.diff(og.rowptr)
+    hub = int(np.argmax(deg))
+    iso = int(np.nonzero(deg == 0)[0][0])
+    srcs = [hub, base, base + 300, iso, hub, base + plen - 1, 17]
+    out, st = rg.bfs_many_host(srcs)
+    assert out.shape == (len(srcs), og.n)
+    for i, x in enumerate(srcs):
+        assert np.array_equal(out[i], O.bfs(og, x)), i
+    assert st["edges_reached"] == sum(rg.bfs(x)[1]["edges_reached"] for x in srcs)
+    assert st["levels"] >= plen - 1
+    out3, _ = rg.bfs_many_host(srcs, max_depth=3, host_threads=1)
+    for i, x in enumerate(srcs):
+        assert np.array_equal(out3[i], O.bfs(og, x, 3)), i
+    empty, _ = rg.bfs_many_host([])
+    assert empty.shape == (0, og.n)
+    with pytest.raises(G.GhbError):
+        rg.bfs_many_host([0, og.n])
+    rg.close()
+
+
 def test_resident_cdlp_and_wcc_with_repeated_entries(G):
     """A symmetric CSR whose rows repeat some entries (so label counts of 2
     occur in the first CDLP iteration) and a directed graph: CDLP and WCC on
