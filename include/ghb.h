@@ -372,8 +372,9 @@ int ghb_graph_bfs(ghb_workspace* ws, const ghb_graph* g, int32_t src, int32_t ma
  * vector per call (GPU_BFS_csr.cuh:320-327).  The sources are pipelined:
  * the GPU traverses one while the copy engine brings the previous one's
  * depths over as one byte each (traversals under 255 levels; deeper ones
- * as int32) and host_threads host threads (0: up to 16) widen the one
- * before into depth_host.  stats: levels is the maximum, the other counts
+ * as int32) and host_threads host threads (0: half the host's, at most 8)
+ * widen the one before into depth_host, with streaming stores where the
+ * host has AVX2.  stats: levels is the maximum, the other counts
  * are sums, device_ms is the call's wall time.  The workspace keeps two
  * device depth buffers, their byte copies and two pinned byte buffers. */
 int ghb_graph_bfs_many_host(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
