@@ -801,9 +801,10 @@ def dropin_leg(args, srcs):
     except ValueError:
         return {"unavailable": f"dropin_bfs_bench rc={r.returncode}: {r.stderr.strip()[-300:]}"}
     d["rc"] = r.returncode
-    d["note"] = ("Cuda_BFS(graph, csr, name) per source: BFS on the CSR_graph's resident copy, depth vector to a "
-                 "pageable host vector, ids -> names (vector<pair<string,int>>); bfs_plus_copy = the same call's "
-                 "device work and copy without the naming")
+    d["note"] = ("Cuda_BFS(graph, csr, name) per source: BFS on the CSR_graph's resident copy, the depths to a "
+                 "host vector (one byte each over PCIe, widened on host threads), ids -> names "
+                 "(vector<pair<string,int>>); bfs_plus_copy = the same call's BFS and depth transfer without the "
+                 "naming")
     return d
 
 

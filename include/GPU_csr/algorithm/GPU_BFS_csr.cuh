@@ -42,8 +42,14 @@ inline std::vector<std::pair<std::string, int>> Cuda_BFS(graph_structure<double>
     // The CSR_graph's resident relabelled copy (built on its first call; the
     // in-CSR, aliasing the out-CSR when undirected, enables bottom-up levels).
     ghb_graph* g = resident(csr_graph, V);
-    int* d = result_buffer<int>((std::size_t)V);
-    if (g && d && ghb_ok(ghb_graph_bfs(workspace(), g, src, max_depth, d, nullptr, nullptr), "ghb_graph_bfs"))
-        result_to_host(d, (std::size_t)V, depth);
+    // The depths come over as one byte each and are widened on host threads
+    // (ghb_graph_bfs_many_host with one source) into a host vector that this
+    // thread keeps between calls, so no page of it is first touched per call.
+    static thread_local std::vector<int> host_depth;
+    host_depth.resize((std::size_t)V);
+    if (g && ghb_ok(ghb_graph_bfs_many_host(workspace(), g, &src, 1, max_depth, host_depth.data(), 0, nullptr,
+                                            nullptr),
+                    "ghb_graph_bfs_many_host"))
+        return trans_id_val(graph, host_depth);
     return trans_id_val(graph, depth);
 }
