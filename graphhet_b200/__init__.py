@@ -59,6 +59,13 @@ class TraversalStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class MsbfsOptions(ctypes.Structure):
+    _fields_ = [("schedule", _p), ("schedule_len", _i32), ("trace", _p), ("trace_cap", _i32)]
+
+
+MS_TRACE_COLS = 6
+
+
 class PrOptions(ctypes.Structure):
     _fields_ = [("iterations", _i32), ("damping", _f64), ("precision", _i32),
                 ("tolerance", _f64), ("l1_history", _p)]
@@ -116,6 +123,7 @@ _SIGS = {
     "ghb_graph_bfs": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p]),
     "ghb_graph_bfs_pred": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p, _p]),
     "ghb_graph_bfs_many_host": (ctypes.c_int, [_p, _p, _p, _i32, _i32, _p, _i32, _p, _p]),
+    "ghb_graph_msbfs_ex": (ctypes.c_int, [_p, _p, _p, _i32, _p, _p, _p]),
     "ghb_graph_msbfs": (ctypes.c_int, [_p, _p, _p, _i32, _p, _p]),
     "ghb_graph_msbfs_reserve": (ctypes.c_int, [_p, _p, _i32]),
     "ghb_graph_msbfs_launch": (ctypes.c_int, [_p, _p, _p, _i32, _p]),
@@ -685,6 +693,32 @@ class ResidentGraph:
         _check(lib().ghb_graph_msbfs(_ws(ws), self._h, _ptr(sd), len(sd), _ptr(depth), ctypes.byref(st)),
                "ghb_graph_msbfs")
         return depth[: len(sd) * self.n].view(len(sd), self.n), st.as_dict()
+
+    def msbfs_ex(self, srcs, schedule=None, trace_cap=0, out=None, ws=None):
+        """Multi-source BFS with forced per-level directions (schedule: 0
+        push, 1 pull per level; None: the rule) and a per-level trace of the
+        first pass (rows: direction, ms, frontier vertices and out-entries,
+        vertices and out-entries found).  Returns (depth, stats, trace)."""
+        import numpy as np
+        sd = torch.as_tensor(srcs, dtype=torch.int32, device=self._dev)
+        depth = out if out is not None else self._i32(len(sd))
+        opt = MsbfsOptions()
+        sched = None
+        if schedule is not None:
+            sched = torch.as_tensor(list(schedule), dtype=torch.int8, device=self._dev)
+            opt.schedule, opt.schedule_len = _ptr(sched), sched.numel()
+        tr = None
+        if trace_cap > 0:
+            tr = torch.zeros(trace_cap * MS_TRACE_COLS, dtype=torch.float32, device=self._dev)
+            opt.trace, opt.trace_cap = _ptr(tr), trace_cap
+        st = TraversalStats()
+        _check(lib().ghb_graph_msbfs_ex(_ws(ws), self._h, _ptr(sd), len(sd), _ptr(depth), ctypes.byref(opt),
+                                        ctypes.byref(st)), "ghb_graph_msbfs_ex")
+        trace = None
+        if tr is not None:
+            rows = min(trace_cap, st.levels)
+            trace = tr.view(trace_cap, MS_TRACE_COLS)[:rows].cpu().numpy()
+        return depth[: len(sd) * self.n].view(len(sd), self.n), st.as_dict(), trace
 
     def msbfs_reserve(self, n_src, ws=None):
         """Size the workspace for msbfs_launch with up to n_src sources."""

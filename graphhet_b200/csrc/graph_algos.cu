@@ -52,6 +52,11 @@ int msbfs_batch(ghb_workspace* ws, int32_t n, int32_t n_active, const int32_t* o
                 const int32_t* in_rp, const int32_t* in_col, const int32_t* srcs_dev, int32_t k,
                 const int32_t* perm, int32_t* depth, int64_t* levels_out, int64_t* examined_out);
 size_t msbfs_persistent_bytes(int32_t n, int64_t m, int32_t n_src);
+int msbfs_persistent_steered(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, const int32_t* out_rp,
+                             const int32_t* out_col, const int32_t* in_rp, const int32_t* in_col,
+                             const int32_t* srcs, int32_t n_src, const int32_t* perm, int32_t* depth,
+                             int64_t* levels_out, int64_t* examined_out, const int8_t* schedule,
+                             int32_t schedule_len, float* trace, int32_t trace_cap);
 bool msbfs_persistent_available(ghb_workspace* ws, int32_t n_src);
 int msbfs_persistent(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, const int32_t* out_rp,
                      const int32_t* out_col, const int32_t* in_rp, const int32_t* in_col, const int32_t* srcs,
@@ -203,6 +208,43 @@ int ghb_graph_msbfs(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, 
                             (const int32_t*)g->perm, depth + (int64_t)s0 * g->n, &levels, &examined));
     }
     GHB_CUDA_TRY(cudaStreamSynchronize(st));  // hs (host) is read by the copies above
+    if (stats) {
+        GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
+        GHB_CUDA_TRY(cudaEventSynchronize(ws->ev_stop));
+        float ms = 0.f;
+        GHB_CUDA_TRY(cudaEventElapsedTime(&ms, ws->ev_start, ws->ev_stop));
+        stats->levels = (int32_t)levels;
+        stats->pull_levels = 0;
+        stats->reached = -1;
+        stats->edges_reached = -1;
+        stats->edges_examined = examined;
+        stats->device_ms = ms;
+    }
+    return GHB_OK;
+}
+
+int ghb_graph_msbfs_ex(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src, int32_t* depth,
+                       const ghb_msbfs_options* options, ghb_traversal_stats* stats) {
+    GRAPH_PRELUDE();
+    GHB_REQUIRE(srcs && depth && n_src >= 1, "bad arguments");
+    GHB_REQUIRE(!options || options->schedule_len >= 0, "schedule_len < 0");
+    GHB_REQUIRE(!options || !options->trace || options->trace_cap >= 0, "trace_cap < 0");
+    if (!msbfs_persistent_available(ws, n_src)) {
+        set_error("whole-pass multi-source BFS unavailable (no cooperative launch, or ms_persistent = 0)");
+        return GHB_ERR_UNSUPPORTED;
+    }
+    cudaStream_t st = ws->stream;
+    std::vector<int32_t> hs(n_src);
+    GHB_CUDA_TRY(cudaMemcpyAsync(hs.data(), srcs, sizeof(int32_t) * n_src, cudaMemcpyDeviceToHost, st));
+    GHB_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int32_t i = 0; i < n_src; ++i) GHB_REQUIRE(hs[i] >= 0 && hs[i] < g->n, "source outside [0, n)");
+    int64_t levels = 0, examined = 0;
+    GHB_TRY(ws_reserve(ws, msbfs_persistent_bytes(g->n, g->m, n_src)));
+    if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
+    GHB_TRY(msbfs_persistent_steered(ws, g->n, g->n_active, g->m, g->rowptr, g->col, g->in_rowptr, g->in_col, srcs,
+                                     n_src, (const int32_t*)g->perm, depth, &levels, &examined,
+                                     options ? options->schedule : nullptr, options ? options->schedule_len : 0,
+                                     options ? options->trace : nullptr, options ? options->trace_cap : 0));
     if (stats) {
         GHB_CUDA_TRY(cudaEventRecord(ws->ev_stop, st));
         GHB_CUDA_TRY(cudaEventSynchronize(ws->ev_stop));

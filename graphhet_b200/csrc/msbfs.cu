@@ -465,6 +465,18 @@ struct MsRunState {
     unsigned long long m_f;       // out-entries of the current frontier
     unsigned long long examined;  // entries read over the pass
     long long pull_levels;
+    unsigned long long t_prev;    // global timer at the previous decision
+};
+
+// Directions forced per level and a per-level trace (device arrays; null:
+// the rule decides, no trace).  Trace row L - 1 describes level L:
+// direction, time (ms), frontier vertices and out-entries it expanded,
+// vertices and out-entries it found.
+struct MsSteer {
+    const int8_t* schedule = nullptr;
+    int32_t schedule_len = 0;
+    float* trace = nullptr;
+    int32_t trace_cap = 0;
 };
 
 template <int W>
@@ -535,7 +547,7 @@ __global__ void __launch_bounds__(kMsThreads, 3) ms_pass_kernel(
     const int32_t* srcs, const int32_t* __restrict__ perm, int32_t* depth, uint64_t* seen, uint64_t* masks,
     int32_t chunk, uint64_t* next, int32_t* qa, int32_t* qb, int4* chunks, uint64_t* all, int32_t* hubs,
     MsCounters* cnt, MsRunState* st, int32_t pull_div, int32_t warp_rest, unsigned long long bar_limit_ns,
-    unsigned bar_extra) {
+    unsigned bar_extra, MsSteer steer) {
     const int64_t words = (int64_t)n * W;
     auto slot = [&](int32_t l) { return masks + (int64_t)(l % chunk) * words; };
     auto barrier = [&]() {
@@ -573,6 +585,17 @@ __global__ void __launch_bounds__(kMsThreads, 3) ms_pass_kernel(
         volatile MsRunState* vs = st;
         const int32_t active = vc->active;
         const unsigned long long mf = vc->m_f;
+        const unsigned long long now = global_timer_ns();
+        if (steer.trace && L >= 1 && L - 1 < steer.trace_cap) {
+            float* row = steer.trace + (size_t)(L - 1) * GHB_MS_TRACE_COLS;
+            row[0] = pulled ? 1.f : 0.f;
+            row[1] = (float)((double)(now - vs->t_prev) * 1e-6);
+            row[2] = (float)vs->active;
+            row[3] = (float)vs->m_f;
+            row[4] = (float)active;
+            row[5] = (float)mf;
+        }
+        st->t_prev = now;
         unsigned long long ex = vs->examined + vc->examined;
         if (L > 0 && !pulled) ex += vs->m_f;  // a push level reads every entry of its frontier
         st->examined = ex;
@@ -588,7 +611,10 @@ __global__ void __launch_bounds__(kMsThreads, 3) ms_pass_kernel(
         cnt->examined = 0;
         st->c_tail = 0;
         int32_t mode = 2;
-        if (active > 0 && L < n) mode = (can_pull && (double)mf * (double)pull_div > (double)m) ? 1 : 0;
+        if (active > 0 && L < n) {
+            if (steer.schedule && L < steer.schedule_len) mode = can_pull ? (steer.schedule[L] & 1) : 0;
+            else mode = (can_pull && (double)mf * (double)pull_div > (double)m) ? 1 : 0;
+        }
         st->mode = mode;
     };
     if (!grid_sync_leader(&st->bar_count, &st->bar_release, &st->status, [&]() { decide(0, false, false); },
@@ -709,7 +735,7 @@ size_t ms_pass_bytes(int32_t n, int64_t m) {
 template <int W>
 int ms_pass_launch(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, const int32_t* out_rp,
                    const int32_t* out_col, const int32_t* in_rp, const int32_t* in_col, const int32_t* srcs, int32_t k,
-                   const int32_t* perm, int32_t* depth) {
+                   const int32_t* perm, int32_t* depth, MsSteer steer = MsSteer()) {
     const int blocks = ms_pass_blocks<W>(ws);
     if (blocks <= 0) {
         set_error("cooperative launch unavailable");
@@ -727,7 +753,8 @@ int ms_pass_launch(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, co
                        out_col, pull ? in_rp : (const int32_t*)nullptr, pull ? in_col : (const int32_t*)nullptr, srcs,
                        perm, depth, s.seen, s.masks, s.chunk, s.next, s.qa, s.qb, s.chunks, s.all, s.hubs, s.cnt,
                        s.rs, ws->tune.ms_pull_div, ws->tune.ms_warp_rest,
-                       (unsigned long long)ws->tune.barrier_limit_us * 1000ull, (unsigned)ws->tune.barrier_extra);
+                       (unsigned long long)ws->tune.barrier_limit_us * 1000ull, (unsigned)ws->tune.barrier_extra,
+                       steer);
 }
 
 // After a launch that was not captured: its status and counters.
@@ -887,24 +914,50 @@ bool msbfs_persistent_available(ghb_workspace* ws, int32_t n_src) {
 int msbfs_persistent(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, const int32_t* out_rp,
                      const int32_t* out_col, const int32_t* in_rp, const int32_t* in_col, const int32_t* srcs,
                      int32_t n_src, const int32_t* perm, int32_t* depth, bool finish, int64_t* levels_out,
-                     int64_t* examined_out) {
+                     int64_t* examined_out, const MsSteer& steer) {
     for (int32_t s0 = 0; s0 < n_src; s0 += kMsPass) {
         const int32_t k = std::min<int32_t>(kMsPass, n_src - s0);
         const int w = ms_words_for(k);
         const int32_t* s = srcs + s0;
         int32_t* d = depth + (int64_t)s0 * n;
+        MsSteer st = steer;
+        if (s0 > 0) st.trace = nullptr;  // the trace describes the first pass
         if (w == 1) {
-            GHB_TRY(ms_pass_launch<1>(ws, n, n_active, m, out_rp, out_col, in_rp, in_col, s, k, perm, d));
+            GHB_TRY(ms_pass_launch<1>(ws, n, n_active, m, out_rp, out_col, in_rp, in_col, s, k, perm, d, st));
             if (finish) GHB_TRY(ms_pass_finish<1>(ws, n, m, levels_out, examined_out));
         } else if (w == 2) {
-            GHB_TRY(ms_pass_launch<2>(ws, n, n_active, m, out_rp, out_col, in_rp, in_col, s, k, perm, d));
+            GHB_TRY(ms_pass_launch<2>(ws, n, n_active, m, out_rp, out_col, in_rp, in_col, s, k, perm, d, st));
             if (finish) GHB_TRY(ms_pass_finish<2>(ws, n, m, levels_out, examined_out));
         } else {
-            GHB_TRY(ms_pass_launch<4>(ws, n, n_active, m, out_rp, out_col, in_rp, in_col, s, k, perm, d));
+            GHB_TRY(ms_pass_launch<4>(ws, n, n_active, m, out_rp, out_col, in_rp, in_col, s, k, perm, d, st));
             if (finish) GHB_TRY(ms_pass_finish<4>(ws, n, m, levels_out, examined_out));
         }
     }
     return GHB_OK;
+}
+
+int msbfs_persistent(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, const int32_t* out_rp,
+                     const int32_t* out_col, const int32_t* in_rp, const int32_t* in_col, const int32_t* srcs,
+                     int32_t n_src, const int32_t* perm, int32_t* depth, bool finish, int64_t* levels_out,
+                     int64_t* examined_out) {
+    return msbfs_persistent(ws, n, n_active, m, out_rp, out_col, in_rp, in_col, srcs, n_src, perm, depth, finish,
+                            levels_out, examined_out, MsSteer());
+}
+
+// Steered variant of ghb_graph_msbfs's one-launch path (schedule and trace
+// are device arrays or null).
+int msbfs_persistent_steered(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, const int32_t* out_rp,
+                             const int32_t* out_col, const int32_t* in_rp, const int32_t* in_col,
+                             const int32_t* srcs, int32_t n_src, const int32_t* perm, int32_t* depth,
+                             int64_t* levels_out, int64_t* examined_out, const int8_t* schedule,
+                             int32_t schedule_len, float* trace, int32_t trace_cap) {
+    MsSteer steer;
+    steer.schedule = schedule;
+    steer.schedule_len = schedule ? schedule_len : 0;
+    steer.trace = trace;
+    steer.trace_cap = trace ? trace_cap : 0;
+    return msbfs_persistent(ws, n, n_active, m, out_rp, out_col, in_rp, in_col, srcs, n_src, perm, depth, true,
+                            levels_out, examined_out, steer);
 }
 
 }  // namespace ghb

@@ -418,6 +418,41 @@ def regret(rg, sources: Sequence[int], repeats: int = 3) -> Dict[str, float]:
                 regret_beamer14=tot["beamer14"] / o - 1.0)
 
 
+def ms_regret(rg, sources: Sequence[int], repeats: int = 3) -> Dict[str, object]:
+    """Regret of the multi-source pass's direction rule against the
+    per-level oracle: a level finds the same vertices pushed or pulled, so
+    the pass is timed level by level under all-push and all-pull schedules
+    (the smallest of `repeats` times per level) and the oracle takes each
+    level's cheaper direction.  Returns the level times, the rule's and the
+    oracle's totals (ms), the oracle schedule run as a check, and the
+    rule's regret."""
+    _, st, _ = rg.msbfs_ex(sources, trace_cap=1)
+    levels = int(st["levels"])
+    cap = max(levels, 1)
+
+    def run(schedule):
+        best, dirs = None, None
+        for _ in range(repeats):
+            _, _, tr = rg.msbfs_ex(sources, schedule=schedule, trace_cap=cap)
+            t = tr[:, 1].astype(np.float64)
+            best = t if best is None else np.minimum(best, t)
+            dirs = tr[:, 0].astype(np.int32)
+        return best, dirs
+
+    t_rule, d_rule = run(None)
+    t_push, _ = run([0] * (levels + 1))
+    t_pull, _ = run([1] * (levels + 1))
+    best = np.where(t_pull < t_push, 1, 0).astype(np.int32)
+    oracle = float(np.minimum(t_push, t_pull).sum())
+    # Level L (trace row L - 1) takes schedule[L - 1].
+    t_sched, _ = run(best.tolist())
+    rule = float(t_rule.sum())
+    return dict(levels=levels, rule_dirs=d_rule.tolist(), oracle_dirs=best.tolist(),
+                ms=dict(rule=rule, oracle=oracle, oracle_run=float(t_sched.sum()), push=float(t_push.sum()),
+                        pull=float(t_pull.sum())),
+                regret_rule=rule / oracle - 1.0)
+
+
 def collect_sssp(specs: Sequence[GraphSpec], sssp_max_scale: int = 22, sssp_sources: int = 3,
                  log=print) -> Dict[str, np.ndarray]:
     """Width-head rows only (sssp_rows on every graph of `specs` up to

@@ -385,6 +385,26 @@ int ghb_graph_bfs_pred(ghb_workspace* ws, const ghb_graph* g, int32_t src, int32
                        ghb_traversal_stats* stats);
 int ghb_graph_msbfs(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
                     int32_t* depth, ghb_traversal_stats* stats);
+/* ghb_graph_msbfs with its levels' directions forced and timed (no
+ * counterpart in the reference): schedule (device int8 array, or NULL for
+ * the direction rule) gives level L's direction at schedule[L] (0 push, 1
+ * pull; levels past schedule_len follow the rule); trace (device float
+ * array, or NULL) receives GHB_MS_TRACE_COLS floats per level of the first
+ * pass (trace_cap rows at most): direction, level time in ms, frontier
+ * vertices and out-entries expanded, vertices and out-entries found.  A
+ * level finds the same vertices in either direction, so timing a pass under
+ * all-push and all-pull schedules gives each level's cheaper direction.
+ * Depths do not depend on the schedule.  Needs the one-launch pass
+ * (ms_persistent = 1 and cooperative launch). */
+#define GHB_MS_TRACE_COLS 6
+typedef struct {
+    const int8_t* schedule;
+    int32_t schedule_len;
+    float* trace;
+    int32_t trace_cap;
+} ghb_msbfs_options;
+int ghb_graph_msbfs_ex(ghb_workspace* ws, const ghb_graph* g, const int32_t* srcs, int32_t n_src,
+                       int32_t* depth, const ghb_msbfs_options* options, ghb_traversal_stats* stats);
 /* The same multi-source BFS as launches only, for CUDA-graph capture (no
  * counterpart in the reference, which runs one source per call): each pass
  * of up to 256 sources is one cooperative launch that runs every level, its

@@ -204,6 +204,32 @@ def test_bfs_many_host_matches_oracle(G):
     rg.close()
 
 
+def test_msbfs_forced_schedules_and_trace(G):
+    """The one-launch multi-source pass under forced directions (all push,
+    all pull, alternating): depths equal the oracle's in every case, the
+    trace's direction column is the schedule, and its counts are the
+    frontier sizes; the rule-steered run matches too."""
+    og = O.rmat_graph(13, 16, 19, directed=False)
+    rg = G.ResidentGraph(to_gpu(G, og))
+    deg = np.diff(og.rowptr)
+    srcs = [int(np.argmax(deg)), 3, 77, int(np.nonzero(deg)[0][-1])] + list(range(100, 160))
+    refs = [O.bfs(og, x) for x in srcs]
+    d0, st0, tr0 = rg.msbfs_ex(srcs, trace_cap=64)
+    levels = st0["levels"]
+    assert tr0.shape == (levels, G.MS_TRACE_COLS)
+    for sched in (None, [0] * 64, [1] * 64, [k & 1 for k in range(64)]):
+        d, st, tr = rg.msbfs_ex(srcs, schedule=sched, trace_cap=64)
+        for i, ref in enumerate(refs):
+            assert np.array_equal(d[i].cpu().numpy(), ref), (sched and sched[:4], i)
+        assert st["levels"] == levels
+        if sched is not None:
+            assert tr[:, 0].astype(int).tolist() == sched[:levels]
+        # The frontier a level finds is the next level's frontier.
+        assert np.array_equal(tr[1:, 2], tr[:-1, 4]) and np.array_equal(tr[1:, 3], tr[:-1, 5])
+        assert np.all(tr[:, 1] >= 0)
+    rg.close()
+
+
 def test_resident_cdlp_and_wcc_with_repeated_entries(G):
     """A symmetric CSR whose rows repeat some entries (so label counts of 2
     occur in the first CDLP iteration) and a directed graph: CDLP and WCC on
