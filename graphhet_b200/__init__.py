@@ -124,6 +124,7 @@ _SIGS = {
     "ghb_graph_bfs_pred": (ctypes.c_int, [_p, _p, _i32, _i32, _p, _p, _p, _p]),
     "ghb_graph_bfs_many_host": (ctypes.c_int, [_p, _p, _p, _i32, _i32, _p, _i32, _p, _p]),
     "ghb_graph_msbfs_ex": (ctypes.c_int, [_p, _p, _p, _i32, _p, _p, _p]),
+    "ghb_ms_policy_load": (ctypes.c_int, [_p, _i32]),
     "ghb_graph_msbfs": (ctypes.c_int, [_p, _p, _p, _i32, _p, _p]),
     "ghb_graph_msbfs_reserve": (ctypes.c_int, [_p, _p, _i32]),
     "ghb_graph_msbfs_launch": (ctypes.c_int, [_p, _p, _p, _i32, _p]),

@@ -78,6 +78,7 @@ struct Tuning {
     int32_t tc_hash = 1;           // TC: 1 = shared-memory hash probes per oriented row, 0 = galloping merges
     int32_t tc_block_row = 8192;   // TC hash path: longest oriented row a block hashes; longer rows gallop
     int32_t ms_persistent = 1;     // multi-source BFS: 1 = one cooperative launch per pass, 0 = host-driven levels
+    int32_t ms_learned = 0;        // multi-source BFS pass: 1 = the installed direction model decides each level
     int32_t bfs_blocks_per_sm = 2; // whole-traversal BFS: 512-thread blocks per SM (1 or 2)
     int32_t pr_gathers = 4;        // PageRank long rows: contribution gathers in flight per lane (4 or 8)
     int32_t mssp_persistent = 1;   // multi-source SSSP: 1 = one cooperative launch per pass, 0 = host-driven

@@ -26,7 +26,9 @@
 // entry is written once: at the flush of the level that reached it, or as
 // INT32_MAX by the final flush.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -446,6 +448,27 @@ __global__ void __launch_bounds__(256) ms_flush_kernel(int32_t n, int32_t n_scan
 // graph.
 
 constexpr int kMsThreads = 256;
+constexpr int kMsPolicyFeatures = 8;
+constexpr int kMsPolicyWeights = kMsPolicyFeatures + 1;
+
+// Features of a multi-source level decision (the same definitions as the
+// trainer's, graphhet_b200/policy.py ms_rows): the next frontier's share of
+// the entries and of the vertices, the mean degree, the pass's source
+// count, the level index, the frontier vertices visited so far, the last
+// level's direction and the frontier's growth, all but two as log2.
+__device__ __forceinline__ void ms_level_features(float* f, double mf, double active, double prev_active,
+                                                  double visits, double n, double m, int k, int level,
+                                                  int prev_pull) {
+    const double tiny = 1.0 / 1073741824.0;
+    f[0] = (float)log2(mf / m + tiny);
+    f[1] = (float)log2(active / n + tiny);
+    f[2] = (float)log2(m / n + tiny);
+    f[3] = (float)log2((double)k);
+    f[4] = (float)(level < 32 ? level : 32) * 0.125f;
+    f[5] = (float)log2(visits / n + tiny);
+    f[6] = (float)prev_pull;
+    f[7] = (float)log2((active + 1.0) / (prev_active + 1.0));
+}
 constexpr int32_t kMsBigRow = 4096;   // push rows this long are cut into chunks
 constexpr int32_t kMsRowChunk = 1024;
 
@@ -466,6 +489,7 @@ struct MsRunState {
     unsigned long long examined;  // entries read over the pass
     long long pull_levels;
     unsigned long long t_prev;    // global timer at the previous decision
+    long long visits;             // frontier vertices summed over the levels so far
 };
 
 // Directions forced per level and a per-level trace (device arrays; null:
@@ -477,6 +501,8 @@ struct MsSteer {
     int32_t schedule_len = 0;
     float* trace = nullptr;
     int32_t trace_cap = 0;
+    int32_t learned = 0;          // 1: the learned direction model below decides
+    float w[kMsPolicyWeights] = {};  // bias, then one weight per ms_level_features entry
 };
 
 template <int W>
@@ -585,6 +611,7 @@ __global__ void __launch_bounds__(kMsThreads, 3) ms_pass_kernel(
         volatile MsRunState* vs = st;
         const int32_t active = vc->active;
         const unsigned long long mf = vc->m_f;
+        const int32_t prev_active = vs->active;  // the frontier level L expanded
         const unsigned long long now = global_timer_ns();
         if (steer.trace && L >= 1 && L - 1 < steer.trace_cap) {
             float* row = steer.trace + (size_t)(L - 1) * GHB_MS_TRACE_COLS;
@@ -611,9 +638,22 @@ __global__ void __launch_bounds__(kMsThreads, 3) ms_pass_kernel(
         cnt->examined = 0;
         st->c_tail = 0;
         int32_t mode = 2;
+        const long long visits = vs->visits + active;
+        st->visits = visits;
         if (active > 0 && L < n) {
-            if (steer.schedule && L < steer.schedule_len) mode = can_pull ? (steer.schedule[L] & 1) : 0;
-            else mode = (can_pull && (double)mf * (double)pull_div > (double)m) ? 1 : 0;
+            if (steer.schedule && L < steer.schedule_len) {
+                mode = can_pull ? (steer.schedule[L] & 1) : 0;
+            } else if (steer.learned) {
+                float f[kMsPolicyFeatures];
+                ms_level_features(f, (double)mf, (double)active, (double)prev_active, (double)visits, (double)n,
+                                  (double)m, k, L + 1, pulled ? 1 : 0);
+                float z = steer.w[0];
+#pragma unroll
+                for (int i = 0; i < kMsPolicyFeatures; ++i) z += steer.w[1 + i] * f[i];
+                mode = (can_pull && z > 0.f) ? 1 : 0;
+            } else {
+                mode = (can_pull && (double)mf * (double)pull_div > (double)m) ? 1 : 0;
+            }
         }
         st->mode = mode;
     };
@@ -732,6 +772,12 @@ size_t ms_pass_bytes(int32_t n, int64_t m) {
 // when given, maps them and the outputs to the graph's ids).  Launch only:
 // the workspace must already hold ms_pass_bytes<W>(n, m) bytes of scratch,
 // and nothing is read back.
+// The installed direction model of the multi-source pass (process-wide,
+// ghb_ms_policy_load); used where the workspace's ms_learned is 1.
+std::mutex g_ms_policy_mu;
+bool g_ms_policy_set = false;
+float g_ms_policy[kMsPolicyWeights];
+
 template <int W>
 int ms_pass_launch(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, const int32_t* out_rp,
                    const int32_t* out_col, const int32_t* in_rp, const int32_t* in_col, const int32_t* srcs, int32_t k,
@@ -744,6 +790,13 @@ int ms_pass_launch(ghb_workspace* ws, int32_t n, int32_t n_active, int64_t m, co
     if (ms_pass_bytes<W>(n, m) > ws->scratch_cap) {
         set_error("multi-source pass: workspace scratch not reserved (ghb_graph_msbfs_reserve)");
         return GHB_ERR_INVALID_ARGUMENT;
+    }
+    if (ws->tune.ms_learned && !steer.schedule) {
+        std::lock_guard<std::mutex> lock(g_ms_policy_mu);
+        if (g_ms_policy_set) {
+            steer.learned = 1;
+            std::memcpy(steer.w, g_ms_policy, sizeof(g_ms_policy));
+        }
     }
     MsPassScratch<W> s = MsPassScratch<W>::carve(ws->scratch, n, m);
     GHB_CUDA_TRY(cudaMemsetAsync(s.cnt, 0, sizeof(MsCounters), ws->stream));
@@ -1010,5 +1063,18 @@ extern "C" int ghb_msbfs(ghb_workspace* ws, int32_t n, const int32_t* out_rowptr
         stats->edges_examined = examined;
         stats->device_ms = ms;
     }
+    return GHB_OK;
+}
+
+extern "C" int ghb_ms_policy_load(const float* weights, int32_t count) {
+    std::lock_guard<std::mutex> lock(ghb::g_ms_policy_mu);
+    if (!weights) {
+        ghb::g_ms_policy_set = false;
+        return GHB_OK;
+    }
+    GHB_REQUIRE(count == ghb::kMsPolicyWeights, "the multi-source direction model has 9 weights");
+    for (int i = 0; i < count; ++i) GHB_REQUIRE(std::isfinite(weights[i]), "weights must be finite");
+    std::memcpy(ghb::g_ms_policy, weights, sizeof(ghb::g_ms_policy));
+    ghb::g_ms_policy_set = true;
     return GHB_OK;
 }

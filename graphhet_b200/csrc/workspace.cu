@@ -141,6 +141,7 @@ const TuneField kTuneFields[] = {
     {"tc_hash", &ghb::Tuning::tc_hash, 0, 1},
     {"tc_block_row", &ghb::Tuning::tc_block_row, 128, 8192},
     {"ms_persistent", &ghb::Tuning::ms_persistent, 0, 1},
+    {"ms_learned", &ghb::Tuning::ms_learned, 0, 1},
     {"bfs_blocks_per_sm", &ghb::Tuning::bfs_blocks_per_sm, 1, 2},
     {"pr_gathers", &ghb::Tuning::pr_gathers, 4, 8},
     {"mssp_persistent", &ghb::Tuning::mssp_persistent, 0, 1},

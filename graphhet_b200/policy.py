@@ -377,11 +377,72 @@ def load(path: str = WEIGHTS_PATH):
 
 
 def install(path: str = WEIGHTS_PATH) -> dict:
-    """Install the trained network for POLICY_LEARNED (this process)."""
+    """Install the trained network for POLICY_LEARNED (this process), and
+    the multi-source pass's direction model when it has been trained."""
     import graphhet_b200 as G
     params, norm, info = load(path)
     G.policy_load(params, norm)
+    if os.path.exists(MS_WEIGHTS_PATH):
+        ms_install()
     return info
+
+
+# ------------------------------------------- multi-source direction model
+MS_WEIGHTS_PATH = os.path.join(_HERE, "policy_ms.npz")
+MS_FEATURES = 8
+
+
+def ms_features(mf, active, prev_active, visits, n, m, k, level, prev_pull) -> np.ndarray:
+    """The multi-source pass's level features, as the kernel computes them
+    (ms_level_features in csrc/msbfs.cu)."""
+    tiny = 1.0 / 1073741824.0
+    return np.array([math.log2(mf / m + tiny), math.log2(active / n + tiny), math.log2(m / n + tiny),
+                     math.log2(k), min(level, 32) * 0.125, math.log2(visits / n + tiny), float(prev_pull),
+                     math.log2((active + 1.0) / (prev_active + 1.0))], dtype=np.float64)
+
+
+def ms_rows(t_push: np.ndarray, t_pull: np.ndarray, trace: np.ndarray, n: int, m: int, k: int,
+            prev_dirs: Sequence[int]) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Training rows of one pass: row r decides level r + 1 from the frontier
+    it expands (trace row r, columns 2-3), the frontier before it and the
+    frontiers visited so far.  Label: 1 where the level pulled faster;
+    weight: what the wrong direction costs there (ms).  prev_dirs[r] is the
+    direction the level before took in the run whose trace is given."""
+    X, y, w = [], [], []
+    visits = 0.0
+    prev = 0.0
+    for r in range(len(trace)):
+        active, mf = float(trace[r, 2]), float(trace[r, 3])
+        visits += active
+        X.append(ms_features(mf, active, prev, visits, n, m, k, r + 1, prev_dirs[r]))
+        y.append(1.0 if t_pull[r] < t_push[r] else 0.0)
+        w.append(abs(float(t_pull[r]) - float(t_push[r])))
+        prev = active
+    return np.array(X), np.array(y), np.array(w)
+
+
+def fit_ms(X: np.ndarray, y: np.ndarray, w: np.ndarray, epochs: int = 20000, lr: float = 0.05,
+           l2: float = 1e-3) -> np.ndarray:
+    """Weighted logistic regression (bias + one weight per feature) by
+    gradient descent on the host; returns the 9 kernel weights."""
+    Xb = np.hstack([np.ones((len(X), 1)), X])
+    ww = w / max(w.mean(), 1e-12)
+    theta = np.zeros(Xb.shape[1])
+    for _ in range(epochs):
+        p = 1.0 / (1.0 + np.exp(-np.clip(Xb @ theta, -40, 40)))
+        g = Xb.T @ ((p - y) * ww) / len(y) + l2 * np.r_[0.0, theta[1:]]
+        theta -= lr * g
+    return theta.astype(np.float32)
+
+
+def ms_install(path: str = MS_WEIGHTS_PATH) -> np.ndarray:
+    """Load the multi-source direction model into the library (this process);
+    a workspace uses it where "ms_learned" is 1."""
+    import ctypes
+    import graphhet_b200 as G
+    wts = np.ascontiguousarray(np.load(path)["weights"].astype(np.float32))
+    G._check(G.lib().ghb_ms_policy_load(wts.ctypes.data_as(ctypes.c_void_p), len(wts)), "ghb_ms_policy_load")
+    return wts
 
 
 # ------------------------------------------------------------- evaluation
@@ -418,14 +479,15 @@ def regret(rg, sources: Sequence[int], repeats: int = 3) -> Dict[str, float]:
                 regret_beamer14=tot["beamer14"] / o - 1.0)
 
 
-def ms_regret(rg, sources: Sequence[int], repeats: int = 3) -> Dict[str, object]:
+def ms_regret(rg, sources: Sequence[int], repeats: int = 3, learned: bool = False) -> Dict[str, object]:
     """Regret of the multi-source pass's direction rule against the
     per-level oracle: a level finds the same vertices pushed or pulled, so
     the pass is timed level by level under all-push and all-pull schedules
     (the smallest of `repeats` times per level) and the oracle takes each
     level's cheaper direction.  Returns the level times, the rule's and the
     oracle's totals (ms), the oracle schedule run as a check, and the
-    rule's regret."""
+    rule's regret; with `learned`, also the installed direction model's
+    (workspace knob ms_learned on the default workspace)."""
     _, st, _ = rg.msbfs_ex(sources, trace_cap=1)
     levels = int(st["levels"])
     cap = max(levels, 1)
@@ -439,6 +501,7 @@ def ms_regret(rg, sources: Sequence[int], repeats: int = 3) -> Dict[str, object]
             dirs = tr[:, 0].astype(np.int32)
         return best, dirs
 
+    import graphhet_b200 as G
     t_rule, d_rule = run(None)
     t_push, _ = run([0] * (levels + 1))
     t_pull, _ = run([1] * (levels + 1))
@@ -447,10 +510,71 @@ def ms_regret(rg, sources: Sequence[int], repeats: int = 3) -> Dict[str, object]
     # Level L (trace row L - 1) takes schedule[L - 1].
     t_sched, _ = run(best.tolist())
     rule = float(t_rule.sum())
-    return dict(levels=levels, rule_dirs=d_rule.tolist(), oracle_dirs=best.tolist(),
-                ms=dict(rule=rule, oracle=oracle, oracle_run=float(t_sched.sum()), push=float(t_push.sum()),
-                        pull=float(t_pull.sum())),
-                regret_rule=rule / oracle - 1.0)
+    out = dict(levels=levels, rule_dirs=d_rule.tolist(), oracle_dirs=best.tolist(),
+               ms=dict(rule=rule, oracle=oracle, oracle_run=float(t_sched.sum()), push=float(t_push.sum()),
+                       pull=float(t_pull.sum())),
+               regret_rule=rule / oracle - 1.0)
+    if learned:
+        G.tune_set("ms_learned", 1)
+        try:
+            t_l, d_l = run(None)
+        finally:
+            G.tune_set("ms_learned", 0)
+        out["learned_dirs"] = d_l.tolist()
+        out["ms"]["learned"] = float(t_l.sum())
+        out["regret_learned"] = float(t_l.sum()) / oracle - 1.0
+    return out
+
+
+def collect_ms(specs: Sequence[GraphSpec], ks: Sequence[int] = (16, 64, 256), max_scale: int = 21,
+               repeats: int = 2, log=print) -> Dict[str, np.ndarray]:
+    """Rows for the multi-source direction model: every graph of `specs` up
+    to max_scale, one pass of k seeded sources per k, timed level by level
+    under all-push and all-pull schedules (the smallest of `repeats` runs)."""
+    import torch
+    import graphhet_b200 as G
+    Xs, ys, ws_, gs, rs = [], [], [], [], []
+    run = 0
+    t0 = time.time()
+    for gi, spec in enumerate(specs):
+        if spec.scale > max_scale:
+            continue
+        g = build_graph(spec, weighted=False)
+        rg = G.ResidentGraph(g)
+        for k in ks:
+            srcs = pick_sources(g, k, spec.seed + k)
+            if len(srcs) < 2:
+                continue
+            _, st, _ = rg.msbfs_ex(srcs, trace_cap=1)
+            levels = int(st["levels"])
+            if levels < 1:
+                continue
+            times, traces = {}, {}
+            for d in (0, 1):
+                best = None
+                for _ in range(repeats):
+                    _, _, tr = rg.msbfs_ex(srcs, schedule=[d] * (levels + 1), trace_cap=levels)
+                    t = tr[:, 1].astype(np.float64)
+                    best = t if best is None else np.minimum(best, t)
+                times[d], traces[d] = best, tr
+            # The previous direction is a feature: rows from both runs.
+            for d in (0, 1):
+                X, y, w = ms_rows(times[0], times[1], traces[d], g.n, g.m, len(srcs), [d] * levels)
+                if d == 1:
+                    X[0, 6] = 0.0  # level 1 follows the set-up, not a pull
+                Xs.append(X)
+                ys.append(y)
+                ws_.append(w)
+                gs.append(np.full(len(y), gi, np.int32))
+                rs.append(np.full(len(y), run, np.int32))
+            run += 1
+        rg.close()
+        del rg, g
+        torch.cuda.empty_cache()
+        if log and gi % 10 == 0:
+            log("ms graph %d/%d %s scale %d (%.0f s)" % (gi + 1, len(specs), spec.kind, spec.scale, time.time() - t0))
+    return dict(X=np.concatenate(Xs), y=np.concatenate(ys), w=np.concatenate(ws_), G=np.concatenate(gs),
+                R=np.concatenate(rs))
 
 
 def collect_sssp(specs: Sequence[GraphSpec], sssp_max_scale: int = 22, sssp_sources: int = 3,
@@ -555,7 +679,40 @@ def main(argv=None) -> int:
     ap.add_argument("--refit-width", action="store_true",
                     help="re-time the SSSP widths on the training graphs with the current kernels and refit the "
                          "width head of the installed network (the BFS heads are kept)")
+    ap.add_argument("--ms-steer", action="store_true",
+                    help="time the multi-source pass's levels under all-push and all-pull schedules on the "
+                         "training graphs (scale <= 20) and fit its direction model (policy_ms.npz)")
     a = ap.parse_args(argv)
+    if a.ms_steer:
+        if a.data and os.path.exists(a.data):
+            z = np.load(a.data)
+            d = dict(X=z["X"], y=z["y"], w=z["w"], G=z["G"], R=z["R"] if "R" in z else z["G"])
+        else:
+            d = collect_ms(training_specs(a.graphs))
+            if a.data:
+                np.savez(a.data, **d)
+        # Every pass (graph, source count) weighs the same in total, so the
+        # grids' thousands of levels do not outvote the few levels of the
+        # low-diameter graphs; inside a pass a level weighs what its wrong
+        # direction costs.
+        run_sum = np.bincount(d["R"], weights=d["w"])
+        d["w"] = d["w"] / np.maximum(run_sum[d["R"]], 1e-12)
+        val = d["G"] % 10 == 0  # every tenth graph held out
+
+        def wacc(th, X, y, w):  # accuracy weighted by what a wrong choice costs
+            pred = (np.hstack([np.ones((len(X), 1)), X]) @ th) > 0
+            return float((w * (pred == (y > 0.5))).sum() / max(w.sum(), 1e-12))
+
+        th = fit_ms(d["X"][~val], d["y"][~val], d["w"][~val])
+        acc = dict(train=wacc(th, d["X"][~val], d["y"][~val], d["w"][~val]),
+                   val=wacc(th, d["X"][val], d["y"][val], d["w"][val]),
+                   always_pull_val=float((d["w"][val] * (d["y"][val] > 0.5)).sum() / max(d["w"][val].sum(), 1e-12)))
+        th_all = fit_ms(d["X"], d["y"], d["w"])
+        info = dict(rows=int(len(d["y"])), graphs=int(len(np.unique(d["G"]))), pull_share=float(d["y"].mean()),
+                    weighted_accuracy=acc)
+        np.savez(MS_WEIGHTS_PATH, weights=th_all, info=json.dumps(info))
+        print(json.dumps(dict(info, weights=th_all.tolist())))
+        return 0
     if a.refit_width:
         params, norm, info = load(WEIGHTS_PATH)
         if a.data and os.path.exists(a.data):

@@ -90,7 +90,9 @@ ghb_workspace* ghb_default_workspace(void);
  * kernel for oriented rows of 129 - 1,024 entries, "sssp_adapt" (0 or 1;
  * default 0) whether the one-launch SSSP halves or doubles the bucket width
  * from one bucket to the next (the light/heavy split stays at the width
- * chosen for the call).
+ * chosen for the call), "ms_learned" (0 or 1; default 0) whether the
+ * multi-source pass's directions come from the model installed by
+ * ghb_ms_policy_load.
  * Results do not depend on them.  "barrier_extra" (0 or 1) is a test knob:
  * 1 makes every grid barrier of the persistent kernels wait for one arrival
  * more than there are blocks, so every wait runs out after barrier_limit_us
@@ -532,6 +534,14 @@ int ghb_gpma_find(ghb_workspace* ws, const ghb_gpma* g, const uint64_t* keys, in
 int ghb_policy_load(const float* params, const float* norm);
 /* 1 when a network is installed. */
 int ghb_policy_loaded(void);
+/* Install the multi-source pass's learned direction model (host array of 9
+ * floats: a bias, then one weight per level feature; NULL uninstalls).  A
+ * workspace with "ms_learned" = 1 then pulls a level when the model's score
+ * is positive instead of following the direction rule; depths do not
+ * change.  Trained by graphhet_b200/policy.py from levels timed under
+ * all-push and all-pull schedules (ghb_graph_msbfs_ex).  No counterpart in
+ * the reference. */
+int ghb_ms_policy_load(const float* weights, int32_t count);
 
 /* Device arrays: logits[batch][20] = network(x[batch][12]). */
 int ghb_mlp_forward(ghb_workspace* ws, const float* params, const float* norm, const float* x,

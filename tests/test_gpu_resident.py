@@ -227,6 +227,18 @@ def test_msbfs_forced_schedules_and_trace(G):
         # The frontier a level finds is the next level's frontier.
         assert np.array_equal(tr[1:, 2], tr[:-1, 4]) and np.array_equal(tr[1:, 3], tr[:-1, 5])
         assert np.all(tr[:, 1] >= 0)
+    # The learned direction model (the shipped weights) steering the pass.
+    from graphhet_b200 import policy as P
+    P.ms_install()
+    G.tune_set("ms_learned", 1)
+    try:
+        d, st, tr = rg.msbfs_ex(srcs, trace_cap=64)
+        d2, _ = rg.msbfs(srcs)
+    finally:
+        G.tune_set("ms_learned", 0)
+        G.lib().ghb_ms_policy_load(None, 0)
+    for i, ref in enumerate(refs):
+        assert np.array_equal(d[i].cpu().numpy(), ref) and np.array_equal(d2[i].cpu().numpy(), ref), i
     rg.close()
 
 
