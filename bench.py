@@ -544,6 +544,17 @@ def extras(args, G, g, rg, srcs, ws, parity=None):
     ex["batch256_rmat22_msbfs_gteps"] = round(mr_b / (ms256 / 1e3) / 1e9, 3)
     ex["batch64_rmat22_msbfs_gteps"] = round(mr_64 / (ms64 / 1e3) / 1e9, 3)
     ex["batch256_vs_plain"] = round(t_single / ms256, 3)
+    # The 256-source pass's directions: the rule and the learned model
+    # against the per-level oracle (levels timed pushed and pulled).
+    from graphhet_b200 import policy as P
+    if os.path.exists(P.MS_WEIGHTS_PATH):
+        P.ms_install()
+        r = P.ms_regret(gb, bsrc, learned=True)
+        ex["regret_msbfs256_rmat22"] = {"ms": {a: round(b, 3) for a, b in r["ms"].items()},
+                                        "regret_rule": round(r["regret_rule"], 4),
+                                        "regret_learned": round(r["regret_learned"], 4),
+                                        "rule_dirs": r["rule_dirs"], "learned_dirs": r["learned_dirs"],
+                                        "oracle_dirs": r["oracle_dirs"]}
     del ob
     # 256 SSSP sources on the same graph: one bucketed multi-source pass
     # against 256 single-source runs (weight rule's width in both).
