@@ -114,3 +114,42 @@ def test_width_head_refit_keeps_bfs_decisions_and_learns_labels():
     assert np.array_equal(W3o[:, :4], W3p[:, :4])
     assert np.array_equal(out[o3 + 1280:o3 + 1284], params[o3 + 1280:o3 + 1284])
     assert P.width_accuracy(out, norm, X, L) > P.width_accuracy(params, norm, X, L) + 0.3
+
+
+def test_ms_rows_features_labels_and_weights():
+    """Rows of the multi-source direction model from one pass's traces:
+    row r decides level r + 1 from the frontier trace row r expands, the
+    frontier before it and the frontiers visited so far; the label is the
+    faster direction, the weight what the other one costs."""
+    n, m, k = 1024, 16384, 64
+    tr = np.array([[0, 0.1, 1, 16, 40, 700],
+                   [0, 0.2, 40, 700, 600, 9000],
+                   [1, 0.3, 600, 9000, 100, 1500]], np.float32)
+    t_push = np.array([0.10, 0.50, 0.20])
+    t_pull = np.array([0.30, 0.20, 0.25])
+    X, y, w = P.ms_rows(t_push, t_pull, tr, n, m, k, [0, 0, 1])
+    assert X.shape == (3, P.MS_FEATURES)
+    assert y.tolist() == [0.0, 1.0, 0.0]
+    assert np.allclose(w, [0.20, 0.30, 0.05])
+    # Row 1: frontier 40 vertices / 700 entries, after 1, visits 41, level 2.
+    ref = P.ms_features(700, 40, 1, 41, n, m, k, 2, 0)
+    assert np.allclose(X[1], ref)
+    assert ref[4] == 0.25 and ref[6] == 0.0
+    assert np.isclose(ref[0], np.log2(700 / m + 2.0**-30)) and np.isclose(ref[7], np.log2(41 / 2))
+
+
+def test_ms_fit_learns_a_separable_direction():
+    rng = np.random.default_rng(5)
+    X = rng.normal(size=(500, P.MS_FEATURES))
+    y = (X[:, 0] - 0.5 * X[:, 5] > 0.2).astype(np.float64)
+    w = rng.uniform(0.1, 1.0, 500)
+    th = P.fit_ms(X, y, w, epochs=4000)
+    assert th.shape == (P.MS_FEATURES + 1,) and th.dtype == np.float32
+    pred = (np.hstack([np.ones((500, 1)), X]) @ th) > 0
+    assert (pred == (y > 0.5)).mean() > 0.95
+
+
+def test_shipped_ms_model_has_nine_finite_weights():
+    z = np.load(P.MS_WEIGHTS_PATH)
+    wts = z["weights"]
+    assert wts.shape == (P.MS_FEATURES + 1,) and np.all(np.isfinite(wts))
