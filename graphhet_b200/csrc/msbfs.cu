@@ -566,8 +566,11 @@ __device__ __forceinline__ void ms_push_walk(const int32_t* __restrict__ rp, con
     }
 }
 
+// Four blocks per SM (64 registers; the 4-word variant spills 76 bytes):
+// 256 sources on RMAT-22 10.3-10.5 ms and 64 on RMAT-24 9.2-10.2 ms, against
+// 10.5-10.7 and 10.2-10.7 ms at three blocks per SM with 80 registers.
 template <int W>
-__global__ void __launch_bounds__(kMsThreads, 3) ms_pass_kernel(
+__global__ void __launch_bounds__(kMsThreads, 4) ms_pass_kernel(
     int32_t n, int32_t n_active, int32_t k, int64_t m, const int32_t* __restrict__ out_rp,
     const int32_t* __restrict__ out_col, const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col,
     const int32_t* srcs, const int32_t* __restrict__ perm, int32_t* depth, uint64_t* seen, uint64_t* masks,
