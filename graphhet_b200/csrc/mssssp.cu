@@ -273,9 +273,12 @@ __device__ __forceinline__ double mp_pmin(const MsspCounters* c) {
     return b == kInfBits ? INFINITY : __longlong_as_double((long long)b);
 }
 
-// Six blocks per SM (40 registers, a 36-byte spill): 256 sources on RMAT-22
-// in 1.32 s against 1.66 s at four blocks per SM with 64 registers.
-__global__ void __launch_bounds__(kMsspThreads, 6) mssp_pass_kernel(
+// Eight blocks per SM, every thread slot of the SM (32 registers, a
+// 148-byte spill): 256 sources on RMAT-22 in 1.08 s, against 1.30-1.34 s at
+// six blocks per SM (40 registers) and 1.66 s at four (64 registers).  The
+// pass waits on its gathers and atomics, so resident warps pay for the
+// spill.
+__global__ void __launch_bounds__(kMsspThreads, 8) mssp_pass_kernel(
     int32_t n, int32_t n_active, int32_t k, int32_t ks, int32_t words, const int32_t* __restrict__ rp,
     const int32_t* __restrict__ col, const double* __restrict__ wt, const int32_t* srcs, const int32_t* __restrict__ perm,
     double inf, double* dist_out, unsigned long long* d, unsigned long long* act_a, unsigned long long* act_b,
@@ -460,7 +463,7 @@ static int mssp_pass_blocks(ghb_workspace* ws) {
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
         if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mssp_pass_kernel, kMsspThreads, 0) ==
                         cudaSuccess)
-            cached[dev] = std::max(0, std::min(per_sm, 6)) * ws->num_sms;
+            cached[dev] = std::max(0, std::min(per_sm, 8)) * ws->num_sms;
         if (!cached[dev]) cached[dev] = -1;
     }
     return cached[dev] > 0 ? cached[dev] : 0;
