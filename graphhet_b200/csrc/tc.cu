@@ -255,7 +255,9 @@ constexpr int kTcBlockThreads = 128;
 constexpr int32_t kTcSlice = 512;     // entries of N+(a) per slice-kernel item
 constexpr int32_t kTcMidRow = 1024;   // rows up to this many entries: a 2,048-slot hash
 constexpr int kTcMidLog2 = 11;
-constexpr int kTcBigLog2 = 14;        // 16,384 slots for rows up to kTcBlockRow
+constexpr int32_t kTcMid2Row = 4096;  // rows up to this many entries: an 8,192-slot hash (32 KB, six blocks per SM)
+constexpr int kTcMid2Log2 = 13;
+constexpr int kTcBigLog2 = 14;        // 16,384 slots for rows up to kTcBlockRow (64 KB, three blocks per SM)
 
 __device__ __forceinline__ uint32_t tc_hash(int32_t w, int shift) {
     return ((uint32_t)w * 2654435761u) >> shift;
@@ -377,10 +379,11 @@ __device__ __forceinline__ unsigned long long tc_row_share(const int32_t* __rest
 
 // Rows of 1..kTcWarpRow oriented entries, a warp each.  Longer rows, up to
 // block_row <= kTcBlockRow entries, are listed for the slice kernels as
-// (row, first entry) items of kTcSlice entries each, in two classes by the
-// hash the row needs (items[0..]: up to kTcMidRow entries, items[item_cap..]:
-// longer); rows over block_row go to huge[] for the galloping walk.
-// tails: [0], [1] the two item counts, [2] the huge rows.
+// (row, first entry) items of kTcSlice entries each, in three classes by the
+// hash the row needs (items[0..]: up to kTcMidRow entries,
+// items[item_cap..]: up to kTcMid2Row, items[2 item_cap..]: longer); rows
+// over block_row go to huge[] for the galloping walk.
+// tails: [0], [1], [2] the three item counts, [3] the huge rows.
 // (Eight blocks per SM, 32 registers: 774-787 ms for RMAT-24 TC against
 // 789-797 ms at six blocks.)
 __global__ void __launch_bounds__(kTcWarpBlock, 8) tc_hash_warp_kernel(int32_t n, const int32_t* __restrict__ orp,
@@ -400,7 +403,7 @@ __global__ void __launch_bounds__(kTcWarpBlock, 8) tc_hash_warp_kernel(int32_t n
         if (k == 0) continue;
         if (k > kTcWarpRow) {
             if (k <= block_row) {
-                const int cls = k <= kTcMidRow ? 0 : 1;
+                const int cls = k <= kTcMidRow ? 0 : (k <= kTcMid2Row ? 1 : 2);
                 const int32_t ns = (k + kTcSlice - 1) / kTcSlice;
                 int32_t pos = 0;
                 if (lane == 0) pos = atomicAdd(tails + cls, ns);
@@ -408,7 +411,7 @@ __global__ void __launch_bounds__(kTcWarpBlock, 8) tc_hash_warp_kernel(int32_t n
                 for (int32_t s = lane; s < ns; s += 32)
                     items[cls * item_cap + pos + s] = make_int2((int32_t)a, s * kTcSlice);
             } else if (lane == 0) {
-                huge[atomicAdd(tails + 2, 1)] = (int32_t)a;
+                huge[atomicAdd(tails + 3, 1)] = (int32_t)a;
             }
             continue;
         }
@@ -476,7 +479,7 @@ __global__ void __launch_bounds__(kTcBlockThreads) tc_hash_slice_kernel(const in
 
 // Triangles of the oriented CSR into cnt (zeroed by the caller): the
 // hash-probe kernels above, then the load-balanced walk with the galloping
-// visitor below for rows longer than kTcBlockRow.  `lists` holds 2n + 8
+// visitor below for rows longer than kTcBlockRow.  `lists` holds tc_lists_ints(n, m)
 // ints of scratch.  (A warp-per-row shared-memory hash variant measured 25 % slower
 // on RMAT scale 24: most oriented rows hold a few entries, so a warp per row
 // leaves most lanes idle, where the walker packs short rows warp-wide.
@@ -493,7 +496,7 @@ int64_t tc_item_cap(int32_t n, int64_t m) { return (int64_t)n + m / kTcSlice + 6
 }  // namespace
 
 // Scratch ints that tc_count_oriented's `lists` must hold.
-size_t tc_lists_ints(int32_t n, int64_t m) { return (size_t)(4 * tc_item_cap(n, m) + n + 8); }
+size_t tc_lists_ints(int32_t n, int64_t m) { return (size_t)(6 * tc_item_cap(n, m) + n + 8); }
 
 namespace {
 
@@ -504,7 +507,7 @@ int tc_count_oriented(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* or
                     OrientedVisitor{orp, ocol, cnt});
     const int64_t item_cap = tc_item_cap(n, m);
     int2* items = reinterpret_cast<int2*>(lists);
-    int32_t* huge = lists + 4 * item_cap;
+    int32_t* huge = lists + 6 * item_cap;
     int32_t* tails = huge + n;
     GHB_CUDA_TRY(cudaMemsetAsync(tails, 0, 4 * sizeof(int32_t), ws->stream));
     GHB_TRY(launch(ws, tc_hash_warp_kernel, dim3(grid_for((int64_t)n * 32, kTcWarpBlock, ws->num_sms * 8)),
@@ -521,11 +524,14 @@ int tc_count_oriented(ghb_workspace* ws, int32_t n, int64_t m, const int32_t* or
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set[ws->device] = true;
     }
-    GHB_TRY(launch(ws, tc_hash_slice_kernel<kTcBigLog2, true>, dim3(ws->num_sms * 3), dim3(kTcBlockThreads), smem,
+    GHB_TRY(launch(ws, tc_hash_slice_kernel<kTcMid2Log2, false>, dim3(ws->num_sms * 6), dim3(kTcBlockThreads), 0,
                    orp, ocol, cnt, (const int2*)(items + item_cap), (const int32_t*)(tails + 1),
                    ws->tune.tc_trim_min));
+    GHB_TRY(launch(ws, tc_hash_slice_kernel<kTcBigLog2, true>, dim3(ws->num_sms * 3), dim3(kTcBlockThreads), smem,
+                   orp, ocol, cnt, (const int2*)(items + 2 * item_cap), (const int32_t*)(tails + 2),
+                   ws->tune.tc_trim_min));
     // Rows over the block path's length: the galloping walk.
-    return walk(ws, orp, ocol, (const int32_t*)huge, (const int32_t*)(tails + 2), (int64_t)0,
+    return walk(ws, orp, ocol, (const int32_t*)huge, (const int32_t*)(tails + 3), (int64_t)0,
                 (int64_t)ws->num_sms * 64, wb, OrientedVisitor{orp, ocol, cnt});
 }
 
