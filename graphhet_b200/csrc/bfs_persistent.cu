@@ -233,7 +233,7 @@ __device__ __noinline__ void level_eval(const float* pol, const float* feat, flo
 __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(
     int32_t n, int32_t n_active, const int32_t* __restrict__ out_rp, const int32_t* __restrict__ out_col,
     const int32_t* __restrict__ in_rp, const int32_t* __restrict__ in_col, int32_t src, int32_t max_depth,
-    int32_t* depth, uint32_t* visited, uint32_t* f0, uint32_t* f1, uint32_t* f2, int32_t* qa, int32_t* qb,
+    int32_t* depth, uint32_t* visited, uint32_t* f0, uint32_t* f1, uint32_t* f2, int32_t* qa, int32_t* qb, int32_t* qc,
     int32_t* big, int policy, float alpha, float beta, float gamma, float band, int64_t m_total,
     const int8_t* __restrict__ schedule,
     int32_t schedule_len, const int32_t* __restrict__ perm, int32_t* depth_out, BfsRunState* st,
@@ -300,6 +300,10 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(
     volatile BfsRunState* vs = st;
     // One iteration per level in every block; the level's state arrived
     // with the previous barrier's release (s_pl).
+    // Frontier L - 1's size and whether that level ran top-down (its
+    // vertices are then listed in queue (L + 2) % 3); level 0 has none.
+    int32_t last_nf = 0;
+    bool last_top = true;
     for (int32_t L = 0;; ++L) {
         const unsigned long long pl = s_pl;
         if (pl & kPlDone) break;
@@ -312,8 +316,24 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(
         uint32_t* f_cur = slot == 0 ? f0 : (slot == 1 ? f1 : f2);
         uint32_t* f_next = nslot == 0 ? f0 : (nslot == 1 ? f1 : f2);
         uint32_t* f_clear = cslot == 0 ? f0 : (cslot == 1 ? f1 : f2);
-        int32_t* q_cur = (L & 1) ? qb : qa;
-        int32_t* q_next = (L & 1) ? qa : qb;
+        // Queues triple-buffered like the bitmaps: level L reads queue L % 3,
+        // appends to (L + 1) % 3, and queue (L + 2) % 3 still lists frontier
+        // L - 1, whose bitmap (f_clear) is cleared through it when that level
+        // ran top-down and its frontier was small.
+        int32_t* q_cur = slot == 0 ? qa : (slot == 1 ? qb : qc);
+        int32_t* q_next = nslot == 0 ? qa : (nslot == 1 ? qb : qc);
+        const int32_t* q_clear = cslot == 0 ? qa : (cslot == 1 ? qb : qc);
+        const int32_t clear_nf = last_nf;
+        const bool clear_sparse = last_top && (int64_t)clear_nf * 4 < words;
+        last_nf = n_f;
+        last_top = dir == 0;
+        auto clear_frontier_bitmap = [&]() {
+            if (clear_sparse) {
+                for (int64_t i = gtid; i < clear_nf; i += gsize) f_clear[__ldcg(q_clear + i) >> 5] = 0u;
+            } else {
+                for (int64_t w = gtid; w < words; w += gsize) f_clear[w] = 0u;
+            }
+        };
         const int32_t next_depth = L + 1;
         PAcc acc;
         // Level decision, run by every thread of the last block to reach the
@@ -508,7 +528,7 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(
                                 append, out_rp, acc, filter);
                 }
             }
-            for (int64_t w = gtid; w < words; w += gsize) f_clear[w] = 0u;
+            clear_frontier_bitmap();
             p_flush(acc, st, nslot, !append);
             acc = PAcc();
             // Decide now unless long rows were deferred (then after them).
@@ -680,7 +700,7 @@ __global__ void __launch_bounds__(512, 2) bfs_persistent_kernel(
                     }
                 }
             }
-            for (int64_t w = gtid; w < words; w += gsize) f_clear[w] = 0u;
+            clear_frontier_bitmap();
             p_flush(acc, st, nslot, true);
             if (!p_sync(st, decide, &s_pl)) return;
         }
@@ -732,27 +752,28 @@ int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int
     const bool want_trace = opt && opt->record_trace && opt->trace && opt->trace_cap > 0;
     const int32_t tcap = want_trace ? std::min<int32_t>(opt->trace_cap, 1 << 16) : 0;
     auto carve = [&](Carver& c, uint32_t** vis, uint32_t** f0, uint32_t** f1, uint32_t** f2, int32_t** qa,
-                     int32_t** qb, int32_t** big, BfsRunState** rs, int8_t** sched, float** tr) {
+                     int32_t** qb, int32_t** qc, int32_t** big, BfsRunState** rs, int8_t** sched, float** tr) {
         *vis = c.take<uint32_t>(words);
         *f0 = c.take<uint32_t>(words);
         *f1 = c.take<uint32_t>(words);
         *f2 = c.take<uint32_t>(words);
         *qa = c.take<int32_t>(n);
         *qb = c.take<int32_t>(n);
+        *qc = c.take<int32_t>(n);
         *big = c.take<int32_t>(n);
         *rs = c.take<BfsRunState>(1);
         *sched = c.take<int8_t>(4096);
         *tr = c.take<float>((size_t)(tcap > 0 ? tcap : 1) * GHB_TRACE_COLS);
     };
     uint32_t *vis, *f0, *f1, *f2;
-    int32_t *qa, *qb, *big;
+    int32_t *qa, *qb, *qc, *big;
     BfsRunState* rs;
     int8_t* sched;
     float* tr;
-    carve(sizing, &vis, &f0, &f1, &f2, &qa, &qb, &big, &rs, &sched, &tr);
+    carve(sizing, &vis, &f0, &f1, &f2, &qa, &qb, &qc, &big, &rs, &sched, &tr);
     GHB_TRY(ws_reserve(ws, sizing.off));
     Carver c(ws->scratch);
-    carve(c, &vis, &f0, &f1, &f2, &qa, &qb, &big, &rs, &sched, &tr);
+    carve(c, &vis, &f0, &f1, &f2, &qa, &qb, &qc, &big, &rs, &sched, &tr);
 
     int policy = opt ? opt->policy : GHB_POLICY_HEURISTIC;
     float alpha = (opt && opt->alpha > 0) ? opt->alpha : 256.0f;
@@ -783,7 +804,7 @@ int bfs_persistent_run(ghb_workspace* ws, int32_t n, int32_t n_active, const int
     const int64_t m_total = hp[0];
     if (stats) GHB_CUDA_TRY(cudaEventRecord(ws->ev_start, st));
     GHB_TRY(launch_coop(ws, bfs_persistent_kernel, dim3(blocks), dim3(512), 0, n,
-                        n_active, out_rp, out_col, in_rp, in_col, src, max_depth, depth, vis, f0, f1, f2, qa, qb, big,
+                        n_active, out_rp, out_col, in_rp, in_col, src, max_depth, depth, vis, f0, f1, f2, qa, qb, qc, big,
                         policy, alpha, beta, gamma, (float)ws->tune.pol_band, m_total,
                         (const int8_t*)(sched_len ? sched : nullptr), sched_len,
                         perm,
